@@ -1,0 +1,261 @@
+"""ctypes binding of libbzgrav.so (the C ABI declared in include/bzgrav.h).
+
+The library is the product; this module only marshals host arrays.  Loading fails loudly if
+the shared object has not been built -- there is no CPU fallback path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libbzgrav.so")
+
+BZ_OK, BZ_INVALID_ARGUMENT, BZ_NOT_READY, BZ_TIMEOUT, BZ_INTERNAL_ERROR = 0, 1, 2, 3, 4
+BZ_CUDA_ERROR, BZ_OUT_OF_MEMORY, BZ_DEVICE_LIMIT, BZ_UNSUPPORTED = 5, 6, 7, 8
+SOLVER_OCTREE, SOLVER_TREEPM, SOLVER_OCTREE_REFERENCE = 0, 1, 2
+KEYS_PRODUCTION, KEYS_REFERENCE = 0, 1
+
+#: every symbol include/bzgrav.h declares
+EXPORTS = (
+    "bz_config_init", "bz_create", "bz_destroy", "bz_set_state", "bz_set_state_f64", "bz_step",
+    "bz_accelerations", "bz_get_state", "bz_get_state_f64", "bz_morton_keys", "bz_tree_topology",
+    "bz_reference_tree", "bz_interaction_counts", "bz_enable_phase_timing", "bz_phase_times",
+    "bz_force_errors", "bz_pm_mesh", "bz_particle_count", "bz_device_bytes", "bz_last_error",
+    "bz_status_string", "bz_version",
+)
+
+PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
+
+
+class BzConfig(C.Structure):
+    _fields_ = [
+        ("struct_size", C.c_uint32),
+        ("solver", C.c_int32),
+        ("octree_theta", C.c_float),
+        ("octree_softening", C.c_float),
+        ("octree_opening_criterion", C.c_int32),
+        ("linear_octree_leaf_capacity", C.c_int32),
+        ("leaf_capacity", C.c_int32),
+        ("multipole_order", C.c_int32),
+        ("physics_max_acceleration", C.c_float),
+        ("physics_min_softening", C.c_float),
+        ("physics_min_distance2", C.c_float),
+        ("physics_min_theta", C.c_float),
+        ("treepm_grid_size", C.c_int32),
+        ("treepm_r_split_cells", C.c_float),
+        ("treepm_r_cut_factor", C.c_float),
+        ("box_length", C.c_double),
+        ("key_mode", C.c_int32),
+        ("device", C.c_int32),
+        ("stream", C.c_uint64),
+        ("use_graph", C.c_int32),
+    ]
+
+
+class BzError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{message} (status {status})")
+        self.status = status
+
+
+_LIB = None
+_vp = C.c_void_p
+
+
+def load():
+    """Load libbzgrav.so; raise if it is missing (build it with ``python -m blitzar_b200.build``)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is not built; run `python -m blitzar_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    L.bz_config_init.argtypes = [C.POINTER(BzConfig)]
+    L.bz_create.argtypes = [C.POINTER(BzConfig), C.c_size_t, C.POINTER(_vp)]
+    L.bz_destroy.argtypes = [_vp]
+    L.bz_set_state.argtypes = [_vp, _vp, _vp, _vp, C.c_size_t]
+    L.bz_set_state_f64.argtypes = [_vp, _vp, _vp, _vp, C.c_size_t]
+    L.bz_step.argtypes = [_vp, C.c_double, C.c_uint32]
+    L.bz_accelerations.argtypes = [_vp, _vp, _vp]
+    L.bz_get_state.argtypes = [_vp, _vp, _vp]
+    L.bz_get_state_f64.argtypes = [_vp, _vp, _vp]
+    L.bz_morton_keys.argtypes = [_vp, _vp, _vp]
+    L.bz_tree_topology.argtypes = [_vp, C.POINTER(C.c_int64)] + [_vp] * 8
+    L.bz_reference_tree.argtypes = [_vp, C.POINTER(C.c_int64)] + [_vp] * 6
+    L.bz_interaction_counts.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.bz_enable_phase_timing.argtypes = [_vp, C.c_int]
+    L.bz_phase_times.argtypes = [_vp, _vp, C.c_int]
+    L.bz_force_errors.argtypes = [_vp, C.c_int32, C.c_uint64, _vp, _vp, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_double)]
+    L.bz_pm_mesh.argtypes = [_vp, C.c_int, _vp]
+    L.bz_particle_count.argtypes = [_vp]
+    L.bz_particle_count.restype = C.c_size_t
+    L.bz_device_bytes.argtypes = [_vp]
+    L.bz_device_bytes.restype = C.c_size_t
+    L.bz_last_error.argtypes = [_vp, C.c_char_p, C.c_size_t]
+    L.bz_last_error.restype = C.c_size_t
+    L.bz_status_string.argtypes = [C.c_int]
+    L.bz_status_string.restype = C.c_char_p
+    L.bz_version.restype = C.c_char_p
+    _LIB = L
+    return L
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data
+
+
+def default_config(**kw) -> BzConfig:
+    cfg = BzConfig()
+    load().bz_config_init(C.byref(cfg))
+    for k, v in kw.items():
+        if not hasattr(cfg, k):
+            raise KeyError(k)
+        setattr(cfg, k, v)
+    return cfg
+
+
+class Engine:
+    """One engine handle (one particle system on one GPU)."""
+
+    def __init__(self, capacity: int, **cfg):
+        self.L = load()
+        self.cfg = default_config(**cfg)
+        h = _vp()
+        st = self.L.bz_create(C.byref(self.cfg), capacity, C.byref(h))
+        if st != BZ_OK:
+            raise BzError(st, f"bz_create: {self.L.bz_status_string(st).decode()}")
+        self.h = h
+        self.n = 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.bz_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, st, what):
+        if st != BZ_OK:
+            buf = C.create_string_buffer(1024)
+            self.L.bz_last_error(self.h, buf, 1024)
+            raise BzError(st, f"{what}: {buf.value.decode(errors='replace')}")
+
+    # -- state
+    def set_state(self, pos, vel=None, mass=None, f64=False):
+        pos = np.asarray(pos)
+        n = pos.shape[0]
+        if f64:
+            p = np.ascontiguousarray(pos.T, np.float64)
+            v = None if vel is None else np.ascontiguousarray(np.asarray(vel).T, np.float64)
+            m = np.ascontiguousarray(mass, np.float32)
+            self._check(self.L.bz_set_state_f64(self.h, _ptr(p), _ptr(v), _ptr(m), n), "bz_set_state_f64")
+        else:
+            p = np.ascontiguousarray(pos.T, np.float32)
+            v = None if vel is None else np.ascontiguousarray(np.asarray(vel).T, np.float32)
+            m = np.ascontiguousarray(mass, np.float32)
+            self._check(self.L.bz_set_state(self.h, _ptr(p), _ptr(v), _ptr(m), n), "bz_set_state")
+        self.n = n
+
+    def set_state_soa(self, pos_soa3, vel_soa3, mass):
+        """Upload from caller-owned SoA float32 buffers (no copies on the Python side)."""
+        n = mass.shape[0]
+        self._check(self.L.bz_set_state(self.h, _ptr(pos_soa3), _ptr(vel_soa3), _ptr(mass), n),
+                    "bz_set_state")
+        self.n = n
+
+    def get_state(self, f64=False, with_vel=True):
+        n = self.n
+        dt = np.float64 if f64 else np.float32
+        p = np.empty(3 * n, dt)
+        v = np.empty(3 * n, dt) if with_vel else None
+        fn = self.L.bz_get_state_f64 if f64 else self.L.bz_get_state
+        self._check(fn(self.h, _ptr(p), _ptr(v)), "bz_get_state")
+        return p.reshape(3, n).T.copy(), (None if v is None else v.reshape(3, n).T.copy())
+
+    def get_state_soa(self, pos_soa3, vel_soa3):
+        self._check(self.L.bz_get_state(self.h, _ptr(pos_soa3), _ptr(vel_soa3)), "bz_get_state")
+
+    def step(self, dt, nsteps=1):
+        self._check(self.L.bz_step(self.h, dt, nsteps), "bz_step")
+
+    def accelerations(self, want_pot=False):
+        a = np.empty(3 * self.n, np.float32)
+        p = np.empty(self.n, np.float32) if want_pot else None
+        self._check(self.L.bz_accelerations(self.h, _ptr(a), _ptr(p)), "bz_accelerations")
+        acc = a.reshape(3, self.n).T.copy()
+        return (acc, p) if want_pot else acc
+
+    def morton_keys(self):
+        k = np.empty(self.n, np.uint64)
+        p = np.empty(self.n, np.int32)
+        self._check(self.L.bz_morton_keys(self.h, _ptr(k), _ptr(p)), "bz_morton_keys")
+        return k, p
+
+    def tree(self):
+        nn = C.c_int64(0)
+        self._check(self.L.bz_tree_topology(self.h, C.byref(nn), *([None] * 8)), "bz_tree_topology")
+        k = nn.value
+        t = {name: np.empty(k, np.int32) for name in ("start", "count", "child", "nchild")}
+        t["mono"] = np.empty((k, 4), np.float32)
+        t["bmin"] = np.empty((k, 3), np.float32)
+        t["bmax"] = np.empty((k, 3), np.float32)
+        t["quad"] = np.empty((k, 6), np.float32)
+        self._check(self.L.bz_tree_topology(self.h, C.byref(nn), _ptr(t["start"]), _ptr(t["count"]),
+                                            _ptr(t["child"]), _ptr(t["nchild"]), _ptr(t["mono"]),
+                                            _ptr(t["bmin"]), _ptr(t["bmax"]), _ptr(t["quad"])),
+                    "bz_tree_topology")
+        t["nodes"] = k
+        return t
+
+    def reference_tree(self):
+        nn = C.c_int64(0)
+        hot = np.empty(8, np.float32)
+        arrs = [np.empty(1, np.int32) for _ in range(5)]
+        self._check(self.L.bz_reference_tree(self.h, C.byref(nn), _ptr(hot), *[_ptr(a) for a in arrs]),
+                    "bz_reference_tree")
+        return dict(nodes=nn.value, hot=hot.reshape(1, 8), next=arrs[0], mask=arrs[1],
+                    first=arrs[2], lstart=arrs[3], lcount=arrs[4])
+
+    def interaction_counts(self):
+        a, b = C.c_uint64(0), C.c_uint64(0)
+        self._check(self.L.bz_interaction_counts(self.h, C.byref(a), C.byref(b)), "bz_interaction_counts")
+        return a.value, b.value
+
+    def enable_timing(self, on=True):
+        self._check(self.L.bz_enable_phase_timing(self.h, 1 if on else 0), "bz_enable_phase_timing")
+
+    def phase_times(self):
+        ms = np.zeros(len(PHASES), np.float32)
+        self._check(self.L.bz_phase_times(self.h, _ptr(ms), len(PHASES)), "bz_phase_times")
+        return dict(zip(PHASES, ms.tolist()))
+
+    def force_errors(self, nsample=4096, seed=1):
+        errs = np.empty(nsample, np.float32)
+        idx = np.empty(nsample, np.int32)
+        med, p99 = C.c_double(0), C.c_double(0)
+        self._check(self.L.bz_force_errors(self.h, nsample, seed, _ptr(errs), _ptr(idx), C.byref(med),
+                                           C.byref(p99)), "bz_force_errors")
+        return dict(median=med.value, p99=p99.value, errs=errs, idx=idx)
+
+    def pm_mesh(self, which):
+        M = self.cfg.treepm_grid_size
+        out = np.empty(M ** 3, np.float32)
+        self._check(self.L.bz_pm_mesh(self.h, which, _ptr(out)), "bz_pm_mesh")
+        return out
+
+    def device_bytes(self):
+        return self.L.bz_device_bytes(self.h)

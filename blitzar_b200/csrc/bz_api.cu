@@ -1,0 +1,1062 @@
+// C ABI of the engine (include/bzgrav.h): handle lifetime, device memory plan, the per-step
+// pipeline and its CUDA graph, host <-> device transfers, parity entry points.
+//
+// Per step (production):
+//   kick_drift (FP64, cached force) -> [bbox] -> keys63 -> radix sort -> permute state into
+//   Morton order -> octree build -> [PM mesh forces] -> group walk (+=) -> closing kick.
+// All of it is enqueued on the handle's stream without host synchronisation, so a whole step
+// is captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <string>
+#include <vector>
+
+#include "../../include/bzgrav.h"
+#include "bz_common.cuh"
+#include "bz_kernels.h"
+
+using namespace bz;
+
+namespace {
+
+enum Phase { kPhKeys = 0, kPhSort, kPhPermute, kPhTree, kPhMesh, kPhWalk, kPhIntegrate, kPhTotal };
+constexpr int kNumPhases = 8;
+constexpr int kEvStepStart = kNumPhases + 1;  // event slot before the opening kick-drift
+
+struct DeviceBuffers {
+    // state in Morton order, two copies (the permutation gathers from one into the other)
+    double* st[2][6] = {};
+    float* mass[2] = {};
+    int* id[2] = {};
+    float4* pos4 = nullptr;
+    float* acc[3] = {};
+    float* pot = nullptr;
+    unsigned long long* keys = nullptr;
+    uint32_t* perm = nullptr;
+    BoxF64* box = nullptr;
+    unsigned* bbox32 = nullptr;
+    int* err = nullptr;
+    double* dt = nullptr;  // {dt, dt/2}
+    unsigned* queue = nullptr;
+    int* spill = nullptr;
+    unsigned long long* counters = nullptr;  // [2] pp, pn
+    float* stage = nullptr;                  // 7n floats for host transfers
+    float* ref_xyzm = nullptr;               // 4n floats, caller order, reference mode
+    float4* ref_orig = nullptr;              // n float4, caller order
+    float* ref_hot8 = nullptr;               // 8 floats
+};
+
+} // namespace
+
+struct bz_handle {
+    bz_config cfg{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    size_t capacity = 0;
+    size_t n = 0;
+    int cur = 0;
+    bool forces_valid = false;
+    DeviceBuffers d;
+    SortWorkspace sort{};
+    TreeArrays tree{};
+    PmPlan* pm = nullptr;
+    int spill_slots = 0;
+    size_t bytes = 0;
+    std::vector<void*> allocations;
+    std::string last_error;
+    // timing
+    bool timing = false;
+    cudaEvent_t ev[kNumPhases + 2] = {};
+    bool stepping = false;  // last timed call was bz_step (has an opening kick-drift)
+    float phase_ms[kNumPhases] = {};
+    // graphs (one per state-buffer parity)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    bool graph_failed = false;
+    double* h_dt = nullptr;  // pinned {dt, dt/2}
+    unsigned long long last_pp = 0, last_pn = 0;
+    bool ref_tree_valid = false;
+};
+
+namespace {
+
+bz_status fail(bz_handle* h, bz_status s, const std::string& msg)
+{
+    if (h)
+        h->last_error = msg;
+    return s;
+}
+
+bz_status cuda_fail(bz_handle* h, cudaError_t e, const char* what)
+{
+    return fail(h, BZ_CUDA_ERROR, std::string("[cuda] ") + what + " failed: " + cudaGetErrorString(e));
+}
+
+template <class T> bool dalloc(bz_handle* h, T** p, size_t count)
+{
+    void* q = nullptr;
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (cudaMalloc(&q, bytes) != cudaSuccess) {
+        *p = nullptr;
+        return false;
+    }
+    h->allocations.push_back(q);
+    h->bytes += bytes;
+    *p = static_cast<T*>(q);
+    return true;
+}
+
+bool periodic(const bz_handle* h) { return h->cfg.solver == BZ_SOLVER_TREEPM && h->cfg.box_length > 0.0; }
+
+float rsplit_len(const bz_handle* h)
+{
+    return static_cast<float>(h->cfg.treepm_r_split_cells * h->cfg.box_length / h->cfg.treepm_grid_size);
+}
+
+void record(bz_handle* h, int i)
+{
+    if (h->timing)
+        cudaEventRecord(h->ev[i], h->stream);
+}
+
+WalkParams walk_params(const bz_handle* h, bool want_pot)
+{
+    WalkParams p{};
+    const float th = std::max(h->cfg.octree_theta, h->cfg.physics_min_theta);
+    p.theta2 = th * th;
+    const float eps = std::max(h->cfg.octree_softening, h->cfg.physics_min_softening);
+    p.eps2 = eps * eps;
+    p.min_dist2 = h->cfg.physics_min_distance2;
+    p.quadrupole = h->cfg.multipole_order >= 2 ? 1 : 0;
+    p.want_pot = want_pot ? 1 : 0;
+    if (h->cfg.solver == BZ_SOLVER_TREEPM) {
+        const float rs = rsplit_len(h);
+        const float rc = h->cfg.treepm_r_cut_factor * rs;
+        p.rsplit = rs;
+        p.rcut2 = rc * rc;
+        p.box = static_cast<float>(h->cfg.box_length);
+    }
+    return p;
+}
+
+// Keys, sort and permutation: the state ends up in Morton order in buffer `cur`.
+void enqueue_order(bz_handle* h)
+{
+    const int n = static_cast<int>(h->n);
+    DeviceBuffers& d = h->d;
+    double* const* s = d.st[h->cur];
+    record(h, kPhKeys);
+    if (!periodic(h))
+        launch_bbox_f64(s[0], s[1], s[2], n, d.box, h->stream);
+    launch_keys63(s[0], s[1], s[2], n, d.box, periodic(h) ? h->cfg.box_length : 0.0, d.keys,
+                  d.perm, h->stream);
+    record(h, kPhSort);
+    launch_radix_sort(d.keys, d.perm, n, 64, h->sort, d.err, h->stream);
+    record(h, kPhPermute);
+    const int nxt = h->cur ^ 1;
+    launch_permute(d.perm, n, d.st[h->cur], d.st[nxt], 6, d.mass[h->cur], d.mass[nxt],
+                   d.id[h->cur], d.id[nxt], d.pos4, 0.0, h->stream);
+    h->cur = nxt;
+}
+
+// Forces of the (already ordered) state into d.acc; optional closing kick.
+void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
+{
+    const int n = static_cast<int>(h->n);
+    DeviceBuffers& d = h->d;
+    record(h, kPhTree);
+    launch_tree_build(d.keys, d.pos4, n, h->cfg.leaf_capacity, kMaxLevels, h->tree, d.err,
+                      h->stream);
+    record(h, kPhMesh);
+    if (h->cfg.solver == BZ_SOLVER_TREEPM && h->pm) {
+        pm_forces(h->pm, d.pos4, n, d.acc[0], d.acc[1], d.acc[2], h->stream);
+    } else {
+        for (int a = 0; a < 3; ++a)
+            cudaMemsetAsync(d.acc[a], 0, sizeof(float) * n, h->stream);
+    }
+    if (want_pot)
+        cudaMemsetAsync(d.pot, 0, sizeof(float) * n, h->stream);
+    record(h, kPhWalk);
+    cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), h->stream);
+    WalkOutputs o{};
+    o.ax = d.acc[0];
+    o.ay = d.acc[1];
+    o.az = d.acc[2];
+    o.pot = want_pot ? d.pot : nullptr;
+    o.totals = d.counters;
+    launch_walk(d.pos4, n, h->tree, walk_params(h, want_pot), o, d.queue, d.spill, d.err,
+                h->stream);
+    record(h, kPhIntegrate);
+    if (kick) {
+        double* const* s = d.st[h->cur];
+        launch_kick(s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt + 1, h->stream);
+    }
+}
+
+void enqueue_step(bz_handle* h)
+{
+    const int n = static_cast<int>(h->n);
+    DeviceBuffers& d = h->d;
+    double* const* s = d.st[h->cur];
+    launch_kick_drift(s[0], s[1], s[2], s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt,
+                      periodic(h) ? h->cfg.box_length : 0.0, nullptr, h->stream);
+    enqueue_order(h);
+    enqueue_forces(h, true, false);
+}
+
+bz_status check_device(bz_handle* h, const char* what)
+{
+    cudaError_t e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess)
+        return cuda_fail(h, e, what);
+    e = cudaGetLastError();
+    if (e != cudaSuccess)
+        return cuda_fail(h, e, what);
+    int err = 0;
+    e = cudaMemcpy(&err, h->d.err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess)
+        return cuda_fail(h, e, what);
+    if (err) {
+        cudaMemset(h->d.err, 0, sizeof(int));
+        std::string m = std::string("[device] ") + what + ":";
+        if (err & kErrWalkStack)
+            m += " walk traversal stack exhausted;";
+        if (err & kErrSortSpin)
+            m += " radix-sort look-back wait limit reached;";
+        if (err & kErrTreeCapacity)
+            m += " octree node capacity exceeded;";
+        if (err & kErrTreeSpin)
+            m += " octree look-back wait limit reached;";
+        if (err & kErrBulkWait)
+            m += " bulk-copy wait limit reached;";
+        if (err & kErrListCapacity)
+            m += " interaction list capacity exceeded;";
+        return fail(h, BZ_DEVICE_LIMIT, m);
+    }
+    return BZ_OK;
+}
+
+void collect_timing(bz_handle* h)
+{
+    if (!h->timing)
+        return;
+    cudaEventSynchronize(h->ev[kNumPhases]);
+    float total = 0.0f;
+    for (int i = 0; i < kPhTotal; ++i) {
+        float ms = 0.0f;
+        const int next = i + 1 <= kPhIntegrate ? i + 1 : kNumPhases;
+        cudaEventElapsedTime(&ms, h->ev[i], h->ev[next]);
+        h->phase_ms[i] = ms;
+        total += ms;
+    }
+    if (h->stepping) {  // opening kick-drift of the last step
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, h->ev[kEvStepStart], h->ev[kPhKeys]);
+        h->phase_ms[kPhIntegrate] += ms;
+        total += ms;
+    }
+    h->phase_ms[kPhTotal] = total;
+}
+
+void read_counters(bz_handle* h)
+{
+    unsigned long long c[2] = {0, 0};
+    cudaMemcpy(c, h->d.counters, sizeof(c), cudaMemcpyDeviceToHost);
+    h->last_pp = c[0];
+    h->last_pn = c[1];
+}
+
+bz_status ensure_forces(bz_handle* h)
+{
+    if (h->forces_valid)
+        return BZ_OK;
+    enqueue_order(h);
+    enqueue_forces(h, false, false);
+    bz_status s = check_device(h, "initial force evaluation");
+    if (s != BZ_OK)
+        return s;
+    h->forces_valid = true;
+    return BZ_OK;
+}
+
+// One-time capture of a step for each state-buffer parity.  Capturing records the work
+// without executing it; the host-side parity is restored afterwards.
+void build_graphs(bz_handle* h)
+{
+    if (h->graph_failed || (h->graph[0] && h->graph[1]))
+        return;
+    const int orig = h->cur;
+    const bool saved = h->timing;
+    h->timing = false;
+    for (int parity = 0; parity < 2 && !h->graph_failed; ++parity) {
+        if (h->graph[parity])
+            continue;
+        h->cur = parity;
+        cudaGraph_t g = nullptr;
+        if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+            h->graph_failed = true;
+            break;
+        }
+        enqueue_step(h);
+        const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        cudaGraphExec_t ex = nullptr;
+        if (e != cudaSuccess || !g || cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
+            h->graph_failed = true;
+            if (g)
+                cudaGraphDestroy(g);
+            break;
+        }
+        cudaGraphDestroy(g);
+        h->graph[parity] = ex;
+    }
+    if (h->graph_failed)
+        cudaGetLastError();
+    h->timing = saved;
+    h->cur = orig;
+}
+
+} // namespace
+
+extern "C" {
+
+const char* bz_version(void) { return "bzgrav 0.1 (sm_100a)"; }
+
+const char* bz_status_string(bz_status s)
+{
+    switch (s) {
+    case BZ_OK: return "ok";
+    case BZ_INVALID_ARGUMENT: return "invalid argument";
+    case BZ_NOT_READY: return "not ready";
+    case BZ_TIMEOUT: return "timeout";
+    case BZ_INTERNAL_ERROR: return "internal error";
+    case BZ_CUDA_ERROR: return "cuda error";
+    case BZ_OUT_OF_MEMORY: return "out of memory";
+    case BZ_DEVICE_LIMIT: return "device limit";
+    case BZ_UNSUPPORTED: return "unsupported";
+    }
+    return "unknown";
+}
+
+bz_status bz_config_init(bz_config* c)
+{
+    if (!c)
+        return BZ_INVALID_ARGUMENT;
+    std::memset(c, 0, sizeof(*c));
+    c->struct_size = sizeof(bz_config);
+    c->solver = BZ_SOLVER_OCTREE;
+    c->octree_theta = 0.5f;
+    c->octree_softening = 0.01f;
+    c->octree_opening_criterion = 0;
+    c->linear_octree_leaf_capacity = 256;
+    c->leaf_capacity = 16;
+    c->multipole_order = 2;
+    c->physics_max_acceleration = 1e30f;
+    c->physics_min_softening = 0.0f;
+    c->physics_min_distance2 = 1.0e-12f;
+    c->physics_min_theta = 0.05f;
+    c->treepm_grid_size = 128;
+    c->treepm_r_split_cells = 1.25f;
+    c->treepm_r_cut_factor = 4.5f;
+    c->box_length = 0.0;
+    c->key_mode = BZ_KEYS_PRODUCTION;
+    c->device = 0;
+    c->stream = 0;
+    c->use_graph = 1;
+    return BZ_OK;
+}
+
+size_t bz_last_error(const bz_handle* h, char* buf, size_t cap)
+{
+    const std::string& e = h ? h->last_error : std::string();
+    if (buf && cap > 0) {
+        const size_t k = std::min(cap - 1, e.size());
+        std::memcpy(buf, e.data(), k);
+        buf[k] = '\0';
+    }
+    return e.size();
+}
+
+bz_status bz_destroy(bz_handle* h)
+{
+    if (!h)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    if (h->stream)
+        cudaStreamSynchronize(h->stream);
+    for (int i = 0; i < 2; ++i)
+        if (h->graph[i])
+            cudaGraphExecDestroy(h->graph[i]);
+    for (int i = 0; i <= kEvStepStart; ++i)
+        if (h->ev[i])
+            cudaEventDestroy(h->ev[i]);
+    pm_destroy(h->pm);
+    for (void* p : h->allocations)
+        cudaFree(p);
+    if (h->h_dt)
+        cudaFreeHost(h->h_dt);
+    if (h->own_stream && h->stream)
+        cudaStreamDestroy(h->stream);
+    delete h;
+    return BZ_OK;
+}
+
+bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
+{
+    if (!cfg || !out || capacity == 0 || cfg->struct_size != sizeof(bz_config))
+        return BZ_INVALID_ARGUMENT;
+    if (capacity > (1u << 25))
+        return BZ_UNSUPPORTED;  // node indices are packed in 26 bits by the walk
+    *out = nullptr;
+    bz_handle* h = new bz_handle();
+    h->cfg = *cfg;
+    h->device = cfg->device;
+    h->capacity = capacity;
+    if (cfg->solver == BZ_SOLVER_TREEPM) {
+        const int M = cfg->treepm_grid_size;
+        if (cfg->box_length <= 0.0 || M < 8 || (M & (M - 1)) != 0 || cfg->treepm_r_split_cells <= 0.0f ||
+            cfg->treepm_r_cut_factor <= 0.0f) {
+            delete h;
+            return BZ_INVALID_ARGUMENT;
+        }
+    }
+    if (cfg->leaf_capacity < 1 || cfg->octree_theta <= 0.0f) {
+        delete h;
+        return BZ_INVALID_ARGUMENT;
+    }
+    cudaError_t e = cudaSetDevice(h->device);
+    if (e != cudaSuccess) {
+        delete h;
+        return BZ_CUDA_ERROR;
+    }
+    if (cfg->stream) {
+        h->stream = reinterpret_cast<cudaStream_t>(cfg->stream);
+    } else {
+        if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+            delete h;
+            return BZ_CUDA_ERROR;
+        }
+        h->own_stream = true;
+    }
+    const size_t n = capacity;
+    DeviceBuffers& d = h->d;
+    bool ok = true;
+    for (int b = 0; b < 2; ++b) {
+        for (int c = 0; c < 6; ++c)
+            ok = ok && dalloc(h, &d.st[b][c], n);
+        ok = ok && dalloc(h, &d.mass[b], n) && dalloc(h, &d.id[b], n);
+    }
+    ok = ok && dalloc(h, &d.pos4, n);
+    for (int a = 0; a < 3; ++a)
+        ok = ok && dalloc(h, &d.acc[a], n);
+    ok = ok && dalloc(h, &d.pot, n) && dalloc(h, &d.keys, n) && dalloc(h, &d.perm, n) &&
+         dalloc(h, &d.box, 1) && dalloc(h, &d.bbox32, 8) && dalloc(h, &d.err, 1) &&
+         dalloc(h, &d.dt, 2) && dalloc(h, &d.queue, 1) && dalloc(h, &d.counters, 2) &&
+         dalloc(h, &d.stage, 7 * n) && dalloc(h, &d.ref_xyzm, 4 * n) && dalloc(h, &d.ref_orig, n) &&
+         dalloc(h, &d.ref_hot8, 8);
+    // sort workspace
+    SortWorkspace& sw = h->sort;
+    const size_t words = sort_state_words(static_cast<int>(n));
+    ok = ok && dalloc(h, &sw.keys_alt, n) && dalloc(h, &sw.vals_alt, n) && dalloc(h, &sw.hist, 8 * 256) &&
+         dalloc(h, &sw.base, 8 * 256) && dalloc(h, &sw.ticket, 8) && dalloc(h, &sw.epoch, 1) &&
+         dalloc(h, &sw.trivial, 8) && dalloc(h, &sw.state, words);
+    sw.max_tiles = static_cast<int>(words / 256);
+    // tree
+    TreeArrays& t = h->tree;
+    t.cap = static_cast<int>(2 * n + 1024);
+    const size_t cap = static_cast<size_t>(t.cap);
+    ok = ok && dalloc(h, &t.start, cap) && dalloc(h, &t.count, cap) && dalloc(h, &t.child, cap) &&
+         dalloc(h, &t.nchild, cap) && dalloc(h, &t.parent, cap) && dalloc(h, &t.level, cap) &&
+         dalloc(h, &t.lvl_first, kMaxLevels + 2) && dalloc(h, &t.lvl_count, kMaxLevels + 2) &&
+         dalloc(h, &t.n_nodes, 1) && dalloc(h, &t.ticket, kMaxLevels + 2) &&
+         dalloc(h, &t.lookback, cap / 256 + kMaxLevels + 4) && dalloc(h, &t.arrive, cap) &&
+         dalloc(h, &t.m64, cap) && dalloc(h, &t.s64, 3 * cap) && dalloc(h, &t.c64, 3 * cap) &&
+         dalloc(h, &t.q64, 6 * cap) && dalloc(h, &t.box0, cap) && dalloc(h, &t.box1, cap) &&
+         dalloc(h, &t.mono, cap) && dalloc(h, &t.quadA, cap) && dalloc(h, &t.quadB, cap);
+    // walk spill area: one slot per warp the persistent walk grid can hold
+    h->spill_slots = walk_spill_slots();
+    ok = ok && dalloc(h, &d.spill, static_cast<size_t>(h->spill_slots) * walk_spill_entries());
+    if (!ok) {
+        bz_destroy(h);
+        return BZ_OUT_OF_MEMORY;
+    }
+    cudaMemsetAsync(sw.state, 0, words * sizeof(unsigned long long), h->stream);
+    cudaMemsetAsync(sw.epoch, 0, sizeof(uint32_t), h->stream);
+    cudaMemsetAsync(d.err, 0, sizeof(int), h->stream);
+    if (cfg->solver == BZ_SOLVER_TREEPM) {
+        int perr = 0;
+        h->pm = pm_create(cfg->treepm_grid_size, cfg->box_length, rsplit_len(h), h->stream, &perr);
+        if (!h->pm) {
+            bz_destroy(h);
+            return BZ_OUT_OF_MEMORY;
+        }
+        h->bytes += pm_bytes(h->pm);
+    }
+    for (int i = 0; i <= kEvStepStart; ++i)
+        cudaEventCreate(&h->ev[i]);
+    cudaMallocHost(&h->h_dt, 2 * sizeof(double));
+    e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        bz_destroy(h);
+        return BZ_CUDA_ERROR;
+    }
+    *out = h;
+    return BZ_OK;
+}
+
+size_t bz_particle_count(const bz_handle* h) { return h ? h->n : 0; }
+size_t bz_device_bytes(const bz_handle* h) { return h ? h->bytes : 0; }
+
+}  // extern "C"
+
+namespace {
+
+__global__ void k_unpack_state(const float* __restrict__ st, int n, int have_vel, double* x,
+                               double* y, double* z, double* vx, double* vy, double* vz,
+                               float* m, int* id, double box)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double p[3] = {st[i], st[n + i], st[2 * n + i]};
+        if (box > 0.0)
+            for (int a = 0; a < 3; ++a) {
+                p[a] -= box * floor(p[a] / box);
+                if (p[a] >= box)
+                    p[a] = 0.0;
+            }
+        x[i] = p[0];
+        y[i] = p[1];
+        z[i] = p[2];
+        vx[i] = have_vel ? st[3 * n + i] : 0.0;
+        vy[i] = have_vel ? st[4 * n + i] : 0.0;
+        vz[i] = have_vel ? st[5 * n + i] : 0.0;
+        m[i] = st[6 * n + i];
+        id[i] = i;
+    }
+}
+
+__global__ void k_pack_state(const double* x, const double* y, const double* z,
+                             const double* vx, const double* vy, const double* vz,
+                             const int* __restrict__ id, int n, float* out, int want_vel)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int o = id[i];
+        out[o] = static_cast<float>(x[i]);
+        out[n + o] = static_cast<float>(y[i]);
+        out[2 * n + o] = static_cast<float>(z[i]);
+        if (want_vel) {
+            out[3 * n + o] = static_cast<float>(vx[i]);
+            out[4 * n + o] = static_cast<float>(vy[i]);
+            out[5 * n + o] = static_cast<float>(vz[i]);
+        }
+    }
+}
+
+__global__ void k_gather_f64(const double* const* __restrict__ src_unused, const double* x,
+                             const double* y, const double* z, const double* vx,
+                             const double* vy, const double* vz, const int* __restrict__ id,
+                             int n, double* out, int want_vel)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int o = id[i];
+        out[o] = x[i];
+        out[n + o] = y[i];
+        out[2 * n + o] = z[i];
+        if (want_vel) {
+            out[3 * n + o] = vx[i];
+            out[4 * n + o] = vy[i];
+            out[5 * n + o] = vz[i];
+        }
+    }
+}
+
+// caller-order FP32 positions + mass (reference mode / key parity)
+__global__ void k_caller_xyzm(const double* x, const double* y, const double* z,
+                              const float* m, const int* __restrict__ id, int n, float* xyzm,
+                              float4* orig)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int o = id[i];
+        const float px = static_cast<float>(x[i]), py = static_cast<float>(y[i]),
+                    pz = static_cast<float>(z[i]);
+        xyzm[o] = px;
+        xyzm[n + o] = py;
+        xyzm[2 * n + o] = pz;
+        xyzm[3 * n + o] = m[i];
+        orig[o] = make_float4(px, py, pz, m[i]);
+    }
+}
+
+__global__ void k_gather_pos4(const float4* __restrict__ orig, const uint32_t* __restrict__ perm,
+                              int n, float4* sorted)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        sorted[i] = orig[perm[i]];
+}
+
+__global__ void k_f64_from_f64soa(const double* src, double* dst, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+int blocks_for(size_t n) { return static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 8)); }
+
+bz_status upload_common(bz_handle* h, size_t n)
+{
+    h->n = n;
+    h->cur = 0;
+    h->forces_valid = false;
+    h->ref_tree_valid = false;
+    return BZ_OK;
+}
+
+// Reference mode: caller-order FP32 copy, reference keys + stable sort, one-leaf tree.
+void enqueue_reference_order(bz_handle* h)
+{
+    const int n = static_cast<int>(h->n);
+    DeviceBuffers& d = h->d;
+    double* const* s = d.st[h->cur];
+    k_caller_xyzm<<<blocks_for(n), 256, 0, h->stream>>>(s[0], s[1], s[2], d.mass[h->cur], d.id[h->cur],
+                                                        n, d.ref_xyzm, d.ref_orig);
+    launch_keys_reference(d.ref_xyzm, d.ref_xyzm + n, d.ref_xyzm + 2 * n, n, d.bbox32, d.keys,
+                          d.perm, h->stream);
+    launch_radix_sort(d.keys, d.perm, n, 32, h->sort, d.err, h->stream);
+    k_gather_pos4<<<blocks_for(n), 256, 0, h->stream>>>(d.ref_orig, d.perm, n, d.pos4);
+    launch_reference_leaf(d.ref_xyzm, d.ref_xyzm + n, d.ref_xyzm + 2 * n, d.ref_xyzm + 3 * n,
+                          d.perm, n, d.ref_hot8, h->stream);
+}
+
+} // namespace
+
+extern "C" {
+
+bz_status bz_set_state(bz_handle* h, const float* pos, const float* vel, const float* mass,
+                       size_t n)
+{
+    if (!h || !pos || !mass || n == 0 || n > h->capacity)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    DeviceBuffers& d = h->d;
+    cudaMemcpyAsync(d.stage, pos, 3 * n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    if (vel)
+        cudaMemcpyAsync(d.stage + 3 * n, vel, 3 * n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(d.stage + 6 * n, mass, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    upload_common(h, n);
+    double* const* s = d.st[0];
+    k_unpack_state<<<blocks_for(n), 256, 0, h->stream>>>(d.stage, static_cast<int>(n), vel ? 1 : 0,
+                                                         s[0], s[1], s[2], s[3], s[4], s[5],
+                                                         d.mass[0], d.id[0],
+                                                         periodic(h) ? h->cfg.box_length : 0.0);
+    return check_device(h, "bz_set_state");
+}
+
+bz_status bz_set_state_f64(bz_handle* h, const double* pos, const double* vel, const float* mass,
+                           size_t n)
+{
+    if (!h || !pos || !mass || n == 0 || n > h->capacity)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    DeviceBuffers& d = h->d;
+    double* const* s = d.st[0];
+    for (int a = 0; a < 3; ++a) {
+        cudaMemcpyAsync(s[a], pos + a * n, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+        if (vel)
+            cudaMemcpyAsync(s[3 + a], vel + a * n, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+        else
+            cudaMemsetAsync(s[3 + a], 0, n * sizeof(double), h->stream);
+    }
+    cudaMemcpyAsync(d.stage + 6 * n, mass, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(d.mass[0], mass, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    upload_common(h, n);
+    std::vector<int> ids(n);
+    for (size_t i = 0; i < n; ++i)
+        ids[i] = static_cast<int>(i);
+    cudaMemcpyAsync(d.id[0], ids.data(), n * sizeof(int), cudaMemcpyHostToDevice, h->stream);
+    return check_device(h, "bz_set_state_f64");
+}
+
+bz_status bz_get_state(bz_handle* h, float* pos, float* vel)
+{
+    if (!h || !pos || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    const size_t n = h->n;
+    DeviceBuffers& d = h->d;
+    double* const* s = d.st[h->cur];
+    k_pack_state<<<blocks_for(n), 256, 0, h->stream>>>(s[0], s[1], s[2], s[3], s[4], s[5], d.id[h->cur],
+                                                       static_cast<int>(n), d.stage, vel ? 1 : 0);
+    cudaMemcpyAsync(pos, d.stage, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (vel)
+        cudaMemcpyAsync(vel, d.stage + 3 * n, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    return check_device(h, "bz_get_state");
+}
+
+bz_status bz_get_state_f64(bz_handle* h, double* pos, double* vel)
+{
+    if (!h || !pos || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    const size_t n = h->n;
+    DeviceBuffers& d = h->d;
+    double* const* s = d.st[h->cur];
+    // reuse the alternate state buffers as a 6n-double staging area
+    double* tmp = nullptr;
+    if (!dalloc(h, &tmp, 6 * n))
+        return fail(h, BZ_OUT_OF_MEMORY, "bz_get_state_f64 staging");
+    k_gather_f64<<<blocks_for(n), 256, 0, h->stream>>>(nullptr, s[0], s[1], s[2], s[3], s[4], s[5],
+                                                       d.id[h->cur], static_cast<int>(n), tmp,
+                                                       vel ? 1 : 0);
+    cudaMemcpyAsync(pos, tmp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (vel)
+        cudaMemcpyAsync(vel, tmp + 3 * n, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    const bz_status st = check_device(h, "bz_get_state_f64");
+    cudaFree(tmp);
+    h->allocations.pop_back();
+    h->bytes -= 6 * n * sizeof(double);
+    return st;
+}
+
+bz_status bz_enable_phase_timing(bz_handle* h, int enable)
+{
+    if (!h)
+        return BZ_INVALID_ARGUMENT;
+    h->timing = enable != 0;
+    return BZ_OK;
+}
+
+bz_status bz_phase_times(bz_handle* h, float* ms, int n)
+{
+    if (!h || !ms)
+        return BZ_INVALID_ARGUMENT;
+    for (int i = 0; i < n && i < kNumPhases; ++i)
+        ms[i] = h->phase_ms[i];
+    return BZ_OK;
+}
+
+bz_status bz_interaction_counts(bz_handle* h, uint64_t* n_pp, uint64_t* n_pn)
+{
+    if (!h)
+        return BZ_INVALID_ARGUMENT;
+    if (n_pp)
+        *n_pp = h->last_pp;
+    if (n_pn)
+        *n_pn = h->last_pn;
+    return BZ_OK;
+}
+
+bz_status bz_accelerations(bz_handle* h, float* acc, float* pot)
+{
+    if (!h || !acc || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    const int n = static_cast<int>(h->n);
+    DeviceBuffers& d = h->d;
+    if (h->cfg.solver == BZ_SOLVER_OCTREE_REFERENCE) {
+        if (pot)
+            return fail(h, BZ_UNSUPPORTED, "potentials are not part of the reference formulation");
+        enqueue_reference_order(h);
+        const float eps = std::max(h->cfg.octree_softening, h->cfg.physics_min_softening);
+        launch_reference_walk(d.ref_orig, d.pos4, d.perm, n, eps, h->cfg.physics_min_distance2, 0.0f,
+                              0.0f, h->cfg.physics_max_acceleration, d.stage, d.stage + n,
+                              d.stage + 2 * n, h->stream);
+        cudaMemcpyAsync(acc, d.stage, 3 * static_cast<size_t>(n) * sizeof(float),
+                        cudaMemcpyDeviceToHost, h->stream);
+        bz_status s = check_device(h, "bz_accelerations (reference)");
+        if (s == BZ_OK)
+            h->ref_tree_valid = true;
+        return s;
+    }
+    h->stepping = false;
+    enqueue_order(h);
+    enqueue_forces(h, false, pot != nullptr);
+    record(h, kNumPhases);
+    launch_scatter3(d.acc[0], d.acc[1], d.acc[2], d.id[h->cur], n, d.stage, h->stream);
+    cudaMemcpyAsync(acc, d.stage, 3 * static_cast<size_t>(n) * sizeof(float), cudaMemcpyDeviceToHost,
+                    h->stream);
+    if (pot) {
+        launch_scatter3(d.pot, d.pot, d.pot, d.id[h->cur], n, d.stage + 3 * n, h->stream);
+        cudaMemcpyAsync(pot, d.stage + 3 * n, static_cast<size_t>(n) * sizeof(float),
+                        cudaMemcpyDeviceToHost, h->stream);
+    }
+    bz_status s = check_device(h, "bz_accelerations");
+    if (s != BZ_OK)
+        return s;
+    collect_timing(h);
+    read_counters(h);
+    h->forces_valid = true;
+    return BZ_OK;
+}
+
+bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps)
+{
+    if (!h || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    if (h->cfg.solver == BZ_SOLVER_OCTREE_REFERENCE)
+        return fail(h, BZ_UNSUPPORTED, "the reference formulation is a parity mode; step with BZ_SOLVER_OCTREE");
+    if (nsteps == 0)
+        return BZ_OK;
+    cudaSetDevice(h->device);
+    h->h_dt[0] = dt;
+    h->h_dt[1] = 0.5 * dt;
+    cudaMemcpyAsync(h->d.dt, h->h_dt, 2 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    bz_status s = ensure_forces(h);
+    if (s != BZ_OK)
+        return s;
+    h->stepping = true;
+    uint32_t done = 0;
+    if (h->cfg.use_graph && !h->timing) {
+        build_graphs(h);
+        if (!h->graph_failed)
+            for (; done < nsteps; ++done) {
+                cudaGraphLaunch(h->graph[h->cur], h->stream);
+                h->cur ^= 1;
+            }
+    }
+    for (; done < nsteps; ++done) {
+        record(h, kEvStepStart);
+        enqueue_step(h);
+    }
+    if (h->timing)
+        record(h, kNumPhases);
+    s = check_device(h, "bz_step");
+    if (s != BZ_OK)
+        return s;
+    collect_timing(h);
+    read_counters(h);
+    return BZ_OK;
+}
+
+bz_status bz_morton_keys(bz_handle* h, uint64_t* sorted_keys, int32_t* perm)
+{
+    if (!h || h->n == 0 || !sorted_keys || !perm)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    const int n = static_cast<int>(h->n);
+    DeviceBuffers& d = h->d;
+    if (h->cfg.key_mode == BZ_KEYS_REFERENCE || h->cfg.solver == BZ_SOLVER_OCTREE_REFERENCE) {
+        enqueue_reference_order(h);
+        h->ref_tree_valid = true;
+    } else {
+        // production keys computed in the caller's order (stable ties follow caller order)
+        double* const* s = d.st[h->cur];
+        double* tmp = nullptr;
+        if (!dalloc(h, &tmp, 3 * static_cast<size_t>(n)))
+            return fail(h, BZ_OUT_OF_MEMORY, "bz_morton_keys staging");
+        k_gather_f64<<<blocks_for(n), 256, 0, h->stream>>>(nullptr, s[0], s[1], s[2], s[3], s[4], s[5],
+                                                           d.id[h->cur], n, tmp, 0);
+        if (!periodic(h))
+            launch_bbox_f64(tmp, tmp + n, tmp + 2 * n, n, d.box, h->stream);
+        launch_keys63(tmp, tmp + n, tmp + 2 * n, n, d.box, periodic(h) ? h->cfg.box_length : 0.0,
+                      d.keys, d.perm, h->stream);
+        launch_radix_sort(d.keys, d.perm, n, 64, h->sort, d.err, h->stream);
+        cudaStreamSynchronize(h->stream);
+        cudaFree(tmp);
+        h->allocations.pop_back();
+        h->bytes -= 3 * static_cast<size_t>(n) * sizeof(double);
+        h->forces_valid = false;  // keys buffer reused
+    }
+    cudaMemcpyAsync(sorted_keys, d.keys, n * sizeof(uint64_t), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(perm, d.perm, n * sizeof(int32_t), cudaMemcpyDeviceToHost, h->stream);
+    return check_device(h, "bz_morton_keys");
+}
+
+bz_status bz_reference_tree(bz_handle* h, int64_t* node_count, float* hot8, int32_t* next,
+                            int32_t* child_mask, int32_t* first_child, int32_t* leaf_start,
+                            int32_t* leaf_count)
+{
+    if (!h || !node_count || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    if (!h->ref_tree_valid) {
+        enqueue_reference_order(h);
+        bz_status s = check_device(h, "bz_reference_tree");
+        if (s != BZ_OK)
+            return s;
+        h->ref_tree_valid = true;
+    }
+    *node_count = 1;
+    if (hot8) {
+        cudaMemcpy(hot8, h->d.ref_hot8, 8 * sizeof(float), cudaMemcpyDeviceToHost);
+    }
+    if (next)
+        next[0] = -1;
+    if (child_mask)
+        child_mask[0] = 0;
+    if (first_child)
+        first_child[0] = -1;
+    if (leaf_start)
+        leaf_start[0] = 0;
+    if (leaf_count)
+        leaf_count[0] = static_cast<int32_t>(h->n);
+    return BZ_OK;
+}
+
+bz_status bz_tree_topology(bz_handle* h, int64_t* node_count, int32_t* start, int32_t* count,
+                           int32_t* child, int32_t* nchild, float* mono4, float* bmin3,
+                           float* bmax3, float* quad6)
+{
+    if (!h || !node_count || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    if (h->cfg.solver == BZ_SOLVER_OCTREE_REFERENCE)
+        return fail(h, BZ_UNSUPPORTED, "use bz_reference_tree in reference mode");
+    cudaSetDevice(h->device);
+    bz_status s = ensure_forces(h);
+    if (s != BZ_OK)
+        return s;
+    int nn = 0;
+    cudaMemcpy(&nn, h->tree.n_nodes, sizeof(int), cudaMemcpyDeviceToHost);
+    *node_count = nn;
+    if (!start && !count && !child && !nchild && !mono4 && !bmin3 && !bmax3 && !quad6)
+        return BZ_OK;
+    const size_t k = static_cast<size_t>(nn);
+    if (start)
+        cudaMemcpy(start, h->tree.start, k * sizeof(int), cudaMemcpyDeviceToHost);
+    if (count)
+        cudaMemcpy(count, h->tree.count, k * sizeof(int), cudaMemcpyDeviceToHost);
+    if (child)
+        cudaMemcpy(child, h->tree.child, k * sizeof(int), cudaMemcpyDeviceToHost);
+    if (nchild)
+        cudaMemcpy(nchild, h->tree.nchild, k * sizeof(int), cudaMemcpyDeviceToHost);
+    if (mono4)
+        cudaMemcpy(mono4, h->tree.mono, k * sizeof(float4), cudaMemcpyDeviceToHost);
+    std::vector<float4> b(k);
+    if (bmin3) {
+        cudaMemcpy(b.data(), h->tree.box0, k * sizeof(float4), cudaMemcpyDeviceToHost);
+        for (size_t i = 0; i < k; ++i) {
+            bmin3[3 * i] = b[i].x;
+            bmin3[3 * i + 1] = b[i].y;
+            bmin3[3 * i + 2] = b[i].z;
+        }
+    }
+    if (bmax3) {
+        cudaMemcpy(b.data(), h->tree.box1, k * sizeof(float4), cudaMemcpyDeviceToHost);
+        for (size_t i = 0; i < k; ++i) {
+            bmax3[3 * i] = b[i].x;
+            bmax3[3 * i + 1] = b[i].y;
+            bmax3[3 * i + 2] = b[i].z;
+        }
+    }
+    if (quad6) {
+        std::vector<float4> qa(k);
+        std::vector<float2> qb(k);
+        cudaMemcpy(qa.data(), h->tree.quadA, k * sizeof(float4), cudaMemcpyDeviceToHost);
+        cudaMemcpy(qb.data(), h->tree.quadB, k * sizeof(float2), cudaMemcpyDeviceToHost);
+        for (size_t i = 0; i < k; ++i) {
+            quad6[6 * i] = qa[i].x;
+            quad6[6 * i + 1] = qa[i].y;
+            quad6[6 * i + 2] = qa[i].z;
+            quad6[6 * i + 3] = qa[i].w;
+            quad6[6 * i + 4] = qb[i].x;
+            quad6[6 * i + 5] = qb[i].y;
+        }
+    }
+    return check_device(h, "bz_tree_topology");
+}
+
+bz_status bz_pm_mesh(bz_handle* h, int which, float* out)
+{
+    if (!h || !out || !h->pm || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    bz_status s = ensure_forces(h);
+    if (s != BZ_OK)
+        return s;
+    pm_deposit(h->pm, h->d.pos4, static_cast<int>(h->n), h->stream);
+    if (which == 1 && pm_solve(h->pm, h->stream) != 0)
+        return fail(h, BZ_CUDA_ERROR, "[cufft] mesh solve failed");
+    const size_t M = static_cast<size_t>(h->cfg.treepm_grid_size);
+    cudaMemcpyAsync(out, pm_mesh(h->pm), M * M * M * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    return check_device(h, "bz_pm_mesh");
+}
+
+bz_status bz_force_errors(bz_handle* h, int32_t nsample, uint64_t seed, float* errs,
+                          int32_t* idx, double* median, double* p99)
+{
+    if (!h || nsample <= 0 || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    bz_status s = ensure_forces(h);
+    if (s != BZ_OK)
+        return s;
+    const int n = static_cast<int>(h->n);
+    const int ns = std::min(nsample, n);
+    // sample caller indices without replacement, then map to sorted slots
+    std::mt19937_64 rng(seed);
+    std::vector<int> all(n);
+    for (int i = 0; i < n; ++i)
+        all[i] = i;
+    for (int i = 0; i < ns; ++i) {
+        std::uniform_int_distribution<int> u(i, n - 1);
+        std::swap(all[i], all[u(rng)]);
+    }
+    std::vector<int> ids(n);
+    cudaMemcpy(ids.data(), h->d.id[h->cur], n * sizeof(int), cudaMemcpyDeviceToHost);
+    std::vector<int> slot_of(n);
+    for (int i = 0; i < n; ++i)
+        slot_of[ids[i]] = i;
+    std::vector<int> slots(ns);
+    for (int i = 0; i < ns; ++i)
+        slots[i] = slot_of[all[i]];
+    int* dslots = nullptr;
+    double* dref = nullptr;
+    double* sk = nullptr;
+    const int kmax = 8;
+    const bool per = periodic(h);
+    if (cudaMalloc(&dslots, ns * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&dref, 3 * ns * sizeof(double)) != cudaSuccess ||
+        (per && cudaMalloc(&sk, 5 * static_cast<size_t>(ewald_num_k(kmax)) * sizeof(double)) != cudaSuccess)) {
+        cudaFree(dslots);
+        cudaFree(dref);
+        cudaFree(sk);
+        return fail(h, BZ_OUT_OF_MEMORY, "bz_force_errors scratch");
+    }
+    cudaMemcpy(dslots, slots.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
+    const double eps = std::max(h->cfg.octree_softening, h->cfg.physics_min_softening);
+    if (per)
+        launch_ewald_f64(h->d.pos4, n, dslots, ns, eps, h->cfg.box_length, 6.4 / h->cfg.box_length,
+                         kmax, sk, dref, h->stream);
+    else
+        launch_direct_f64(h->d.pos4, n, dslots, ns, eps, dref, h->stream);
+    std::vector<double> ref(3 * ns);
+    std::vector<float> ax(n), ay(n), az(n);
+    cudaMemcpyAsync(ref.data(), dref, 3 * ns * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(ax.data(), h->d.acc[0], n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(ay.data(), h->d.acc[1], n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(az.data(), h->d.acc[2], n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    s = check_device(h, "bz_force_errors");
+    cudaFree(dslots);
+    cudaFree(dref);
+    cudaFree(sk);
+    if (s != BZ_OK)
+        return s;
+    std::vector<double> e(ns);
+    for (int i = 0; i < ns; ++i) {
+        const int k = slots[i];
+        const double dx = ax[k] - ref[3 * i], dy = ay[k] - ref[3 * i + 1], dz = az[k] - ref[3 * i + 2];
+        const double rn = std::sqrt(ref[3 * i] * ref[3 * i] + ref[3 * i + 1] * ref[3 * i + 1] +
+                                    ref[3 * i + 2] * ref[3 * i + 2]);
+        e[i] = std::sqrt(dx * dx + dy * dy + dz * dz) / (rn > 0 ? rn : 1.0);
+        if (errs)
+            errs[i] = static_cast<float>(e[i]);
+        if (idx)
+            idx[i] = all[i];
+    }
+    std::vector<double> sorted = e;
+    std::sort(sorted.begin(), sorted.end());
+    auto pct = [&](double q) {
+        const double pos = q * (ns - 1);
+        const int lo = static_cast<int>(std::floor(pos));
+        const int hi = std::min(lo + 1, ns - 1);
+        return sorted[lo] + (sorted[hi] - sorted[lo]) * (pos - lo);
+    };
+    if (median)
+        *median = pct(0.5);
+    if (p99)
+        *p99 = pct(0.99);
+    return BZ_OK;
+}
+
+}  // extern "C"

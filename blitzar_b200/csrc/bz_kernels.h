@@ -1,0 +1,150 @@
+// Internal launch interface between the C-ABI layer (bz_api.cu) and the kernel files.
+// Every launcher enqueues on the given stream and never synchronises.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace bz {
+
+// ---------------------------------------------------------------- keys (bz_keys.cu)
+struct BoxF64 {
+    unsigned long long mn[3];  // ordered-integer images of the FP64 minima
+    unsigned long long mx[3];  // ... and maxima
+};
+void launch_bbox_f64(const double* x, const double* y, const double* z, int n, BoxF64* box,
+                     cudaStream_t s);
+// Production keys: 21 bits per axis, floor quantisation of a cube.  periodic_len > 0 uses
+// the cube [0, L)^3; otherwise the cube is derived on the device from *box.
+void launch_keys63(const double* x, const double* y, const double* z, int n,
+                   const BoxF64* box, double periodic_len, unsigned long long* keys,
+                   uint32_t* perm, cudaStream_t s);
+// Reference-compatible keys (FP32 bbox, the reference's quantisation and bit spread).
+void launch_keys_reference(const float* x, const float* y, const float* z, int n,
+                           unsigned* bbox_ordered6, unsigned long long* keys, uint32_t* perm,
+                           cudaStream_t s);
+
+// ---------------------------------------------------------------- sort (bz_sort.cu)
+struct SortWorkspace {
+    unsigned long long* keys_alt;
+    uint32_t* vals_alt;
+    uint32_t* hist;              // [8][256] digit counts
+    uint32_t* base;              // [8][256] exclusive digit bases
+    uint32_t* ticket;            // [8] tile tickets
+    uint32_t* epoch;             // [1] sort-call counter (look-back state tag)
+    int* trivial;                // [8] pass-is-identity flags
+    unsigned long long* state;   // [max_tiles][256] look-back words
+    int max_tiles;
+};
+size_t sort_state_words(int n);
+int sort_tile_items();
+// Stable LSD radix sort of (keys, vals) on the low `bits` key bits (multiple of 8).  The
+// sorted result lands back in (keys, vals).
+void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits,
+                       SortWorkspace& ws, int* err, cudaStream_t s);
+
+// ---------------------------------------------------------------- tree (bz_tree.cu)
+struct TreeArrays {
+    int cap;           // node capacity
+    int* start;        // particle range of each node
+    int* count;
+    int* child;        // first child (-1 for leaves)
+    int* nchild;
+    int* parent;
+    int* level;
+    int* lvl_first;    // [kMaxLevels+2]
+    int* lvl_count;    // [kMaxLevels+2]
+    int* n_nodes;      // [1]
+    uint32_t* ticket;  // [kMaxLevels+2]
+    unsigned long long* lookback;  // [cap/256 + kMaxLevels + 2]
+    int* arrive;       // [cap] bottom-up arrival counters
+    double* m64;       // [cap] FP64 mass
+    double* s64;       // [3*cap] FP64 first moments
+    double* c64;       // [3*cap] FP64 centre of mass
+    double* q64;       // [6*cap] FP64 second moments about the COM
+    float4* box0;      // {bmin.xyz, link}
+    float4* box1;      // {bmax.xyz, info}
+    float4* mono;      // {com.xyz, mass}
+    float4* quadA;     // {qxx, qxy, qxz, qyy}
+    float2* quadB;     // {qyz, qzz}
+};
+constexpr int kMaxLevels = 21;
+void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
+                       int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s);
+
+// Reference-mode topology: the single leaf the reference builds for its own keys.
+void launch_reference_leaf(const float* x, const float* y, const float* z, const float* m,
+                           const uint32_t* sorted_index, int n, float* hot8, cudaStream_t s);
+
+// ---------------------------------------------------------------- walk (bz_walk.cu)
+struct WalkParams {
+    float theta2;
+    float eps2;
+    float rcut2;      // 0 disables the cutoff
+    float box;        // periodic length, 0 = open
+    float rsplit;     // Gaussian split scale, 0 = Newtonian
+    float min_dist2;
+    int quadrupole;
+    int want_pot;
+};
+struct WalkOutputs {
+    float* ax;        // accumulated into (+=)
+    float* ay;
+    float* az;
+    float* pot;       // optional (+=)
+    unsigned long long* n_pp;  // optional per-group counters
+    unsigned long long* n_pn;
+    unsigned long long* totals; // optional [2] sums of the above
+};
+void launch_walk(const float4* pos4, int n, const TreeArrays& t, const WalkParams& p,
+                 const WalkOutputs& o, unsigned* queue, int* spill, int* err, cudaStream_t s);
+int walk_spill_slots();       // warp slots that need a spill area
+size_t walk_spill_entries();  // ints per slot
+
+// Reference-formulation direct sum (the walk the reference runs on its one-leaf tree).
+void launch_reference_walk(const float4* pos_orig, const float4* pos_sorted,
+                           const uint32_t* sorted_index, int n, float softening,
+                           float min_distance2, float split_scale, float cutoff2,
+                           float max_acceleration, float* ax, float* ay, float* az,
+                           cudaStream_t s);
+
+// ---------------------------------------------------------------- PM (bz_pm.cu)
+struct PmPlan;
+PmPlan* pm_create(int mesh, double box, double rsplit, cudaStream_t s, int* cuda_err);
+void pm_destroy(PmPlan* p);
+size_t pm_bytes(const PmPlan* p);
+// Deposit, FFT Poisson solve with split + deconvolution, then interpolate the centred-
+// difference gradient at each particle; writes (=) ax, ay, az.
+int pm_forces(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float* az,
+              cudaStream_t s);
+// The three stages separately (tests read the mesh between them): the mesh buffer holds the
+// density after pm_deposit and the potential after pm_solve.
+void pm_deposit(PmPlan* p, const float4* pos4, int n, cudaStream_t s);
+int pm_solve(PmPlan* p, cudaStream_t s);
+void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float* az,
+               cudaStream_t s);
+float* pm_mesh(PmPlan* p);
+
+// ---------------------------------------------------------------- state (bz_state.cu)
+void launch_permute(const uint32_t* perm, int n, const double* const* src, double* const* dst,
+                    int ndouble, const float* msrc, float* mdst, const int* idsrc, int* iddst,
+                    float4* pos4, double periodic_len, cudaStream_t s);
+void launch_kick(double* vx, double* vy, double* vz, const float* ax, const float* ay,
+                 const float* az, int n, const double* dt_half, cudaStream_t s);
+void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                       const float* ax, const float* ay, const float* az, int n,
+                       const double* dt, double periodic_len, BoxF64* box, cudaStream_t s);
+void launch_scatter3(const float* ax, const float* ay, const float* az, const int* id, int n,
+                     float* out_soa3, cudaStream_t s);
+void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s);
+
+// ---------------------------------------------------------------- diagnostics (bz_diag.cu)
+// FP64 reference accelerations for the listed (sorted-order) targets: direct sum (open) or
+// Ewald (periodic).
+void launch_direct_f64(const float4* pos4, int n, const int* targets, int nt, double eps,
+                       double* acc3, cudaStream_t s);
+void launch_ewald_f64(const float4* pos4, int n, const int* targets, int nt, double eps,
+                      double box, double alpha, int kmax, double* sk_scratch, double* acc3,
+                      cudaStream_t s);
+int ewald_num_k(int kmax);
+
+} // namespace bz

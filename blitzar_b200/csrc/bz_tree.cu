@@ -1,0 +1,414 @@
+// Adaptive linear octree over Morton-sorted particles: top-down topology (one kernel per
+// level, decoupled look-back over the level's child counts, no host round trip) and a single
+// bottom-up moments kernel (last-arriving child computes its parent).
+//
+// This file is compiled with --fmad=false: the FP64 moment sums must round exactly as written
+// (fixed order, no contraction) so that node moments are bit-identical to the oracle's.
+//
+// Replaces the reference's level loop with a host sync per level
+// (engine/physics/octree/cuda/linear/OctBuild.inl:156-199, OctLeafKernels.inl:7-81,
+// OctParentKernels.inl:7-103, OctLinkKernels.inl): same idea (node = Morton cell, children
+// from the next 3 key bits, FP64 mass/COM), but leaves are adaptive (<= leaf_cap particles),
+// children of a node are contiguous (breadth-first layout, no `next` links needed) and the
+// moments include the quadrupole.
+#include "bz_common.cuh"
+#include "bz_kernels.h"
+
+namespace bz {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr unsigned long long kAgg = 1ull << 30;
+constexpr unsigned long long kPrefix = 2ull << 30;
+constexpr unsigned long long kMask = (1ull << 30) - 1;
+
+__global__ void k_tree_init(TreeArrays t, int n)
+{
+    const int i = threadIdx.x;
+    if (i < kMaxLevels + 2) {
+        t.lvl_first[i] = 0;
+        t.lvl_count[i] = 0;
+        t.ticket[i] = 0;
+    }
+    if (i == 0) {
+        t.lvl_count[0] = 1;
+        t.n_nodes[0] = 1;
+        t.start[0] = 0;
+        t.count[0] = n;
+        t.parent[0] = -1;
+        t.level[0] = 0;
+        t.arrive[0] = 0;
+    }
+}
+
+__device__ __forceinline__ int lower_bound_digit(const unsigned long long* __restrict__ keys,
+                                                 int lo, int hi, int shift, unsigned d)
+{
+    // first i in [lo, hi) with digit(i) >= d (digits are non-decreasing inside a cell)
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const unsigned dm = static_cast<unsigned>((keys[mid] >> shift) & 7u);
+        if (dm < d)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ unsigned long long vload(const unsigned long long* p)
+{
+    return *reinterpret_cast<const volatile unsigned long long*>(p);
+}
+__device__ __forceinline__ void vstore(unsigned long long* p, unsigned long long v)
+{
+    *reinterpret_cast<volatile unsigned long long*>(p) = v;
+}
+
+// Split every node of level `l` with more than leaf_cap particles into its non-empty octant
+// cells.  Children of the level are appended in (parent, octant) order.
+__global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long long* __restrict__ keys,
+                                                          int l, int leaf_cap, int max_level,
+                                                          TreeArrays t, int* err)
+{
+    __shared__ int s_tile;
+    __shared__ int s_scan[kThreads];
+    __shared__ int s_prefix;
+    const int first = t.lvl_first[l];
+    // after a capacity overflow the recorded count can exceed the arrays: clamp
+    const int cnt = min(t.lvl_count[l], t.cap - first);
+    if (cnt <= 0)
+        return;
+    const int ntiles = (cnt + kThreads - 1) / kThreads;
+    const int next_first = first + cnt;
+    unsigned long long* lb = t.lookback + (first / kThreads + l);
+    const int shift = 3 * (max_level - l - 1);
+    for (;;) {
+        if (threadIdx.x == 0)
+            s_tile = static_cast<int>(atomicAdd(&t.ticket[l], 1u));
+        __syncthreads();
+        const int tile = s_tile;
+        __syncthreads();
+        if (tile >= ntiles)
+            break;
+        const int k = first + tile * kThreads + threadIdx.x;
+        int b[9];
+        int nch = 0;
+        bool split = false;
+        if (k < next_first) {
+            const int s = t.start[k], c = t.count[k];
+            split = c > leaf_cap && l < max_level;
+            if (split) {
+                b[0] = s;
+                b[8] = s + c;
+#pragma unroll
+                for (int d = 1; d < 8; ++d)
+                    b[d] = lower_bound_digit(keys, b[d - 1], s + c, shift, static_cast<unsigned>(d));
+#pragma unroll
+                for (int d = 0; d < 8; ++d)
+                    nch += b[d + 1] > b[d] ? 1 : 0;
+            }
+        }
+        // block exclusive scan of child counts
+        s_scan[threadIdx.x] = nch;
+        __syncthreads();
+        for (int o = 1; o < kThreads; o <<= 1) {
+            const int v = threadIdx.x >= o ? s_scan[threadIdx.x - o] : 0;
+            __syncthreads();
+            s_scan[threadIdx.x] += v;
+            __syncthreads();
+        }
+        const int incl = s_scan[threadIdx.x];
+        const int total = s_scan[kThreads - 1];
+        if (threadIdx.x == 0) {
+            unsigned long long excl = 0;
+            if (tile == 0) {
+                vstore(&lb[0], kPrefix | static_cast<unsigned long long>(total));
+            } else {
+                vstore(&lb[tile], kAgg | static_cast<unsigned long long>(total));
+                int tt = tile - 1, spins = 0;
+                while (tt >= 0) {
+                    const unsigned long long v = vload(&lb[tt]);
+                    if ((v & (3ull << 30)) == 0) {
+                        if (++spins > kSpinLimit) {
+                            raise_error(err, kErrTreeSpin);
+                            break;
+                        }
+                        if (spins > 32)
+                            __nanosleep(32);
+                        continue;
+                    }
+                    excl += v & kMask;
+                    if (v & kPrefix)
+                        break;
+                    --tt;
+                }
+                vstore(&lb[tile], kPrefix | (excl + static_cast<unsigned long long>(total)));
+            }
+            s_prefix = static_cast<int>(excl);
+            if (tile == ntiles - 1) {
+                const int children = static_cast<int>(excl) + total;
+                t.lvl_first[l + 1] = next_first;
+                t.lvl_count[l + 1] = children;
+                t.n_nodes[0] = min(next_first + children, t.cap);
+                if (next_first + children > t.cap)
+                    raise_error(err, kErrTreeCapacity);
+            }
+        }
+        __syncthreads();
+        if (k < next_first) {
+            int c0 = next_first + s_prefix + incl - nch;
+            if (split && c0 + nch > t.cap)
+                nch = 0;  // capacity exceeded (error raised above): keep the node a leaf
+            t.child[k] = nch > 0 ? c0 : -1;
+            t.nchild[k] = nch;
+            if (nch > 0) {
+#pragma unroll
+                for (int d = 0; d < 8; ++d) {
+                    if (b[d + 1] > b[d]) {
+                        t.start[c0] = b[d];
+                        t.count[c0] = b[d + 1] - b[d];
+                        t.parent[c0] = k;
+                        t.level[c0] = l + 1;
+                        t.arrive[c0] = 0;
+                        ++c0;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Leaves of the deepest level are never visited by k_tree_level (it stops at max_level), so
+// their child fields are written here before the moments pass reads them.
+__global__ void k_tree_finish_last(TreeArrays t, int max_level)
+{
+    const int first = t.lvl_first[max_level];
+    const int cnt = min(t.lvl_count[max_level], t.cap - first);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x) {
+        t.child[first + i] = -1;
+        t.nchild[first + i] = 0;
+    }
+}
+
+__device__ void leaf_moments(const float4* __restrict__ pos4, int k, TreeArrays& t)
+{
+    const int s = t.start[k], e = s + t.count[k];
+    float mn[3] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
+    float mx[3] = {-3.402823466e38f, -3.402823466e38f, -3.402823466e38f};
+    double tm = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int i = s; i < e; ++i) {
+        const float4 p = pos4[i];
+        mn[0] = fminf(mn[0], p.x);
+        mn[1] = fminf(mn[1], p.y);
+        mn[2] = fminf(mn[2], p.z);
+        mx[0] = fmaxf(mx[0], p.x);
+        mx[1] = fmaxf(mx[1], p.y);
+        mx[2] = fmaxf(mx[2], p.z);
+        tm += (double)p.w;
+        sx += (double)p.w * (double)p.x;
+        sy += (double)p.w * (double)p.y;
+        sz += (double)p.w * (double)p.z;
+    }
+    const double cx = tm > 0.0 ? sx / tm : 0.5 * ((double)mn[0] + (double)mx[0]);
+    const double cy = tm > 0.0 ? sy / tm : 0.5 * ((double)mn[1] + (double)mx[1]);
+    const double cz = tm > 0.0 ? sz / tm : 0.5 * ((double)mn[2] + (double)mx[2]);
+    double q[6] = {0, 0, 0, 0, 0, 0};
+    for (int i = s; i < e; ++i) {
+        const float4 p = pos4[i];
+        const double dx = (double)p.x - cx, dy = (double)p.y - cy, dz = (double)p.z - cz;
+        const double w = (double)p.w;
+        q[0] += w * dx * dx;
+        q[1] += w * dx * dy;
+        q[2] += w * dx * dz;
+        q[3] += w * dy * dy;
+        q[4] += w * dy * dz;
+        q[5] += w * dz * dz;
+    }
+    t.m64[k] = tm;
+    t.s64[3 * k] = sx;
+    t.s64[3 * k + 1] = sy;
+    t.s64[3 * k + 2] = sz;
+    t.c64[3 * k] = cx;
+    t.c64[3 * k + 1] = cy;
+    t.c64[3 * k + 2] = cz;
+    for (int j = 0; j < 6; ++j)
+        t.q64[6 * k + j] = q[j];
+    t.box0[k] = make_float4(mn[0], mn[1], mn[2], __int_as_float(s));
+    t.box1[k] = make_float4(mx[0], mx[1], mx[2], __int_as_float(-(e - s)));
+    t.mono[k] = make_float4((float)cx, (float)cy, (float)cz, (float)tm);
+    t.quadA[k] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+    t.quadB[k] = make_float2((float)q[4], (float)q[5]);
+}
+
+__device__ void internal_moments(int k, TreeArrays& t)
+{
+    const int c0 = t.child[k], c1 = c0 + t.nchild[k];
+    float mn[3] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
+    float mx[3] = {-3.402823466e38f, -3.402823466e38f, -3.402823466e38f};
+    double tm = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
+    for (int c = c0; c < c1; ++c) {
+        const float4 b0 = __ldcg(&t.box0[c]);
+        const float4 b1 = __ldcg(&t.box1[c]);
+        mn[0] = fminf(mn[0], b0.x);
+        mn[1] = fminf(mn[1], b0.y);
+        mn[2] = fminf(mn[2], b0.z);
+        mx[0] = fmaxf(mx[0], b1.x);
+        mx[1] = fmaxf(mx[1], b1.y);
+        mx[2] = fmaxf(mx[2], b1.z);
+        tm += __ldcg(&t.m64[c]);
+        sx += __ldcg(&t.s64[3 * c]);
+        sy += __ldcg(&t.s64[3 * c + 1]);
+        sz += __ldcg(&t.s64[3 * c + 2]);
+    }
+    const double cx = tm > 0.0 ? sx / tm : 0.5 * ((double)mn[0] + (double)mx[0]);
+    const double cy = tm > 0.0 ? sy / tm : 0.5 * ((double)mn[1] + (double)mx[1]);
+    const double cz = tm > 0.0 ? sz / tm : 0.5 * ((double)mn[2] + (double)mx[2]);
+    double q[6] = {0, 0, 0, 0, 0, 0};
+    for (int c = c0; c < c1; ++c) {
+        const double dx = __ldcg(&t.c64[3 * c]) - cx;
+        const double dy = __ldcg(&t.c64[3 * c + 1]) - cy;
+        const double dz = __ldcg(&t.c64[3 * c + 2]) - cz;
+        const double w = __ldcg(&t.m64[c]);
+        q[0] += __ldcg(&t.q64[6 * c]) + w * dx * dx;
+        q[1] += __ldcg(&t.q64[6 * c + 1]) + w * dx * dy;
+        q[2] += __ldcg(&t.q64[6 * c + 2]) + w * dx * dz;
+        q[3] += __ldcg(&t.q64[6 * c + 3]) + w * dy * dy;
+        q[4] += __ldcg(&t.q64[6 * c + 4]) + w * dy * dz;
+        q[5] += __ldcg(&t.q64[6 * c + 5]) + w * dz * dz;
+    }
+    t.m64[k] = tm;
+    t.s64[3 * k] = sx;
+    t.s64[3 * k + 1] = sy;
+    t.s64[3 * k + 2] = sz;
+    t.c64[3 * k] = cx;
+    t.c64[3 * k + 1] = cy;
+    t.c64[3 * k + 2] = cz;
+    for (int j = 0; j < 6; ++j)
+        t.q64[6 * k + j] = q[j];
+    t.box0[k] = make_float4(mn[0], mn[1], mn[2], __int_as_float(c0));
+    t.box1[k] = make_float4(mx[0], mx[1], mx[2], __int_as_float(c1 - c0));
+    t.mono[k] = make_float4((float)cx, (float)cy, (float)cz, (float)tm);
+    t.quadA[k] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
+    t.quadB[k] = make_float2((float)q[4], (float)q[5]);
+}
+
+// One thread per leaf computes its moments, then climbs: the child that arrives last at a
+// parent (atomic counter) computes the parent from all children in octant order.
+__global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restrict__ pos4,
+                                                            TreeArrays t)
+{
+    const int nn = t.n_nodes[0];
+    for (int k = blockIdx.x * kThreads + threadIdx.x; k < nn; k += gridDim.x * kThreads) {
+        if (t.nchild[k] != 0)
+            continue;
+        leaf_moments(pos4, k, t);
+        int node = k;
+        for (;;) {
+            const int p = t.parent[node];
+            if (p < 0)
+                break;
+            __threadfence();
+            const int old = atomicAdd(&t.arrive[p], 1);
+            if (old != t.nchild[p] - 1)
+                break;
+            __threadfence();
+            internal_moments(p, t);
+            node = p;
+        }
+    }
+}
+
+} // namespace
+
+void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
+                       int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t lbw = static_cast<size_t>(t.cap) / kThreads + kMaxLevels + 4;
+    cudaMemsetAsync(t.lookback, 0, lbw * sizeof(unsigned long long), s);
+    k_tree_init<<<1, 32, 0, s>>>(t, n);
+    // Level l holds at most min(8^l, n) nodes; the persistent grid covers that with tiles.
+    for (int l = 0; l < max_level; ++l) {
+        long long bound = 1;
+        for (int j = 0; j < l && bound < n; ++j)
+            bound *= 8;
+        if (bound > n)
+            bound = n;
+        long long blocks = (bound + kThreads - 1) / kThreads;
+        if (blocks > 2LL * sms)
+            blocks = 2LL * sms;
+        k_tree_level<<<static_cast<int>(blocks), kThreads, 0, s>>>(sorted_keys, l, leaf_cap,
+                                                                   max_level, t, err);
+    }
+    k_tree_finish_last<<<sms, 256, 0, s>>>(t, max_level);
+    long long mb = (static_cast<long long>(t.cap) + kThreads - 1) / kThreads;
+    if (mb > 16LL * sms)
+        mb = 16LL * sms;
+    k_tree_moments<<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+}
+
+} // namespace bz
+
+// ---- reference-mode topology ------------------------------------------------------------
+// The reference's linear octree for its own keys.  Its bit spread keeps 10 bits per axis, so
+// keys are < 2^30, while the leaf prefix is key >> 3*(21 - leafDepth) with leafDepth <= 11
+// for any n below 16*8^11: every key has prefix 0, the build yields exactly one leaf holding
+// all particles in sorted order, the parent loop never runs and that leaf is the root
+// (engine/physics/octree/cuda/linear/OctBuild.inl:109-199).  This kernel builds that node as
+// buildLinearOctreeLeafNodesKernel does (OctLeafKernels.inl:7-81): FP32 tight box, FP64 mass
+// and weighted position sums in sorted order.  The reference is compiled with nvcc's default
+// contraction, so its `w += x * m` sums and `0.5f * ext + 1e-6f` execute as fused
+// multiply-adds; they are written as explicit fmas here (this file is otherwise compiled
+// without contraction).
+namespace bz {
+namespace {
+__global__ void k_reference_leaf(const float* __restrict__ x, const float* __restrict__ y,
+                                 const float* __restrict__ z, const float* __restrict__ m,
+                                 const uint32_t* __restrict__ sorted_index, int n, float* hot8)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0)
+        return;
+    float mn[3] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
+    float mx[3] = {-3.402823466e38f, -3.402823466e38f, -3.402823466e38f};
+    double tm = 0.0, wx = 0.0, wy = 0.0, wz = 0.0;
+    for (int j = 0; j < n; ++j) {
+        const uint32_t p = sorted_index[j];
+        const float px = x[p], py = y[p], pz = z[p], pm = m[p];
+        mn[0] = fminf(mn[0], px);
+        mn[1] = fminf(mn[1], py);
+        mn[2] = fminf(mn[2], pz);
+        mx[0] = fmaxf(mx[0], px);
+        mx[1] = fmaxf(mx[1], py);
+        mx[2] = fmaxf(mx[2], pz);
+        tm += (double)pm;
+        wx = __fma_rn((double)px, (double)pm, wx);
+        wy = __fma_rn((double)py, (double)pm, wy);
+        wz = __fma_rn((double)pz, (double)pm, wz);
+    }
+    const float cx = 0.5f * (mn[0] + mx[0]);
+    const float cy = 0.5f * (mn[1] + mx[1]);
+    const float cz = 0.5f * (mn[2] + mx[2]);
+    const float half = __fmaf_rn(0.5f, fmaxf(fmaxf(mx[0] - mn[0], mx[1] - mn[1]), mx[2] - mn[2]), 1.0e-6f);
+    hot8[0] = cx;
+    hot8[1] = cy;
+    hot8[2] = cz;
+    hot8[3] = half;
+    hot8[4] = (float)tm;
+    hot8[5] = tm > 0.0 ? (float)(wx / tm) : cx;
+    hot8[6] = tm > 0.0 ? (float)(wy / tm) : cy;
+    hot8[7] = tm > 0.0 ? (float)(wz / tm) : cz;
+}
+} // namespace
+
+void launch_reference_leaf(const float* x, const float* y, const float* z, const float* m,
+                           const uint32_t* sorted_index, int n, float* hot8, cudaStream_t s)
+{
+    k_reference_leaf<<<1, 32, 0, s>>>(x, y, z, m, sorted_index, n, hot8);
+}
+
+} // namespace bz

@@ -1,0 +1,707 @@
+// Warp-cooperative group tree walk (the force hot path).
+//
+// One warp owns a group of 32 consecutive Morton-sorted targets.  It walks the tree once for
+// the whole group: each step pops up to 32 nodes (one per lane), tests them against the
+// group's bounding box, and sorts them with warp votes into
+//   - pruned (beyond the short-range cutoff),
+//   - accepted multipoles  -> appended to a shared-memory node list,
+//   - leaves to sum directly -> appended to a shared-memory leaf list,
+//   - opened internal nodes -> children pushed on a shared-memory stack (shuffle scan).
+// Full lists are flushed: every lane evaluates its own target against each listed node, and
+// leaf particles are pulled into a shared-memory tile with cp.async.bulk (global -> shared,
+// completing on an mbarrier; no cluster multicast) and summed with FP32 pair arithmetic.
+// Per-flush partial sums are folded into the running force with a two-sum (compensated
+// accumulation).
+//
+// Decisions are computed with round-to-nearest intrinsics (no contraction) so that the set
+// of accepted nodes and direct leaves is bit-identical to the oracle's; the reference's
+// per-particle stackless walk is engine/physics/octree/cuda/force/OctGpu.inl:100-228 and the
+// TreePM pair law with the Gaussian split is engine/physics/core/cuda/prelude/
+// CudForceKernels.inl:62-89.
+#include "bz_common.cuh"
+#include "bz_kernels.h"
+
+namespace bz {
+
+namespace {
+
+constexpr int kWarps = 4;
+constexpr int kStack = 1024;      // shared-memory part of the traversal stack
+constexpr int kSpill = 8192;      // per-warp global spill area (oldest entries)
+constexpr int kList = 64;
+constexpr int kTile = 256;
+constexpr int kIndexBits = 26;
+constexpr int kIndexMask = (1 << kIndexBits) - 1;
+constexpr int kPerPairImage = 64;  // leaf code: periodic image chosen per pair
+
+struct __align__(16) WarpSmem {
+    float4 tile[kTile];
+    float4 nd_mono[32];
+    float4 nd_qa[32];
+    float2 nd_qb[32];
+    int stack[kStack];
+    int nlist[kList];
+    int lstart[kList];
+    int lcount[kList];
+    int lcode[kList];
+    int lpre[kList];
+    unsigned long long bar;
+};
+
+// erfc(u) ~= t (a1 + t (a2 + t (a3 + t (a4 + t a5)))) e^{-u^2},  t = 1/(1 + p u)
+// (Abramowitz & Stegun 7.1.26, |error| <= 1.5e-7).
+__device__ __forceinline__ float erfc_as(float u, float e)
+{
+    const float t = rcp_approx(fmaf(0.3275911f, u, 1.0f));
+    float p = 1.061405429f;
+    p = fmaf(p, t, -1.453152027f);
+    p = fmaf(p, t, 1.421413741f);
+    p = fmaf(p, t, -0.284496736f);
+    p = fmaf(p, t, 0.254829592f);
+    return t * p * e;
+}
+
+constexpr float kTwoOverSqrtPi = 1.1283791670955126f;
+constexpr float kFourOverSqrtPi = 2.2567583341910252f;
+constexpr float kEightOverSqrtPi = 4.5135166683820503f;
+
+template <bool SPLIT, bool POT>
+__device__ __forceinline__ void pair_pp(const float4 s, float tx, float ty, float tz,
+                                        const WalkParams& p, float inv2rs, bool cut, bool self,
+                                        float& fx, float& fy, float& fz, float& fp)
+{
+    const float dx = s.x - tx, dy = s.y - ty, dz = s.z - tz;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float s2 = r2 + p.eps2;
+    float m = s.w;
+    if (cut && r2 > p.rcut2)
+        m = 0.0f;
+    float rinv = rsqrt_approx(s2);
+    if (s2 <= p.min_dist2) {
+        m = 0.0f;
+        rinv = 0.0f;
+    }
+    const float rinv2 = rinv * rinv;
+    float f = m * rinv * rinv2;
+    if (SPLIT) {
+        const float u = s2 * rinv * inv2rs;
+        const float e = __expf(-u * u);
+        const float ec = erfc_as(u, e);
+        const float w = fmaf(kTwoOverSqrtPi * u, e, ec);
+        f *= w;
+        if (POT && !self)
+            fp = fmaf(-m * ec, rinv, fp);
+    } else {
+        if (POT && !self)
+            fp = fmaf(-m, rinv, fp);
+    }
+    fx = fmaf(f, dx, fx);
+    fy = fmaf(f, dy, fy);
+    fz = fmaf(f, dz, fz);
+}
+
+template <bool SPLIT, bool QUAD, bool POT>
+__device__ __forceinline__ void pair_pn(const float4 mo, const float4 qa, const float2 qb,
+                                        float tx, float ty, float tz, const WalkParams& p,
+                                        float inv2rs, float& fx, float& fy, float& fz, float& fp)
+{
+    const float dx = mo.x - tx, dy = mo.y - ty, dz = mo.z - tz;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float s2 = r2 + p.eps2;
+    float rinv = rsqrt_approx(s2);
+    float m = mo.w;
+    if (s2 <= p.min_dist2) {
+        rinv = 0.0f;
+        m = 0.0f;
+    }
+    const float rinv2 = rinv * rinv;
+    float D0, D1, D2 = 0.0f, D3 = 0.0f;
+    if (SPLIT) {
+        const float u = s2 * rinv * inv2rs;
+        const float e = __expf(-u * u);
+        const float ec = erfc_as(u, e);
+        const float h = fmaf(kTwoOverSqrtPi * u, e, ec);
+        D0 = ec * rinv;
+        D1 = h * rinv * rinv2;
+        if (QUAD) {
+            const float u2 = u * u;
+            const float k = fmaf(kFourOverSqrtPi * u2 * u, e, 3.0f * h);
+            const float l = fmaf(kEightOverSqrtPi * u2 * u2 * u, e, 5.0f * k);
+            D2 = k * rinv2 * rinv2 * rinv;
+            D3 = l * rinv2 * rinv2 * rinv2 * rinv;
+        }
+    } else {
+        D0 = rinv;
+        D1 = rinv * rinv2;
+        if (QUAD) {
+            D2 = 3.0f * D1 * rinv2;
+            D3 = 5.0f * D2 * rinv2;
+        }
+    }
+    float c0 = m * D1;
+    if (QUAD) {
+        const float qdx = fmaf(qa.x, dx, fmaf(qa.y, dy, qa.z * dz));
+        const float qdy = fmaf(qa.y, dx, fmaf(qa.w, dy, qb.x * dz));
+        const float qdz = fmaf(qa.z, dx, fmaf(qb.x, dy, qb.y * dz));
+        const float dqd = fmaf(dx, qdx, fmaf(dy, qdy, dz * qdz));
+        const float tr = qa.x + qa.w + qb.y;
+        if (m == 0.0f) {
+            D1 = D2 = D3 = 0.0f;
+        }
+        c0 = fmaf(0.5f * D3, dqd, fmaf(-0.5f * D2, tr, c0));
+        fx = fmaf(c0, dx, fmaf(-D2, qdx, fx));
+        fy = fmaf(c0, dy, fmaf(-D2, qdy, fy));
+        fz = fmaf(c0, dz, fmaf(-D2, qdz, fz));
+        if (POT)
+            fp += fmaf(-m, D0, fmaf(0.5f * D1, tr, -0.5f * D2 * dqd));
+    } else {
+        fx = fmaf(c0, dx, fx);
+        fy = fmaf(c0, dy, fy);
+        fz = fmaf(c0, dz, fz);
+        if (POT)
+            fp = fmaf(-m, D0, fp);
+    }
+}
+
+struct Acc {
+    float s[4];
+    float e[4];
+    __device__ void zero()
+    {
+        for (int i = 0; i < 4; ++i)
+            s[i] = e[i] = 0.0f;
+    }
+    __device__ void add(int i, float v)
+    {
+        float ss, ee;
+        two_sum(s[i], v, ss, ee);
+        s[i] = ss;
+        e[i] += ee;
+    }
+    __device__ float total(int i) const { return s[i] + e[i]; }
+};
+
+__device__ __forceinline__ float shift_of(int code, int axis, float box)
+{
+    return box * static_cast<float>(((code >> (2 * axis)) & 3) - 1);
+}
+
+template <bool PERIODIC, bool SPLIT, bool QUAD, bool POT>
+__device__ __forceinline__ void flush_nodes(WarpSmem& w, int nn, const TreeArrays& t,
+                                            const WalkParams& p, float inv2rs, float tx,
+                                            float ty, float tz, Acc& acc)
+{
+    const int lane = threadIdx.x & 31;
+    for (int base = 0; base < nn; base += 32) {
+        const int m = min(32, nn - base);
+        if (lane < m) {
+            const int e = w.nlist[base + lane];
+            const int k = e & kIndexMask;
+            float4 mo = t.mono[k];
+            if (PERIODIC) {
+                const int code = static_cast<int>(static_cast<unsigned>(e) >> kIndexBits);
+                mo.x -= shift_of(code, 0, p.box);
+                mo.y -= shift_of(code, 1, p.box);
+                mo.z -= shift_of(code, 2, p.box);
+            }
+            w.nd_mono[lane] = mo;
+            if (QUAD) {
+                w.nd_qa[lane] = t.quadA[k];
+                w.nd_qb[lane] = t.quadB[k];
+            }
+        }
+        __syncwarp();
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f, fp = 0.0f;
+        for (int j = 0; j < m; ++j) {
+            const float4 qa = QUAD ? w.nd_qa[j] : make_float4(0, 0, 0, 0);
+            const float2 qb = QUAD ? w.nd_qb[j] : make_float2(0, 0);
+            pair_pn<SPLIT, QUAD, POT>(w.nd_mono[j], qa, qb, tx, ty, tz, p, inv2rs, fx, fy, fz, fp);
+        }
+        acc.add(0, fx);
+        acc.add(1, fy);
+        acc.add(2, fz);
+        if (POT)
+            acc.add(3, fp);
+        __syncwarp();
+    }
+}
+
+template <bool PERIODIC, bool SPLIT, bool POT>
+__device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* __restrict__ pos4,
+                                             const WalkParams& p, float inv2rs, bool cut,
+                                             float tx, float ty, float tz, int self_index,
+                                             Acc& acc, uint32_t& phase, int* err)
+{
+    const int lane = threadIdx.x & 31;
+    // exclusive prefix of the leaf sizes (list holds at most 64 entries)
+    const int c0 = lane < nl ? w.lcount[lane] : 0;
+    const int c1 = lane + 32 < nl ? w.lcount[lane + 32] : 0;
+    const int i0 = warp_incl_scan(c0);
+    const int t0 = __shfl_sync(kFullMask, i0, 31);
+    const int i1 = warp_incl_scan(c1) + t0;
+    const int total = __shfl_sync(kFullMask, i1, 31);
+    if (lane < nl)
+        w.lpre[lane] = i0 - c0;
+    if (lane + 32 < nl)
+        w.lpre[lane + 32] = i1 - c1;
+    __syncwarp();
+    int jfirst = 0;
+    for (int cbase = 0; cbase < total; cbase += kTile) {
+        const int cend = min(cbase + kTile, total);
+        // make earlier generic-proxy reads of the tile visible before the async writes
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0)
+            mbar_arrive_expect_tx(&w.bar, static_cast<uint32_t>(cend - cbase) * 16u);
+        __syncwarp();
+        for (int j = lane; j < nl; j += 32) {
+            const int lo = max(w.lpre[j], cbase);
+            const int hi = min(w.lpre[j] + w.lcount[j], cend);
+            if (hi > lo)
+                bulk_g2s(&w.tile[lo - cbase], pos4 + (w.lstart[j] + (lo - w.lpre[j])),
+                         static_cast<uint32_t>(hi - lo) * 16u, &w.bar);
+        }
+        mbar_wait_bounded(&w.bar, phase, err);
+        phase ^= 1u;
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f, fp = 0.0f;
+        for (int j = jfirst; j < nl; ++j) {
+            const int pre = w.lpre[j];
+            if (pre >= cend)
+                break;
+            const int lo = max(pre, cbase);
+            const int hi = min(pre + w.lcount[j], cend);
+            if (hi <= lo)
+                continue;
+            float sx = tx, sy = ty, sz = tz;
+            const int gsrc0 = w.lstart[j] + (lo - pre);
+            const int off = lo - cbase;
+            const int cntp = hi - lo;
+            if (PERIODIC) {
+                const int code = w.lcode[j];
+                if (code == kPerPairImage) {
+                    // rare slow path: nearest image chosen per pair
+                    const float inv_box = 1.0f / p.box;
+                    for (int q = 0; q < cntp; ++q) {
+                        float4 s4 = w.tile[off + q];
+                        s4.x = tx + (s4.x - tx - p.box * rintf((s4.x - tx) * inv_box));
+                        s4.y = ty + (s4.y - ty - p.box * rintf((s4.y - ty) * inv_box));
+                        s4.z = tz + (s4.z - tz - p.box * rintf((s4.z - tz) * inv_box));
+                        pair_pp<SPLIT, POT>(s4, tx, ty, tz, p, inv2rs, cut,
+                                            POT && gsrc0 + q == self_index, fx, fy, fz, fp);
+                    }
+                    if (pre + w.lcount[j] <= cend)
+                        jfirst = j + 1;
+                    continue;
+                }
+                sx += shift_of(code, 0, p.box);
+                sy += shift_of(code, 1, p.box);
+                sz += shift_of(code, 2, p.box);
+            }
+            int q = 0;
+            for (; q + 1 < cntp; q += 2) {
+                pair_pp<SPLIT, POT>(w.tile[off + q], sx, sy, sz, p, inv2rs, cut,
+                                    POT && gsrc0 + q == self_index, fx, fy, fz, fp);
+                pair_pp<SPLIT, POT>(w.tile[off + q + 1], sx, sy, sz, p, inv2rs, cut,
+                                    POT && gsrc0 + q + 1 == self_index, fx, fy, fz, fp);
+            }
+            for (; q < cntp; ++q)
+                pair_pp<SPLIT, POT>(w.tile[off + q], sx, sy, sz, p, inv2rs, cut,
+                                    POT && gsrc0 + q == self_index, fx, fy, fz, fp);
+            if (pre + w.lcount[j] <= cend)
+                jfirst = j + 1;
+        }
+        acc.add(0, fx);
+        acc.add(1, fy);
+        acc.add(2, fz);
+        if (POT)
+            acc.add(3, fp);
+        __syncwarp();
+    }
+}
+
+// Persistent kernel: each warp takes groups from a global queue until none are left.  The
+// traversal stack lives in shared memory; when it would overflow, its oldest half is spilled
+// to a per-warp-slot global area and refilled when the shared part runs dry.
+template <bool PERIODIC, bool SPLIT, bool QUAD, bool POT>
+__global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__ pos4, int n,
+                                                       TreeArrays t, WalkParams p, float inv_box,
+                                                       WalkOutputs o, unsigned* queue,
+                                                       int* spill_base, int* err)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
+    int* spill = spill_base + static_cast<size_t>(blockIdx.x * kWarps + warp) * kSpill;
+    const int ngroups = (n + 31) >> 5;
+    if (lane == 0)
+        mbar_init(&w.bar, 1);
+    fence_mbar_init();
+    __syncwarp();
+    const bool cut = p.rcut2 > 0.0f;
+    const float inv2rs = SPLIT ? 0.5f / p.rsplit : 0.0f;
+    const float rcut = __fsqrt_rn(p.rcut2);
+    const float half_box = __fmul_rn(0.5f, p.box);
+    const unsigned lt = lanemask_lt();
+    uint32_t phase = 0;
+
+    for (;;) {
+        int g = 0;
+        if (lane == 0)
+            g = static_cast<int>(atomicAdd(queue, 1u));
+        g = __shfl_sync(kFullMask, g, 0);
+        if (g >= ngroups)
+            break;
+        const int ti = g * 32 + lane;
+        const bool valid = ti < n;
+        const float4 me = pos4[valid ? ti : g * 32];
+        float gmin[3] = {me.x, me.y, me.z}, gmax[3] = {me.x, me.y, me.z};
+#pragma unroll
+        for (int a = 0; a < 3; ++a)
+            for (int off = 16; off > 0; off >>= 1) {
+                gmin[a] = fminf(gmin[a], __shfl_xor_sync(kFullMask, gmin[a], off));
+                gmax[a] = fmaxf(gmax[a], __shfl_xor_sync(kFullMask, gmax[a], off));
+            }
+        float gc[3], ghalf[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            gc[a] = __fmul_rn(0.5f, __fadd_rn(gmin[a], gmax[a]));
+            ghalf[a] = __fmul_rn(0.5f, __fsub_rn(gmax[a], gmin[a]));
+        }
+
+        if (lane == 0)
+            w.stack[0] = 0;
+        __syncwarp();
+        int top = 1, gtop = 0, nn = 0, nl = 0, lp = 0;
+        unsigned long long cnt_pp = 0, cnt_pn = 0;
+        Acc acc;
+        acc.zero();
+        bool bail = false;
+        while (top > 0 || gtop > 0) {
+            if (top == 0) {  // refill from the spill area (uniform branch)
+                const int m = min(gtop, kStack / 2);
+                for (int i = lane; i < m; i += 32)
+                    w.stack[i] = spill[gtop - m + i];
+                gtop -= m;
+                top = m;
+                __syncwarp();
+            }
+            const int take = min(top, 32);
+            const int k = lane < take ? w.stack[top - take + lane] : -1;
+            top -= take;
+            __syncwarp();
+            bool accept = false, leaf = false;
+            int nch = 0, link = 0, info = 0, code = 0;
+            if (k >= 0) {
+                const float4 b0 = t.box0[k];
+                const float4 b1 = t.box1[k];
+                const float4 mo = t.mono[k];
+                link = __float_as_int(b0.w);
+                info = __float_as_int(b1.w);
+                const float bmin[3] = {b0.x, b0.y, b0.z}, bmax[3] = {b1.x, b1.y, b1.z};
+                const float com[3] = {mo.x, mo.y, mo.z};
+                float sh[3] = {0.0f, 0.0f, 0.0f};
+                bool amb = false;
+                if (PERIODIC) {
+                    // Image-ambiguous node (its extent + the group's + the cutoff reaches half
+                    // the box): always opened; a leaf is summed with per-pair minimum images.
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const float nh = __fmul_rn(0.5f, __fsub_rn(bmax[a], bmin[a]));
+                        if (__fadd_rn(__fadd_rn(ghalf[a], nh), rcut) > half_box)
+                            amb = true;
+                    }
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const float cn = __fmul_rn(0.5f, __fadd_rn(bmin[a], bmax[a]));
+                        const float r = rintf(__fmul_rn(__fsub_rn(cn, gc[a]), inv_box));
+                        sh[a] = __fmul_rn(p.box, r);
+                        code |= (static_cast<int>(r) + 1) << (2 * a);
+                    }
+                    if (amb)
+                        code = kPerPairImage;
+                }
+                bool pruned = false;
+                if (PERIODIC && amb) {
+                    if (info < 0)
+                        leaf = true;
+                    else
+                        nch = info;
+                } else if (cut) {
+                    float d2 = 0.0f;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const float lo = __fsub_rn(bmin[a], sh[a]), hi = __fsub_rn(bmax[a], sh[a]);
+                        const float d = fmaxf(fmaxf(__fsub_rn(lo, gmax[a]), __fsub_rn(gmin[a], hi)), 0.0f);
+                        d2 = __fadd_rn(d2, __fmul_rn(d, d));
+                    }
+                    pruned = d2 > p.rcut2;
+                }
+                if (!pruned && !(PERIODIC && amb)) {
+                    float e2 = 0.0f, l = 0.0f;
+#pragma unroll
+                    for (int a = 0; a < 3; ++a) {
+                        const float c = __fsub_rn(com[a], sh[a]);
+                        const float e = fmaxf(fmaxf(__fsub_rn(gmin[a], c), __fsub_rn(c, gmax[a])), 0.0f);
+                        e2 = __fadd_rn(e2, __fmul_rn(e, e));
+                        l = fmaxf(l, __fsub_rn(bmax[a], bmin[a]));
+                    }
+                    accept = __fmul_rn(l, l) < __fmul_rn(p.theta2, e2);
+                    if (!accept) {
+                        if (info < 0)
+                            leaf = true;
+                        else
+                            nch = info;
+                    }
+                }
+            }
+            const unsigned am = __ballot_sync(kFullMask, accept);
+            const unsigned lm = __ballot_sync(kFullMask, leaf);
+            if (accept)
+                w.nlist[nn + __popc(am & lt)] = k | (code << kIndexBits);
+            if (leaf) {
+                const int pos = nl + __popc(lm & lt);
+                w.lstart[pos] = link;
+                w.lcount[pos] = -info;
+                w.lcode[pos] = code;
+            }
+            nn += __popc(am);
+            nl += __popc(lm);
+            int lsum = leaf ? -info : 0;
+            for (int off = 16; off > 0; off >>= 1)
+                lsum += __shfl_xor_sync(kFullMask, lsum, off);
+            lp += lsum;
+            cnt_pp += static_cast<unsigned long long>(lsum);
+            cnt_pn += static_cast<unsigned long long>(__popc(am));
+            const int incl = warp_incl_scan(nch);
+            const int tot = __shfl_sync(kFullMask, incl, 31);
+            if (top + tot > kStack) {  // spill the oldest half (uniform branch)
+                const int half = kStack / 2;
+                if (gtop + half > kSpill) {
+                    if (lane == 0)
+                        raise_error(err, kErrWalkStack);
+                    bail = true;
+                    break;
+                }
+                for (int i = lane; i < half; i += 32)
+                    spill[gtop + i] = w.stack[i];
+                __syncwarp();
+                for (int i = lane; i < top - half; i += 32)
+                    w.stack[i] = w.stack[i + half];
+                __syncwarp();
+                gtop += half;
+                top -= half;
+            }
+            for (int c = 0; c < nch; ++c)
+                w.stack[top + incl - nch + c] = link + c;
+            top += tot;
+            __syncwarp();
+            if (nn >= 32) {
+                flush_nodes<PERIODIC, SPLIT, QUAD, POT>(w, nn, t, p, inv2rs, me.x, me.y, me.z, acc);
+                nn = 0;
+            }
+            if (nl >= 32 || lp >= kTile) {
+                flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, p, inv2rs, cut, me.x, me.y, me.z,
+                                                   ti, acc, phase, err);
+                nl = 0;
+                lp = 0;
+            }
+        }
+        if (!bail) {
+            if (nn > 0)
+                flush_nodes<PERIODIC, SPLIT, QUAD, POT>(w, nn, t, p, inv2rs, me.x, me.y, me.z, acc);
+            if (nl > 0)
+                flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, p, inv2rs, cut, me.x, me.y, me.z,
+                                                   ti, acc, phase, err);
+        }
+        if (valid) {
+            o.ax[ti] += acc.total(0);
+            o.ay[ti] += acc.total(1);
+            o.az[ti] += acc.total(2);
+            if (POT && o.pot)
+                o.pot[ti] += acc.total(3);
+        }
+        if (lane == 0) {
+            if (o.n_pp)
+                o.n_pp[g] = cnt_pp;
+            if (o.n_pn)
+                o.n_pn[g] = cnt_pn;
+            if (o.totals) {
+                const unsigned long long ng = static_cast<unsigned long long>(min(32, n - g * 32));
+                atomicAdd(&o.totals[0], cnt_pp * ng);
+                atomicAdd(&o.totals[1], cnt_pn * ng);
+            }
+        }
+        __syncwarp();
+    }
+}
+
+__global__ void k_zero_u32(unsigned* p) { *p = 0u; }
+
+struct WalkLaunch {
+    int blocks = 0;
+    size_t smem = 0;
+};
+
+template <bool PERIODIC, bool SPLIT, bool QUAD, bool POT>
+WalkLaunch walk_shape(int n)
+{
+    static WalkLaunch cached;
+    if (cached.blocks == 0) {
+        const size_t smem = sizeof(WarpSmem) * kWarps;
+        cudaFuncSetAttribute(k_walk<PERIODIC, SPLIT, QUAD, POT>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        int dev = 0, sms = 148, per_sm = 1;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<PERIODIC, SPLIT, QUAD, POT>,
+                                                      kWarps * 32, smem);
+        cached.blocks = sms * (per_sm > 0 ? per_sm : 1);
+        cached.smem = smem;
+    }
+    WalkLaunch l = cached;
+    const int groups = (n + 31) / 32;
+    const int need = (groups + kWarps - 1) / kWarps;
+    if (l.blocks > need)
+        l.blocks = need < 1 ? 1 : need;
+    return l;
+}
+
+template <bool PERIODIC, bool SPLIT, bool QUAD, bool POT>
+void launch_variant(const float4* pos4, int n, const TreeArrays& t, const WalkParams& p,
+                    const WalkOutputs& o, unsigned* queue, int* spill, int* err, cudaStream_t s)
+{
+    const WalkLaunch l = walk_shape<PERIODIC, SPLIT, QUAD, POT>(n);
+    const float inv_box = p.box > 0.0f ? 1.0f / p.box : 0.0f;
+    k_zero_u32<<<1, 1, 0, s>>>(queue);
+    k_walk<PERIODIC, SPLIT, QUAD, POT><<<l.blocks, kWarps * 32, l.smem, s>>>(pos4, n, t, p, inv_box,
+                                                                            o, queue, spill, err);
+}
+
+template <bool PERIODIC, bool SPLIT>
+void dispatch_qp(const float4* pos4, int n, const TreeArrays& t, const WalkParams& p,
+                 const WalkOutputs& o, unsigned* queue, int* spill, int* err, cudaStream_t s)
+{
+    if (p.quadrupole) {
+        if (p.want_pot)
+            launch_variant<PERIODIC, SPLIT, true, true>(pos4, n, t, p, o, queue, spill, err, s);
+        else
+            launch_variant<PERIODIC, SPLIT, true, false>(pos4, n, t, p, o, queue, spill, err, s);
+    } else {
+        if (p.want_pot)
+            launch_variant<PERIODIC, SPLIT, false, true>(pos4, n, t, p, o, queue, spill, err, s);
+        else
+            launch_variant<PERIODIC, SPLIT, false, false>(pos4, n, t, p, o, queue, spill, err, s);
+    }
+}
+
+// ---- reference formulation: the reference's walk on its one-leaf tree, i.e. a direct sum
+// over the Morton-sorted order with the reference pair law (rsqrtf, erfcf, expf), FP32
+// accumulation in leaf order, then the acceleration clamp (OctGpu.inl:138-227,
+// CudForceKernels.inl:7-89).  One thread per particle in original order.
+constexpr int kRefThreads = 256;
+__global__ void __launch_bounds__(kRefThreads) k_reference_walk(
+    const float4* __restrict__ orig, const float4* __restrict__ sorted,
+    const uint32_t* __restrict__ sorted_index, int n, float softening, float min_distance2,
+    float split_scale, float cutoff2, float max_acc, float* ax, float* ay, float* az)
+{
+    __shared__ float4 tile[kRefThreads];
+    __shared__ int tile_id[kRefThreads];
+    const int i = blockIdx.x * kRefThreads + threadIdx.x;
+    const float4 self = i < n ? orig[i] : make_float4(0, 0, 0, 0);
+    float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+    const bool cutoff = cutoff2 > 0.0f;
+    for (int base = 0; base < n; base += kRefThreads) {
+        const int j = base + threadIdx.x;
+        if (j < n) {
+            tile[threadIdx.x] = sorted[j];
+            tile_id[threadIdx.x] = static_cast<int>(sorted_index[j]);
+        }
+        __syncthreads();
+        const int m = min(kRefThreads, n - base);
+        if (i < n) {
+            for (int q = 0; q < m; ++q) {
+                if (tile_id[q] == i)
+                    continue;
+                const float4 s = tile[q];
+                if (cutoff) {
+                    const float ddx = self.x - s.x, ddy = self.y - s.y, ddz = self.z - s.z;
+                    if (ddx * ddx + ddy * ddy + ddz * ddz > cutoff2)
+                        continue;
+                }
+                const float dx = s.x - self.x, dy = s.y - self.y, dz = s.z - self.z;
+                const float d2 = dx * dx + dy * dy + dz * dz + softening * softening;
+                if (d2 <= min_distance2)
+                    continue;
+                const float inv = rsqrtf(d2);
+                const float inv3 = inv * inv * inv;
+                float wgt = 1.0f;
+                if (split_scale > 0.0f) {
+                    const float dist = 1.0f / inv;
+                    const float arg = 0.5f * dist / split_scale;
+                    wgt = erfcf(arg) + dist * 0.5641895835477563f / split_scale * expf(-arg * arg);
+                }
+                const float f = s.w * inv3 * wgt;
+                fx += dx * f;
+                fy += dy * f;
+                fz += dz * f;
+            }
+        }
+        __syncthreads();
+    }
+    if (i < n) {
+        const float norm = sqrtf(fx * fx + fy * fy + fz * fz);
+        if (norm > max_acc && norm > 1e-12f) {
+            const float sc = max_acc / norm;
+            fx *= sc;
+            fy *= sc;
+            fz *= sc;
+        }
+        ax[i] = fx;
+        ay[i] = fy;
+        az[i] = fz;
+    }
+}
+
+} // namespace
+
+int walk_spill_slots()
+{
+    // upper bound on concurrently resident warps of any walk variant
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    return sms * (2048 / 32);
+}
+size_t walk_spill_entries() { return static_cast<size_t>(kSpill); }
+
+void launch_walk(const float4* pos4, int n, const TreeArrays& t, const WalkParams& p,
+                 const WalkOutputs& o, unsigned* queue, int* spill, int* err, cudaStream_t s)
+{
+    const bool periodic = p.box > 0.0f;
+    const bool split = p.rsplit > 0.0f;
+    if (periodic) {
+        if (split)
+            dispatch_qp<true, true>(pos4, n, t, p, o, queue, spill, err, s);
+        else
+            dispatch_qp<true, false>(pos4, n, t, p, o, queue, spill, err, s);
+    } else {
+        if (split)
+            dispatch_qp<false, true>(pos4, n, t, p, o, queue, spill, err, s);
+        else
+            dispatch_qp<false, false>(pos4, n, t, p, o, queue, spill, err, s);
+    }
+}
+
+void launch_reference_walk(const float4* pos_orig, const float4* pos_sorted,
+                           const uint32_t* sorted_index, int n, float softening,
+                           float min_distance2, float split_scale, float cutoff2,
+                           float max_acceleration, float* ax, float* ay, float* az,
+                           cudaStream_t s)
+{
+    const int blocks = (n + kRefThreads - 1) / kRefThreads;
+    k_reference_walk<<<blocks, kRefThreads, 0, s>>>(pos_orig, pos_sorted, sorted_index, n,
+                                                    softening, min_distance2, split_scale,
+                                                    cutoff2, max_acceleration, ax, ay, az);
+}
+
+} // namespace bz

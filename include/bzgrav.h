@@ -1,0 +1,168 @@
+/* bzgrav.h -- C ABI of the B200 Barnes-Hut / TreePM gravity engine (libbzgrav.so).
+ *
+ * The library sits behind BLITZAR's solver dispatch as the engine of the `octree_gpu` /
+ * TreePM path.  Plain C types only: host pointers and sizes in, status codes out.  One
+ * handle owns all device memory of one particle system on one GPU and one CUDA stream;
+ * handles are not thread-safe (one host thread drives a handle, as one host thread drives a
+ * reference ParticleSystem).
+ *
+ * Reference interfaces each entry point replaces are cited as paths inside the BLITZAR
+ * project.
+ */
+#ifndef BZGRAV_H
+#define BZGRAV_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes; 0..4 mirror blitzar_core_result_t (runtime/ffi/core/FfiApi.hpp:15-21). */
+typedef enum bz_status {
+    BZ_OK = 0,
+    BZ_INVALID_ARGUMENT = 1,
+    BZ_NOT_READY = 2,
+    BZ_TIMEOUT = 3,
+    BZ_INTERNAL_ERROR = 4,
+    BZ_CUDA_ERROR = 5,        /* a CUDA/cuFFT call failed (text in bz_last_error) */
+    BZ_OUT_OF_MEMORY = 6,
+    BZ_DEVICE_LIMIT = 7,      /* a bounded device-side loop gave up (stack, wait, capacity) */
+    BZ_UNSUPPORTED = 8
+} bz_status;
+
+/* Which solver the handle runs (the `--solver` / simulation(solver=...) selection,
+ * engine/config/registry/entries/CfgEntriesCore.cpp:22, mapped to ParticleSystem::SolverMode
+ * by engine/server/simulation/runtime/SrvHelpers.cpp:91-102). */
+typedef enum bz_solver {
+    BZ_SOLVER_OCTREE = 0,           /* Barnes-Hut octree (drop-in for octree_gpu) */
+    BZ_SOLVER_TREEPM = 1,           /* periodic TreePM: mesh long range + tree short range */
+    BZ_SOLVER_OCTREE_REFERENCE = 2  /* the reference octree_gpu formulation: reference keys,
+                                       reference topology and its walk (parity mode) */
+} bz_solver;
+
+typedef enum bz_key_mode {
+    BZ_KEYS_PRODUCTION = 0, /* FP64 quantisation, 21 bits per axis (63-bit keys) */
+    BZ_KEYS_REFERENCE = 1   /* bit-exact reference keys (FP32 quantisation and bit spread of
+                               engine/physics/octree/cuda/linear/OctKeyKernels.inl:22-46) */
+} bz_key_mode;
+
+/* Configuration; field names follow the simulation.ini keys they mirror. */
+typedef struct bz_config {
+    uint32_t struct_size;          /* sizeof(bz_config), set by bz_config_init */
+    int32_t solver;                /* bz_solver */
+    float octree_theta;            /* octree_theta */
+    float octree_softening;        /* octree_softening (Plummer epsilon) */
+    int32_t octree_opening_criterion; /* octree_opening_criterion: 0 com, 1 bounds (reference mode) */
+    int32_t linear_octree_leaf_capacity; /* reference-mode leaf rule (default 256) */
+    int32_t leaf_capacity;         /* production adaptive octree: particles per leaf */
+    int32_t multipole_order;       /* 1 monopole, 2 monopole + quadrupole */
+    float physics_max_acceleration;/* physics_max_acceleration (clamp; 1e30 disables) */
+    float physics_min_softening;   /* physics_min_softening */
+    float physics_min_distance2;   /* physics_min_distance2 */
+    float physics_min_theta;       /* physics_min_theta */
+    int32_t treepm_grid_size;      /* treepm_grid_size: PM mesh cells per side */
+    float treepm_r_split_cells;    /* Gaussian split scale r_s in mesh cells */
+    float treepm_r_cut_factor;     /* short-range cutoff r_cut = factor * r_s */
+    double box_length;             /* periodic box length (TreePM); 0 = open boundaries */
+    int32_t key_mode;              /* bz_key_mode */
+    int32_t device;                /* CUDA device ordinal */
+    uint64_t stream;               /* cudaStream_t to run on, or 0 for a private stream */
+    int32_t use_graph;             /* capture bz_step's per-step work in a CUDA graph */
+} bz_config;
+
+typedef struct bz_handle bz_handle;
+
+/* Default configuration (reference defaults: theta 0.5, softening 0.01, leaf capacity 256,
+ * TreePM grid 128, split 1.25 cells, cutoff 4.5 r_s, quadrupole on). */
+bz_status bz_config_init(bz_config* cfg);
+
+/* Create an engine for up to `capacity` particles.  Replaces ParticleSystem construction +
+ * runtime buffer planning (engine/physics/core/particle/PhyParticleSystem.hpp:146,
+ * engine/physics/core/cuda/core/CudSolverConfiguration.inl:116-156) and the solver setters
+ * setOctreeTheta/Softening/OpeningCriterion, setTreePmParameters,
+ * setLinearOctreeLeafCapacity, setPhysicsStabilityConstants (PhyParticleSystem.hpp:187-252). */
+bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out);
+bz_status bz_destroy(bz_handle* h);
+
+/* Upload particles in the reference SoA layout (engine/physics/core/particle/
+ * PhyParticleSoAView.hpp:18-33): pos = x[n], y[n], z[n] back to back; vel likewise; mass[n].
+ * vel may be NULL (zero velocities).  The _f64 variant keeps full FP64 state. */
+bz_status bz_set_state(bz_handle* h, const float* pos_soa3, const float* vel_soa3,
+                       const float* mass, size_t n);
+bz_status bz_set_state_f64(bz_handle* h, const double* pos_soa3, const double* vel_soa3,
+                           const float* mass, size_t n);
+
+/* Advance nsteps leapfrog (KDK) steps of size dt.  Replaces ParticleSystem::update
+ * (PhyParticleSystem.hpp:163; octree_gpu leapfrog in engine/physics/core/cuda/integration/
+ * CudOctreeGpuIntegrators.inl:121-195).  The force at the end of a step is reused at the
+ * start of the next, so each step evaluates the force once. */
+bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps);
+
+/* Accelerations (and optionally potentials) of the current state, caller's particle order,
+ * SoA 3n floats.  Replaces computeOctreeAccelerationKernel (engine/physics/octree/cuda/force/
+ * OctGpu.inl:230-245) / the TreePM force kernels (engine/physics/treepm/short_range/
+ * TpmTreeForce.inl:142-159).  pot may be NULL. */
+bz_status bz_accelerations(bz_handle* h, float* acc_soa3, float* pot);
+
+/* Download the state in the caller's particle order (ParticleSystem::syncHostState /
+ * getParticles, PhyParticleSystem.hpp:351,377).  vel may be NULL.  _f64 returns FP64 state. */
+bz_status bz_get_state(bz_handle* h, float* pos_soa3, float* vel_soa3);
+bz_status bz_get_state_f64(bz_handle* h, double* pos_soa3, double* vel_soa3);
+
+/* Morton keys of the current state, sorted, with the stable sort permutation (sorted
+ * position -> caller index): buildMortonCodesKernel + thrust::sort_by_key
+ * (engine/physics/octree/cuda/linear/OctKeyKernels.inl:22-46, OctBuild.inl:96). */
+bz_status bz_morton_keys(bz_handle* h, uint64_t* sorted_keys, int32_t* perm);
+
+/* Tree of the current state.  First call with all arrays NULL to learn the node count.
+ * Production octree (breadth-first, node 0 = root):
+ *   start/count = particle range in sorted order, child = first child or -1, nchild,
+ *   mono4 = {com.xyz, mass}, bmin3/bmax3 = tight box, quad6 = second moments about the COM.
+ * Reference mode (BZ_SOLVER_OCTREE_REFERENCE): the reference's node arrays
+ *   (engine/physics/octree/cuda/linear/OctLinkKernels.inl:61-113): mono4 <- hot {cx,cy,cz,half}
+ *   and bmin3[0..2] unused; see bz_reference_tree. */
+bz_status bz_tree_topology(bz_handle* h, int64_t* node_count, int32_t* start, int32_t* count,
+                           int32_t* child, int32_t* nchild, float* mono4, float* bmin3,
+                           float* bmax3, float* quad6);
+
+/* Reference-mode tree in the reference's packed layout: hot8 = {cx,cy,cz,half,mass,comx,
+ * comy,comz}, next, child_mask, first_child, leaf_start, leaf_count (OctLinkKernels.inl:61-113). */
+bz_status bz_reference_tree(bz_handle* h, int64_t* node_count, float* hot8, int32_t* next,
+                            int32_t* child_mask, int32_t* first_child, int32_t* leaf_start,
+                            int32_t* leaf_count);
+
+/* Interaction counts of the last force evaluation (particle-particle, particle-node). */
+bz_status bz_interaction_counts(bz_handle* h, uint64_t* n_pp, uint64_t* n_pn);
+
+/* Per-phase device times of the last bz_step/bz_accelerations call, in milliseconds, from
+ * CUDA events on the handle's stream: [0] keys, [1] sort, [2] permute, [3] tree, [4] mesh,
+ * [5] walk, [6] integrate, [7] total.  Timing is recorded only when enabled. */
+bz_status bz_enable_phase_timing(bz_handle* h, int enable);
+bz_status bz_phase_times(bz_handle* h, float* ms, int n);
+
+/* Relative force errors of the current state's accelerations against an FP64 reference on
+ * `nsample` seeded targets: direct sum (open) or Ewald (periodic).  Writes the per-target
+ * errors |a - a_ref| / |a_ref| (caller order of the sampled targets) if errs != NULL, and
+ * the sampled caller indices if idx != NULL. */
+bz_status bz_force_errors(bz_handle* h, int32_t nsample, uint64_t seed, float* errs,
+                          int32_t* idx, double* median, double* p99);
+
+/* Debug access to the PM mesh of the last force evaluation: which = 0 density after the
+ * deposit, 1 potential after the solve.  out holds grid^3 floats, index (z*M + y)*M + x. */
+bz_status bz_pm_mesh(bz_handle* h, int which, float* out);
+
+size_t bz_particle_count(const bz_handle* h);
+size_t bz_device_bytes(const bz_handle* h);
+
+/* Last error text (blitzar_core_get_last_error, runtime/ffi/core/FfiApi.hpp:99-100).
+ * Returns the full length; writes at most cap-1 bytes plus NUL. */
+size_t bz_last_error(const bz_handle* h, char* buf, size_t cap);
+const char* bz_status_string(bz_status s);
+const char* bz_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

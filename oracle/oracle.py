@@ -1,0 +1,283 @@
+"""ctypes bindings for the oracle libraries -- TEST INFRASTRUCTURE ONLY.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this module,
+and only as the checker: the product (``blitzar_b200``) never calls into it.
+
+* ``liboracle.so`` -- the C restatement in ``bz_oracle.c`` (built from committed sources).
+* ``_ref/libbzref.so`` -- the reference's own sources compiled where they lie
+  (``ref_shim.cpp``); present only where the reference tree was available at build time.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF = None
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_i64p = np.ctypeslib.ndpointer(np.int64, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+
+
+class WalkParams(C.Structure):
+    _fields_ = [("theta2", C.c_float), ("eps2", C.c_float), ("rcut2", C.c_float),
+                ("box", C.c_float), ("rsplit", C.c_float), ("min_dist2", C.c_float),
+                ("quadrupole", C.c_int), ("group", C.c_int)]
+
+
+def build(ref: bool = False) -> None:
+    """Compile the restatement (and, with ref=True, the reference shim) in place."""
+    target = ["all", "ref"] if ref else ["all"]
+    subprocess.run(["make", "-s", "-C", HERE] + target, check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        src = os.path.join(HERE, "bz_oracle.c")
+        if not os.path.exists(path) or os.path.getmtime(path) < os.path.getmtime(src):
+            build()
+        L = C.CDLL(path)
+        L.or_bbox_f32.argtypes = [_f32p, _f32p, _f32p, C.c_int64, _f32p]
+        L.or_morton_ref.argtypes = [_f32p, _f32p, _f32p, C.c_int64, _f32p, C.c_int, _u64p]
+        L.or_morton63.argtypes = [_f64p, _f64p, _f64p, C.c_int64, _f64p, C.c_double, _u64p]
+        L.or_stable_sort_u64.argtypes = [_u64p, C.c_int64, _i32p]
+        L.or_ref_linear_octree.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int64, C.c_int, C.c_int,
+                                           C.c_int64, _f32p, _i32p, _i32p, _i32p, _i32p, _i32p,
+                                           _u64p, _i32p, _i32p]
+        L.or_ref_linear_octree.restype = C.c_int64
+        L.or_ref_walk.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int64, _f32p, _i32p, _i32p,
+                                  _i32p, _i32p, _i32p, _i32p, C.c_int32, C.c_float, C.c_float,
+                                  C.c_float, C.c_float, C.c_int, C.c_float, C.c_float, _f64p]
+        L.or_build_tree.argtypes = [_u64p, _f32p, C.c_int64, C.c_int, C.c_int, C.c_int64,
+                                    _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _f32p, _f32p,
+                                    _f32p, _f32p]
+        L.or_build_tree.restype = C.c_int64
+        L.or_walk.argtypes = [_f32p, C.c_int64, _i32p, _i32p, _i32p, _i32p, _f32p, _f32p,
+                              _f32p, _f32p, C.POINTER(WalkParams), _f64p, C.c_void_p, _i64p,
+                              _i64p]
+        L.or_direct_f64.argtypes = [_f32p, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
+                                    C.c_double, C.c_double, C.c_double, _f64p, C.c_void_p]
+        L.or_ewald_f64.argtypes = [_f32p, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
+                                   C.c_double, C.c_double, C.c_int, _f64p]
+        L.or_fft3d.argtypes = [_f64p, C.c_int, C.c_int]
+        L.or_pm_periodic.argtypes = [_f32p, C.c_int64, C.c_int, C.c_double, C.c_double, _f64p,
+                                     C.c_void_p, C.c_void_p]
+        L.or_split_weight.argtypes = [C.c_double, C.c_double]
+        L.or_split_weight.restype = C.c_double
+        _LIB = L
+    return _LIB
+
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libbzref.so"))
+
+
+def ref():
+    """The reference's own code (compiled from its sources), or None when not built."""
+    global _REF
+    if _REF is None:
+        path = os.path.join(HERE, "_ref", "libbzref.so")
+        if not os.path.exists(path):
+            return None
+        R = C.CDLL(path)
+        R.ref_morton_keys.argtypes = [_f32p, _f32p, _f32p, C.c_int, _u64p, _i32p, _f32p]
+        R.ref_linear_octree.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_int,
+                                        _f32p, _i32p, _i32p, _i32p, _i32p, _i32p, _u64p, _i32p,
+                                        _i32p]
+        R.ref_octree_gpu_accel.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int,
+                                           C.c_float, C.c_float, C.c_float, C.c_float, C.c_int,
+                                           C.c_float, C.c_float, _f32p, _f32p, _f32p,
+                                           C.POINTER(C.c_int)]
+        R.ref_octree_cpu_accel.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_float,
+                                           C.c_float, C.c_float, C.c_float, C.c_int, C.c_float,
+                                           C.c_float, C.c_void_p, C.c_int, _f32p, _f32p, _f32p]
+        R.ref_fp64_pairwise.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_float,
+                                        C.c_float, _f32p, _f32p, _f32p]
+        R.ref_pm_periodic.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_double,
+                                      C.c_double, C.c_int, C.c_char_p, _f32p, _f32p, _f32p,
+                                      C.c_void_p, C.c_void_p]
+        R.ref_fft3d.argtypes = [_f64p, C.c_int, C.c_int]
+        R.ref_short_range_pair.argtypes = [_f32p, _f32p, C.c_float, C.c_float, C.c_float,
+                                           C.c_float, _f32p]
+        R.ref_omp_threads.restype = C.c_int
+        _REF = R
+    return _REF
+
+
+# ------------------------------------------------------------------------- helpers
+
+def _soa(pos):
+    pos = np.asarray(pos, np.float32)
+    return [np.ascontiguousarray(pos[:, a]) for a in range(3)]
+
+
+def pos4(pos, mass):
+    out = np.empty((len(mass), 4), np.float32)
+    out[:, :3] = pos
+    out[:, 3] = mass
+    return out
+
+
+def morton_ref(pos, fused=True):
+    """Reference keys; fused=True models the reference CUDA kernel (nvcc contraction)."""
+    x, y, z = _soa(pos)
+    bb = np.zeros(6, np.float32)
+    lib().or_bbox_f32(x, y, z, len(x), bb)
+    keys = np.zeros(len(x), np.uint64)
+    lib().or_morton_ref(x, y, z, len(x), bb, 1 if fused else 0, keys)
+    return keys, bb
+
+
+def morton63(pos64, origin, size):
+    pos64 = np.asarray(pos64, np.float64)
+    keys = np.zeros(len(pos64), np.uint64)
+    lib().or_morton63(np.ascontiguousarray(pos64[:, 0]), np.ascontiguousarray(pos64[:, 1]),
+                      np.ascontiguousarray(pos64[:, 2]), len(pos64),
+                      np.asarray(origin, np.float64), float(size), keys)
+    return keys
+
+
+def stable_sort(keys):
+    perm = np.zeros(len(keys), np.int32)
+    lib().or_stable_sort_u64(np.ascontiguousarray(keys, np.uint64), len(keys), perm)
+    return perm
+
+
+def ref_linear_octree(pos, mass, leaf_capacity=256, fused=True):
+    """Restated reference topology (fused=True: as its CUDA build rounds).  Returns a dict."""
+    x, y, z = _soa(pos)
+    n = len(x)
+    cap = 8 * n + 64
+    out = dict(hot=np.zeros(8 * cap, np.float32), next=np.zeros(cap, np.int32),
+               mask=np.zeros(cap, np.int32), first=np.zeros(cap, np.int32),
+               lstart=np.zeros(cap, np.int32), lcount=np.zeros(cap, np.int32),
+               keys=np.zeros(n, np.uint64), index=np.zeros(n, np.int32))
+    depth = np.zeros(1, np.int32)
+    nn = lib().or_ref_linear_octree(x, y, z, np.asarray(mass, np.float32), n, leaf_capacity,
+                                    1 if fused else 0, cap,
+                                    out["hot"], out["next"], out["mask"], out["first"],
+                                    out["lstart"], out["lcount"], out["keys"], out["index"], depth)
+    if nn < 0:
+        raise RuntimeError("reference octree capacity overflow")
+    res = {k: (v[: 8 * nn].reshape(nn, 8) if k == "hot" else v[:nn]) for k, v in out.items()
+           if k not in ("keys", "index")}
+    res["keys"], res["index"], res["leaf_depth"], res["nodes"] = out["keys"], out["index"], int(depth[0]), int(nn)
+    return res
+
+
+def ref_walk(pos, mass, tree, theta=0.5, softening=0.01, min_distance2=1e-12,
+             max_acceleration=1e30, criterion=0, split_scale=0.0, cutoff2=0.0):
+    x, y, z = _soa(pos)
+    acc = np.zeros(3 * len(x), np.float64)
+    lib().or_ref_walk(x, y, z, np.asarray(mass, np.float32), len(x),
+                      np.ascontiguousarray(tree["hot"].reshape(-1)), tree["next"], tree["mask"],
+                      tree["first"], tree["lstart"], tree["lcount"], tree["index"],
+                      tree["nodes"] - 1, theta, softening, min_distance2, max_acceleration,
+                      criterion, split_scale, cutoff2, acc)
+    return acc.reshape(-1, 3)
+
+
+def build_tree(sorted_keys, sorted_pos4, leaf_cap=16, max_level=21):
+    n = len(sorted_keys)
+    cap = 2 * n + 64
+    a = {k: np.zeros(cap, np.int32) for k in ("start", "count", "child", "nchild", "parent", "level")}
+    mono = np.zeros(4 * cap, np.float32)
+    bmin = np.zeros(3 * cap, np.float32)
+    bmax = np.zeros(3 * cap, np.float32)
+    quad = np.zeros(6 * cap, np.float32)
+    nn = lib().or_build_tree(np.ascontiguousarray(sorted_keys, np.uint64),
+                             np.ascontiguousarray(sorted_pos4, np.float32), n, leaf_cap, max_level,
+                             cap, a["start"], a["count"], a["child"], a["nchild"], a["parent"],
+                             a["level"], mono, bmin, bmax, quad)
+    if nn < 0:
+        raise RuntimeError("tree capacity overflow")
+    t = {k: v[:nn] for k, v in a.items()}
+    t["mono"] = mono[: 4 * nn].reshape(nn, 4)
+    t["bmin"] = bmin[: 3 * nn].reshape(nn, 3)
+    t["bmax"] = bmax[: 3 * nn].reshape(nn, 3)
+    t["quad"] = quad[: 6 * nn].reshape(nn, 6)
+    t["nodes"] = int(nn)
+    return t
+
+
+def walk(sorted_pos4, tree, theta=0.5, eps=0.01, rcut=0.0, box=0.0, rsplit=0.0,
+         min_dist2=1e-12, quadrupole=True, group=32, want_pot=False):
+    n = len(sorted_pos4)
+    prm = WalkParams(np.float32(theta) * np.float32(theta), np.float32(eps) * np.float32(eps),
+                     np.float32(rcut) * np.float32(rcut), box, rsplit, min_dist2,
+                     1 if quadrupole else 0, group)
+    acc = np.zeros(3 * n, np.float64)
+    pot = np.zeros(n, np.float64) if want_pot else None
+    ng = (n + group - 1) // group
+    npp = np.zeros(ng, np.int64)
+    npn = np.zeros(ng, np.int64)
+    lib().or_walk(np.ascontiguousarray(sorted_pos4, np.float32), n, tree["start"], tree["count"],
+                  tree["child"], tree["nchild"], np.ascontiguousarray(tree["mono"].reshape(-1)),
+                  np.ascontiguousarray(tree["bmin"].reshape(-1)),
+                  np.ascontiguousarray(tree["bmax"].reshape(-1)),
+                  np.ascontiguousarray(tree["quad"].reshape(-1)), C.byref(prm), acc,
+                  pot.ctypes.data if pot is not None else None, npp, npn)
+    out = dict(acc=acc.reshape(n, 3), n_pp=npp, n_pn=npn)
+    if pot is not None:
+        out["pot"] = pot
+    return out
+
+
+def direct(pos4_, targets=None, eps=0.01, box=0.0, rsplit=0.0, rcut=0.0, want_pot=False):
+    p = np.ascontiguousarray(pos4_, np.float32)
+    if targets is None:
+        nt, tptr, tg = len(p), None, None
+    else:
+        tg = np.ascontiguousarray(targets, np.int64)
+        nt, tptr = len(tg), tg.ctypes.data
+    acc = np.zeros(3 * nt, np.float64)
+    pot = np.zeros(nt, np.float64) if want_pot else None
+    lib().or_direct_f64(p, len(p), tptr, nt, eps, box, rsplit, rcut, acc,
+                        pot.ctypes.data if pot is not None else None)
+    return (acc.reshape(nt, 3), pot) if want_pot else acc.reshape(nt, 3)
+
+
+def ewald(pos4_, targets=None, eps=0.0, box=1.0, alpha=None, kmax=8):
+    p = np.ascontiguousarray(pos4_, np.float32)
+    if alpha is None:
+        alpha = 6.4 / box
+    tg = None if targets is None else np.ascontiguousarray(targets, np.int64)
+    nt = len(p) if tg is None else len(tg)
+    acc = np.zeros(3 * nt, np.float64)
+    lib().or_ewald_f64(p, len(p), None if tg is None else tg.ctypes.data, nt, eps, box, alpha,
+                       kmax, acc)
+    return acc.reshape(nt, 3)
+
+
+def pm_periodic(pos4_, mesh, box, rsplit, want_fields=False):
+    p = np.ascontiguousarray(pos4_, np.float32)
+    acc = np.zeros(3 * len(p), np.float64)
+    cells = mesh ** 3
+    dens = np.zeros(cells, np.float64) if want_fields else None
+    phi = np.zeros(cells, np.float64) if want_fields else None
+    lib().or_pm_periodic(p, len(p), mesh, box, rsplit, acc,
+                         None if dens is None else dens.ctypes.data,
+                         None if phi is None else phi.ctypes.data)
+    if want_fields:
+        return acc.reshape(-1, 3), dens, phi
+    return acc.reshape(-1, 3)
+
+
+def fft3d(cube_complex, inverse=False):
+    a = np.ascontiguousarray(np.stack([cube_complex.real, cube_complex.imag], -1).reshape(-1), np.float64)
+    lib().or_fft3d(a, cube_complex.shape[0], 1 if inverse else 0)
+    a = a.reshape(-1, 2)
+    return (a[:, 0] + 1j * a[:, 1]).reshape(cube_complex.shape)
+
+
+def split_weight(s, rsplit):
+    return lib().or_split_weight(float(s), float(rsplit))
