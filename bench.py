@@ -1,0 +1,431 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the periodic TreePM leapfrog step on one B200.
+
+Workload (default ``treepm128``): N = 128^3 = 2,097,152 equal-mass particles on a unit
+periodic box, grid positions displaced by a Zel'dovich field of a Gaussian random field with
+P(k) ~ k^-2 (3-D rms displacement 0.2 cell, seed 2), zero velocities; PM mesh 128^3 CIC with
+Gaussian split r_s = 1.25 cells, short-range cutoff 4.5 r_s, theta = 0.5 with quadrupoles,
+Plummer softening 0.02 cell, FP64 leapfrog with dt = 5e-4.  Inputs are seeded synthetic data.
+
+A "step" is one KDK leapfrog step of the whole system (keys, sort, permutation, octree,
+mesh, group walk, kicks and drift), replayed from a CUDA graph.  The state (about 230 B per
+particle, ~480 MB) is larger than the 126 MB L2, so no flush is needed between steps.
+
+Under torchrun (N > 1) every rank steps an independent replica (the single-system path does
+not shard) and `value` sums all ranks' particle-steps over the slowest rank's
+device time.  ``--impl reference`` times the reference's CPU TreePM path instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+FLOP_PP = {True: 35, False: 20}          # pair: monopole 20 (rsqrt = 1), + 15 with the split
+FLOP_PN = {(True, True): 80, (True, False): 35, (False, True): 65, (False, False): 20}
+FP32_LANES_PER_SM = 128
+SMS = 148
+NOMINAL_SM_MHZ = 1965.0
+
+WORKLOADS = {
+    "treepm128": dict(kind="treepm", n_side=128, mesh=128, r_split_cells=1.25, r_cut_factor=4.5,
+                      theta=0.5, eps_cells=0.02, dt=5e-4, seed=2, rms_cells=0.2),
+    "treepm64": dict(kind="treepm", n_side=64, mesh=64, r_split_cells=1.25, r_cut_factor=4.5,
+                     theta=0.5, eps_cells=0.02, dt=5e-4, seed=2, rms_cells=0.2),
+    "plummer65k": dict(kind="octree", n=65536, theta=0.5, eps=0.01, dt=1e-3, seed=1),
+}
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="treepm128")
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--error-sample", type=int, default=2048)
+    ap.add_argument("--cpu-sample", type=int, default=16384)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# --------------------------------------------------------------------------- setup
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def init_dist(world, local, backend="nccl"):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    if backend == "nccl":
+        torch.cuda.set_device(local)
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return dist
+
+
+def make_ics(w, rank):
+    from blitzar_b200 import ics
+
+    if w["kind"] == "treepm":
+        pos, vel, mass = ics.grf_grid(w["n_side"], seed=w["seed"] + rank, rms_cells=w["rms_cells"])
+    else:
+        pos, vel, mass = ics.plummer(w["n"], seed=w["seed"] + rank)
+    return pos, vel, mass.astype(np.float32)
+
+
+def engine_config(w):
+    if w["kind"] == "treepm":
+        return dict(solver=1, box_length=1.0, treepm_grid_size=w["mesh"],
+                    treepm_r_split_cells=w["r_split_cells"], treepm_r_cut_factor=w["r_cut_factor"],
+                    octree_theta=w["theta"], octree_softening=w["eps_cells"] / w["mesh"],
+                    multipole_order=2)
+    return dict(solver=0, octree_theta=w["theta"], octree_softening=w["eps"], multipole_order=2)
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle-reason samples taken while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index=0):
+        self.dev = device_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100",
+                                          "-i", str(self.dev)],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, ValueError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def load_traffic(name):
+    path = os.path.join(ROOT, "profiles", f"{name}.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f)
+    return None
+
+
+# --------------------------------------------------------------------------- CPU baseline
+
+def cpu_baseline(w, pos, mass, sample, seed=7):
+    """Reference CPU path on a bounded sample: returns (particle-steps/s, cores, kind, text)."""
+    from oracle import oracle as O
+
+    n = len(mass)
+    rng = np.random.default_rng(seed)
+    targets = np.sort(rng.choice(n, size=min(sample, n), replace=False)).astype(np.int32)
+    p32 = pos.astype(np.float32)
+    x, y, z = [np.ascontiguousarray(p32[:, a]) for a in range(3)]
+    m = np.ascontiguousarray(mass, np.float32)
+    R = O.ref() if O.ref_available() else None
+    if w["kind"] == "treepm":
+        M = w["mesh"]
+        rs = w["r_split_cells"] / M
+        rc = w["r_cut_factor"] * rs
+        eps = w["eps_cells"] / M
+        if R is not None:
+            ax, ay, az = [np.zeros(n, np.float32) for _ in range(3)]
+            t0 = time.perf_counter()
+            R.ref_pm_periodic(x, y, z, m, n, M, 1.0, rs, 0, b"cic", ax, ay, az, None, None)
+            t_pm = time.perf_counter() - t0
+            bx, by, bz = [np.zeros(len(targets), np.float32) for _ in range(3)]
+            t0 = time.perf_counter()
+            R.ref_octree_cpu_accel(x, y, z, m, n, w["theta"], eps, 1e-12, 1e30, 0, rs, rc * rc,
+                                   targets.ctypes.data, len(targets), bx, by, bz)
+            t_tree = time.perf_counter() - t0
+            cores = int(R.ref_omp_threads())
+            kind = "reference"
+            text = (f"reference CPU TreePM pieces built from the reference sources: periodic PM "
+                    f"(templates TpmAssignment/TpmField, FP32, mesh {M}^3) over all {n} particles "
+                    f"+ octree_cpu build over all {n} and its cutoff/erfc-split walk for "
+                    f"{len(targets)} seeded targets, walk time scaled to N (open-boundary short "
+                    f"range: the reference has no periodic split)")
+        else:
+            p4 = O.pos4(p32, m)
+            t0 = time.perf_counter()
+            O.pm_periodic(p4, M, 1.0, rs)
+            t_pm = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            O.direct(p4, targets[:1024].astype(np.int64), eps=eps, box=1.0, rsplit=rs, rcut=rc)
+            t_tree = (time.perf_counter() - t0) * len(targets) / 1024
+            cores = os.cpu_count() or 1
+            kind = "port"
+            text = "oracle port: FP64 PM + FP64 direct short range on a target sample, scaled to N"
+        t_step = t_pm + t_tree * n / len(targets)
+    else:
+        if R is None:
+            return None
+        ax, ay, az = [np.zeros(len(targets), np.float32) for _ in range(3)]
+        t0 = time.perf_counter()
+        R.ref_octree_cpu_accel(x, y, z, m, n, w["theta"], w["eps"], 1e-12, 1e30, 0, 0.0, 0.0,
+                               targets.ctypes.data, len(targets), ax, ay, az)
+        t_tree = time.perf_counter() - t0
+        t_step = t_tree * n / len(targets)
+        cores = int(R.ref_omp_threads())
+        kind = "reference"
+        text = f"reference octree_cpu build over all {n} + walk for {len(targets)} targets, scaled to N"
+    return n / t_step, cores, kind, text
+
+
+# --------------------------------------------------------------------------- arms
+
+def run_reference(args, w, rank, world):
+    if rank != 0:
+        return 0
+    pos, vel, mass = make_ics(w, 0)
+    n = len(mass)
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        pass
+    vals = []
+    res = None
+    for _ in range(max(1, min(args.steps, 3))):
+        res = cpu_baseline(w, pos, mass, args.cpu_sample)
+        if res is None:
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU library not built"}))
+            return 0
+        vals.append(res[0])
+    value = float(np.median(vals))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * n / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_dict(w, args, n),
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": res[1], "kind": res[2],
+                         "sample": res[3]},
+        "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+METRIC = "particle-steps/s at <=1e-3 median force err: learned/mixed vs plain GPU TreePM"
+
+
+def config_dict(w, args, n):
+    c = {"workload": args.workload, "particles": n, "parallelism": f"replicas{args.gpus}",
+         "l2": "inputs larger than L2 (state ~230 B/particle)"}
+    c.update({k: v for k, v in w.items() if k != "kind"})
+    return c
+
+
+def run_ours(args, w, rank, world, local):
+    import torch
+
+    dist = init_dist(world, local)
+    torch.cuda.set_device(local)
+    from blitzar_b200._lib import Engine
+
+    pos, vel, mass = make_ics(w, rank)
+    n = len(mass)
+    stream = torch.cuda.Stream()
+    cfg = engine_config(w)
+    eng = Engine(n, stream=stream.cuda_stream, device=local, **cfg)
+    eng.set_state(pos, vel, mass, f64=True)
+    dt = w["dt"]
+    with torch.cuda.stream(stream):
+        for _ in range(max(3, args.warmup)):
+            eng.step(dt, 1)
+    torch.cuda.synchronize()
+
+    clocks = ClockSampler(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    time.sleep(0.3)
+    start = torch.cuda.Event(enable_timing=True)
+    end = torch.cuda.Event(enable_timing=True)
+    start.record(stream)
+    eng.step(dt, args.steps)
+    end.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = start.elapsed_time(end)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = n * world * args.steps / (ms / 1e3)
+
+    launches_step = eng.launches_per_step()
+    # phase-timed eager pass for the per-kernel roofline
+    eng.enable_timing(True)
+    eng.step(dt, 3)
+    ph = eng.phase_times()
+    pp, pn = eng.interaction_counts()
+    eng.enable_timing(False)
+    split = w["kind"] == "treepm"
+    flops = pp * FLOP_PP[split] + pn * FLOP_PN[(split, True)]
+    walk_ms = ph["walk"]
+    achieved_tf = flops / (walk_ms * 1e-3) / 1e12
+    peak_tf = SMS * FP32_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
+    traffic = load_traffic(f"walk_{args.workload}")
+    roofline = {
+        "kernel": "k_walk (group tree walk + pair/multipole arithmetic)",
+        "bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
+        "frac": achieved_tf / peak_tf,
+        "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak is provided",
+        "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
+        "interactions_per_launch": {"particle_particle": pp, "particle_node": pn},
+        "flops_per_interaction": {"pp": FLOP_PP[split], "pn": FLOP_PN[(split, True)]},
+        "launch_ms": walk_ms,
+    }
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except OSError:
+        pass
+    hbm_peak = peaks.get("hbm_gbs", 6650.0)
+    sort_bytes = n * (8 + 8 * 24)      # histogram read + 8 passes x (12 B read + 12 B write)
+    keys_bytes = n * (24 + 12)
+    permute_bytes = n * (2 * (48 + 4 + 4) + 16)
+    secondary = {
+        "sort": {"bound": "hbm", "achieved": sort_bytes / (ph["sort"] * 1e-3) / 1e9, "peak": hbm_peak,
+                 "unit": "GB/s", "ms": ph["sort"]},
+        "keys": {"bound": "hbm", "achieved": keys_bytes / (ph["keys"] * 1e-3) / 1e9, "peak": hbm_peak,
+                 "unit": "GB/s", "ms": ph["keys"]},
+        "permute": {"bound": "hbm", "achieved": permute_bytes / (ph["permute"] * 1e-3) / 1e9,
+                    "peak": hbm_peak, "unit": "GB/s", "ms": ph["permute"]},
+    }
+    for k in secondary.values():
+        k["frac"] = k["achieved"] / k["peak"]
+
+    errs = eng.force_errors(nsample=args.error_sample, seed=11)
+
+    # end to end through the C ABI with pinned host buffers: upload state, one step, download
+    e2e = None
+    if args.e2e_steps > 0:
+        hp = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
+        hv = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
+        hm = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
+        eng.get_state_soa(hp, hv)
+        hm[:] = mass
+        eng.set_state_soa(hp, hv, hm)
+        eng.step(dt, 1)
+        eng.get_state_soa(hp, hv)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            eng.set_state_soa(hp, hv, hm)
+            eng.step(dt, 1)
+            eng.get_state_soa(hp, hv)
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([sec], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            sec = float(t.item())
+        e2e = {"value": n * world * args.e2e_steps / sec, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": 7 * 4 * n, "d2h_bytes_per_step": 6 * 4 * n,
+               "note": "each step uploads the full state, which forces a fresh force evaluation "
+                       "before the leapfrog step (two evaluations per step)"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        res = cpu_baseline(w, pos, mass, args.cpu_sample)
+        if res is not None:
+            cpu = {"value": res[0], "unit": "particle-steps/s", "cores": res[1], "kind": res[2],
+                   "sample": res[3]}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded GRF-displaced grid)" if w["kind"] == "treepm" else "synthetic (seeded Plummer)",
+        "config": config_dict(w, args, n),
+        "force_error": {"median": errs["median"], "p99": errs["p99"], "sample": args.error_sample,
+                        "reference": "FP64 Ewald" if w["kind"] == "treepm" else "FP64 direct sum"},
+        "roofline": roofline, "roofline_secondary": secondary,
+        "phase_ms": ph, "gpu_launches": launches_step * args.steps, "launches_per_step": launches_step,
+        "clocks": clk, "e2e": e2e, "cpu_baseline": cpu,
+    }
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    w = WORKLOADS[args.workload]
+    if args.impl == "reference":
+        return run_reference(args, w, rank, world)
+    return run_ours(args, w, rank, world, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -24,7 +24,7 @@ EXPORTS = (
     "bz_accelerations", "bz_get_state", "bz_get_state_f64", "bz_morton_keys", "bz_tree_topology",
     "bz_reference_tree", "bz_interaction_counts", "bz_enable_phase_timing", "bz_phase_times",
     "bz_force_errors", "bz_pm_mesh", "bz_particle_count", "bz_device_bytes", "bz_last_error",
-    "bz_status_string", "bz_version",
+    "bz_status_string", "bz_version", "bz_kernel_launches", "bz_launches_per_step",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -100,6 +100,8 @@ def load():
     L.bz_status_string.argtypes = [C.c_int]
     L.bz_status_string.restype = C.c_char_p
     L.bz_version.restype = C.c_char_p
+    L.bz_kernel_launches.restype = C.c_uint64
+    L.bz_launches_per_step.argtypes = [_vp, C.POINTER(C.c_uint64)]
     _LIB = L
     return L
 
@@ -256,6 +258,11 @@ class Engine:
         out = np.empty(M ** 3, np.float32)
         self._check(self.L.bz_pm_mesh(self.h, which, _ptr(out)), "bz_pm_mesh")
         return out
+
+    def launches_per_step(self):
+        k = C.c_uint64(0)
+        self._check(self.L.bz_launches_per_step(self.h, C.byref(k)), "bz_launches_per_step")
+        return k.value
 
     def device_bytes(self):
         return self.L.bz_device_bytes(self.h)

@@ -22,6 +22,10 @@
 
 using namespace bz;
 
+namespace bz {
+std::atomic<unsigned long long> g_kernel_launches{0};
+}
+
 namespace {
 
 enum Phase { kPhKeys = 0, kPhSort, kPhPermute, kPhTree, kPhMesh, kPhWalk, kPhIntegrate, kPhTotal };
@@ -326,6 +330,32 @@ extern "C" {
 
 const char* bz_version(void) { return "bzgrav 0.1 (sm_100a)"; }
 
+uint64_t bz_kernel_launches(void) { return g_kernel_launches.load(); }
+
+bz_status bz_launches_per_step(bz_handle* h, uint64_t* launches)
+{
+    if (!h || !launches || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    // count one eagerly enqueued step into a throw-away capture (nothing executes)
+    cudaSetDevice(h->device);
+    const unsigned long long before = g_kernel_launches.load();
+    const int cur = h->cur;
+    const bool timing = h->timing;
+    h->timing = false;
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return fail(h, BZ_CUDA_ERROR, "capture for launch count");
+    enqueue_step(h);
+    cudaStreamEndCapture(h->stream, &g);
+    if (g)
+        cudaGraphDestroy(g);
+    h->cur = cur;
+    h->timing = timing;
+    *launches = g_kernel_launches.load() - before;
+    g_kernel_launches.fetch_sub(*launches);
+    return BZ_OK;
+}
+
 const char* bz_status_string(bz_status s)
 {
     switch (s) {
@@ -620,11 +650,13 @@ void enqueue_reference_order(bz_handle* h)
     const int n = static_cast<int>(h->n);
     DeviceBuffers& d = h->d;
     double* const* s = d.st[h->cur];
+    count_launch();
     k_caller_xyzm<<<blocks_for(n), 256, 0, h->stream>>>(s[0], s[1], s[2], d.mass[h->cur], d.id[h->cur],
                                                         n, d.ref_xyzm, d.ref_orig);
     launch_keys_reference(d.ref_xyzm, d.ref_xyzm + n, d.ref_xyzm + 2 * n, n, d.bbox32, d.keys,
                           d.perm, h->stream);
     launch_radix_sort(d.keys, d.perm, n, 32, h->sort, d.err, h->stream);
+    count_launch();
     k_gather_pos4<<<blocks_for(n), 256, 0, h->stream>>>(d.ref_orig, d.perm, n, d.pos4);
     launch_reference_leaf(d.ref_xyzm, d.ref_xyzm + n, d.ref_xyzm + 2 * n, d.ref_xyzm + 3 * n,
                           d.perm, n, d.ref_hot8, h->stream);
@@ -647,6 +679,7 @@ bz_status bz_set_state(bz_handle* h, const float* pos, const float* vel, const f
     cudaMemcpyAsync(d.stage + 6 * n, mass, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
     upload_common(h, n);
     double* const* s = d.st[0];
+    count_launch();
     k_unpack_state<<<blocks_for(n), 256, 0, h->stream>>>(d.stage, static_cast<int>(n), vel ? 1 : 0,
                                                          s[0], s[1], s[2], s[3], s[4], s[5],
                                                          d.mass[0], d.id[0],
@@ -687,6 +720,7 @@ bz_status bz_get_state(bz_handle* h, float* pos, float* vel)
     const size_t n = h->n;
     DeviceBuffers& d = h->d;
     double* const* s = d.st[h->cur];
+    count_launch();
     k_pack_state<<<blocks_for(n), 256, 0, h->stream>>>(s[0], s[1], s[2], s[3], s[4], s[5], d.id[h->cur],
                                                        static_cast<int>(n), d.stage, vel ? 1 : 0);
     cudaMemcpyAsync(pos, d.stage, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
@@ -707,6 +741,7 @@ bz_status bz_get_state_f64(bz_handle* h, double* pos, double* vel)
     double* tmp = nullptr;
     if (!dalloc(h, &tmp, 6 * n))
         return fail(h, BZ_OUT_OF_MEMORY, "bz_get_state_f64 staging");
+    count_launch();
     k_gather_f64<<<blocks_for(n), 256, 0, h->stream>>>(nullptr, s[0], s[1], s[2], s[3], s[4], s[5],
                                                        d.id[h->cur], static_cast<int>(n), tmp,
                                                        vel ? 1 : 0);
@@ -846,6 +881,7 @@ bz_status bz_morton_keys(bz_handle* h, uint64_t* sorted_keys, int32_t* perm)
         double* tmp = nullptr;
         if (!dalloc(h, &tmp, 3 * static_cast<size_t>(n)))
             return fail(h, BZ_OUT_OF_MEMORY, "bz_morton_keys staging");
+        count_launch();
         k_gather_f64<<<blocks_for(n), 256, 0, h->stream>>>(nullptr, s[0], s[1], s[2], s[3], s[4], s[5],
                                                            d.id[h->cur], n, tmp, 0);
         if (!periodic(h))

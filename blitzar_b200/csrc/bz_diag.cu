@@ -156,8 +156,10 @@ int ewald_num_k(int kmax)
 void launch_direct_f64(const float4* pos4, int n, const int* targets, int nt, double eps,
                        double* acc3, cudaStream_t s)
 {
-    if (nt > 0)
+    if (nt > 0) {
+        count_launch();
         k_direct_f64<<<nt, kThreads, 0, s>>>(pos4, n, targets, eps * eps, acc3);
+    }
 }
 
 void launch_ewald_f64(const float4* pos4, int n, const int* targets, int nt, double eps,
@@ -165,10 +167,13 @@ void launch_ewald_f64(const float4* pos4, int n, const int* targets, int nt, dou
                       cudaStream_t s)
 {
     const int nk = ewald_num_k(kmax);
+    count_launch();
     k_ewald_sk<<<nk, kThreads, 0, s>>>(pos4, n, kmax, 2.0 * kPi / box, sk_scratch);
-    if (nt > 0)
+    if (nt > 0) {
+        count_launch();
         k_ewald_target<<<nt, kThreads, 0, s>>>(pos4, n, targets, eps * eps, box, alpha, nk,
                                                sk_scratch, acc3);
+    }
 }
 
 } // namespace bz

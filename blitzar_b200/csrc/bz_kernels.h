@@ -1,10 +1,16 @@
 // Internal launch interface between the C-ABI layer (bz_api.cu) and the kernel files.
 // Every launcher enqueues on the given stream and never synchronises.
 #pragma once
+#include <atomic>
 #include <cstdint>
 #include <cuda_runtime.h>
 
 namespace bz {
+
+// Number of this library's kernel launches enqueued so far (cuFFT's own kernels are not
+// counted).  Launches recorded into a CUDA graph are counted once, at capture.
+extern std::atomic<unsigned long long> g_kernel_launches;
+inline void count_launch(unsigned long long k = 1) { g_kernel_launches.fetch_add(k, std::memory_order_relaxed); }
 
 // ---------------------------------------------------------------- keys (bz_keys.cu)
 struct BoxF64 {

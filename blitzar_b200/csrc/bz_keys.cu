@@ -229,7 +229,9 @@ int grid_for(int n)
 void launch_bbox_f64(const double* x, const double* y, const double* z, int n, BoxF64* box,
                      cudaStream_t s)
 {
+    count_launch();
     k_bbox_init<<<1, 32, 0, s>>>(box);
+    count_launch();
     k_bbox_f64<<<grid_for(n), kThreads, 0, s>>>(x, y, z, n, box);
 }
 
@@ -237,6 +239,7 @@ void launch_keys63(const double* x, const double* y, const double* z, int n,
                    const BoxF64* box, double periodic_len, unsigned long long* keys,
                    uint32_t* perm, cudaStream_t s)
 {
+    count_launch();
     k_keys63<<<grid_for(n), kThreads, 0, s>>>(x, y, z, n, box, periodic_len, keys, perm);
 }
 
@@ -244,8 +247,11 @@ void launch_keys_reference(const float* x, const float* y, const float* z, int n
                            unsigned* bbox_ordered6, unsigned long long* keys, uint32_t* perm,
                            cudaStream_t s)
 {
+    count_launch();
     k_bbox32_init<<<1, 32, 0, s>>>(bbox_ordered6);
+    count_launch();
     k_bbox_f32<<<grid_for(n), kThreads, 0, s>>>(x, y, z, n, bbox_ordered6);
+    count_launch();
     k_keys_reference<<<grid_for(n), kThreads, 0, s>>>(x, y, z, n, bbox_ordered6, keys, perm);
 }
 

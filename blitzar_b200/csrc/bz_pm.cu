@@ -208,6 +208,7 @@ PmPlan* pm_create(int mesh, double box, double rsplit, cudaStream_t s, int* cuda
     cufftGetSize(p->r2c, &ws1);
     cufftGetSize(p->c2r, &ws2);
     p->bytes = cells * sizeof(float) + half * (sizeof(cufftComplex) + sizeof(double)) + ws1 + ws2;
+    count_launch();
     k_green_table<<<sm_count() * 4, 256, 0, s>>>(mesh, box, rsplit, p->green);
     return p;
 }
@@ -240,6 +241,7 @@ void pm_deposit(PmPlan* p, const float4* pos4, int n, cudaStream_t s)
     cudaMemsetAsync(p->rho, 0, cells * sizeof(float), s);
     int b = (n + kThreads - 1) / kThreads;
     b = b < sms * 8 ? b : sms * 8;
+    count_launch();
     k_deposit<<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, inv_h3, p->rho);
 }
 
@@ -249,6 +251,7 @@ int pm_solve(PmPlan* p, cudaStream_t s)
     const size_t half = static_cast<size_t>(M) * M * (M / 2 + 1);
     if (cufftExecR2C(p->r2c, p->rho, p->spec) != CUFFT_SUCCESS)
         return 1;
+    count_launch();
     k_apply_green<<<sm_count() * 4, kThreads, 0, s>>>(p->spec, p->green, half);
     if (cufftExecC2R(p->c2r, p->spec, p->rho) != CUFFT_SUCCESS)
         return 2;
@@ -263,6 +266,7 @@ void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float
     const int sms = sm_count();
     int b = (n + kThreads - 1) / kThreads;
     b = b < sms * 8 ? b : sms * 8;
+    count_launch();
     k_interp_gradient<<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->rho, ax, ay, az);
 }
 

@@ -253,10 +253,13 @@ void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    count_launch();
     k_sort_init<<<1, 256, 0, s>>>(ws);
     int hb = (n + kThreads - 1) / kThreads;
     hb = hb < 2 * sms ? hb : 2 * sms;
+    count_launch();
     k_histogram<<<hb, kThreads, 0, s>>>(keys, n, passes, ws);
+    count_launch();
     k_scan_hist<<<passes, 256, 0, s>>>(n, ws);
     const int tiles = (n + kTile - 1) / kTile;
     const size_t smem = sizeof(PassSmem);
@@ -266,11 +269,14 @@ void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits
                              static_cast<int>(smem));
         attr_set = true;
     }
-    for (int p = 0; p < passes; ++p)
+    for (int p = 0; p < passes; ++p) {
+        count_launch();
         k_onesweep<<<tiles, kThreads, smem, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, p, ws,
                                                  err);
+    }
     int fb = (n + 255) / 256;
     fb = fb < 4 * sms ? fb : 4 * sms;
+    count_launch();
     k_fixup<<<fb, 256, 0, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, passes, ws);
 }
 

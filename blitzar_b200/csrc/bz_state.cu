@@ -170,12 +170,14 @@ void launch_permute(const uint32_t* perm, int n, const double* const* src, doubl
         a.src[c] = src[c];
         a.dst[c] = dst[c];
     }
+    count_launch();
     k_permute<<<grid_for(n), kThreads, 0, s>>>(perm, n, a, ndouble, msrc, mdst, idsrc, iddst, pos4);
 }
 
 void launch_kick(double* vx, double* vy, double* vz, const float* ax, const float* ay,
                  const float* az, int n, const double* dt_half, cudaStream_t s)
 {
+    count_launch();
     k_kick<<<grid_for(n), kThreads, 0, s>>>(vx, vy, vz, ax, ay, az, n, dt_half);
 }
 
@@ -183,8 +185,11 @@ void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, 
                        const float* ax, const float* ay, const float* az, int n,
                        const double* dt, double periodic_len, BoxF64* box, cudaStream_t s)
 {
-    if (box)
+    if (box) {
+        count_launch();
         k_box_reset<<<1, 32, 0, s>>>(box);
+    }
+    count_launch();
     k_kick_drift<<<grid_for(n), kThreads, 0, s>>>(x, y, z, vx, vy, vz, ax, ay, az, n, dt,
                                                   periodic_len, box);
 }
@@ -192,11 +197,13 @@ void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, 
 void launch_scatter3(const float* ax, const float* ay, const float* az, const int* id, int n,
                      float* out_soa3, cudaStream_t s)
 {
+    count_launch();
     k_scatter3<<<grid_for(n), kThreads, 0, s>>>(ax, ay, az, id, n, out_soa3);
 }
 
 void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s)
 {
+    count_launch();
     k_f64_to_f32<<<grid_for(n), kThreads, 0, s>>>(src, dst, n);
 }
 

@@ -331,6 +331,7 @@ void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const size_t lbw = static_cast<size_t>(t.cap) / kThreads + kMaxLevels + 4;
     cudaMemsetAsync(t.lookback, 0, lbw * sizeof(unsigned long long), s);
+    count_launch();
     k_tree_init<<<1, 32, 0, s>>>(t, n);
     // Level l holds at most min(8^l, n) nodes; the persistent grid covers that with tiles.
     for (int l = 0; l < max_level; ++l) {
@@ -342,13 +343,16 @@ void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4
         long long blocks = (bound + kThreads - 1) / kThreads;
         if (blocks > 2LL * sms)
             blocks = 2LL * sms;
+        count_launch();
         k_tree_level<<<static_cast<int>(blocks), kThreads, 0, s>>>(sorted_keys, l, leaf_cap,
                                                                    max_level, t, err);
     }
+    count_launch();
     k_tree_finish_last<<<sms, 256, 0, s>>>(t, max_level);
     long long mb = (static_cast<long long>(t.cap) + kThreads - 1) / kThreads;
     if (mb > 16LL * sms)
         mb = 16LL * sms;
+    count_launch();
     k_tree_moments<<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
 }
 
@@ -408,6 +412,7 @@ __global__ void k_reference_leaf(const float* __restrict__ x, const float* __res
 void launch_reference_leaf(const float* x, const float* y, const float* z, const float* m,
                            const uint32_t* sorted_index, int n, float* hot8, cudaStream_t s)
 {
+    count_launch();
     k_reference_leaf<<<1, 32, 0, s>>>(x, y, z, m, sorted_index, n, hot8);
 }
 

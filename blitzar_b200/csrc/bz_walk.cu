@@ -572,7 +572,9 @@ void launch_variant(const float4* pos4, int n, const TreeArrays& t, const WalkPa
 {
     const WalkLaunch l = walk_shape<PERIODIC, SPLIT, QUAD, POT>(n);
     const float inv_box = p.box > 0.0f ? 1.0f / p.box : 0.0f;
+    count_launch();
     k_zero_u32<<<1, 1, 0, s>>>(queue);
+    count_launch();
     k_walk<PERIODIC, SPLIT, QUAD, POT><<<l.blocks, kWarps * 32, l.smem, s>>>(pos4, n, t, p, inv_box,
                                                                             o, queue, spill, err);
 }
@@ -699,6 +701,7 @@ void launch_reference_walk(const float4* pos_orig, const float4* pos_sorted,
                            cudaStream_t s)
 {
     const int blocks = (n + kRefThreads - 1) / kRefThreads;
+    count_launch();
     k_reference_walk<<<blocks, kRefThreads, 0, s>>>(pos_orig, pos_sorted, sorted_index, n,
                                                     softening, min_distance2, split_scale,
                                                     cutoff2, max_acceleration, ax, ay, az);

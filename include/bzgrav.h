@@ -153,6 +153,11 @@ bz_status bz_force_errors(bz_handle* h, int32_t nsample, uint64_t seed, float* e
  * deposit, 1 potential after the solve.  out holds grid^3 floats, index (z*M + y)*M + x. */
 bz_status bz_pm_mesh(bz_handle* h, int which, float* out);
 
+/* Kernel launches of this library enqueued so far (cuFFT's own kernels excluded), and the
+ * number one bz_step step enqueues. */
+uint64_t bz_kernel_launches(void);
+bz_status bz_launches_per_step(bz_handle* h, uint64_t* launches);
+
 size_t bz_particle_count(const bz_handle* h);
 size_t bz_device_bytes(const bz_handle* h);
 
