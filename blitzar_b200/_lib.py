@@ -47,6 +47,10 @@ class BzConfig(C.Structure):
         ("treepm_grid_size", C.c_int32),
         ("treepm_r_split_cells", C.c_float),
         ("treepm_r_cut_factor", C.c_float),
+        ("treepm_assignment", C.c_int32),
+        ("treepm_gradient", C.c_int32),
+        ("treepm_window_floor", C.c_float),
+        ("treepm_node_size_factor", C.c_float),
         ("box_length", C.c_double),
         ("key_mode", C.c_int32),
         ("device", C.c_int32),

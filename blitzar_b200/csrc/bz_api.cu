@@ -143,6 +143,7 @@ WalkParams walk_params(const bz_handle* h, bool want_pot)
         const float rc = h->cfg.treepm_r_cut_factor * rs;
         p.rsplit = rs;
         p.rcut2 = rc * rc;
+        p.max_node_size = h->cfg.treepm_node_size_factor > 0.0f ? h->cfg.treepm_node_size_factor * rs : 0.0f;
         p.box = static_cast<float>(h->cfg.box_length);
     }
     return p;
@@ -392,6 +393,10 @@ bz_status bz_config_init(bz_config* c)
     c->treepm_grid_size = 128;
     c->treepm_r_split_cells = 1.25f;
     c->treepm_r_cut_factor = 4.5f;
+    c->treepm_assignment = 0;
+    c->treepm_gradient = 0;
+    c->treepm_window_floor = 0.08f;
+    c->treepm_node_size_factor = 0.0f;
     c->box_length = 0.0;
     c->key_mode = BZ_KEYS_PRODUCTION;
     c->device = 0;
@@ -449,7 +454,8 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     if (cfg->solver == BZ_SOLVER_TREEPM) {
         const int M = cfg->treepm_grid_size;
         if (cfg->box_length <= 0.0 || M < 8 || (M & (M - 1)) != 0 || cfg->treepm_r_split_cells <= 0.0f ||
-            cfg->treepm_r_cut_factor <= 0.0f) {
+            cfg->treepm_r_cut_factor <= 0.0f || cfg->treepm_assignment < 0 || cfg->treepm_assignment > 2 ||
+            cfg->treepm_r_cut_factor * cfg->treepm_r_split_cells * 2.0 >= M) {
             delete h;
             return BZ_INVALID_ARGUMENT;
         }
@@ -519,7 +525,9 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     cudaMemsetAsync(d.err, 0, sizeof(int), h->stream);
     if (cfg->solver == BZ_SOLVER_TREEPM) {
         int perr = 0;
-        h->pm = pm_create(cfg->treepm_grid_size, cfg->box_length, rsplit_len(h), h->stream, &perr);
+        h->pm = pm_create(cfg->treepm_grid_size, cfg->box_length, rsplit_len(h),
+                          cfg->treepm_assignment + 2, cfg->treepm_gradient,
+                          cfg->treepm_window_floor, h->stream, &perr);
         if (!h->pm) {
             bz_destroy(h);
             return BZ_OUT_OF_MEMORY;
@@ -994,18 +1002,35 @@ bz_status bz_tree_topology(bz_handle* h, int64_t* node_count, int32_t* start, in
 
 bz_status bz_pm_mesh(bz_handle* h, int which, float* out)
 {
-    if (!h || !out || !h->pm || h->n == 0)
+    if (!h || !out || !h->pm || h->n == 0 || which < 0 || which > 4)
         return BZ_INVALID_ARGUMENT;
+    if (which == 1 && h->cfg.treepm_gradient != 0)
+        return fail(h, BZ_UNSUPPORTED, "the potential mesh exists in centred-difference mode only");
     cudaSetDevice(h->device);
     bz_status s = ensure_forces(h);
     if (s != BZ_OK)
         return s;
-    pm_deposit(h->pm, h->d.pos4, static_cast<int>(h->n), h->stream);
-    if (which == 1 && pm_solve(h->pm, h->stream) != 0)
-        return fail(h, BZ_CUDA_ERROR, "[cufft] mesh solve failed");
     const size_t M = static_cast<size_t>(h->cfg.treepm_grid_size);
-    cudaMemcpyAsync(out, pm_mesh(h->pm), M * M * M * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
-    return check_device(h, "bz_pm_mesh");
+    pm_deposit(h->pm, h->d.pos4, static_cast<int>(h->n), h->stream);
+    if (which == 0) {
+        cudaMemcpyAsync(out, pm_mesh(h->pm), M * M * M * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+        return check_device(h, "bz_pm_mesh");
+    }
+    if (pm_solve(h->pm, h->stream) != 0)
+        return fail(h, BZ_CUDA_ERROR, "[cufft] mesh solve failed");
+    if (which == 1) {
+        cudaMemcpyAsync(out, pm_mesh(h->pm), M * M * M * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+        return check_device(h, "bz_pm_mesh");
+    }
+    std::vector<float4> f(M * M * M);
+    cudaMemcpyAsync(f.data(), pm_force_mesh(h->pm), f.size() * sizeof(float4), cudaMemcpyDeviceToHost,
+                    h->stream);
+    s = check_device(h, "bz_pm_mesh");
+    if (s != BZ_OK)
+        return s;
+    for (size_t c = 0; c < f.size(); ++c)
+        out[c] = which == 2 ? f[c].x : (which == 3 ? f[c].y : f[c].z);
+    return BZ_OK;
 }
 
 bz_status bz_force_errors(bz_handle* h, int32_t nsample, uint64_t seed, float* errs,

@@ -89,6 +89,7 @@ struct WalkParams {
     float box;        // periodic length, 0 = open
     float rsplit;     // Gaussian split scale, 0 = Newtonian
     float min_dist2;
+    float max_node_size;  // > 0: nodes at least this large are never accepted as multipoles
     int quadrupole;
     int want_pot;
 };
@@ -115,7 +116,10 @@ void launch_reference_walk(const float4* pos_orig, const float4* pos_sorted,
 
 // ---------------------------------------------------------------- PM (bz_pm.cu)
 struct PmPlan;
-PmPlan* pm_create(int mesh, double box, double rsplit, cudaStream_t s, int* cuda_err);
+// order: 2 CIC, 3 TSC, 4 PCS; gradient: 0 centred differences of phi, 1 spectral (i k);
+// window_floor: lower bound of the deconvolution window (the reference uses 0.08).
+PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, double window_floor,
+                  cudaStream_t s, int* cuda_err);
 void pm_destroy(PmPlan* p);
 size_t pm_bytes(const PmPlan* p);
 // Deposit, FFT Poisson solve with split + deconvolution, then interpolate the centred-
@@ -123,12 +127,15 @@ size_t pm_bytes(const PmPlan* p);
 int pm_forces(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float* az,
               cudaStream_t s);
 // The three stages separately (tests read the mesh between them): the mesh buffer holds the
-// density after pm_deposit and the potential after pm_solve.
+// density after pm_deposit and, in centred-difference mode, the potential after pm_solve.
 void pm_deposit(PmPlan* p, const float4* pos4, int n, cudaStream_t s);
+// particles per deposit block, chosen so that a block's stencils fit a shared-memory tile
+int pm_deposit_chunk(const PmPlan* p, int n);
 int pm_solve(PmPlan* p, cudaStream_t s);
 void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float* az,
                cudaStream_t s);
 float* pm_mesh(PmPlan* p);
+const float4* pm_force_mesh(PmPlan* p);
 
 // ---------------------------------------------------------------- state (bz_state.cu)
 void launch_permute(const uint32_t* perm, int n, const double* const* src, double* const* dst,

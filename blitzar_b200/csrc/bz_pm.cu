@@ -1,16 +1,26 @@
-// Periodic particle-mesh (long-range) leg of TreePM:
-//   CIC deposit (float atomics onto the mesh, Morton-sorted particles for locality)
-//   -> cuFFT R2C -> Green's function with Gaussian split, CIC window deconvolution and the
-//      1/M^3 normalisation folded in (normalisation constant in FP64)
-//   -> cuFFT C2R -> potential
-//   -> per-particle CIC interpolation of the centred-difference gradient, fused: the three
-//      gradient meshes of the reference are never written.
+// Periodic particle-mesh (long-range) leg of TreePM.
+//
+//   deposit  : mass assignment of order p (2 CIC, 3 TSC, 4 PCS) onto an M^3 mesh.  Each block
+//              takes 2048 consecutive Morton-sorted particles, accumulates them into a
+//              shared-memory tile covering their stencils (shared atomics), then adds the tile
+//              to the mesh (one global atomic per tile cell instead of p^3 per particle);
+//              blocks whose stencils do not fit a tile use global atomics directly.
+//   solve    : cuFFT R2C -> Green's function with Gaussian split, window deconvolution and 1/M^3
+//              (precomputed in FP64) -> either the potential (reference centred differences,
+//              then a gradient kernel) or, fused in the same k-space pass, the three spectral
+//              gradients i k phi_k -> cuFFT C2R -> interleaved float4 force mesh.
+//   interp   : the same order-p stencil gathers the force mesh at each particle.
+//
 // Formulas follow the reference CPU templates driven with a periodic grid
-// (engine/physics/treepm/deposit/TpmAssignment.inl:104-199,
-//  engine/physics/treepm/field/TpmField.inl:6-89): mesh node i sits at i*h, density is
-// mass/h^3, phi_k = 4 pi e^{-k^2 r_s^2} rho_k / (k^2 max(W, 0.08)), W = prod sinc^4(k h/2),
-// acceleration = +centred difference of that phi.
+// (engine/physics/treepm/deposit/TpmAssignment.inl:39-199, engine/physics/treepm/field/
+// TpmField.inl:6-89): node i at i*h, density mass/h^3, phi_k = 4 pi e^{-k^2 r_s^2} rho_k /
+// (k^2 max(W, floor)), W = prod sinc^{2p}(k h / 2), acceleration = +gradient of that phi.
+// The reference's PCS stencil starts at floor(s + 0.5) - 1 and so drops the node floor(s) - 1
+// when frac(s) >= 0.5; here every order uses the full support (TSC: nearest node +-1, CIC and
+// PCS: floor(s) - (p/2 - 1) ... floor(s) + p/2).
 #include <cufft.h>
+
+#include <cmath>
 
 #include "bz_common.cuh"
 #include "bz_kernels.h"
@@ -21,9 +31,15 @@ struct PmPlan {
     int mesh = 0;
     double box = 0.0;
     double rsplit = 0.0;
-    float* rho = nullptr;          // M^3, later reused for phi
-    cufftComplex* spec = nullptr;  // M*M*(M/2+1)
-    double* green = nullptr;       // M*M*(M/2+1) precomputed Green x window x normalisation
+    int order = 2;
+    int gradient = 0;          // 0 centred differences of phi (reference), 1 spectral
+    double floor = 0.08;
+    float* rho = nullptr;      // M^3: density, then potential (centred-difference mode)
+    cufftComplex* spec = nullptr;     // M*M*(M/2+1)
+    cufftComplex* spec3 = nullptr;    // 3 x M*M*(M/2+1) spectral gradients
+    float* field3 = nullptr;          // 3 x M^3 real gradients
+    float4* force = nullptr;          // M^3 interleaved force mesh
+    double* green = nullptr;          // M*M*(M/2+1)
     cufftHandle r2c = 0, c2r = 0;
     size_t bytes = 0;
 };
@@ -31,52 +47,148 @@ struct PmPlan {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr int kTileCells = 12000;      // 47 KB of float accumulators (static shared memory <= 48 KB)
 
-__device__ __forceinline__ void cic_axis(float coord, float inv_h, int mesh, int& i0, int& i1,
-                                         float& w0, float& w1)
+__device__ __forceinline__ float tsc_w(float d)
+{
+    const float a = fabsf(d);
+    if (a < 0.5f)
+        return 0.75f - a * a;
+    if (a < 1.5f) {
+        const float t = 1.5f - a;
+        return 0.5f * t * t;
+    }
+    return 0.0f;
+}
+__device__ __forceinline__ float pcs_w(float d)
+{
+    const float a = fabsf(d);
+    if (a < 1.0f)
+        return (4.0f - 6.0f * a * a + 3.0f * a * a * a) * (1.0f / 6.0f);
+    if (a < 2.0f) {
+        const float t = 2.0f - a;
+        return t * t * t * (1.0f / 6.0f);
+    }
+    return 0.0f;
+}
+
+// Stencil of order P along one axis: first (unwrapped) node index and P weights.
+template <int P>
+__device__ __forceinline__ int stencil(float coord, float inv_h, int mesh, float* w)
 {
     const float raw = coord * inv_h;
     const float m = static_cast<float>(mesh);
-    const float s = raw - floorf(raw / m) * m;
-    const float fl = floorf(s);
-    int a = static_cast<int>(fl);
-    a = a >= mesh ? a - mesh : (a < 0 ? a + mesh : a);
-    i0 = a;
-    i1 = a + 1 == mesh ? 0 : a + 1;
-    w1 = s - fl;
-    w0 = 1.0f - w1;
+    const float s = raw - floorf(raw / m) * m;  // [0, M]
+    if (P == 2) {
+        const float fl = floorf(s);
+        const float f = s - fl;
+        w[0] = 1.0f - f;
+        w[1] = f;
+        return static_cast<int>(fl);
+    } else if (P == 3) {
+        const float c = floorf(s + 0.5f);
+        w[0] = tsc_w(s - (c - 1.0f));
+        w[1] = tsc_w(s - c);
+        w[2] = tsc_w(s - (c + 1.0f));
+        return static_cast<int>(c) - 1;
+    } else {
+        const float fl = floorf(s);
+        w[0] = pcs_w(s - (fl - 1.0f));
+        w[1] = pcs_w(s - fl);
+        w[2] = pcs_w(s - (fl + 1.0f));
+        w[3] = pcs_w(s - (fl + 2.0f));
+        return static_cast<int>(fl) - 1;
+    }
 }
 
-__global__ void __launch_bounds__(kThreads) k_deposit(const float4* __restrict__ pos4, int n,
-                                                       int mesh, float inv_h, float inv_h3,
-                                                       float* __restrict__ rho)
+__device__ __forceinline__ int wrapm(int i, int m)
 {
-    for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+    i %= m;
+    return i < 0 ? i + m : i;
+}
+
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __restrict__ pos4, int n,
+                                                             int chunk, int mesh, float inv_h,
+                                                             float inv_h3, float* __restrict__ rho)
+{
+    __shared__ float tile[kTileCells];
+    __shared__ int s_lo[3], s_hi[3];
+    const int base = blockIdx.x * chunk;
+    const int end = min(base + chunk, n);
+    if (threadIdx.x < 3) {
+        s_lo[threadIdx.x] = 1 << 30;
+        s_hi[threadIdx.x] = -(1 << 30);
+    }
+    __syncthreads();
+    int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
+    for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
-        int x0, x1, y0, y1, z0, z1;
-        float wx0, wx1, wy0, wy1, wz0, wz1;
-        cic_axis(p.x, inv_h, mesh, x0, x1, wx0, wx1);
-        cic_axis(p.y, inv_h, mesh, y0, y1, wy0, wy1);
-        cic_axis(p.z, inv_h, mesh, z0, z1, wz0, wz1);
+        float w[P];
+        const int b[3] = {stencil<P>(p.x, inv_h, mesh, w), stencil<P>(p.y, inv_h, mesh, w),
+                          stencil<P>(p.z, inv_h, mesh, w)};
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = min(lo[a], b[a]);
+            hi[a] = max(hi[a], b[a] + P - 1);
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        atomicMin(&s_lo[a], lo[a]);
+        atomicMax(&s_hi[a], hi[a]);
+    }
+    __syncthreads();
+    const int ex = s_hi[0] - s_lo[0] + 1, ey = s_hi[1] - s_lo[1] + 1, ez = s_hi[2] - s_lo[2] + 1;
+    const bool tiled = ex > 0 && ey > 0 && ez > 0 && static_cast<long long>(ex) * ey * ez <= kTileCells;
+    const int ox = s_lo[0], oy = s_lo[1], oz = s_lo[2];
+    if (tiled)
+        for (int c = threadIdx.x; c < ex * ey * ez; c += kThreads)
+            tile[c] = 0.0f;
+    __syncthreads();
+    const size_t M = static_cast<size_t>(mesh);
+    for (int i = base + threadIdx.x; i < end; i += kThreads) {
+        const float4 p = pos4[i];
+        float wx[P], wy[P], wz[P];
+        const int bx = stencil<P>(p.x, inv_h, mesh, wx);
+        const int by = stencil<P>(p.y, inv_h, mesh, wy);
+        const int bz = stencil<P>(p.z, inv_h, mesh, wz);
         const float m = p.w * inv_h3;
-        const size_t M = static_cast<size_t>(mesh);
-        const size_t r00 = (static_cast<size_t>(z0) * M + y0) * M, r01 = (static_cast<size_t>(z0) * M + y1) * M;
-        const size_t r10 = (static_cast<size_t>(z1) * M + y0) * M, r11 = (static_cast<size_t>(z1) * M + y1) * M;
-        atomicAdd(&rho[r00 + x0], m * wx0 * wy0 * wz0);
-        atomicAdd(&rho[r00 + x1], m * wx1 * wy0 * wz0);
-        atomicAdd(&rho[r01 + x0], m * wx0 * wy1 * wz0);
-        atomicAdd(&rho[r01 + x1], m * wx1 * wy1 * wz0);
-        atomicAdd(&rho[r10 + x0], m * wx0 * wy0 * wz1);
-        atomicAdd(&rho[r10 + x1], m * wx1 * wy0 * wz1);
-        atomicAdd(&rho[r11 + x0], m * wx0 * wy1 * wz1);
-        atomicAdd(&rho[r11 + x1], m * wx1 * wy1 * wz1);
+#pragma unroll
+        for (int c = 0; c < P; ++c)
+#pragma unroll
+            for (int b = 0; b < P; ++b) {
+                const float wzy = m * wz[c] * wy[b];
+#pragma unroll
+                for (int a = 0; a < P; ++a) {
+                    const float v = wzy * wx[a];
+                    if (tiled) {
+                        atomicAdd(&tile[((bz + c - oz) * ey + (by + b - oy)) * ex + (bx + a - ox)], v);
+                    } else {
+                        const size_t g = (static_cast<size_t>(wrapm(bz + c, mesh)) * M + wrapm(by + b, mesh)) * M +
+                                         wrapm(bx + a, mesh);
+                        atomicAdd(&rho[g], v);
+                    }
+                }
+            }
+    }
+    if (!tiled)
+        return;
+    __syncthreads();
+    for (int c = threadIdx.x; c < ex * ey * ez; c += kThreads) {
+        const float v = tile[c];
+        if (v != 0.0f) {
+            const int x = c % ex, y = (c / ex) % ey, z = c / (ex * ey);
+            const size_t g = (static_cast<size_t>(wrapm(oz + z, mesh)) * M + wrapm(oy + y, mesh)) * M +
+                             wrapm(ox + x, mesh);
+            atomicAdd(&rho[g], v);
+        }
     }
 }
 
 __device__ __forceinline__ double sinc_d(double v) { return fabs(v) < 1.0e-5 ? 1.0 : sin(v) / v; }
 
-// Green x deconvolution x 1/M^3, once per plan (depends only on mesh, box, r_s).
-__global__ void k_green_table(int mesh, double box, double rsplit, double* green)
+// Green x window deconvolution x 1/M^3, once per plan.
+__global__ void k_green_table(int mesh, double box, double rsplit, int order, double floor_w,
+                              double* green)
 {
     const int hx = mesh / 2 + 1;
     const size_t total = static_cast<size_t>(mesh) * mesh * hx;
@@ -97,13 +209,12 @@ __global__ void k_green_table(int mesh, double box, double rsplit, double* green
             green[idx] = 0.0;
             continue;
         }
-        double wx = sinc_d(0.5 * kx * h), wy = sinc_d(0.5 * ky * h), wz = sinc_d(0.5 * kz * h);
-        wx = wx * wx * wx * wx;
-        wy = wy * wy * wy * wy;
-        wz = wz * wz * wz * wz;
-        double W = wx * wy * wz;
-        if (W < 0.08)
-            W = 0.08;
+        const double s3 = sinc_d(0.5 * kx * h) * sinc_d(0.5 * ky * h) * sinc_d(0.5 * kz * h);
+        double W = 1.0;
+        for (int i = 0; i < 2 * order; ++i)
+            W *= s3;
+        if (W < floor_w)
+            W = floor_w;
         green[idx] = 4.0 * 3.14159265358979323846 * exp(-k2 * rsplit * rsplit) / (k2 * W) * norm;
     }
 }
@@ -122,51 +233,104 @@ __global__ void __launch_bounds__(kThreads) k_apply_green(cufftComplex* __restri
     }
 }
 
-// Interpolate the centred-difference gradient of phi with the CIC stencil.
-__global__ void __launch_bounds__(kThreads) k_interp_gradient(const float4* __restrict__ pos4,
-                                                               int n, int mesh, float inv_h,
-                                                               const float* __restrict__ phi,
-                                                               float* __restrict__ ax,
-                                                               float* __restrict__ ay,
-                                                               float* __restrict__ az)
+// Fused Green x spectral gradient: F_a = i k_a G rho_k for a = x, y, z (Nyquist derivative
+// terms set to zero).
+__global__ void __launch_bounds__(kThreads) k_green_gradient(const cufftComplex* __restrict__ spec,
+                                                              const double* __restrict__ green,
+                                                              int mesh, double box,
+                                                              cufftComplex* __restrict__ out3)
 {
-    const float half_inv_h = 0.5f * inv_h;
+    const int hx = mesh / 2 + 1;
+    const size_t total = static_cast<size_t>(mesh) * mesh * hx;
+    const float ks = static_cast<float>(2.0 * 3.14159265358979323846 / box);
+    for (size_t i = blockIdx.x * static_cast<size_t>(kThreads) + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * kThreads) {
+        const int x = static_cast<int>(i % hx);
+        const size_t pl = i / hx;
+        const int y = static_cast<int>(pl % mesh);
+        const int z = static_cast<int>(pl / mesh);
+        const int sx = x == mesh / 2 ? 0 : x;
+        const int sy = y == mesh / 2 ? 0 : (y < mesh / 2 ? y : y - mesh);
+        const int sz = z == mesh / 2 ? 0 : (z < mesh / 2 ? z : z - mesh);
+        const float g = static_cast<float>(green[i]);
+        const cufftComplex c = spec[i];
+        const float pr = c.x * g, pi = c.y * g;
+        const float k[3] = {sx * ks, sy * ks, sz * ks};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            cufftComplex o;
+            o.x = -k[a] * pi;  // i k (pr + i pi) = -k pi + i k pr
+            o.y = k[a] * pr;
+            out3[a * total + i] = o;
+        }
+    }
+}
+
+// Centred-difference gradient of phi into the interleaved force mesh (reference mode).
+__global__ void __launch_bounds__(kThreads) k_fd_gradient(const float* __restrict__ phi, int mesh,
+                                                           float half_inv_h, float4* __restrict__ force)
+{
+    const size_t M = static_cast<size_t>(mesh), total = M * M * M;
+    for (size_t i = blockIdx.x * static_cast<size_t>(kThreads) + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * kThreads) {
+        const int x = static_cast<int>(i % M), y = static_cast<int>((i / M) % M), z = static_cast<int>(i / (M * M));
+        const int xp = x + 1 == mesh ? 0 : x + 1, xm = x == 0 ? mesh - 1 : x - 1;
+        const int yp = y + 1 == mesh ? 0 : y + 1, ym = y == 0 ? mesh - 1 : y - 1;
+        const int zp = z + 1 == mesh ? 0 : z + 1, zm = z == 0 ? mesh - 1 : z - 1;
+        const size_t row = (static_cast<size_t>(z) * M + y) * M;
+        const float gx = (phi[row + xp] - phi[row + xm]) * half_inv_h;
+        const float gy = (phi[(static_cast<size_t>(z) * M + yp) * M + x] - phi[(static_cast<size_t>(z) * M + ym) * M + x]) * half_inv_h;
+        const float gz = (phi[(static_cast<size_t>(zp) * M + y) * M + x] - phi[(static_cast<size_t>(zm) * M + y) * M + x]) * half_inv_h;
+        force[i] = make_float4(gx, gy, gz, 0.0f);
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_pack_force(const float* __restrict__ f3, size_t total,
+                                                          float4* __restrict__ force)
+{
+    for (size_t i = blockIdx.x * static_cast<size_t>(kThreads) + threadIdx.x; i < total;
+         i += static_cast<size_t>(gridDim.x) * kThreads)
+        force[i] = make_float4(f3[i], f3[total + i], f3[2 * total + i], 0.0f);
+}
+
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ pos4, int n, int mesh,
+                                                      float inv_h, const float4* __restrict__ force,
+                                                      float* __restrict__ ax, float* __restrict__ ay,
+                                                      float* __restrict__ az)
+{
     const size_t M = static_cast<size_t>(mesh);
     for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
         const float4 p = pos4[i];
-        int xs[2], ys[2], zs[2];
-        float wx[2], wy[2], wz[2];
-        cic_axis(p.x, inv_h, mesh, xs[0], xs[1], wx[0], wx[1]);
-        cic_axis(p.y, inv_h, mesh, ys[0], ys[1], wy[0], wy[1]);
-        cic_axis(p.z, inv_h, mesh, zs[0], zs[1], wz[0], wz[1]);
-        const int xm = xs[0] == 0 ? mesh - 1 : xs[0] - 1, xp = xs[1] + 1 == mesh ? 0 : xs[1] + 1;
-        const int ym = ys[0] == 0 ? mesh - 1 : ys[0] - 1, yp = ys[1] + 1 == mesh ? 0 : ys[1] + 1;
-        const int zm = zs[0] == 0 ? mesh - 1 : zs[0] - 1, zp = zs[1] + 1 == mesh ? 0 : zs[1] + 1;
-        const int xa[4] = {xm, xs[0], xs[1], xp};
-        const int ya[4] = {ym, ys[0], ys[1], yp};
-        const int za[4] = {zm, zs[0], zs[1], zp};
+        float wx[P], wy[P], wz[P];
+        const int bx = stencil<P>(p.x, inv_h, mesh, wx);
+        const int by = stencil<P>(p.y, inv_h, mesh, wy);
+        const int bz = stencil<P>(p.z, inv_h, mesh, wz);
+        int xs[P];
+#pragma unroll
+        for (int a = 0; a < P; ++a)
+            xs[a] = wrapm(bx + a, mesh);
         float gx = 0.0f, gy = 0.0f, gz = 0.0f;
 #pragma unroll
-        for (int c = 0; c < 2; ++c)
+        for (int c = 0; c < P; ++c) {
+            const size_t zrow = static_cast<size_t>(wrapm(bz + c, mesh)) * M;
 #pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                const size_t row = (static_cast<size_t>(za[c + 1]) * M + ya[b + 1]) * M;
+            for (int b = 0; b < P; ++b) {
+                const size_t row = (zrow + wrapm(by + b, mesh)) * M;
+                const float wzy = wz[c] * wy[b];
 #pragma unroll
-                for (int a = 0; a < 2; ++a) {
-                    const float w = wx[a] * wy[b] * wz[c];
-                    const float dxp = __ldg(&phi[row + xa[a + 2]]) - __ldg(&phi[row + xa[a]]);
-                    const float dyp = __ldg(&phi[(static_cast<size_t>(za[c + 1]) * M + ya[b + 2]) * M + xa[a + 1]]) -
-                                      __ldg(&phi[(static_cast<size_t>(za[c + 1]) * M + ya[b]) * M + xa[a + 1]]);
-                    const float dzp = __ldg(&phi[(static_cast<size_t>(za[c + 2]) * M + ya[b + 1]) * M + xa[a + 1]]) -
-                                      __ldg(&phi[(static_cast<size_t>(za[c]) * M + ya[b + 1]) * M + xa[a + 1]]);
-                    gx = fmaf(w, dxp, gx);
-                    gy = fmaf(w, dyp, gy);
-                    gz = fmaf(w, dzp, gz);
+                for (int a = 0; a < P; ++a) {
+                    const float4 f = __ldg(&force[row + xs[a]]);
+                    const float w = wzy * wx[a];
+                    gx = fmaf(w, f.x, gx);
+                    gy = fmaf(w, f.y, gy);
+                    gz = fmaf(w, f.z, gz);
                 }
             }
-        ax[i] = gx * half_inv_h;
-        ay[i] = gy * half_inv_h;
-        az[i] = gz * half_inv_h;
+        }
+        ax[i] = gx;
+        ay[i] = gy;
+        az[i] = gz;
     }
 }
 
@@ -180,18 +344,27 @@ int sm_count()
 
 } // namespace
 
-PmPlan* pm_create(int mesh, double box, double rsplit, cudaStream_t s, int* cuda_err)
+PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, double window_floor,
+                  cudaStream_t s, int* cuda_err)
 {
     PmPlan* p = new PmPlan();
     p->mesh = mesh;
     p->box = box;
     p->rsplit = rsplit;
+    p->order = order < 2 ? 2 : (order > 4 ? 4 : order);
+    p->gradient = gradient ? 1 : 0;
+    p->floor = window_floor;
     const size_t cells = static_cast<size_t>(mesh) * mesh * mesh;
     const size_t half = static_cast<size_t>(mesh) * mesh * (mesh / 2 + 1);
     *cuda_err = 0;
-    if (cudaMalloc(&p->rho, cells * sizeof(float)) != cudaSuccess ||
-        cudaMalloc(&p->spec, half * sizeof(cufftComplex)) != cudaSuccess ||
-        cudaMalloc(&p->green, half * sizeof(double)) != cudaSuccess) {
+    bool ok = cudaMalloc(&p->rho, cells * sizeof(float)) == cudaSuccess &&
+              cudaMalloc(&p->spec, half * sizeof(cufftComplex)) == cudaSuccess &&
+              cudaMalloc(&p->green, half * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&p->force, cells * sizeof(float4)) == cudaSuccess;
+    if (ok && p->gradient)
+        ok = cudaMalloc(&p->spec3, 3 * half * sizeof(cufftComplex)) == cudaSuccess &&
+             cudaMalloc(&p->field3, 3 * cells * sizeof(float)) == cudaSuccess;
+    if (!ok) {
         *cuda_err = 1;
         pm_destroy(p);
         return nullptr;
@@ -207,9 +380,10 @@ PmPlan* pm_create(int mesh, double box, double rsplit, cudaStream_t s, int* cuda
     size_t ws1 = 0, ws2 = 0;
     cufftGetSize(p->r2c, &ws1);
     cufftGetSize(p->c2r, &ws2);
-    p->bytes = cells * sizeof(float) + half * (sizeof(cufftComplex) + sizeof(double)) + ws1 + ws2;
+    p->bytes = cells * (sizeof(float) + sizeof(float4)) + half * (sizeof(cufftComplex) + sizeof(double)) +
+               (p->gradient ? 3 * (half * sizeof(cufftComplex) + cells * sizeof(float)) : 0) + ws1 + ws2;
     count_launch();
-    k_green_table<<<sm_count() * 4, 256, 0, s>>>(mesh, box, rsplit, p->green);
+    k_green_table<<<sm_count() * 4, 256, 0, s>>>(mesh, box, rsplit, p->order, window_floor, p->green);
     return p;
 }
 
@@ -223,12 +397,16 @@ void pm_destroy(PmPlan* p)
         cufftDestroy(p->c2r);
     cudaFree(p->rho);
     cudaFree(p->spec);
+    cudaFree(p->spec3);
+    cudaFree(p->field3);
+    cudaFree(p->force);
     cudaFree(p->green);
     delete p;
 }
 
 size_t pm_bytes(const PmPlan* p) { return p ? p->bytes : 0; }
 float* pm_mesh(PmPlan* p) { return p->rho; }
+const float4* pm_force_mesh(PmPlan* p) { return p->force; }
 
 void pm_deposit(PmPlan* p, const float4* pos4, int n, cudaStream_t s)
 {
@@ -237,24 +415,57 @@ void pm_deposit(PmPlan* p, const float4* pos4, int n, cudaStream_t s)
     const double h = p->box / M;
     const float inv_h = static_cast<float>(1.0 / h);
     const float inv_h3 = static_cast<float>(1.0 / (h * h * h));
-    const int sms = sm_count();
     cudaMemsetAsync(p->rho, 0, cells * sizeof(float), s);
-    int b = (n + kThreads - 1) / kThreads;
-    b = b < sms * 8 ? b : sms * 8;
+    const int chunk = pm_deposit_chunk(p, n);
+    const int b = (n + chunk - 1) / chunk;
     count_launch();
-    k_deposit<<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, inv_h3, p->rho);
+    if (p->order == 2)
+        k_deposit_tiled<2><<<b, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, inv_h3, p->rho);
+    else if (p->order == 3)
+        k_deposit_tiled<3><<<b, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, inv_h3, p->rho);
+    else
+        k_deposit_tiled<4><<<b, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, inv_h3, p->rho);
+}
+
+int pm_deposit_chunk(const PmPlan* p, int n)
+{
+    // A chunk of c Morton-consecutive particles spans about c / (n / M^3) cells of a roughly
+    // uniform distribution; keep (cbrt(cells) + p)^3 within the tile with margin.
+    const double cells_per_particle = static_cast<double>(p->mesh) * p->mesh * p->mesh / (n > 0 ? n : 1);
+    int chunk = 4096;
+    while (chunk > 128) {
+        const double side = std::cbrt(chunk * cells_per_particle) + p->order + 1.0;
+        if (side * side * side <= 0.6 * kTileCells)
+            break;
+        chunk >>= 1;
+    }
+    return chunk;
 }
 
 int pm_solve(PmPlan* p, cudaStream_t s)
 {
     const int M = p->mesh;
     const size_t half = static_cast<size_t>(M) * M * (M / 2 + 1);
+    const size_t cells = static_cast<size_t>(M) * M * M;
+    const int sms = sm_count();
     if (cufftExecR2C(p->r2c, p->rho, p->spec) != CUFFT_SUCCESS)
         return 1;
-    count_launch();
-    k_apply_green<<<sm_count() * 4, kThreads, 0, s>>>(p->spec, p->green, half);
-    if (cufftExecC2R(p->c2r, p->spec, p->rho) != CUFFT_SUCCESS)
-        return 2;
+    if (p->gradient) {
+        count_launch();
+        k_green_gradient<<<sms * 4, kThreads, 0, s>>>(p->spec, p->green, M, p->box, p->spec3);
+        for (int a = 0; a < 3; ++a)
+            if (cufftExecC2R(p->c2r, p->spec3 + a * half, p->field3 + a * cells) != CUFFT_SUCCESS)
+                return 2;
+        count_launch();
+        k_pack_force<<<sms * 4, kThreads, 0, s>>>(p->field3, cells, p->force);
+    } else {
+        count_launch();
+        k_apply_green<<<sms * 4, kThreads, 0, s>>>(p->spec, p->green, half);
+        if (cufftExecC2R(p->c2r, p->spec, p->rho) != CUFFT_SUCCESS)
+            return 2;
+        count_launch();
+        k_fd_gradient<<<sms * 4, kThreads, 0, s>>>(p->rho, M, static_cast<float>(0.5 * M / p->box), p->force);
+    }
     return 0;
 }
 
@@ -262,12 +473,16 @@ void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float
                cudaStream_t s)
 {
     const int M = p->mesh;
-    const float inv_h = static_cast<float>(1.0 / (p->box / M));
-    const int sms = sm_count();
+    const float inv_h = static_cast<float>(M / p->box);
     int b = (n + kThreads - 1) / kThreads;
-    b = b < sms * 8 ? b : sms * 8;
+    b = b < sm_count() * 8 ? b : sm_count() * 8;
     count_launch();
-    k_interp_gradient<<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->rho, ax, ay, az);
+    if (p->order == 2)
+        k_interp<2><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->force, ax, ay, az);
+    else if (p->order == 3)
+        k_interp<3><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->force, ax, ay, az);
+    else
+        k_interp<4><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->force, ax, ay, az);
 }
 
 int pm_forces(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float* az,

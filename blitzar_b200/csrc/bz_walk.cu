@@ -445,7 +445,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                         e2 = __fadd_rn(e2, __fmul_rn(e, e));
                         l = fmaxf(l, __fsub_rn(bmax[a], bmin[a]));
                     }
-                    accept = __fmul_rn(l, l) < __fmul_rn(p.theta2, e2);
+                    // The split kernel varies on the scale r_s, so its expansion error depends on
+                    // the node size itself, not only on l/d: nodes at least max_node_size large
+                    // are never accepted.
+                    accept = __fmul_rn(l, l) < __fmul_rn(p.theta2, e2) &&
+                             (p.max_node_size <= 0.0f || l < p.max_node_size);
                     if (!accept) {
                         if (info < 0)
                             leaf = true;

@@ -65,6 +65,12 @@ typedef struct bz_config {
     int32_t treepm_grid_size;      /* treepm_grid_size: PM mesh cells per side */
     float treepm_r_split_cells;    /* Gaussian split scale r_s in mesh cells */
     float treepm_r_cut_factor;     /* short-range cutoff r_cut = factor * r_s */
+    int32_t treepm_assignment;     /* treepm_assignment: 0 cic, 1 tsc, 2 pcs */
+    int32_t treepm_gradient;       /* 0 centred differences of the potential (reference),
+                                      1 spectral i k gradient fused with the Green's function */
+    float treepm_window_floor;     /* lower bound of the deconvolution window (reference 0.08) */
+    float treepm_node_size_factor; /* short range: tree nodes at least this many r_s across are
+                                      never accepted as multipoles (0 = no cap) */
     double box_length;             /* periodic box length (TreePM); 0 = open boundaries */
     int32_t key_mode;              /* bz_key_mode */
     int32_t device;                /* CUDA device ordinal */
@@ -149,8 +155,9 @@ bz_status bz_phase_times(bz_handle* h, float* ms, int n);
 bz_status bz_force_errors(bz_handle* h, int32_t nsample, uint64_t seed, float* errs,
                           int32_t* idx, double* median, double* p99);
 
-/* Debug access to the PM mesh of the last force evaluation: which = 0 density after the
- * deposit, 1 potential after the solve.  out holds grid^3 floats, index (z*M + y)*M + x. */
+/* Debug access to the PM mesh of the current state: which = 0 density after the deposit,
+ * 1 potential after the solve (centred-difference mode only), 2/3/4 the x/y/z force mesh.
+ * out holds grid^3 floats, index (z*M + y)*M + x. */
 bz_status bz_pm_mesh(bz_handle* h, int which, float* out);
 
 /* Kernel launches of this library enqueued so far (cuFFT's own kernels excluded), and the

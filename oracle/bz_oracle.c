@@ -822,7 +822,9 @@ static void walk_node(walk_ctx* w, int32_t k)
         e2 = e2 + rn_mul(e, e);
         l = fmaxf_(l, bmax[a] - bmin[a]);
     }
-    const int accept = rn_mul(l, l) < rn_mul(p->theta2, e2);
+    /* split kernel: its multipole expansion is governed by the node size relative to r_s as
+     * well as by l/d, so nodes larger than max_node_size are never accepted */
+    const int accept = rn_mul(l, l) < rn_mul(p->theta2, e2) && (p->max_node_size <= 0.0f || l < p->max_node_size);
     if (accept) {
         w->pn++;
         const double m = mono[3];
@@ -1122,44 +1124,79 @@ static inline int wrapi(int v, int m)
     return w < 0 ? w + m : w;
 }
 
-/* CIC stencil (TpmAssignment.inl:104-117): lower = floor(s), weights 1-f, f, periodic. */
-static void cic_stencil(double coord01, double inv_cell, int mesh, int idx[2], double w[2])
+/* Assignment stencil of order p (2 CIC, 3 TSC, 4 PCS) along one axis: first node index
+ * (wrapped) and p weights.  CIC and TSC are the reference's stencils
+ * (TpmAssignment.inl:64-117); PCS uses the full support floor(s)-1 .. floor(s)+2 (the
+ * reference starts at floor(s+0.5)-1, which drops a node when frac(s) >= 0.5). */
+static double tsc_w(double d)
+{
+    const double a = fabs(d);
+    if (a < 0.5)
+        return 0.75 - a * a;
+    if (a < 1.5)
+        return 0.5 * (1.5 - a) * (1.5 - a);
+    return 0.0;
+}
+static double pcs_w(double d)
+{
+    const double a = fabs(d);
+    if (a < 1.0)
+        return (4.0 - 6.0 * a * a + 3.0 * a * a * a) / 6.0;
+    if (a < 2.0)
+        return (2.0 - a) * (2.0 - a) * (2.0 - a) / 6.0;
+    return 0.0;
+}
+static void stencil_p(double coord01, double inv_cell, int mesh, int order, int idx[4], double w[4])
 {
     const double raw = coord01 * inv_cell;
     const double s = raw - floor(raw / (double)mesh) * (double)mesh;
-    const double fl = floor(s);
-    idx[0] = wrapi((int)fl, mesh);
-    idx[1] = wrapi((int)fl + 1, mesh);
-    const double f = s - fl;
-    w[0] = 1.0 - f;
-    w[1] = f;
+    if (order == 2) {
+        const double fl = floor(s);
+        idx[0] = wrapi((int)fl, mesh);
+        idx[1] = wrapi((int)fl + 1, mesh);
+        w[1] = s - fl;
+        w[0] = 1.0 - w[1];
+    } else if (order == 3) {
+        const double c = floor(s + 0.5);
+        for (int k = 0; k < 3; ++k) {
+            idx[k] = wrapi((int)c - 1 + k, mesh);
+            w[k] = tsc_w(s - (c - 1.0 + k));
+        }
+    } else {
+        const double fl = floor(s);
+        for (int k = 0; k < 4; ++k) {
+            idx[k] = wrapi((int)fl - 1 + k, mesh);
+            w[k] = pcs_w(s - (fl - 1.0 + k));
+        }
+    }
 }
 
 static inline double sinc(double v) { return fabs(v) < 1.0e-5 ? 1.0 : sin(v) / v; }
 
-int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rsplit,
-                   double* acc3, double* density, double* phi)
+/* Periodic PM accelerations.  order: 2/3/4; gradient: 0 centred differences of the potential
+ * (TpmField.inl:48-89), 1 spectral i k (Nyquist derivative terms zero); floor_w: lower bound
+ * of the deconvolution window.  density/phi (optional) receive the deposited density and
+ * (centred-difference mode) the potential. */
+int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rsplit, int order,
+                   int gradient, double floor_w, double* acc3, double* density, double* phi)
 {
     const int64_t M = mesh, cells = M * M * M;
     const double h = box / (double)mesh, inv = 1.0 / h;
     double* rho = (double*)calloc((size_t)cells, sizeof(double));
-    /* deposit (TpmAssignment.inl:160-199) */
     for (int64_t i = 0; i < n; ++i) {
-        int ix[2], iy[2], iz[2];
-        double wx[2], wy[2], wz[2];
-        cic_stencil(pos4[4 * i], inv, mesh, ix, wx);
-        cic_stencil(pos4[4 * i + 1], inv, mesh, iy, wy);
-        cic_stencil(pos4[4 * i + 2], inv, mesh, iz, wz);
+        int ix[4], iy[4], iz[4];
+        double wx[4], wy[4], wz[4];
+        stencil_p(pos4[4 * i], inv, mesh, order, ix, wx);
+        stencil_p(pos4[4 * i + 1], inv, mesh, order, iy, wy);
+        stencil_p(pos4[4 * i + 2], inv, mesh, order, iz, wz);
         const double sc = (double)pos4[4 * i + 3] / (h * h * h);
-        for (int c = 0; c < 2; ++c)
-            for (int b = 0; b < 2; ++b)
-                for (int a = 0; a < 2; ++a)
+        for (int c = 0; c < order; ++c)
+            for (int b = 0; b < order; ++b)
+                for (int a = 0; a < order; ++a)
                     rho[(iz[c] * M + iy[b]) * M + ix[a]] += sc * wx[a] * wy[b] * wz[c];
     }
     if (density)
         memcpy(density, rho, sizeof(double) * (size_t)cells);
-    /* Green's function with Gaussian split and CIC window deconvolution (TpmField.inl:6-47):
-     * phi_k = 4 pi e^{-k^2 r_s^2} rho_k / (k^2 max(W, 0.08)), W = prod sinc^4(k h / 2). */
     double* sp = (double*)malloc(sizeof(double) * 2 * (size_t)cells);
     for (int64_t c = 0; c < cells; ++c) {
         sp[2 * c] = rho[c];
@@ -1179,52 +1216,80 @@ int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rs
                     sp[2 * c] = sp[2 * c + 1] = 0.0;
                     continue;
                 }
-                const double g = 4.0 * M_PI * exp(-k2 * rsplit * rsplit);
-                double wx = sinc(0.5 * kx * h), wy = sinc(0.5 * ky * h), wz = sinc(0.5 * kz * h);
-                wx = wx * wx * wx * wx;
-                wy = wy * wy * wy * wy;
-                wz = wz * wz * wz * wz;
-                double W = wx * wy * wz;
-                if (W < 0.08)
-                    W = 0.08;
-                const double f = g / (k2 * W);
+                const double s3 = sinc(0.5 * kx * h) * sinc(0.5 * ky * h) * sinc(0.5 * kz * h);
+                double W = 1.0;
+                for (int i = 0; i < 2 * order; ++i)
+                    W *= s3;
+                if (W < floor_w)
+                    W = floor_w;
+                const double f = 4.0 * M_PI * exp(-k2 * rsplit * rsplit) / (k2 * W);
                 sp[2 * c] *= f;
                 sp[2 * c + 1] *= f;
             }
-    or_fft3d(sp, mesh, 1);
-    double* p = (double*)malloc(sizeof(double) * (size_t)cells);
-    for (int64_t c = 0; c < cells; ++c)
-        p[c] = sp[2 * c];
-    if (phi)
-        memcpy(phi, p, sizeof(double) * (size_t)cells);
-    /* centred difference (TpmField.inl:48-89) sampled with the CIC stencil
-     * (TpmAssignment.inl:120-158); acceleration = +gradient of this +4 pi potential. */
+    double* field[3] = {NULL, NULL, NULL};
+    for (int a = 0; a < 3; ++a)
+        field[a] = (double*)malloc(sizeof(double) * (size_t)cells);
+    if (gradient == 0) {
+        double* q = (double*)malloc(sizeof(double) * 2 * (size_t)cells);
+        memcpy(q, sp, sizeof(double) * 2 * (size_t)cells);
+        or_fft3d(q, mesh, 1);
+        double* p = (double*)malloc(sizeof(double) * (size_t)cells);
+        for (int64_t c = 0; c < cells; ++c)
+            p[c] = q[2 * c];
+        if (phi)
+            memcpy(phi, p, sizeof(double) * (size_t)cells);
+        for (int64_t Z = 0; Z < M; ++Z)
+            for (int64_t Y = 0; Y < M; ++Y)
+                for (int64_t X = 0; X < M; ++X) {
+                    const int64_t c = (Z * M + Y) * M + X;
+                    field[0][c] = (p[(Z * M + Y) * M + wrapi((int)X + 1, mesh)] - p[(Z * M + Y) * M + wrapi((int)X - 1, mesh)]) * 0.5 * inv;
+                    field[1][c] = (p[(Z * M + wrapi((int)Y + 1, mesh)) * M + X] - p[(Z * M + wrapi((int)Y - 1, mesh)) * M + X]) * 0.5 * inv;
+                    field[2][c] = (p[(wrapi((int)Z + 1, mesh) * M + Y) * M + X] - p[(wrapi((int)Z - 1, mesh) * M + Y) * M + X]) * 0.5 * inv;
+                }
+        free(q);
+        free(p);
+    } else {
+        double* q = (double*)malloc(sizeof(double) * 2 * (size_t)cells);
+        for (int a = 0; a < 3; ++a) {
+            for (int64_t z = 0; z < M; ++z)
+                for (int64_t y = 0; y < M; ++y)
+                    for (int64_t x = 0; x < M; ++x) {
+                        const int64_t idx3[3] = {x, y, z};
+                        const int64_t v = idx3[a];
+                        const int64_t sv = v == M / 2 ? 0 : (v < M / 2 ? v : v - M);
+                        const double k = sv * ks;
+                        const int64_t c = (z * M + y) * M + x;
+                        q[2 * c] = -k * sp[2 * c + 1];
+                        q[2 * c + 1] = k * sp[2 * c];
+                    }
+            or_fft3d(q, mesh, 1);
+            for (int64_t c = 0; c < cells; ++c)
+                field[a][c] = q[2 * c];
+        }
+        free(q);
+    }
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; ++i) {
-        int ix[2], iy[2], iz[2];
-        double wx[2], wy[2], wz[2];
-        cic_stencil(pos4[4 * i], inv, mesh, ix, wx);
-        cic_stencil(pos4[4 * i + 1], inv, mesh, iy, wy);
-        cic_stencil(pos4[4 * i + 2], inv, mesh, iz, wz);
-        double a[3] = {0, 0, 0};
-        for (int c = 0; c < 2; ++c)
-            for (int b = 0; b < 2; ++b)
-                for (int q = 0; q < 2; ++q) {
-                    const int X = ix[q], Y = iy[b], Z = iz[c];
-                    const double w = wx[q] * wy[b] * wz[c];
-                    const double gx = (p[(Z * M + Y) * M + wrapi(X + 1, mesh)] - p[(Z * M + Y) * M + wrapi(X - 1, mesh)]) * 0.5 * inv;
-                    const double gy = (p[(Z * M + wrapi(Y + 1, mesh)) * M + X] - p[(Z * M + wrapi(Y - 1, mesh)) * M + X]) * 0.5 * inv;
-                    const double gz = (p[(wrapi(Z + 1, mesh) * M + Y) * M + X] - p[(wrapi(Z - 1, mesh) * M + Y) * M + X]) * 0.5 * inv;
-                    a[0] += gx * w;
-                    a[1] += gy * w;
-                    a[2] += gz * w;
+        int ix[4], iy[4], iz[4];
+        double wx[4], wy[4], wz[4];
+        stencil_p(pos4[4 * i], inv, mesh, order, ix, wx);
+        stencil_p(pos4[4 * i + 1], inv, mesh, order, iy, wy);
+        stencil_p(pos4[4 * i + 2], inv, mesh, order, iz, wz);
+        double acc[3] = {0, 0, 0};
+        for (int c = 0; c < order; ++c)
+            for (int b = 0; b < order; ++b)
+                for (int q2 = 0; q2 < order; ++q2) {
+                    const int64_t cell = (iz[c] * M + iy[b]) * M + ix[q2];
+                    const double w = wx[q2] * wy[b] * wz[c];
+                    for (int a = 0; a < 3; ++a)
+                        acc[a] += w * field[a][cell];
                 }
-        acc3[3 * i] = a[0];
-        acc3[3 * i + 1] = a[1];
-        acc3[3 * i + 2] = a[2];
+        for (int a = 0; a < 3; ++a)
+            acc3[3 * i + a] = acc[a];
     }
+    for (int a = 0; a < 3; ++a)
+        free(field[a]);
     free(rho);
     free(sp);
-    free(p);
     return 0;
 }

@@ -56,6 +56,7 @@ typedef struct {
     float min_dist2; /* pairs with softened r^2 <= this are skipped */
     int quadrupole;  /* 1 = monopole + quadrupole for accepted nodes */
     int group;       /* targets per group (32) */
+    float max_node_size; /* > 0: nodes with extent >= this are never accepted */
 } or_walk_params;
 
 void or_walk(const float* pos4, int64_t n, const int32_t* start, const int32_t* count,
@@ -73,8 +74,8 @@ void or_ewald_f64(const float* pos4, int64_t n, const int64_t* targets, int64_t 
 
 /* ---- periodic particle-mesh leg ------------------------------------------------------- */
 void or_fft3d(double* re_im, int size, int inverse);
-int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rsplit,
-                   double* acc3, double* density, double* phi);
+int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rsplit, int order,
+                   int gradient, double floor_w, double* acc3, double* density, double* phi);
 
 /* ---- split kernel helpers ---------------------------------------------------------------- */
 double or_split_weight(double s, double rsplit);

@@ -29,7 +29,7 @@ _u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
 class WalkParams(C.Structure):
     _fields_ = [("theta2", C.c_float), ("eps2", C.c_float), ("rcut2", C.c_float),
                 ("box", C.c_float), ("rsplit", C.c_float), ("min_dist2", C.c_float),
-                ("quadrupole", C.c_int), ("group", C.c_int)]
+                ("quadrupole", C.c_int), ("group", C.c_int), ("max_node_size", C.c_float)]
 
 
 def build(ref: bool = False) -> None:
@@ -69,8 +69,8 @@ def lib():
         L.or_ewald_f64.argtypes = [_f32p, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
                                    C.c_double, C.c_double, C.c_int, _f64p]
         L.or_fft3d.argtypes = [_f64p, C.c_int, C.c_int]
-        L.or_pm_periodic.argtypes = [_f32p, C.c_int64, C.c_int, C.c_double, C.c_double, _f64p,
-                                     C.c_void_p, C.c_void_p]
+        L.or_pm_periodic.argtypes = [_f32p, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int,
+                                     C.c_int, C.c_double, _f64p, C.c_void_p, C.c_void_p]
         L.or_split_weight.argtypes = [C.c_double, C.c_double]
         L.or_split_weight.restype = C.c_double
         _LIB = L
@@ -210,11 +210,11 @@ def build_tree(sorted_keys, sorted_pos4, leaf_cap=16, max_level=21):
 
 
 def walk(sorted_pos4, tree, theta=0.5, eps=0.01, rcut=0.0, box=0.0, rsplit=0.0,
-         min_dist2=1e-12, quadrupole=True, group=32, want_pot=False):
+         min_dist2=1e-12, quadrupole=True, group=32, want_pot=False, max_node_size=0.0):
     n = len(sorted_pos4)
     prm = WalkParams(np.float32(theta) * np.float32(theta), np.float32(eps) * np.float32(eps),
                      np.float32(rcut) * np.float32(rcut), box, rsplit, min_dist2,
-                     1 if quadrupole else 0, group)
+                     1 if quadrupole else 0, group, max_node_size)
     acc = np.zeros(3 * n, np.float64)
     pot = np.zeros(n, np.float64) if want_pot else None
     ng = (n + group - 1) // group
@@ -258,13 +258,18 @@ def ewald(pos4_, targets=None, eps=0.0, box=1.0, alpha=None, kmax=8):
     return acc.reshape(nt, 3)
 
 
-def pm_periodic(pos4_, mesh, box, rsplit, want_fields=False):
+ASSIGNMENT_ORDER = {"cic": 2, "tsc": 3, "pcs": 4}
+
+
+def pm_periodic(pos4_, mesh, box, rsplit, want_fields=False, assignment="cic", spectral=False,
+                window_floor=0.08):
     p = np.ascontiguousarray(pos4_, np.float32)
     acc = np.zeros(3 * len(p), np.float64)
     cells = mesh ** 3
     dens = np.zeros(cells, np.float64) if want_fields else None
     phi = np.zeros(cells, np.float64) if want_fields else None
-    lib().or_pm_periodic(p, len(p), mesh, box, rsplit, acc,
+    lib().or_pm_periodic(p, len(p), mesh, box, rsplit, ASSIGNMENT_ORDER[assignment],
+                         1 if spectral else 0, window_floor, acc,
                          None if dens is None else dens.ctypes.data,
                          None if phi is None else phi.ctypes.data)
     if want_fields:
