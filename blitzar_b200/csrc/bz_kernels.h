@@ -61,7 +61,7 @@ struct TreeArrays {
     int* lvl_count;    // [kMaxLevels+2]
     int* n_nodes;      // [1]
     uint32_t* ticket;  // [kMaxLevels+2]
-    unsigned long long* lookback;  // [cap/256 + kMaxLevels + 2]
+    unsigned long long* lookback;  // [tree_lookback_words(cap)]
     int* arrive;       // [cap] bottom-up arrival counters
     double* m64;       // [cap] FP64 mass
     double* s64;       // [3*cap] FP64 first moments
@@ -74,6 +74,7 @@ struct TreeArrays {
     float2* quadB;     // {qyz, qzz}
 };
 constexpr int kMaxLevels = 21;
+size_t tree_lookback_words(int cap);
 void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
                        int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s);
 
@@ -135,7 +136,7 @@ int pm_solve(PmPlan* p, cudaStream_t s);
 void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float* az,
                cudaStream_t s);
 float* pm_mesh(PmPlan* p);
-const float4* pm_force_mesh(PmPlan* p);
+const float4* pm_force_mesh(PmPlan* p);  // interleaved {ax, ay, az, 0}
 
 // ---------------------------------------------------------------- state (bz_state.cu)
 void launch_permute(const uint32_t* perm, int n, const double* const* src, double* const* dst,

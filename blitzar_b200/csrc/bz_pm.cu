@@ -8,7 +8,7 @@
 //   solve    : cuFFT R2C -> Green's function with Gaussian split, window deconvolution and 1/M^3
 //              (precomputed in FP64) -> either the potential (reference centred differences,
 //              then a gradient kernel) or, fused in the same k-space pass, the three spectral
-//              gradients i k phi_k -> cuFFT C2R -> interleaved float4 force mesh.
+//              gradients i k phi_k -> three cuFFT C2R -> interleaved float4 force mesh.
 //   interp   : the same order-p stencil gathers the force mesh at each particle.
 //
 // Formulas follow the reference CPU templates driven with a periodic grid
@@ -37,9 +37,9 @@ struct PmPlan {
     float* rho = nullptr;      // M^3: density, then potential (centred-difference mode)
     cufftComplex* spec = nullptr;     // M*M*(M/2+1)
     cufftComplex* spec3 = nullptr;    // 3 x M*M*(M/2+1) spectral gradients
-    float* field3 = nullptr;          // 3 x M^3 real gradients
-    float4* force = nullptr;          // M^3 interleaved force mesh
-    double* green = nullptr;          // M*M*(M/2+1)
+    float* field3 = nullptr;          // 3 x M^3 spectral gradient meshes
+    float4* force = nullptr;          // M^3 interleaved force mesh {ax, ay, az, 0}
+    float* green = nullptr;           // M*M*(M/2+1), computed in FP64
     cufftHandle r2c = 0, c2r = 0;
     size_t bytes = 0;
 };
@@ -173,13 +173,36 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
     if (!tiled)
         return;
     __syncthreads();
-    for (int c = threadIdx.x; c < ex * ey * ez; c += kThreads) {
-        const float v = tile[c];
-        if (v != 0.0f) {
-            const int x = c % ex, y = (c / ex) % ey, z = c / (ex * ey);
-            const size_t g = (static_cast<size_t>(wrapm(oz + z, mesh)) * M + wrapm(oy + y, mesh)) * M +
-                             wrapm(ox + x, mesh);
-            atomicAdd(&rho[g], v);
+    // Flush the tile row by row.  Where a row segment is contiguous in the mesh (no periodic
+    // wrap) and 16-byte aligned, four cells go in one vector atomic (red.global.add.v4.f32).
+    const int quads = (ex + 3 + 3) / 4;  // enough 4-cell groups to cover a row from any alignment
+    for (int r = threadIdx.x; r < ey * ez * quads; r += kThreads) {
+        const int q = r % quads, row = r / quads;
+        const int y = row % ey, z = row / ey;
+        const size_t rowbase = (static_cast<size_t>(wrapm(oz + z, mesh)) * M + wrapm(oy + y, mesh)) * M;
+        // group q covers mesh x in [xa, xa + 4) with xa 4-aligned relative to the unwrapped origin
+        const int xa = ((ox >> 2) << 2) + 4 * q;
+        float v[4];
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int tx = xa + j - ox;
+            v[j] = (tx >= 0 && tx < ex) ? tile[(z * ey + y) * ex + tx] : 0.0f;
+            any = any || v[j] != 0.0f;
+        }
+        if (!any)
+            continue;
+        const int gx = wrapm(xa, mesh);
+        if (gx + 3 < mesh && (mesh & 3) == 0) {
+            float* dst = rho + rowbase + gx;
+            asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst), "f"(v[0]), "f"(v[1]),
+                         "f"(v[2]), "f"(v[3])
+                         : "memory");
+        } else {
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (v[j] != 0.0f)
+                    atomicAdd(&rho[rowbase + wrapm(xa + j, mesh)], v[j]);
         }
     }
 }
@@ -188,7 +211,7 @@ __device__ __forceinline__ double sinc_d(double v) { return fabs(v) < 1.0e-5 ? 1
 
 // Green x window deconvolution x 1/M^3, once per plan.
 __global__ void k_green_table(int mesh, double box, double rsplit, int order, double floor_w,
-                              double* green)
+                              float* green)
 {
     const int hx = mesh / 2 + 1;
     const size_t total = static_cast<size_t>(mesh) * mesh * hx;
@@ -206,7 +229,7 @@ __global__ void k_green_table(int mesh, double box, double rsplit, int order, do
         const double kx = x * ks, ky = sy * ks, kz = sz * ks;
         const double k2 = kx * kx + ky * ky + kz * kz;
         if (k2 <= 1.0e-12) {
-            green[idx] = 0.0;
+            green[idx] = 0.0f;
             continue;
         }
         const double s3 = sinc_d(0.5 * kx * h) * sinc_d(0.5 * ky * h) * sinc_d(0.5 * kz * h);
@@ -215,17 +238,17 @@ __global__ void k_green_table(int mesh, double box, double rsplit, int order, do
             W *= s3;
         if (W < floor_w)
             W = floor_w;
-        green[idx] = 4.0 * 3.14159265358979323846 * exp(-k2 * rsplit * rsplit) / (k2 * W) * norm;
+        green[idx] = static_cast<float>(4.0 * 3.14159265358979323846 * exp(-k2 * rsplit * rsplit) / (k2 * W) * norm);
     }
 }
 
 __global__ void __launch_bounds__(kThreads) k_apply_green(cufftComplex* __restrict__ spec,
-                                                           const double* __restrict__ green,
+                                                           const float* __restrict__ green,
                                                            size_t total)
 {
     for (size_t i = blockIdx.x * static_cast<size_t>(kThreads) + threadIdx.x; i < total;
          i += static_cast<size_t>(gridDim.x) * kThreads) {
-        const float g = static_cast<float>(green[i]);
+        const float g = green[i];
         cufftComplex c = spec[i];
         c.x *= g;
         c.y *= g;
@@ -236,7 +259,7 @@ __global__ void __launch_bounds__(kThreads) k_apply_green(cufftComplex* __restri
 // Fused Green x spectral gradient: F_a = i k_a G rho_k for a = x, y, z (Nyquist derivative
 // terms set to zero).
 __global__ void __launch_bounds__(kThreads) k_green_gradient(const cufftComplex* __restrict__ spec,
-                                                              const double* __restrict__ green,
+                                                              const float* __restrict__ green,
                                                               int mesh, double box,
                                                               cufftComplex* __restrict__ out3)
 {
@@ -252,7 +275,7 @@ __global__ void __launch_bounds__(kThreads) k_green_gradient(const cufftComplex*
         const int sx = x == mesh / 2 ? 0 : x;
         const int sy = y == mesh / 2 ? 0 : (y < mesh / 2 ? y : y - mesh);
         const int sz = z == mesh / 2 ? 0 : (z < mesh / 2 ? z : z - mesh);
-        const float g = static_cast<float>(green[i]);
+        const float g = green[i];
         const cufftComplex c = spec[i];
         const float pr = c.x * g, pi = c.y * g;
         const float k[3] = {sx * ks, sy * ks, sz * ks};
@@ -293,6 +316,9 @@ __global__ void __launch_bounds__(kThreads) k_pack_force(const float* __restrict
         force[i] = make_float4(f3[i], f3[total + i], f3[2 * total + i], 0.0f);
 }
 
+// Interpolation: the same order-p stencil gathers the interleaved force mesh at each
+// particle (Morton order keeps neighbouring threads on neighbouring cells, so the gathers hit
+// L1/L2).
 template <int P>
 __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ pos4, int n, int mesh,
                                                       float inv_h, const float4* __restrict__ force,
@@ -359,7 +385,7 @@ PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, 
     *cuda_err = 0;
     bool ok = cudaMalloc(&p->rho, cells * sizeof(float)) == cudaSuccess &&
               cudaMalloc(&p->spec, half * sizeof(cufftComplex)) == cudaSuccess &&
-              cudaMalloc(&p->green, half * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&p->green, half * sizeof(float)) == cudaSuccess &&
               cudaMalloc(&p->force, cells * sizeof(float4)) == cudaSuccess;
     if (ok && p->gradient)
         ok = cudaMalloc(&p->spec3, 3 * half * sizeof(cufftComplex)) == cudaSuccess &&
@@ -380,7 +406,7 @@ PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, 
     size_t ws1 = 0, ws2 = 0;
     cufftGetSize(p->r2c, &ws1);
     cufftGetSize(p->c2r, &ws2);
-    p->bytes = cells * (sizeof(float) + sizeof(float4)) + half * (sizeof(cufftComplex) + sizeof(double)) +
+    p->bytes = cells * (sizeof(float) + sizeof(float4)) + half * (sizeof(cufftComplex) + sizeof(float)) +
                (p->gradient ? 3 * (half * sizeof(cufftComplex) + cells * sizeof(float)) : 0) + ws1 + ws2;
     count_launch();
     k_green_table<<<sm_count() * 4, 256, 0, s>>>(mesh, box, rsplit, p->order, window_floor, p->green);
@@ -446,13 +472,13 @@ int pm_solve(PmPlan* p, cudaStream_t s)
 {
     const int M = p->mesh;
     const size_t half = static_cast<size_t>(M) * M * (M / 2 + 1);
-    const size_t cells = static_cast<size_t>(M) * M * M;
     const int sms = sm_count();
     if (cufftExecR2C(p->r2c, p->rho, p->spec) != CUFFT_SUCCESS)
         return 1;
     if (p->gradient) {
         count_launch();
         k_green_gradient<<<sms * 4, kThreads, 0, s>>>(p->spec, p->green, M, p->box, p->spec3);
+        const size_t cells = static_cast<size_t>(M) * M * M;
         for (int a = 0; a < 3; ++a)
             if (cufftExecC2R(p->c2r, p->spec3 + a * half, p->field3 + a * cells) != CUFFT_SUCCESS)
                 return 2;

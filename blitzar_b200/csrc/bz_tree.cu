@@ -67,11 +67,18 @@ __device__ __forceinline__ void vstore(unsigned long long* p, unsigned long long
 }
 
 // Split every node of level `l` with more than leaf_cap particles into its non-empty octant
-// cells.  Children of the level are appended in (parent, octant) order.
+// cells.  Children of the level are appended in (parent, octant) order.  On the top levels
+// (few, very large nodes) TPN = 8 threads serve one node: thread d (1..7) finds the first
+// particle whose digit is >= d, so the seven binary searches run side by side; deeper levels
+// use one thread per node.  Look-back tiles are indexed in units of kLookbackNodes nodes.
+constexpr int kLookbackNodes = kThreads / 8;
+
+template <int TPN>
 __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long long* __restrict__ keys,
                                                           int l, int leaf_cap, int max_level,
                                                           TreeArrays t, int* err)
 {
+    constexpr int kNodesPerTile = kThreads / TPN;
     __shared__ int s_tile;
     __shared__ int s_scan[kThreads];
     __shared__ int s_prefix;
@@ -80,10 +87,11 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
     const int cnt = min(t.lvl_count[l], t.cap - first);
     if (cnt <= 0)
         return;
-    const int ntiles = (cnt + kThreads - 1) / kThreads;
+    const int ntiles = (cnt + kNodesPerTile - 1) / kNodesPerTile;
     const int next_first = first + cnt;
-    unsigned long long* lb = t.lookback + (first / kThreads + l);
+    unsigned long long* lb = t.lookback + (first / kLookbackNodes + 2 * l);
     const int shift = 3 * (max_level - l - 1);
+    const int slot = threadIdx.x / TPN, sub = threadIdx.x % TPN, lane = threadIdx.x & 31;
     for (;;) {
         if (threadIdx.x == 0)
             s_tile = static_cast<int>(atomicAdd(&t.ticket[l], 1u));
@@ -92,25 +100,39 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
         __syncthreads();
         if (tile >= ntiles)
             break;
-        const int k = first + tile * kThreads + threadIdx.x;
-        int b[9];
-        int nch = 0;
+        const int k = first + tile * kNodesPerTile + slot;
+        int s0 = 0, c0 = 0;
         bool split = false;
+        int bsub = 0;
+        int b[9];
         if (k < next_first) {
-            const int s = t.start[k], c = t.count[k];
-            split = c > leaf_cap && l < max_level;
-            if (split) {
-                b[0] = s;
-                b[8] = s + c;
+            s0 = t.start[k];
+            c0 = t.count[k];
+            split = c0 > leaf_cap && l < max_level;
+            if (TPN == 8) {
+                if (split && sub > 0)
+                    bsub = lower_bound_digit(keys, s0, s0 + c0, shift, static_cast<unsigned>(sub));
+            } else if (split) {
+                b[0] = s0;
 #pragma unroll
                 for (int d = 1; d < 8; ++d)
-                    b[d] = lower_bound_digit(keys, b[d - 1], s + c, shift, static_cast<unsigned>(d));
-#pragma unroll
-                for (int d = 0; d < 8; ++d)
-                    nch += b[d + 1] > b[d] ? 1 : 0;
+                    b[d] = lower_bound_digit(keys, b[d - 1], s0 + c0, shift, static_cast<unsigned>(d));
             }
         }
-        // block exclusive scan of child counts
+        if (TPN == 8) {
+#pragma unroll
+            for (int d = 1; d < 8; ++d)
+                b[d] = __shfl_sync(kFullMask, bsub, (lane & ~7) + d);
+        }
+        b[0] = s0;
+        b[8] = s0 + c0;
+        int nch = 0;
+        if (split && sub == 0) {
+#pragma unroll
+            for (int d = 0; d < 8; ++d)
+                nch += b[d + 1] > b[d] ? 1 : 0;
+        }
+        // block exclusive scan of child counts (only the leader of each node contributes)
         s_scan[threadIdx.x] = nch;
         __syncthreads();
         for (int o = 1; o < kThreads; o <<= 1) {
@@ -157,22 +179,22 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
             }
         }
         __syncthreads();
-        if (k < next_first) {
-            int c0 = next_first + s_prefix + incl - nch;
-            if (split && c0 + nch > t.cap)
+        if (k < next_first && sub == 0) {
+            int c = next_first + s_prefix + incl - nch;
+            if (split && c + nch > t.cap)
                 nch = 0;  // capacity exceeded (error raised above): keep the node a leaf
-            t.child[k] = nch > 0 ? c0 : -1;
+            t.child[k] = nch > 0 ? c : -1;
             t.nchild[k] = nch;
             if (nch > 0) {
 #pragma unroll
                 for (int d = 0; d < 8; ++d) {
                     if (b[d + 1] > b[d]) {
-                        t.start[c0] = b[d];
-                        t.count[c0] = b[d + 1] - b[d];
-                        t.parent[c0] = k;
-                        t.level[c0] = l + 1;
-                        t.arrive[c0] = 0;
-                        ++c0;
+                        t.start[c] = b[d];
+                        t.count[c] = b[d + 1] - b[d];
+                        t.parent[c] = k;
+                        t.level[c] = l + 1;
+                        t.arrive[c] = 0;
+                        ++c;
                     }
                 }
             }
@@ -245,39 +267,50 @@ __device__ void leaf_moments(const float4* __restrict__ pos4, int k, TreeArrays&
 
 __device__ void internal_moments(int k, TreeArrays& t)
 {
-    const int c0 = t.child[k], c1 = c0 + t.nchild[k];
+    const int c0 = t.child[k], nc = t.nchild[k];
+    // Both passes are unrolled over the (at most 8) children with predication, so the loads of
+    // all children issue together and one climb step costs about one memory round trip; the
+    // sums still run in octant order.
     float mn[3] = {3.402823466e38f, 3.402823466e38f, 3.402823466e38f};
     float mx[3] = {-3.402823466e38f, -3.402823466e38f, -3.402823466e38f};
     double tm = 0.0, sx = 0.0, sy = 0.0, sz = 0.0;
-    for (int c = c0; c < c1; ++c) {
-        const float4 b0 = __ldcg(&t.box0[c]);
-        const float4 b1 = __ldcg(&t.box1[c]);
-        mn[0] = fminf(mn[0], b0.x);
-        mn[1] = fminf(mn[1], b0.y);
-        mn[2] = fminf(mn[2], b0.z);
-        mx[0] = fmaxf(mx[0], b1.x);
-        mx[1] = fmaxf(mx[1], b1.y);
-        mx[2] = fmaxf(mx[2], b1.z);
-        tm += __ldcg(&t.m64[c]);
-        sx += __ldcg(&t.s64[3 * c]);
-        sy += __ldcg(&t.s64[3 * c + 1]);
-        sz += __ldcg(&t.s64[3 * c + 2]);
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        if (j < nc) {
+            const int c = c0 + j;
+            const float4 b0 = __ldcg(&t.box0[c]);
+            const float4 b1 = __ldcg(&t.box1[c]);
+            mn[0] = fminf(mn[0], b0.x);
+            mn[1] = fminf(mn[1], b0.y);
+            mn[2] = fminf(mn[2], b0.z);
+            mx[0] = fmaxf(mx[0], b1.x);
+            mx[1] = fmaxf(mx[1], b1.y);
+            mx[2] = fmaxf(mx[2], b1.z);
+            tm += __ldcg(&t.m64[c]);
+            sx += __ldcg(&t.s64[3 * c]);
+            sy += __ldcg(&t.s64[3 * c + 1]);
+            sz += __ldcg(&t.s64[3 * c + 2]);
+        }
     }
     const double cx = tm > 0.0 ? sx / tm : 0.5 * ((double)mn[0] + (double)mx[0]);
     const double cy = tm > 0.0 ? sy / tm : 0.5 * ((double)mn[1] + (double)mx[1]);
     const double cz = tm > 0.0 ? sz / tm : 0.5 * ((double)mn[2] + (double)mx[2]);
     double q[6] = {0, 0, 0, 0, 0, 0};
-    for (int c = c0; c < c1; ++c) {
-        const double dx = __ldcg(&t.c64[3 * c]) - cx;
-        const double dy = __ldcg(&t.c64[3 * c + 1]) - cy;
-        const double dz = __ldcg(&t.c64[3 * c + 2]) - cz;
-        const double w = __ldcg(&t.m64[c]);
-        q[0] += __ldcg(&t.q64[6 * c]) + w * dx * dx;
-        q[1] += __ldcg(&t.q64[6 * c + 1]) + w * dx * dy;
-        q[2] += __ldcg(&t.q64[6 * c + 2]) + w * dx * dz;
-        q[3] += __ldcg(&t.q64[6 * c + 3]) + w * dy * dy;
-        q[4] += __ldcg(&t.q64[6 * c + 4]) + w * dy * dz;
-        q[5] += __ldcg(&t.q64[6 * c + 5]) + w * dz * dz;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+        if (j < nc) {
+            const int c = c0 + j;
+            const double dx = __ldcg(&t.c64[3 * c]) - cx;
+            const double dy = __ldcg(&t.c64[3 * c + 1]) - cy;
+            const double dz = __ldcg(&t.c64[3 * c + 2]) - cz;
+            const double w = __ldcg(&t.m64[c]);
+            q[0] += __ldcg(&t.q64[6 * c]) + w * dx * dx;
+            q[1] += __ldcg(&t.q64[6 * c + 1]) + w * dx * dy;
+            q[2] += __ldcg(&t.q64[6 * c + 2]) + w * dx * dz;
+            q[3] += __ldcg(&t.q64[6 * c + 3]) + w * dy * dy;
+            q[4] += __ldcg(&t.q64[6 * c + 4]) + w * dy * dz;
+            q[5] += __ldcg(&t.q64[6 * c + 5]) + w * dz * dz;
+        }
     }
     t.m64[k] = tm;
     t.s64[3 * k] = sx;
@@ -289,7 +322,7 @@ __device__ void internal_moments(int k, TreeArrays& t)
     for (int j = 0; j < 6; ++j)
         t.q64[6 * k + j] = q[j];
     t.box0[k] = make_float4(mn[0], mn[1], mn[2], __int_as_float(c0));
-    t.box1[k] = make_float4(mx[0], mx[1], mx[2], __int_as_float(c1 - c0));
+    t.box1[k] = make_float4(mx[0], mx[1], mx[2], __int_as_float(nc));
     t.mono[k] = make_float4((float)cx, (float)cy, (float)cz, (float)tm);
     t.quadA[k] = make_float4((float)q[0], (float)q[1], (float)q[2], (float)q[3]);
     t.quadB[k] = make_float2((float)q[4], (float)q[5]);
@@ -323,14 +356,15 @@ __global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restr
 
 } // namespace
 
+size_t tree_lookback_words(int cap) { return static_cast<size_t>(cap) / kLookbackNodes + 2 * kMaxLevels + 8; }
+
 void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
                        int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s)
 {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t lbw = static_cast<size_t>(t.cap) / kThreads + kMaxLevels + 4;
-    cudaMemsetAsync(t.lookback, 0, lbw * sizeof(unsigned long long), s);
+    cudaMemsetAsync(t.lookback, 0, tree_lookback_words(t.cap) * sizeof(unsigned long long), s);
     count_launch();
     k_tree_init<<<1, 32, 0, s>>>(t, n);
     // Level l holds at most min(8^l, n) nodes; the persistent grid covers that with tiles.
@@ -340,12 +374,18 @@ void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4
             bound *= 8;
         if (bound > n)
             bound = n;
-        long long blocks = (bound + kThreads - 1) / kThreads;
+        const bool wide = bound <= 4096;  // top levels: few, large nodes
+        const long long per_tile = wide ? kThreads / 8 : kThreads;
+        long long blocks = (bound + per_tile - 1) / per_tile;
         if (blocks > 2LL * sms)
             blocks = 2LL * sms;
         count_launch();
-        k_tree_level<<<static_cast<int>(blocks), kThreads, 0, s>>>(sorted_keys, l, leaf_cap,
-                                                                   max_level, t, err);
+        if (wide)
+            k_tree_level<8><<<static_cast<int>(blocks), kThreads, 0, s>>>(sorted_keys, l, leaf_cap,
+                                                                          max_level, t, err);
+        else
+            k_tree_level<1><<<static_cast<int>(blocks), kThreads, 0, s>>>(sorted_keys, l, leaf_cap,
+                                                                          max_level, t, err);
     }
     count_launch();
     k_tree_finish_last<<<sms, 256, 0, s>>>(t, max_level);

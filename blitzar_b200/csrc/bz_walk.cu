@@ -44,6 +44,7 @@ struct __align__(16) WarpSmem {
     int lstart[kList];
     int lcount[kList];
     int lcode[kList];
+    int lnode[kList];
     int lpre[kList];
     unsigned long long bar;
 };
@@ -64,6 +65,20 @@ __device__ __forceinline__ float erfc_as(float u, float e)
 constexpr float kTwoOverSqrtPi = 1.1283791670955126f;
 constexpr float kFourOverSqrtPi = 2.2567583341910252f;
 constexpr float kEightOverSqrtPi = 4.5135166683820503f;
+
+struct SplitK {
+    float inv2rs;  // 1 / (2 r_s)
+    float cexp;    // -log2(e) / (4 r_s^2): e^{-u^2} = 2^{s^2 cexp}
+    float pk;      // 0.3275911 / (2 r_s): A&S t = 1 / (1 + p u)
+    float c2;      // (2/sqrt(pi)) / (2 r_s): 2u/sqrt(pi) = s c2
+};
+
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float r;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
 
 template <bool SPLIT, bool POT>
 __device__ __forceinline__ void pair_pp(const float4 s, float tx, float ty, float tz,
@@ -95,6 +110,37 @@ __device__ __forceinline__ void pair_pp(const float4 s, float tx, float ty, floa
         if (POT && !self)
             fp = fmaf(-m, rinv, fp);
     }
+    fx = fmaf(f, dx, fx);
+    fy = fmaf(f, dy, fy);
+    fz = fmaf(f, dz, fz);
+}
+
+// Force-only pair for softening above the minimum-distance floor (no zero-distance guard
+// needed): the split weight w = e^{-u^2} (t P(t) + 2u/sqrt(pi)) with the A&S 7.1.26 erfc and
+// all scale factors folded into precomputed constants.
+template <bool SPLIT>
+__device__ __forceinline__ void pair_fast(const float4 s, float tx, float ty, float tz, float eps2,
+                                          float rcut2, bool cut, const SplitK& k, float& fx,
+                                          float& fy, float& fz)
+{
+    const float dx = s.x - tx, dy = s.y - ty, dz = s.z - tz;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const float s2 = r2 + eps2;
+    const float m = (cut && r2 > rcut2) ? 0.0f : s.w;
+    const float rinv = rsqrt_approx(s2);
+    float mw = m;
+    if (SPLIT) {
+        const float sd = s2 * rinv;
+        const float e = ex2_approx(s2 * k.cexp);
+        const float t = rcp_approx(fmaf(sd, k.pk, 1.0f));
+        float q = 1.061405429f;
+        q = fmaf(q, t, -1.453152027f);
+        q = fmaf(q, t, 1.421413741f);
+        q = fmaf(q, t, -0.284496736f);
+        q = fmaf(q, t, 0.254829592f);
+        mw = m * (e * fmaf(t, q, sd * k.c2));
+    }
+    const float f = mw * (rinv * rinv * rinv);
     fx = fmaf(f, dx, fx);
     fy = fmaf(f, dy, fy);
     fz = fmaf(f, dz, fz);
@@ -228,11 +274,48 @@ __device__ __forceinline__ void flush_nodes(WarpSmem& w, int nn, const TreeArray
 
 template <bool PERIODIC, bool SPLIT, bool POT>
 __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* __restrict__ pos4,
-                                             const WalkParams& p, float inv2rs, bool cut,
-                                             float tx, float ty, float tz, int self_index,
-                                             Acc& acc, uint32_t& phase, int* err)
+                                             const TreeArrays& t, const WalkParams& p,
+                                             float inv2rs, bool cut, float tx, float ty, float tz,
+                                             int self_index, Acc& acc, uint32_t& phase, int* err)
 {
     const int lane = threadIdx.x & 31;
+    if (cut) {
+        // Drop leaves that no target of this warp can reach: a leaf whose (shifted) box is
+        // farther than the cutoff from every lane's target holds no pair inside the cutoff.
+        int keep = 0;
+        for (int j = 0; j < nl; ++j) {
+            const int code = w.lcode[j];
+            bool need = true;
+            if (!PERIODIC || code != kPerPairImage) {
+                const int k = w.lnode[j];
+                const float4 b0 = t.box0[k];
+                const float4 b1 = t.box1[k];
+                float sxo = 0.0f, syo = 0.0f, szo = 0.0f;
+                if (PERIODIC) {
+                    sxo = shift_of(code, 0, p.box);
+                    syo = shift_of(code, 1, p.box);
+                    szo = shift_of(code, 2, p.box);
+                }
+                const float ddx = fmaxf(fmaxf(b0.x - sxo - tx, tx - (b1.x - sxo)), 0.0f);
+                const float ddy = fmaxf(fmaxf(b0.y - syo - ty, ty - (b1.y - syo)), 0.0f);
+                const float ddz = fmaxf(fmaxf(b0.z - szo - tz, tz - (b1.z - szo)), 0.0f);
+                need = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz)) <= p.rcut2 * 1.0001f;
+            }
+            if (__any_sync(kFullMask, need)) {
+                if (lane == 0 && keep != j) {
+                    w.lstart[keep] = w.lstart[j];
+                    w.lcount[keep] = w.lcount[j];
+                    w.lcode[keep] = code;
+                    w.lnode[keep] = w.lnode[j];
+                }
+                ++keep;
+            }
+        }
+        __syncwarp();
+        nl = keep;
+        if (nl == 0)
+            return;
+    }
     // exclusive prefix of the leaf sizes (list holds at most 64 entries)
     const int c0 = lane < nl ? w.lcount[lane] : 0;
     const int c1 = lane + 32 < nl ? w.lcount[lane + 32] : 0;
@@ -245,6 +328,12 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
     if (lane + 32 < nl)
         w.lpre[lane + 32] = i1 - c1;
     __syncwarp();
+    const bool fast = !POT && p.eps2 > p.min_dist2;
+    SplitK sk;
+    sk.inv2rs = inv2rs;
+    sk.cexp = -1.4426950408889634f * inv2rs * inv2rs;
+    sk.pk = 0.3275911f * inv2rs;
+    sk.c2 = kTwoOverSqrtPi * inv2rs;
     int jfirst = 0;
     for (int cbase = 0; cbase < total; cbase += kTile) {
         const int cend = min(cbase + kTile, total);
@@ -298,15 +387,24 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                 sz += shift_of(code, 2, p.box);
             }
             int q = 0;
-            for (; q + 1 < cntp; q += 2) {
-                pair_pp<SPLIT, POT>(w.tile[off + q], sx, sy, sz, p, inv2rs, cut,
-                                    POT && gsrc0 + q == self_index, fx, fy, fz, fp);
-                pair_pp<SPLIT, POT>(w.tile[off + q + 1], sx, sy, sz, p, inv2rs, cut,
-                                    POT && gsrc0 + q + 1 == self_index, fx, fy, fz, fp);
+            if (fast) {
+                for (; q + 1 < cntp; q += 2) {
+                    pair_fast<SPLIT>(w.tile[off + q], sx, sy, sz, p.eps2, p.rcut2, cut, sk, fx, fy, fz);
+                    pair_fast<SPLIT>(w.tile[off + q + 1], sx, sy, sz, p.eps2, p.rcut2, cut, sk, fx, fy, fz);
+                }
+                if (q < cntp)
+                    pair_fast<SPLIT>(w.tile[off + q], sx, sy, sz, p.eps2, p.rcut2, cut, sk, fx, fy, fz);
+            } else {
+                for (; q + 1 < cntp; q += 2) {
+                    pair_pp<SPLIT, POT>(w.tile[off + q], sx, sy, sz, p, inv2rs, cut,
+                                        POT && gsrc0 + q == self_index, fx, fy, fz, fp);
+                    pair_pp<SPLIT, POT>(w.tile[off + q + 1], sx, sy, sz, p, inv2rs, cut,
+                                        POT && gsrc0 + q + 1 == self_index, fx, fy, fz, fp);
+                }
+                for (; q < cntp; ++q)
+                    pair_pp<SPLIT, POT>(w.tile[off + q], sx, sy, sz, p, inv2rs, cut,
+                                        POT && gsrc0 + q == self_index, fx, fy, fz, fp);
             }
-            for (; q < cntp; ++q)
-                pair_pp<SPLIT, POT>(w.tile[off + q], sx, sy, sz, p, inv2rs, cut,
-                                    POT && gsrc0 + q == self_index, fx, fy, fz, fp);
             if (pre + w.lcount[j] <= cend)
                 jfirst = j + 1;
         }
@@ -465,6 +563,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
             if (leaf) {
                 const int pos = nl + __popc(lm & lt);
                 w.lstart[pos] = link;
+                w.lnode[pos] = k;
                 w.lcount[pos] = -info;
                 w.lcode[pos] = code;
             }
@@ -504,7 +603,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                 nn = 0;
             }
             if (nl >= 32 || lp >= kTile) {
-                flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, p, inv2rs, cut, me.x, me.y, me.z,
+                flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, t, p, inv2rs, cut, me.x, me.y, me.z,
                                                    ti, acc, phase, err);
                 nl = 0;
                 lp = 0;
@@ -514,7 +613,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
             if (nn > 0)
                 flush_nodes<PERIODIC, SPLIT, QUAD, POT>(w, nn, t, p, inv2rs, me.x, me.y, me.z, acc);
             if (nl > 0)
-                flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, p, inv2rs, cut, me.x, me.y, me.z,
+                flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, t, p, inv2rs, cut, me.x, me.y, me.z,
                                                    ti, acc, phase, err);
         }
         if (valid) {

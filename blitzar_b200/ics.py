@@ -41,7 +41,7 @@ def grf_grid(n_side: int, seed: int, rms_cells: float = 0.2, spectral_index: flo
     delta_k = np.fft.rfftn(white) * amp
     disp = np.empty((3, n, n, n))
     for a, K in enumerate((KX, KY, KZ)):
-        disp[a] = np.fft.irfftn(1j * K / k2 * delta_k, s=(n, n, n))
+        disp[a] = np.fft.irfftn(1j * K / k2 * delta_k, s=(n, n, n), axes=(0, 1, 2))
     rms = math.sqrt(float((disp ** 2).sum(0).mean()))
     cell = box / n
     disp *= rms_cells * cell / rms

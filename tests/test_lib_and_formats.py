@@ -1,0 +1,93 @@
+"""CPU-side checks of the product: the C-ABI library loads and exports every symbol its header
+declares, argument validation happens before any CUDA call, and the snapshot formats and IC
+generators behave."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def test_library_exports_header_symbols():
+    from blitzar_b200 import _lib
+    from blitzar_b200 import build as b
+
+    if not os.path.exists(_lib.LIB_PATH):
+        b.build()
+    L = _lib.load()
+    header = open(os.path.join(ROOT, "include", "bzgrav.h")).read()
+    declared = set(re.findall(r"\b(bz_[a-z0-9_]+)\s*\(", header))
+    assert declared >= {"bz_create", "bz_step", "bz_accelerations", "bz_morton_keys"}
+    for name in sorted(declared):
+        assert hasattr(L, name), name
+    assert set(_lib.EXPORTS) == declared
+    assert L.bz_version().startswith(b"bzgrav")
+
+
+def test_config_defaults_and_argument_checks():
+    import ctypes as C
+
+    from blitzar_b200 import _lib
+
+    L = _lib.load()
+    cfg = _lib.default_config()
+    assert cfg.octree_theta == pytest.approx(0.5) and cfg.leaf_capacity == 16
+    assert cfg.struct_size == C.sizeof(_lib.BzConfig)
+    h = C.c_void_p()
+    assert L.bz_create(C.byref(cfg), 0, C.byref(h)) == _lib.BZ_INVALID_ARGUMENT
+    bad = _lib.default_config()
+    bad.struct_size = 4
+    assert L.bz_create(C.byref(bad), 10, C.byref(h)) == _lib.BZ_INVALID_ARGUMENT
+    assert L.bz_destroy(None) == _lib.BZ_INVALID_ARGUMENT
+    assert L.bz_status_string(_lib.BZ_DEVICE_LIMIT) == b"device limit"
+
+
+def test_nbsimbin_round_trip(tmp_path):
+    from blitzar_b200 import snapshot
+
+    rng = np.random.default_rng(0)
+    pos = rng.standard_normal((100, 3)).astype(np.float32)
+    vel = rng.standard_normal((100, 3)).astype(np.float32)
+    m = rng.random(100).astype(np.float32)
+    f = tmp_path / "s.bin"
+    snapshot.write_bin(f, pos, vel, m)
+    raw = f.read_bytes()
+    assert raw[:8] == b"NBSIMBIN" and len(raw) == 16 + 32 * 100
+    p2, v2, m2, t2 = snapshot.read_bin(f)
+    assert np.array_equal(p2, pos) and np.array_equal(v2, vel) and np.array_equal(m2, m)
+    assert np.all(t2 == 0)
+
+
+def test_xyz_format(tmp_path):
+    from blitzar_b200 import snapshot
+
+    pos = np.array([[1.0, -2.5, 3.14159265], [1e-7, 123456789.0, 0.0]], np.float32)
+    m = np.array([1.0, 0.5], np.float32)
+    f = tmp_path / "s.xyz"
+    snapshot.write_xyz(f, pos, m, step=7)
+    lines = f.read_text().splitlines()
+    assert lines[0] == "2" and lines[1] == "solver=octree_gpu integrator=leapfrog step=7"
+    assert lines[2] == "P 1 -2.5 3.14159 1 0"
+    assert lines[3] == "P 1e-07 1.23457e+08 0 0.5 0"
+
+
+def test_ic_generators():
+    from blitzar_b200 import ics
+
+    pos, vel, m = ics.grf_grid(16, 2)
+    assert pos.shape == (4096, 3) and pos.min() >= 0 and pos.max() < 1
+    g = (np.arange(16) + 0.5) / 16
+    grid = np.stack(np.meshgrid(g, g, g, indexing="ij"), -1).reshape(-1, 3)
+    d = pos - grid
+    d -= np.rint(d)
+    assert abs(np.sqrt((d ** 2).sum(1).mean()) * 16 - 0.2) < 1e-9
+    pos, vel, m = ics.plummer(20000, 1)
+    assert abs((m * (vel ** 2).sum(1)).sum() - 3 * np.pi / 32) < 0.02  # 2T for G = M = a = 1
+    pos, vel, m = ics.hernquist(20000, 3)
+    r = np.linalg.norm(pos, axis=1)
+    assert abs(np.median(r) - (1 + np.sqrt(2))) < 0.1  # half-mass radius (untruncated)
+    assert r.max() <= 100.0
+    pos, vel, m = ics.king(3000, 5, 6.0)
+    assert np.isfinite(vel).all() and abs(m.sum() - 1.0) < 1e-12
