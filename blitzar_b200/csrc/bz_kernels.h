@@ -74,6 +74,8 @@ struct TreeArrays {
     float2* quadB;     // {qyz, qzz}
 };
 constexpr int kMaxLevels = 21;
+// Upper bound on device ordinals for per-device caches (function attributes, launch shapes).
+constexpr int kMaxDevices = 64;
 size_t tree_lookback_words(int cap);
 void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
                        int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s);

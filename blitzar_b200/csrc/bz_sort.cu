@@ -263,11 +263,13 @@ void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits
     k_scan_hist<<<passes, 256, 0, s>>>(n, ws);
     const int tiles = (n + kTile - 1) / kTile;
     const size_t smem = sizeof(PassSmem);
-    static bool attr_set = false;
-    if (!attr_set) {
+    // function attributes belong to the device's context: set once per device
+    static std::atomic<bool> attr_set[kMaxDevices];
+    if (dev < 0 || dev >= kMaxDevices || !attr_set[dev].load()) {
         cudaFuncSetAttribute(k_onesweep, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              static_cast<int>(smem));
-        attr_set = true;
+        if (dev >= 0 && dev < kMaxDevices)
+            attr_set[dev].store(true);
     }
     for (int p = 0; p < passes; ++p) {
         count_launch();

@@ -648,20 +648,24 @@ struct WalkLaunch {
 template <bool PERIODIC, bool SPLIT, bool QUAD, bool POT>
 WalkLaunch walk_shape(int n)
 {
-    static WalkLaunch cached;
-    if (cached.blocks == 0) {
+    // function attributes and occupancy belong to the device: one cached shape per device
+    static WalkLaunch cached[kMaxDevices];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    WalkLaunch local;
+    WalkLaunch& c = (dev >= 0 && dev < kMaxDevices) ? cached[dev] : local;
+    if (c.blocks == 0) {
         const size_t smem = sizeof(WarpSmem) * kWarps;
         cudaFuncSetAttribute(k_walk<PERIODIC, SPLIT, QUAD, POT>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
-        int dev = 0, sms = 148, per_sm = 1;
-        cudaGetDevice(&dev);
+        int sms = 148, per_sm = 1;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<PERIODIC, SPLIT, QUAD, POT>,
                                                       kWarps * 32, smem);
-        cached.blocks = sms * (per_sm > 0 ? per_sm : 1);
-        cached.smem = smem;
+        c.smem = smem;
+        c.blocks = sms * (per_sm > 0 ? per_sm : 1);
     }
-    WalkLaunch l = cached;
+    WalkLaunch l = c;
     const int groups = (n + 31) / 32;
     const int need = (groups + kWarps - 1) / kWarps;
     if (l.blocks > need)
