@@ -25,6 +25,7 @@ EXPORTS = (
     "bz_reference_tree", "bz_interaction_counts", "bz_enable_phase_timing", "bz_phase_times",
     "bz_force_errors", "bz_pm_mesh", "bz_particle_count", "bz_device_bytes", "bz_last_error",
     "bz_status_string", "bz_version", "bz_kernel_launches", "bz_launches_per_step",
+    "bz_sort_pairs_noalloc",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -106,6 +107,7 @@ def load():
     L.bz_version.restype = C.c_char_p
     L.bz_kernel_launches.restype = C.c_uint64
     L.bz_launches_per_step.argtypes = [_vp, C.POINTER(C.c_uint64)]
+    L.bz_sort_pairs_noalloc.argtypes = [_vp, _vp, C.c_int64, C.c_int, C.c_uint64]
     _LIB = L
     return L
 

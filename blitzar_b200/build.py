@@ -31,6 +31,7 @@ SOURCES = {
     "bz_state.cu": [],
     "bz_diag.cu": [],
     "bz_api.cu": [],
+    "bz_noalloc.cu": [],
 }
 HEADERS = ["bz_common.cuh", "bz_kernels.h"]
 

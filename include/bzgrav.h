@@ -168,6 +168,34 @@ bz_status bz_launches_per_step(bz_handle* h, uint64_t* launches);
 size_t bz_particle_count(const bz_handle* h);
 size_t bz_device_bytes(const bz_handle* h);
 
+/* Allocation-free stable radix sort of device-resident (key, value) pairs, in place, on the
+ * calling thread's current device.  No counterpart in the reference (its sort,
+ * thrust::sort_by_key, allocates temporary storage on every call).
+ *
+ * For callers that must not allocate device memory: a host application that reserves HBM
+ * for its own pool or arena (a cudaMalloc from a plug-in would fail or escape the pool's
+ * accounting), and step loops where cudaMalloc/cudaFree are too costly (cudaFree waits for
+ * the whole device).  The handle-based API above allocates in bz_create; this call does
+ * not: its scratch is a fixed array in device memory, sized for BZ_SORT_NOALLOC_MAX_KEYS
+ * pairs (about 12.6 MiB), that every process loading this library holds on each device it
+ * uses until exit.  It calls no cudaMalloc, cudaFree or allocating library routine.
+ *
+ * keys/values: device (or managed) memory of the current device, n entries each; sorted by
+ * the low key_bits bits (8, 16, ..., 64), ties kept in input order (the same order as
+ * bz_morton_keys).  stream: a cudaStream_t as an integer (0 = the default stream).  The
+ * call returns once the sort has finished on that stream.
+ * Returns BZ_INVALID_ARGUMENT for n < 0 or n > BZ_SORT_NOALLOC_MAX_KEYS, key_bits not a
+ * multiple of 8 in 8..64, NULL or misaligned pointers, or memory the device cannot address;
+ * BZ_DEVICE_LIMIT if a look-back wait gave up; BZ_CUDA_ERROR if a CUDA call failed.
+ * The first call on each device looks up the scratch's device address (this may load the
+ * library's device code on that device); make that first call before any stream capture.
+ * All calls on a device share the one scratch array and it keeps the last call's contents:
+ * calls that overlap on the GPU (from several host threads or streams at once) race on it
+ * and must be serialised by the caller. */
+#define BZ_SORT_NOALLOC_MAX_KEYS 1048576
+bz_status bz_sort_pairs_noalloc(uint64_t* keys, uint32_t* values, int64_t n, int key_bits,
+                                uint64_t stream);
+
 /* Last error text (blitzar_core_get_last_error, runtime/ffi/core/FfiApi.hpp:99-100).
  * Returns the full length; writes at most cap-1 bytes plus NUL. */
 size_t bz_last_error(const bz_handle* h, char* buf, size_t cap);
