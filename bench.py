@@ -14,8 +14,8 @@ A "step" is one KDK leapfrog step of the whole system (keys, sort, permutation, 
 mesh, group walk, kicks and drift), replayed from a CUDA graph.  The state (about 230 B per
 particle, ~480 MB) is larger than the 126 MB L2, so no flush is needed between steps.
 
-Under torchrun (N > 1) every rank steps an independent replica (the single-system path does
-not shard) and `value` sums all ranks' particle-steps over the slowest rank's
+Under torchrun (N > 1) every rank steps an independent replica (the force evaluation of one
+system does not shard) and `value` sums all ranks' particle-steps over the slowest rank's
 device time.  ``--impl reference`` times the reference's CPU TreePM path instead.
 """
 from __future__ import annotations

@@ -26,18 +26,26 @@ namespace bz {
 namespace {
 
 constexpr int kWarps = 4;
-constexpr int kStack = 1024;      // shared-memory part of the traversal stack
+constexpr int kStack = 512;       // shared-memory part of the traversal stack
 constexpr int kSpill = 8192;      // per-warp global spill area (oldest entries)
 constexpr int kList = 64;
-constexpr int kTile = 256;
+constexpr int kTile = 128;
+constexpr int kFlushParticles = 256;  // listed leaf particles that trigger a flush
 constexpr int kIndexBits = 26;
 constexpr int kIndexMask = (1 << kIndexBits) - 1;
 constexpr int kPerPairImage = 64;  // leaf code: periodic image chosen per pair
 
+constexpr int kNoShift = 21;       // shift code of the central image on all three axes
+
 struct __align__(16) WarpSmem {
     float4 tile[kTile];
-    float4 nd_mono[32];
-    float4 nd_qa[32];
+    union {
+        struct {
+            float4 nd_mono[32];
+            float4 nd_qa[32];
+        };
+        unsigned mask[kTile / 32][32];  // leaf flush: per-lane in-cutoff bits of the tile
+    };
     float2 nd_qb[32];
     int stack[kStack];
     int nlist[kList];
@@ -282,30 +290,55 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
     if (cut) {
         // Drop leaves that no target of this warp can reach: a leaf whose (shifted) box is
         // farther than the cutoff from every lane's target holds no pair inside the cutoff.
-        int keep = 0;
-        for (int j = 0; j < nl; ++j) {
-            const int code = w.lcode[j];
-            bool need = true;
-            if (!PERIODIC || code != kPerPairImage) {
+        // Lane j loads the boxes of list entries j and j + 32 in one round (no serial chain
+        // of loads); each box is then broadcast by shuffle and tested against every target.
+        float4 lo[2], hi[2];
+        bool ppi[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int j = lane + 32 * h;
+            lo[h] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            hi[h] = lo[h];
+            ppi[h] = false;
+            if (j < nl) {
+                const int code = w.lcode[j];
+                ppi[h] = PERIODIC && code == kPerPairImage;
                 const int k = w.lnode[j];
                 const float4 b0 = t.box0[k];
                 const float4 b1 = t.box1[k];
                 float sxo = 0.0f, syo = 0.0f, szo = 0.0f;
-                if (PERIODIC) {
+                if (PERIODIC && !ppi[h]) {
                     sxo = shift_of(code, 0, p.box);
                     syo = shift_of(code, 1, p.box);
                     szo = shift_of(code, 2, p.box);
                 }
-                const float ddx = fmaxf(fmaxf(b0.x - sxo - tx, tx - (b1.x - sxo)), 0.0f);
-                const float ddy = fmaxf(fmaxf(b0.y - syo - ty, ty - (b1.y - syo)), 0.0f);
-                const float ddz = fmaxf(fmaxf(b0.z - szo - tz, tz - (b1.z - szo)), 0.0f);
-                need = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz)) <= p.rcut2 * 1.0001f;
+                lo[h] = make_float4(b0.x - sxo, b0.y - syo, b0.z - szo, 0.0f);
+                hi[h] = make_float4(b1.x - sxo, b1.y - syo, b1.z - szo, 0.0f);
+            }
+        }
+        const float lim2 = p.rcut2 * 1.0001f;
+        int keep = 0;
+        for (int j = 0; j < nl; ++j) {
+            const int h = j >> 5, src = j & 31;
+            const float bx0 = __shfl_sync(kFullMask, h ? lo[1].x : lo[0].x, src);
+            const float by0 = __shfl_sync(kFullMask, h ? lo[1].y : lo[0].y, src);
+            const float bz0 = __shfl_sync(kFullMask, h ? lo[1].z : lo[0].z, src);
+            const float bx1 = __shfl_sync(kFullMask, h ? hi[1].x : hi[0].x, src);
+            const float by1 = __shfl_sync(kFullMask, h ? hi[1].y : hi[0].y, src);
+            const float bz1 = __shfl_sync(kFullMask, h ? hi[1].z : hi[0].z, src);
+            const bool pp = __shfl_sync(kFullMask, h ? ppi[1] : ppi[0], src);
+            bool need = true;
+            if (!pp) {
+                const float ddx = fmaxf(fmaxf(bx0 - tx, tx - bx1), 0.0f);
+                const float ddy = fmaxf(fmaxf(by0 - ty, ty - by1), 0.0f);
+                const float ddz = fmaxf(fmaxf(bz0 - tz, tz - bz1), 0.0f);
+                need = fmaf(ddx, ddx, fmaf(ddy, ddy, ddz * ddz)) <= lim2;
             }
             if (__any_sync(kFullMask, need)) {
                 if (lane == 0 && keep != j) {
                     w.lstart[keep] = w.lstart[j];
                     w.lcount[keep] = w.lcount[j];
-                    w.lcode[keep] = code;
+                    w.lcode[keep] = w.lcode[j];
                     w.lnode[keep] = w.lnode[j];
                 }
                 ++keep;
@@ -352,22 +385,97 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
         }
         mbar_wait_bounded(&w.bar, phase, err);
         phase ^= 1u;
-        float fx = 0.0f, fy = 0.0f, fz = 0.0f, fp = 0.0f;
-        for (int j = jfirst; j < nl; ++j) {
-            const int pre = w.lpre[j];
-            if (pre >= cend)
-                break;
-            const int lo = max(pre, cbase);
-            const int hi = min(pre + w.lcount[j], cend);
-            if (hi <= lo)
-                continue;
-            float sx = tx, sy = ty, sz = tz;
-            const int gsrc0 = w.lstart[j] + (lo - pre);
-            const int off = lo - cbase;
-            const int cntp = hi - lo;
-            if (PERIODIC) {
+        // Periodic images: move the sources of each shifted leaf into the group's image in
+        // place (leaves summed with per-pair images keep their stored positions).
+        bool per_pair = false;
+        if (PERIODIC) {
+            for (int j = jfirst; j < nl; ++j) {
+                const int pre = w.lpre[j];
+                if (pre >= cend)
+                    break;
+                const int lo = max(pre, cbase);
+                const int hi = min(pre + w.lcount[j], cend);
                 const int code = w.lcode[j];
+                if (hi <= lo || code == kNoShift)
+                    continue;
                 if (code == kPerPairImage) {
+                    per_pair = true;
+                    continue;
+                }
+                const float shx = shift_of(code, 0, p.box), shy = shift_of(code, 1, p.box),
+                            shz = shift_of(code, 2, p.box);
+                for (int q = lo + lane; q < hi; q += 32) {
+                    float4& s4 = w.tile[q - cbase];
+                    s4.x = __fsub_rn(s4.x, shx);
+                    s4.y = __fsub_rn(s4.y, shy);
+                    s4.z = __fsub_rn(s4.z, shz);
+                }
+            }
+            __syncwarp();
+        }
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f, fp = 0.0f;
+        if (fast && cut && !per_pair) {
+            // Cutoff filter: each lane marks the tile sources inside its own cutoff sphere
+            // (the same r^2 expression as the pair law, so the set is exact), then sums only
+            // those.  Skipped pairs contribute exactly zero in the unfiltered sum, so the
+            // result is bit-identical to summing every listed source in tile order.
+            const int nb = cend - cbase;
+            const int nw = (nb + 31) >> 5;
+            for (int wd = 0; wd < nw; ++wd) {
+                const int qb = wd << 5;
+                unsigned m = 0u;
+                if (qb + 32 <= nb) {
+#pragma unroll
+                    for (int b = 0; b < 32; ++b) {
+                        const float4 s4 = w.tile[qb + b];
+                        const float dx = s4.x - tx, dy = s4.y - ty, dz = s4.z - tz;
+                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        if (r2 <= p.rcut2)
+                            m |= 1u << b;
+                    }
+                } else {
+                    for (int b = 0; qb + b < nb; ++b) {
+                        const float4 s4 = w.tile[qb + b];
+                        const float dx = s4.x - tx, dy = s4.y - ty, dz = s4.z - tz;
+                        const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+                        if (r2 <= p.rcut2)
+                            m |= 1u << b;
+                    }
+                }
+                w.mask[wd][lane] = m;
+            }
+            int wd = 0;
+            unsigned m = w.mask[0][lane];
+            for (;;) {
+                while (m == 0u && ++wd < nw)
+                    m = w.mask[wd][lane];
+                if (m == 0u)
+                    break;
+                const int b = __ffs(m) - 1;
+                m &= m - 1u;
+                pair_fast<SPLIT>(w.tile[(wd << 5) + b], tx, ty, tz, p.eps2, p.rcut2, false, sk,
+                                 fx, fy, fz);
+            }
+            __syncwarp();
+            for (int j = jfirst; j < nl; ++j) {
+                if (w.lpre[j] >= cend)
+                    break;
+                if (w.lpre[j] + w.lcount[j] <= cend)
+                    jfirst = j + 1;
+            }
+        } else {
+            for (int j = jfirst; j < nl; ++j) {
+                const int pre = w.lpre[j];
+                if (pre >= cend)
+                    break;
+                const int lo = max(pre, cbase);
+                const int hi = min(pre + w.lcount[j], cend);
+                if (hi <= lo)
+                    continue;
+                const int gsrc0 = w.lstart[j] + (lo - pre);
+                const int off = lo - cbase;
+                const int cntp = hi - lo;
+                if (PERIODIC && w.lcode[j] == kPerPairImage) {
                     // rare slow path: nearest image chosen per pair
                     const float inv_box = 1.0f / p.box;
                     for (int q = 0; q < cntp; ++q) {
@@ -382,31 +490,28 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                         jfirst = j + 1;
                     continue;
                 }
-                sx += shift_of(code, 0, p.box);
-                sy += shift_of(code, 1, p.box);
-                sz += shift_of(code, 2, p.box);
-            }
-            int q = 0;
-            if (fast) {
-                for (; q + 1 < cntp; q += 2) {
-                    pair_fast<SPLIT>(w.tile[off + q], sx, sy, sz, p.eps2, p.rcut2, cut, sk, fx, fy, fz);
-                    pair_fast<SPLIT>(w.tile[off + q + 1], sx, sy, sz, p.eps2, p.rcut2, cut, sk, fx, fy, fz);
+                int q = 0;
+                if (fast) {
+                    for (; q + 1 < cntp; q += 2) {
+                        pair_fast<SPLIT>(w.tile[off + q], tx, ty, tz, p.eps2, p.rcut2, cut, sk, fx, fy, fz);
+                        pair_fast<SPLIT>(w.tile[off + q + 1], tx, ty, tz, p.eps2, p.rcut2, cut, sk, fx, fy, fz);
+                    }
+                    if (q < cntp)
+                        pair_fast<SPLIT>(w.tile[off + q], tx, ty, tz, p.eps2, p.rcut2, cut, sk, fx, fy, fz);
+                } else {
+                    for (; q + 1 < cntp; q += 2) {
+                        pair_pp<SPLIT, POT>(w.tile[off + q], tx, ty, tz, p, inv2rs, cut,
+                                            POT && gsrc0 + q == self_index, fx, fy, fz, fp);
+                        pair_pp<SPLIT, POT>(w.tile[off + q + 1], tx, ty, tz, p, inv2rs, cut,
+                                            POT && gsrc0 + q + 1 == self_index, fx, fy, fz, fp);
+                    }
+                    for (; q < cntp; ++q)
+                        pair_pp<SPLIT, POT>(w.tile[off + q], tx, ty, tz, p, inv2rs, cut,
+                                            POT && gsrc0 + q == self_index, fx, fy, fz, fp);
                 }
-                if (q < cntp)
-                    pair_fast<SPLIT>(w.tile[off + q], sx, sy, sz, p.eps2, p.rcut2, cut, sk, fx, fy, fz);
-            } else {
-                for (; q + 1 < cntp; q += 2) {
-                    pair_pp<SPLIT, POT>(w.tile[off + q], sx, sy, sz, p, inv2rs, cut,
-                                        POT && gsrc0 + q == self_index, fx, fy, fz, fp);
-                    pair_pp<SPLIT, POT>(w.tile[off + q + 1], sx, sy, sz, p, inv2rs, cut,
-                                        POT && gsrc0 + q + 1 == self_index, fx, fy, fz, fp);
-                }
-                for (; q < cntp; ++q)
-                    pair_pp<SPLIT, POT>(w.tile[off + q], sx, sy, sz, p, inv2rs, cut,
-                                        POT && gsrc0 + q == self_index, fx, fy, fz, fp);
+                if (pre + w.lcount[j] <= cend)
+                    jfirst = j + 1;
             }
-            if (pre + w.lcount[j] <= cend)
-                jfirst = j + 1;
         }
         acc.add(0, fx);
         acc.add(1, fy);
@@ -602,7 +707,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                 flush_nodes<PERIODIC, SPLIT, QUAD, POT>(w, nn, t, p, inv2rs, me.x, me.y, me.z, acc);
                 nn = 0;
             }
-            if (nl >= 32 || lp >= kTile) {
+            if (nl >= 32 || lp >= kFlushParticles) {
                 flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, t, p, inv2rs, cut, me.x, me.y, me.z,
                                                    ti, acc, phase, err);
                 nl = 0;
