@@ -55,7 +55,9 @@ WORKLOADS = {
     "treepm64": dict(kind="treepm", n_side=64, mesh=128, r_split_cells=1.25, r_cut_factor=5.0,
                      theta=0.5, eps_lattice=0.02, dt=5e-4, seed=2, rms_cells=0.2,
                      assignment="pcs", gradient="spectral", node_size_factor=0.5),
-    "plummer65k": dict(kind="octree", n=65536, theta=0.5, eps=0.01, dt=1e-3, seed=1),
+    "plummer65k": dict(kind="octree", ic="plummer", n=65536, theta=0.5, eps=0.01, dt=1e-3, seed=1),
+    "hernquist4m": dict(kind="octree", ic="hernquist", n=4194304, theta=0.4, eps=0.005, dt=2e-4,
+                        seed=3),
 }
 
 
@@ -102,6 +104,8 @@ def make_ics(w, rank):
 
     if w["kind"] == "treepm":
         pos, vel, mass = ics.grf_grid(w["n_side"], seed=w["seed"] + rank, rms_cells=w["rms_cells"])
+    elif w["ic"] == "hernquist":
+        pos, vel, mass = ics.hernquist(w["n"], seed=w["seed"] + rank)
     else:
         pos, vel, mass = ics.plummer(w["n"], seed=w["seed"] + rank)
     return pos, vel, mass.astype(np.float32)
@@ -312,6 +316,7 @@ def run_ours(args, w, rank, world, local):
         for _ in range(max(3, args.warmup)):
             eng.step(dt, 1)
     torch.cuda.synchronize()
+    energy0 = eng.energy() if w["kind"] == "octree" else None
 
     clocks = ClockSampler(local)
     if dist:
@@ -334,6 +339,13 @@ def run_ours(args, w, rank, world, local):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = n * world * args.steps / (ms / 1e3)
+    drift = None
+    if energy0 is not None:
+        k1, w1, p1 = eng.energy()
+        e0 = energy0[0] + energy0[1]
+        drift = {"relative_energy_drift": (k1 + w1 - e0) / abs(e0), "steps": args.steps,
+                 "momentum_change": float(np.abs(p1 - energy0[2]).max()),
+                 "note": "total energy (FP64 kinetic + tree potential) before and after the timed steps"}
 
     launches_step = eng.launches_per_step()
     # phase-timed eager pass for the per-kernel roofline
@@ -420,7 +432,8 @@ def run_ours(args, w, rank, world, local):
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic (seeded GRF-displaced grid)" if w["kind"] == "treepm" else "synthetic (seeded Plummer)",
+        "data": ("synthetic (seeded GRF-displaced grid)" if w["kind"] == "treepm"
+                 else f"synthetic (seeded {w['ic'].capitalize()} sphere)"),
         "config": config_dict(w, args, n),
         "force_error": {"median": errs["median"], "p99": errs["p99"], "sample": args.error_sample,
                         "reference": "FP64 Ewald" if w["kind"] == "treepm" else "FP64 direct sum"},
@@ -428,6 +441,8 @@ def run_ours(args, w, rank, world, local):
         "phase_ms": ph, "gpu_launches": launches_step * args.steps, "launches_per_step": launches_step,
         "clocks": clk, "e2e": e2e, "cpu_baseline": cpu,
     }
+    if drift is not None:
+        line["energy"] = drift
     eng.close()
     if rank == 0:
         print(json.dumps(line))

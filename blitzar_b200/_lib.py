@@ -25,7 +25,7 @@ EXPORTS = (
     "bz_reference_tree", "bz_interaction_counts", "bz_enable_phase_timing", "bz_phase_times",
     "bz_force_errors", "bz_pm_mesh", "bz_particle_count", "bz_device_bytes", "bz_last_error",
     "bz_status_string", "bz_version", "bz_kernel_launches", "bz_launches_per_step",
-    "bz_sort_pairs_noalloc",
+    "bz_sort_pairs_noalloc", "bz_energy",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -107,6 +107,7 @@ def load():
     L.bz_version.restype = C.c_char_p
     L.bz_kernel_launches.restype = C.c_uint64
     L.bz_launches_per_step.argtypes = [_vp, C.POINTER(C.c_uint64)]
+    L.bz_energy.argtypes = [_vp, _vp, _vp, _vp]
     L.bz_sort_pairs_noalloc.argtypes = [_vp, _vp, C.c_int64, C.c_int, C.c_uint64]
     _LIB = L
     return L
@@ -206,6 +207,15 @@ class Engine:
         self._check(self.L.bz_accelerations(self.h, _ptr(a), _ptr(p)), "bz_accelerations")
         acc = a.reshape(3, self.n).T.copy()
         return (acc, p) if want_pot else acc
+
+    def energy(self, potential=True):
+        """FP64 (kinetic, potential or None, momentum[3]) of the current state."""
+        ke = C.c_double(0.0)
+        pe = C.c_double(0.0)
+        mom = np.zeros(3, np.float64)
+        self._check(self.L.bz_energy(self.h, C.byref(ke), C.byref(pe) if potential else None,
+                                     _ptr(mom)), "bz_energy")
+        return ke.value, (pe.value if potential else None), mom
 
     def morton_keys(self):
         k = np.empty(self.n, np.uint64)

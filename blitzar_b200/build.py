@@ -26,6 +26,7 @@ SOURCES = {
     "bz_keys.cu": [],
     "bz_sort.cu": [],
     "bz_tree.cu": ["--fmad=false"],
+    "bz_groups.cu": [],
     "bz_walk.cu": [],
     "bz_pm.cu": [],
     "bz_state.cu": [],

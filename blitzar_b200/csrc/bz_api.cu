@@ -46,6 +46,7 @@ struct DeviceBuffers {
     unsigned* bbox32 = nullptr;
     int* err = nullptr;
     double* dt = nullptr;  // {dt, dt/2}
+    double* energy = nullptr;  // energy/momentum reduction scratch + results
     unsigned* queue = nullptr;
     int* spill = nullptr;
     unsigned long long* counters = nullptr;  // [2] pp, pn
@@ -69,6 +70,7 @@ struct bz_handle {
     DeviceBuffers d;
     SortWorkspace sort{};
     TreeArrays tree{};
+    GroupTable groups{};
     PmPlan* pm = nullptr;
     int spill_slots = 0;
     size_t bytes = 0;
@@ -177,6 +179,7 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
     record(h, kPhTree);
     launch_tree_build(d.keys, d.pos4, n, h->cfg.leaf_capacity, kMaxLevels, h->tree, d.err,
                       h->stream);
+    launch_groups(h->tree, n, h->groups, h->stream);
     record(h, kPhMesh);
     if (h->cfg.solver == BZ_SOLVER_TREEPM && h->pm) {
         pm_forces(h->pm, d.pos4, n, d.acc[0], d.acc[1], d.acc[2], h->stream);
@@ -194,8 +197,8 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
     o.az = d.acc[2];
     o.pot = want_pot ? d.pot : nullptr;
     o.totals = d.counters;
-    launch_walk(d.pos4, n, h->tree, walk_params(h, want_pot), o, d.queue, d.spill, d.err,
-                h->stream);
+    launch_walk(d.pos4, n, h->tree, h->groups, walk_params(h, want_pot), o, d.queue, d.spill,
+                d.err, h->stream);
     record(h, kPhIntegrate);
     if (kick) {
         double* const* s = d.st[h->cur];
@@ -491,7 +494,8 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
         ok = ok && dalloc(h, &d.acc[a], n);
     ok = ok && dalloc(h, &d.pot, n) && dalloc(h, &d.keys, n) && dalloc(h, &d.perm, n) &&
          dalloc(h, &d.box, 1) && dalloc(h, &d.bbox32, 8) && dalloc(h, &d.err, 1) &&
-         dalloc(h, &d.dt, 2) && dalloc(h, &d.queue, 1) && dalloc(h, &d.counters, 2) &&
+         dalloc(h, &d.dt, 2) && dalloc(h, &d.energy, energy_scratch_doubles()) &&
+         dalloc(h, &d.queue, 1) && dalloc(h, &d.counters, 2) &&
          dalloc(h, &d.stage, 7 * n) && dalloc(h, &d.ref_xyzm, 4 * n) && dalloc(h, &d.ref_orig, n) &&
          dalloc(h, &d.ref_hot8, 8);
     // sort workspace
@@ -513,6 +517,9 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
          dalloc(h, &t.m64, cap) && dalloc(h, &t.s64, 3 * cap) && dalloc(h, &t.c64, 3 * cap) &&
          dalloc(h, &t.q64, 6 * cap) && dalloc(h, &t.box0, cap) && dalloc(h, &t.box1, cap) &&
          dalloc(h, &t.mono, cap) && dalloc(h, &t.quadA, cap) && dalloc(h, &t.quadB, cap);
+    GroupTable& gt = h->groups;
+    ok = ok && dalloc(h, &gt.flag, n) && dalloc(h, &gt.gstart, n + 1) && dalloc(h, &gt.ngroups, 1) &&
+         dalloc(h, &gt.block_sums, static_cast<size_t>(group_count_blocks(static_cast<int>(n))));
     // walk spill area: one slot per warp the persistent walk grid can hold
     h->spill_slots = walk_spill_slots();
     ok = ok && dalloc(h, &d.spill, static_cast<size_t>(h->spill_slots) * walk_spill_entries());
@@ -831,6 +838,45 @@ bz_status bz_accelerations(bz_handle* h, float* acc, float* pot)
     collect_timing(h);
     read_counters(h);
     h->forces_valid = true;
+    return BZ_OK;
+}
+
+bz_status bz_energy(bz_handle* h, double* kinetic, double* potential, double* momentum3)
+{
+    if (!h || h->n == 0 || (!kinetic && !potential && !momentum3))
+        return BZ_INVALID_ARGUMENT;
+    if (h->cfg.solver == BZ_SOLVER_OCTREE_REFERENCE)
+        return fail(h, BZ_UNSUPPORTED, "energies are not part of the reference formulation");
+    if (potential && h->cfg.solver == BZ_SOLVER_TREEPM)
+        return fail(h, BZ_UNSUPPORTED, "bz_energy: the TreePM mesh leg has no potential output");
+    cudaSetDevice(h->device);
+    const int n = static_cast<int>(h->n);
+    DeviceBuffers& d = h->d;
+    h->stepping = false;
+    if (potential) {
+        enqueue_order(h);
+        enqueue_forces(h, false, true);
+    }
+    double* const* st = d.st[h->cur];
+    launch_energy(st[3], st[4], st[5], d.mass[h->cur], potential ? d.pot : nullptr, n, d.energy,
+                  h->stream);
+    double out[5] = {};
+    cudaMemcpyAsync(out, d.energy + energy_scratch_doubles() - 8, 5 * sizeof(double),
+                    cudaMemcpyDeviceToHost, h->stream);
+    const bz_status s = check_device(h, "bz_energy");
+    if (s != BZ_OK)
+        return s;
+    if (potential)
+        h->forces_valid = true;
+    if (kinetic)
+        *kinetic = out[0];
+    if (potential)
+        *potential = out[1];
+    if (momentum3) {
+        momentum3[0] = out[2];
+        momentum3[1] = out[3];
+        momentum3[2] = out[4];
+    }
     return BZ_OK;
 }
 

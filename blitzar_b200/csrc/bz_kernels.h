@@ -96,6 +96,17 @@ struct WalkParams {
     int quadrupole;
     int want_pot;
 };
+// ---------------------------------------------------------------- target groups (bz_groups.cu)
+constexpr int kGroupMax = 32;  // particles per walk group (one warp)
+struct GroupTable {
+    int* flag;        // [n] group-start flags
+    int* gstart;      // [n + 1] group start indices in sorted order, then the end sentinel
+    int* ngroups;     // [1]
+    int* block_sums;  // [group_count_blocks(n)]
+};
+int group_count_blocks(int n);
+void launch_groups(const TreeArrays& t, int n, GroupTable& g, cudaStream_t s);
+
 struct WalkOutputs {
     float* ax;        // accumulated into (+=)
     float* ay;
@@ -105,8 +116,9 @@ struct WalkOutputs {
     unsigned long long* n_pn;
     unsigned long long* totals; // optional [2] sums of the above
 };
-void launch_walk(const float4* pos4, int n, const TreeArrays& t, const WalkParams& p,
-                 const WalkOutputs& o, unsigned* queue, int* spill, int* err, cudaStream_t s);
+void launch_walk(const float4* pos4, int n, const TreeArrays& t, const GroupTable& g,
+                 const WalkParams& p, const WalkOutputs& o, unsigned* queue, int* spill, int* err,
+                 cudaStream_t s);
 int walk_spill_slots();       // warp slots that need a spill area
 size_t walk_spill_entries();  // ints per slot
 
@@ -149,6 +161,11 @@ void launch_kick(double* vx, double* vy, double* vz, const float* ax, const floa
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
                        const float* ax, const float* ay, const float* az, int n,
                        const double* dt, double periodic_len, BoxF64* box, cudaStream_t s);
+// FP64 energy/momentum sums over the sorted state (scratch: energy_scratch_doubles(); the
+// five results land at scratch[5 * 1024 .. 5 * 1024 + 5)).
+size_t energy_scratch_doubles();
+void launch_energy(const double* vx, const double* vy, const double* vz, const float* m,
+                   const float* pot, int n, double* scratch, cudaStream_t s);
 void launch_scatter3(const float* ax, const float* ay, const float* az, const int* id, int n,
                      float* out_soa3, cudaStream_t s);
 void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s);

@@ -207,4 +207,69 @@ void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s)
     k_f64_to_f32<<<grid_for(n), kThreads, 0, s>>>(src, dst, n);
 }
 
+namespace {
+
+constexpr int kEnergyBlocks = 1024;
+
+// Per-block FP64 partial sums of {sum m v^2 / 2, sum m phi / 2, sum m vx, sum m vy, sum m vz};
+// blocks write their partials and a single block adds them in block order (deterministic).
+__global__ void __launch_bounds__(kThreads) k_energy_partials(
+    const double* __restrict__ vx, const double* __restrict__ vy, const double* __restrict__ vz,
+    const float* __restrict__ m, const float* __restrict__ pot, int n, double* __restrict__ part)
+{
+    double acc[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+        const double mi = m[i];
+        const double x = vx[i], y = vy[i], z = vz[i];
+        acc[0] += 0.5 * mi * (x * x + y * y + z * z);
+        if (pot)
+            acc[1] += 0.5 * mi * static_cast<double>(pot[i]);
+        acc[2] += mi * x;
+        acc[3] += mi * y;
+        acc[4] += mi * z;
+    }
+    __shared__ double red[5][kThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+        double v = acc[k];
+        for (int o = 16; o > 0; o >>= 1)
+            v += __shfl_down_sync(kFullMask, v, o);
+        if (lane == 0)
+            red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 5) {
+        double v = 0.0;
+        for (int w = 0; w < kThreads / 32; ++w)
+            v += red[threadIdx.x][w];
+        part[threadIdx.x * kEnergyBlocks + blockIdx.x] = v;
+    }
+}
+
+__global__ void k_energy_final(const double* __restrict__ part, int blocks, double* __restrict__ out)
+{
+    if (threadIdx.x < 5) {
+        double v = 0.0;
+        for (int b = 0; b < blocks; ++b)
+            v += part[threadIdx.x * kEnergyBlocks + b];
+        out[threadIdx.x] = v;
+    }
+}
+
+} // namespace
+
+size_t energy_scratch_doubles() { return 5 * static_cast<size_t>(kEnergyBlocks) + 8; }
+
+void launch_energy(const double* vx, const double* vy, const double* vz, const float* m,
+                   const float* pot, int n, double* scratch, cudaStream_t s)
+{
+    int blocks = grid_for(n);
+    blocks = blocks < kEnergyBlocks ? blocks : kEnergyBlocks;
+    count_launch();
+    k_energy_partials<<<blocks, kThreads, 0, s>>>(vx, vy, vz, m, pot, n, scratch);
+    count_launch();
+    k_energy_final<<<1, 32, 0, s>>>(scratch, blocks, scratch + 5 * kEnergyBlocks);
+}
+
 } // namespace bz

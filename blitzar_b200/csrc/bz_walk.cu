@@ -1,7 +1,7 @@
 // Warp-cooperative group tree walk (the force hot path).
 //
-// One warp owns a group of 32 consecutive Morton-sorted targets.  It walks the tree once for
-// the whole group: each step pops up to 32 nodes (one per lane), tests them against the
+// One warp owns a group of at most 32 consecutive Morton-sorted targets (a run of sibling
+// subtrees cut from the octree, bz_groups.cu).  It walks the tree once for the whole group: each step pops up to 32 nodes (one per lane), tests them against the
 // group's bounding box, and sorts them with warp votes into
 //   - pruned (beyond the short-range cutoff),
 //   - accepted multipoles  -> appended to a shared-memory node list,
@@ -527,7 +527,9 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
 // to a per-warp-slot global area and refilled when the shared part runs dry.
 template <bool PERIODIC, bool SPLIT, bool QUAD, bool POT>
 __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__ pos4, int n,
-                                                       TreeArrays t, WalkParams p, float inv_box,
+                                                       TreeArrays t, const int* __restrict__ gstart,
+                                                       const int* __restrict__ ngroups_ptr,
+                                                       WalkParams p, float inv_box,
                                                        WalkOutputs o, unsigned* queue,
                                                        int* spill_base, int* err)
 {
@@ -535,7 +537,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];
     int* spill = spill_base + static_cast<size_t>(blockIdx.x * kWarps + warp) * kSpill;
-    const int ngroups = (n + 31) >> 5;
+    const int ngroups = *ngroups_ptr;
     if (lane == 0)
         mbar_init(&w.bar, 1);
     fence_mbar_init();
@@ -554,9 +556,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
         g = __shfl_sync(kFullMask, g, 0);
         if (g >= ngroups)
             break;
-        const int ti = g * 32 + lane;
-        const bool valid = ti < n;
-        const float4 me = pos4[valid ? ti : g * 32];
+        const int g0 = gstart[g];
+        const int gn = gstart[g + 1] - g0;
+        const int ti = g0 + lane;
+        const bool valid = lane < gn;
+        const float4 me = pos4[valid ? ti : g0];
         float gmin[3] = {me.x, me.y, me.z}, gmax[3] = {me.x, me.y, me.z};
 #pragma unroll
         for (int a = 0; a < 3; ++a)
@@ -734,7 +738,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
             if (o.n_pn)
                 o.n_pn[g] = cnt_pn;
             if (o.totals) {
-                const unsigned long long ng = static_cast<unsigned long long>(min(32, n - g * 32));
+                const unsigned long long ng = static_cast<unsigned long long>(gn);
                 atomicAdd(&o.totals[0], cnt_pp * ng);
                 atomicAdd(&o.totals[1], cnt_pn * ng);
             }
@@ -771,40 +775,41 @@ WalkLaunch walk_shape(int n)
         c.blocks = sms * (per_sm > 0 ? per_sm : 1);
     }
     WalkLaunch l = c;
-    const int groups = (n + 31) / 32;
-    const int need = (groups + kWarps - 1) / kWarps;
+    const int need = (n + kWarps - 1) / kWarps;  // groups <= n
     if (l.blocks > need)
         l.blocks = need < 1 ? 1 : need;
     return l;
 }
 
 template <bool PERIODIC, bool SPLIT, bool QUAD, bool POT>
-void launch_variant(const float4* pos4, int n, const TreeArrays& t, const WalkParams& p,
-                    const WalkOutputs& o, unsigned* queue, int* spill, int* err, cudaStream_t s)
+void launch_variant(const float4* pos4, int n, const TreeArrays& t, const GroupTable& g,
+                    const WalkParams& p, const WalkOutputs& o, unsigned* queue, int* spill,
+                    int* err, cudaStream_t s)
 {
     const WalkLaunch l = walk_shape<PERIODIC, SPLIT, QUAD, POT>(n);
     const float inv_box = p.box > 0.0f ? 1.0f / p.box : 0.0f;
     count_launch();
     k_zero_u32<<<1, 1, 0, s>>>(queue);
     count_launch();
-    k_walk<PERIODIC, SPLIT, QUAD, POT><<<l.blocks, kWarps * 32, l.smem, s>>>(pos4, n, t, p, inv_box,
-                                                                            o, queue, spill, err);
+    k_walk<PERIODIC, SPLIT, QUAD, POT><<<l.blocks, kWarps * 32, l.smem, s>>>(
+        pos4, n, t, g.gstart, g.ngroups, p, inv_box, o, queue, spill, err);
 }
 
 template <bool PERIODIC, bool SPLIT>
-void dispatch_qp(const float4* pos4, int n, const TreeArrays& t, const WalkParams& p,
-                 const WalkOutputs& o, unsigned* queue, int* spill, int* err, cudaStream_t s)
+void dispatch_qp(const float4* pos4, int n, const TreeArrays& t, const GroupTable& g,
+                 const WalkParams& p, const WalkOutputs& o, unsigned* queue, int* spill, int* err,
+                 cudaStream_t s)
 {
     if (p.quadrupole) {
         if (p.want_pot)
-            launch_variant<PERIODIC, SPLIT, true, true>(pos4, n, t, p, o, queue, spill, err, s);
+            launch_variant<PERIODIC, SPLIT, true, true>(pos4, n, t, g, p, o, queue, spill, err, s);
         else
-            launch_variant<PERIODIC, SPLIT, true, false>(pos4, n, t, p, o, queue, spill, err, s);
+            launch_variant<PERIODIC, SPLIT, true, false>(pos4, n, t, g, p, o, queue, spill, err, s);
     } else {
         if (p.want_pot)
-            launch_variant<PERIODIC, SPLIT, false, true>(pos4, n, t, p, o, queue, spill, err, s);
+            launch_variant<PERIODIC, SPLIT, false, true>(pos4, n, t, g, p, o, queue, spill, err, s);
         else
-            launch_variant<PERIODIC, SPLIT, false, false>(pos4, n, t, p, o, queue, spill, err, s);
+            launch_variant<PERIODIC, SPLIT, false, false>(pos4, n, t, g, p, o, queue, spill, err, s);
     }
 }
 
@@ -888,21 +893,22 @@ int walk_spill_slots()
 }
 size_t walk_spill_entries() { return static_cast<size_t>(kSpill); }
 
-void launch_walk(const float4* pos4, int n, const TreeArrays& t, const WalkParams& p,
-                 const WalkOutputs& o, unsigned* queue, int* spill, int* err, cudaStream_t s)
+void launch_walk(const float4* pos4, int n, const TreeArrays& t, const GroupTable& g,
+                 const WalkParams& p, const WalkOutputs& o, unsigned* queue, int* spill, int* err,
+                 cudaStream_t s)
 {
     const bool periodic = p.box > 0.0f;
     const bool split = p.rsplit > 0.0f;
     if (periodic) {
         if (split)
-            dispatch_qp<true, true>(pos4, n, t, p, o, queue, spill, err, s);
+            dispatch_qp<true, true>(pos4, n, t, g, p, o, queue, spill, err, s);
         else
-            dispatch_qp<true, false>(pos4, n, t, p, o, queue, spill, err, s);
+            dispatch_qp<true, false>(pos4, n, t, g, p, o, queue, spill, err, s);
     } else {
         if (split)
-            dispatch_qp<false, true>(pos4, n, t, p, o, queue, spill, err, s);
+            dispatch_qp<false, true>(pos4, n, t, g, p, o, queue, spill, err, s);
         else
-            dispatch_qp<false, false>(pos4, n, t, p, o, queue, spill, err, s);
+            dispatch_qp<false, false>(pos4, n, t, g, p, o, queue, spill, err, s);
     }
 }
 

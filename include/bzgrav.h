@@ -112,6 +112,13 @@ bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps);
  * TpmTreeForce.inl:142-159).  pot may be NULL. */
 bz_status bz_accelerations(bz_handle* h, float* acc_soa3, float* pot);
 
+/* FP64 diagnostics of the current state, replacing the reference's sampled energy
+ * (engine/physics/thermal/energy/ThmEnergyGpu.inl:77,
+ * engine/server/simulation/telemetry/SrvSnapshotAndEnergy.cpp:321-349) with
+ * full sums: kinetic = sum m v^2 / 2, potential = sum m phi / 2 (runs one potential-evaluating
+ * force pass; octree solver only), momentum3 = sum m v.  Any output may be NULL. */
+bz_status bz_energy(bz_handle* h, double* kinetic, double* potential, double* momentum3);
+
 /* Download the state in the caller's particle order (ParticleSystem::syncHostState /
  * getParticles, PhyParticleSystem.hpp:351,377).  vel may be NULL.  _f64 returns FP64 state. */
 bz_status bz_get_state(bz_handle* h, float* pos_soa3, float* vel_soa3);

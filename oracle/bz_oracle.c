@@ -869,14 +869,89 @@ static void walk_node(walk_ctx* w, int32_t k)
         walk_node(w, c);
 }
 
+/* Target groups cut from the tree (the CUDA rule of blitzar_b200/csrc/bz_groups.cu): a split
+ * node packs its children, in order, into runs of at most gmax particles; a child above gmax,
+ * or a "sparse" child, is split in turn; a split leaf is cut into chunks of gmax (above gmax)
+ * or single particles (sparse).  A node of at most gmax particles is sparse when its tight box
+ * is wider than 0.5 x its distance from the root centre of mass (the root never is).  A root
+ * with at most gmax particles is one group.  Writes the group starts in sorted order followed
+ * by the end sentinel; returns the group count. */
+typedef struct {
+    const int32_t *start, *count, *child, *nchild;
+    const float *bmin3, *bmax3;
+    float com[3];
+    int32_t gmax;
+    int64_t* gstart;
+    int64_t ng;
+} group_ctx;
+
+static int node_sparse(const group_ctx* g, int32_t k)
+{
+    if (k == 0)
+        return 0;
+    const float* lo = g->bmin3 + 3 * (int64_t)k;
+    const float* hi = g->bmax3 + 3 * (int64_t)k;
+    float e = 0.0f, d2 = 0.0f;
+    for (int a = 0; a < 3; ++a) {
+        const float ex = hi[a] - lo[a];
+        e = ex > e ? ex : e;
+    }
+    float dd[3];
+    for (int a = 0; a < 3; ++a) {
+        float v = lo[a] - g->com[a];
+        const float w = g->com[a] - hi[a];
+        v = w > v ? w : v;
+        dd[a] = v > 0.0f ? v : 0.0f;
+    }
+    d2 = (dd[0] * dd[0] + dd[1] * dd[1]) + dd[2] * dd[2];
+    return e > 0.5f * sqrtf(d2);
+}
+
+static void groups_visit(group_ctx* g, int32_t k)
+{
+    if (g->nchild[k] == 0) {
+        const int32_t step = g->count[k] > g->gmax ? g->gmax : 1;
+        for (int32_t i = 0; i < g->count[k]; i += step)
+            g->gstart[g->ng++] = g->start[k] + i;
+        return;
+    }
+    int32_t run = 0;
+    for (int32_t c = g->child[k]; c < g->child[k] + g->nchild[k]; ++c) {
+        if (g->count[c] > g->gmax || node_sparse(g, c)) {
+            run = 0;
+            groups_visit(g, c);
+            continue;
+        }
+        if (run == 0 || run + g->count[c] > g->gmax) {
+            g->gstart[g->ng++] = g->start[c];
+            run = 0;
+        }
+        run += g->count[c];
+    }
+}
+
+int64_t or_tree_groups(const int32_t* start, const int32_t* count, const int32_t* child,
+                       const int32_t* nchild, const float* bmin3, const float* bmax3,
+                       const float* mono4, int32_t gmax, int64_t* gstart)
+{
+    group_ctx g = {start, count, child, nchild, bmin3, bmax3, {mono4[0], mono4[1], mono4[2]},
+                   gmax, gstart, 0};
+    if (count[0] <= gmax)
+        gstart[g.ng++] = start[0];
+    else
+        groups_visit(&g, 0);
+    gstart[g.ng] = start[0] + count[0];
+    return g.ng;
+}
+
 void or_walk(const float* pos4, int64_t n, const int32_t* start, const int32_t* count,
              const int32_t* child, const int32_t* nchild, const float* mono4,
              const float* bmin3, const float* bmax3, const float* quad6,
-             const or_walk_params* prm, double* acc3, double* pot, int64_t* n_pp,
-             int64_t* n_pn)
+             const or_walk_params* prm, const int64_t* gstart, int64_t ngroups, double* acc3,
+             double* pot, int64_t* n_pp, int64_t* n_pn)
 {
     const int G = prm->group > 0 ? prm->group : 32;
-    const int64_t ng = (n + G - 1) / G;
+    const int64_t ng = gstart ? ngroups : (n + G - 1) / G;
 #pragma omp parallel for schedule(dynamic, 4)
     for (int64_t g = 0; g < ng; ++g) {
         walk_ctx w;
@@ -891,8 +966,13 @@ void or_walk(const float* pos4, int64_t n, const int32_t* start, const int32_t* 
         w.child = child;
         w.nchild = nchild;
         w.prm = prm;
-        w.g0 = g * G;
-        w.g1 = w.g0 + G < n ? w.g0 + G : n;
+        if (gstart) {
+            w.g0 = gstart[g];
+            w.g1 = gstart[g + 1];
+        } else {
+            w.g0 = g * G;
+            w.g1 = w.g0 + G < n ? w.g0 + G : n;
+        }
         for (int a = 0; a < 3; ++a) {
             w.gmin[a] = FLT_MAX;
             w.gmax[a] = -FLT_MAX;

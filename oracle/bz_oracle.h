@@ -59,11 +59,16 @@ typedef struct {
     float max_node_size; /* > 0: nodes with extent >= this are never accepted */
 } or_walk_params;
 
+int64_t or_tree_groups(const int32_t* start, const int32_t* count, const int32_t* child,
+                       const int32_t* nchild, const float* bmin3, const float* bmax3,
+                       const float* mono4, int32_t gmax, int64_t* gstart);
+/* gstart == NULL: fixed groups of prm->group consecutive targets; else ngroups tree groups
+ * given by or_tree_groups. */
 void or_walk(const float* pos4, int64_t n, const int32_t* start, const int32_t* count,
              const int32_t* child, const int32_t* nchild, const float* mono4,
              const float* bmin3, const float* bmax3, const float* quad6,
-             const or_walk_params* prm, double* acc3, double* pot, int64_t* n_pp,
-             int64_t* n_pn);
+             const or_walk_params* prm, const int64_t* gstart, int64_t ngroups, double* acc3,
+             double* pot, int64_t* n_pp, int64_t* n_pn);
 
 /* ---- direct sums --------------------------------------------------------------------- */
 void or_direct_f64(const float* pos4, int64_t n, const int64_t* targets, int64_t nt,

@@ -61,9 +61,12 @@ def lib():
                                     _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _f32p, _f32p,
                                     _f32p, _f32p]
         L.or_build_tree.restype = C.c_int64
+        L.or_tree_groups.argtypes = [_i32p, _i32p, _i32p, _i32p, _f32p, _f32p, _f32p, C.c_int32,
+                                     _i64p]
+        L.or_tree_groups.restype = C.c_int64
         L.or_walk.argtypes = [_f32p, C.c_int64, _i32p, _i32p, _i32p, _i32p, _f32p, _f32p,
-                              _f32p, _f32p, C.POINTER(WalkParams), _f64p, C.c_void_p, _i64p,
-                              _i64p]
+                              _f32p, _f32p, C.POINTER(WalkParams), C.c_void_p, C.c_int64, _f64p,
+                              C.c_void_p, _i64p, _i64p]
         L.or_direct_f64.argtypes = [_f32p, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
                                     C.c_double, C.c_double, C.c_double, _f64p, C.c_void_p]
         L.or_ewald_f64.argtypes = [_f32p, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
@@ -209,24 +212,46 @@ def build_tree(sorted_keys, sorted_pos4, leaf_cap=16, max_level=21):
     return t
 
 
+def tree_groups(tree, gmax=32):
+    """Group start indices (plus the end sentinel) cut from the tree, the engine's rule."""
+    n = int(tree["count"][0])
+    g = np.zeros(n + 2, np.int64)
+    ng = lib().or_tree_groups(tree["start"], tree["count"], tree["child"], tree["nchild"],
+                              np.ascontiguousarray(tree["bmin"].reshape(-1)),
+                              np.ascontiguousarray(tree["bmax"].reshape(-1)),
+                              np.ascontiguousarray(tree["mono"].reshape(-1)), gmax, g)
+    return g[: ng + 1].copy()
+
+
 def walk(sorted_pos4, tree, theta=0.5, eps=0.01, rcut=0.0, box=0.0, rsplit=0.0,
-         min_dist2=1e-12, quadrupole=True, group=32, want_pot=False, max_node_size=0.0):
+         min_dist2=1e-12, quadrupole=True, group=None, want_pot=False, max_node_size=0.0):
+    """Group walk.  group=None: groups cut from the tree (as the engine does); an integer:
+    fixed groups of that many consecutive sorted targets."""
     n = len(sorted_pos4)
     prm = WalkParams(np.float32(theta) * np.float32(theta), np.float32(eps) * np.float32(eps),
                      np.float32(rcut) * np.float32(rcut), box, rsplit, min_dist2,
-                     1 if quadrupole else 0, group, max_node_size)
+                     1 if quadrupole else 0, group or 32, max_node_size)
     acc = np.zeros(3 * n, np.float64)
     pot = np.zeros(n, np.float64) if want_pot else None
-    ng = (n + group - 1) // group
+    if group is None:
+        gstart = tree_groups(tree)
+        ng = len(gstart) - 1
+    else:
+        gstart = np.arange(0, n + group, group, dtype=np.int64)
+        gstart[-1] = n
+        gstart = gstart[: (n + group - 1) // group + 1]
+        ng = len(gstart) - 1
     npp = np.zeros(ng, np.int64)
     npn = np.zeros(ng, np.int64)
     lib().or_walk(np.ascontiguousarray(sorted_pos4, np.float32), n, tree["start"], tree["count"],
                   tree["child"], tree["nchild"], np.ascontiguousarray(tree["mono"].reshape(-1)),
                   np.ascontiguousarray(tree["bmin"].reshape(-1)),
                   np.ascontiguousarray(tree["bmax"].reshape(-1)),
-                  np.ascontiguousarray(tree["quad"].reshape(-1)), C.byref(prm), acc,
-                  pot.ctypes.data if pot is not None else None, npp, npn)
-    out = dict(acc=acc.reshape(n, 3), n_pp=npp, n_pn=npn)
+                  np.ascontiguousarray(tree["quad"].reshape(-1)), C.byref(prm),
+                  gstart.ctypes.data, ng, acc, pot.ctypes.data if pot is not None else None,
+                  npp, npn)
+    out = dict(acc=acc.reshape(n, 3), n_pp=npp, n_pn=npn, gstart=gstart,
+               group_sizes=np.diff(gstart))
     if pot is not None:
         out["pot"] = pot
     return out

@@ -78,3 +78,40 @@ def test_periodic_wrap_and_momentum(gpu):
     assert p.min() >= 0.0 and p.max() < 1.0
     mom = (v * m[:, None]).sum(0)
     assert np.abs(mom).max() < 1e-4 * np.abs(v).mean()
+
+
+def test_energy_diagnostics_match_oracle(gpu, oracle):
+    """bz_energy: FP64 kinetic energy and momentum equal the host sums of the same state;
+    the potential energy equals the oracle's direct sum within the walk's multipole error."""
+    from blitzar_b200 import ics
+
+    n = 8192
+    pos, vel, m = ics.plummer(n, seed=3)
+    m = m.astype(np.float32)
+    with _engine(n, octree_theta=0.3) as e:
+        e.set_state(pos, vel, m, f64=True)
+        ke, pe, mom = e.energy()
+        p, v = e.get_state(f64=True)
+    md = m.astype(np.float64)
+    assert abs(ke - 0.5 * (md * (v ** 2).sum(1)).sum()) < 1e-12 * abs(ke)
+    assert np.allclose(mom, (md[:, None] * v).sum(0), rtol=0, atol=1e-12)
+    _, phi = oracle.direct(oracle.pos4(pos.astype(np.float32), m), None, eps=0.01, want_pot=True)
+    pe_ref = 0.5 * (md * phi).sum()
+    assert abs(pe - pe_ref) < 2e-4 * abs(pe_ref)
+    assert -1.6 < 2 * ke / pe < -0.4  # near virial equilibrium: 2T / W = -1 for the Plummer DF
+
+
+def test_energy_drift_is_small(gpu):
+    """A leapfrog run of a Plummer sphere conserves total energy to well below 1e-3."""
+    from blitzar_b200 import ics
+
+    n = 16384
+    pos, vel, m = ics.plummer(n, seed=5)
+    with _engine(n, octree_softening=0.01) as e:
+        e.set_state(pos, vel, m.astype(np.float32), f64=True)
+        k0, w0, p0 = e.energy()
+        e.step(1e-3, 200)
+        k1, w1, p1 = e.energy()
+    e0, e1 = k0 + w0, k1 + w1
+    assert abs(e1 - e0) < 5e-4 * abs(e0)
+    assert np.abs(p1 - p0).max() < 1e-4 * np.sqrt(2 * k0 * m.sum())

@@ -82,8 +82,7 @@ def test_walk_matches_oracle_open(gpu, oracle, quad, theta):
     err = _rel(acc.astype(np.float64), oacc)
     assert err.max() < 1e-5, err.max()
     # identical interaction lists: the device counters equal the oracle's
-    ng = (n + 31) // 32
-    sizes = np.minimum(32, n - 32 * np.arange(ng))
+    sizes = w["group_sizes"]
     assert npp == int((w["n_pp"] * sizes).sum())
     assert npn == int((w["n_pn"] * sizes).sum())
 

@@ -134,7 +134,6 @@ def test_node_size_cap_matches_oracle(gpu, oracle):
     t = oracle.build_tree(keys[perm], p4[perm], leaf_cap=16)
     w = oracle.walk(p4[perm], t, theta=0.5, eps=eps, rcut=np.float32(5.0) * rs, box=1.0, rsplit=rs,
                     max_node_size=np.float32(1.5) * rs)
-    ng = (n + 31) // 32
-    sizes = np.minimum(32, n - 32 * np.arange(ng))
+    sizes = w["group_sizes"]
     assert npp == int((w["n_pp"] * sizes).sum())
     assert npn == int((w["n_pn"] * sizes).sum())

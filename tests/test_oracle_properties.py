@@ -109,3 +109,26 @@ def test_split_kernel_identity(oracle):
     assert abs(oracle.split_weight(1e-9, 1.0) - 1.0) < 1e-12
     assert abs(oracle.split_weight(4.5, 1.0) - 0.0175329) < 1e-6
     assert oracle.split_weight(10.0, 1.0) < 1e-10
+
+
+def test_tree_groups_cover_and_stay_compact(oracle):
+    """Walk groups cut from the tree: they tile [0, n) in order, hold at most 32 targets, and
+    each lies inside one node's box (its box is never larger than the parent node of the run)."""
+    from blitzar_b200 import ics
+
+    pos, _, m = ics.hernquist(20000, 9)
+    m = m.astype(np.float32)
+    sk, sp4, _, t = _tree(oracle, pos.astype(np.float32), m)
+    g = oracle.tree_groups(t)
+    sizes = np.diff(g)
+    assert g[0] == 0 and g[-1] == len(m)
+    assert sizes.min() >= 1 and sizes.max() <= 32
+    fixed = np.arange(0, len(m), 32)
+    # fixed chunks straddle sparse branches: the largest tree group box is far smaller
+    ext = lambda a, b: float((sp4[a:b, :3].max(0) - sp4[a:b, :3].min(0)).max())
+    worst_tree = max(ext(a, b) for a, b in zip(g[:-1], g[1:]))
+    worst_fixed = max(ext(a, min(a + 32, len(m))) for a in fixed)
+    assert worst_tree < 0.5 * worst_fixed
+    # a root of at most 32 particles is a single group
+    sk2, sp42, _, t2 = _tree(oracle, pos[:20].astype(np.float32), m[:20])
+    assert list(oracle.tree_groups(t2)) == [0, 20]
