@@ -25,7 +25,7 @@ EXPORTS = (
     "bz_reference_tree", "bz_interaction_counts", "bz_enable_phase_timing", "bz_phase_times",
     "bz_force_errors", "bz_pm_mesh", "bz_particle_count", "bz_device_bytes", "bz_last_error",
     "bz_status_string", "bz_version", "bz_kernel_launches", "bz_launches_per_step",
-    "bz_sort_pairs_noalloc", "bz_energy",
+    "bz_sort_pairs_noalloc", "bz_energy", "bz_autotune",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -57,6 +57,7 @@ class BzConfig(C.Structure):
         ("device", C.c_int32),
         ("stream", C.c_uint64),
         ("use_graph", C.c_int32),
+        ("walk_group_size", C.c_int32),
     ]
 
 
@@ -108,6 +109,7 @@ def load():
     L.bz_kernel_launches.restype = C.c_uint64
     L.bz_launches_per_step.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_energy.argtypes = [_vp, _vp, _vp, _vp]
+    L.bz_autotune.argtypes = [_vp, C.c_int32, _vp, _vp, _vp]
     L.bz_sort_pairs_noalloc.argtypes = [_vp, _vp, C.c_int64, C.c_int, C.c_uint64]
     _LIB = L
     return L
@@ -207,6 +209,15 @@ class Engine:
         self._check(self.L.bz_accelerations(self.h, _ptr(a), _ptr(p)), "bz_accelerations")
         acc = a.reshape(3, self.n).T.copy()
         return (acc, p) if want_pot else acc
+
+    def autotune(self, trials=3):
+        """Pick the fastest (leaf capacity, walk group size) for the current state."""
+        leaf = C.c_int32(0)
+        grp = C.c_int32(0)
+        ms = C.c_float(0.0)
+        self._check(self.L.bz_autotune(self.h, trials, C.byref(leaf), C.byref(grp), C.byref(ms)),
+                    "bz_autotune")
+        return leaf.value, grp.value, ms.value
 
     def energy(self, potential=True):
         """FP64 (kinetic, potential or None, momentum[3]) of the current state."""

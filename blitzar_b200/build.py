@@ -18,6 +18,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(ROOT, "_build")
 LIB = os.path.join(HERE, "libbzgrav.so")
+HEADLESS = os.path.join(HERE, "bz_headless")  # C++ headless driver (links libbzgrav.so)
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
@@ -77,6 +78,16 @@ def build(force: bool = False, verbose: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError("link failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
+    host_src = os.path.join(HERE, "host", "bz_headless.cpp")
+    host_hdr = os.path.join(HERE, "host", "bz_particle_system.hpp")
+    if force or _stale(HEADLESS, [host_src, host_hdr, LIB, os.path.join(ROOT, "include", "bzgrav.h")]):
+        cxx = shutil.which("g++") or "g++"
+        cmd = [cxx, "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"),
+               "-I", os.path.join(HERE, "host"), host_src, "-L", HERE, "-lbzgrav",
+               "-Wl,-rpath,$ORIGIN", "-o", HEADLESS]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("headless driver build failed:\n" + " ".join(cmd) + "\n" + r.stdout + r.stderr)
     return LIB
 
 

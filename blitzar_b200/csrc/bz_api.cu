@@ -179,7 +179,7 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
     record(h, kPhTree);
     launch_tree_build(d.keys, d.pos4, n, h->cfg.leaf_capacity, kMaxLevels, h->tree, d.err,
                       h->stream);
-    launch_groups(h->tree, n, h->groups, h->stream);
+    launch_groups(h->tree, n, h->cfg.walk_group_size, h->groups, h->stream);
     record(h, kPhMesh);
     if (h->cfg.solver == BZ_SOLVER_TREEPM && h->pm) {
         pm_forces(h->pm, d.pos4, n, d.acc[0], d.acc[1], d.acc[2], h->stream);
@@ -405,6 +405,7 @@ bz_status bz_config_init(bz_config* c)
     c->device = 0;
     c->stream = 0;
     c->use_graph = 1;
+    c->walk_group_size = kGroupMax;
     return BZ_OK;
 }
 
@@ -463,7 +464,8 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
             return BZ_INVALID_ARGUMENT;
         }
     }
-    if (cfg->leaf_capacity < 1 || cfg->octree_theta <= 0.0f) {
+    if (cfg->leaf_capacity < 1 || cfg->octree_theta <= 0.0f || cfg->walk_group_size < 1 ||
+        cfg->walk_group_size > kGroupMax) {
         delete h;
         return BZ_INVALID_ARGUMENT;
     }
@@ -916,6 +918,76 @@ bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps)
         return s;
     collect_timing(h);
     read_counters(h);
+    return BZ_OK;
+}
+
+bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int32_t* group_size,
+                      float* ms_per_evaluation)
+{
+    if (!h || h->n == 0 || trials < 1)
+        return BZ_INVALID_ARGUMENT;
+    if (h->cfg.solver == BZ_SOLVER_OCTREE_REFERENCE)
+        return fail(h, BZ_UNSUPPORTED, "the reference formulation has nothing to tune");
+    cudaSetDevice(h->device);
+    static const int kLeaf[] = {8, 12, 16, 24, 32, 48};
+    static const int kGroup[] = {16, 24, 32};
+    const int leaf0 = h->cfg.leaf_capacity, group0 = h->cfg.walk_group_size;
+    const bool timing0 = h->timing;
+    h->timing = false;
+    h->stepping = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = -1.0f;
+    int best_leaf = leaf0, best_group = group0;
+    bz_status st = BZ_OK;
+    for (int leaf : kLeaf) {
+        for (int group : kGroup) {
+            h->cfg.leaf_capacity = leaf;
+            h->cfg.walk_group_size = group;
+            enqueue_order(h);  // warm-up evaluation with these parameters
+            enqueue_forces(h, false, false);
+            cudaEventRecord(e0, h->stream);
+            for (int r = 0; r < trials; ++r) {
+                enqueue_order(h);
+                enqueue_forces(h, false, false);
+            }
+            cudaEventRecord(e1, h->stream);
+            st = check_device(h, "bz_autotune");
+            if (st != BZ_OK)
+                break;
+            float ms = 0.0f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            ms /= static_cast<float>(trials);
+            if (best < 0.0f || ms < best) {
+                best = ms;
+                best_leaf = leaf;
+                best_group = group;
+            }
+        }
+        if (st != BZ_OK)
+            break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    h->timing = timing0;
+    h->cfg.leaf_capacity = st == BZ_OK ? best_leaf : leaf0;
+    h->cfg.walk_group_size = st == BZ_OK ? best_group : group0;
+    // the captured step holds the old parameters: capture again on the next bz_step
+    for (int i = 0; i < 2; ++i) {
+        if (h->graph[i])
+            cudaGraphExecDestroy(h->graph[i]);
+        h->graph[i] = nullptr;
+    }
+    h->forces_valid = false;
+    if (st != BZ_OK)
+        return st;
+    if (leaf_capacity)
+        *leaf_capacity = best_leaf;
+    if (group_size)
+        *group_size = best_group;
+    if (ms_per_evaluation)
+        *ms_per_evaluation = best;
     return BZ_OK;
 }
 

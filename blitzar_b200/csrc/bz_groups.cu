@@ -1,16 +1,16 @@
 // Target groups for the group walk, cut from the octree.
 //
-// A group is at most kGroupMax (one warp) consecutive sorted particles that the walk treats
+// A group is at most gmax <= kGroupMax (one warp) consecutive sorted particles that the walk treats
 // as one target box.  Fixed chunks of 32 consecutive Morton-ordered particles can straddle
 // distant branches where the particles are sparse, and such a group's box (hence its list of
 // opened nodes) grows without bound.  Groups are instead runs of consecutive sibling subtrees:
-// for every node holding more than kGroupMax particles, its children are visited in order;
-// a child with more than kGroupMax particles forms its own groups (recursively), and the
-// other children are packed greedily into runs of at most kGroupMax particles.  A small child
+// for every node holding more than gmax particles, its children are visited in order;
+// a child with more than gmax particles forms its own groups (recursively), and the
+// other children are packed greedily into runs of at most gmax particles.  A small child
 // whose particles are spread wide compared with its distance from the system's centre of mass
 // ("sparse", below) is cut further in the same way, down to single particles.  A leaf above
-// the limit (possible only at the depth limit) is cut into chunks of kGroupMax.  A root with
-// at most kGroupMax particles is one group.  Every group is thus a contiguous particle range
+// the limit (possible only at the depth limit) is cut into chunks of gmax.  A root with
+// at most gmax particles is one group.  Every group is thus a contiguous particle range
 // inside one node's box, and groups come out in sorted (Morton) order.
 //
 // Construction is one flag per group start (written by the node that owns the run) followed
@@ -29,7 +29,7 @@ constexpr int kChunk = kThreads * kItems;  // flags per compaction block
 
 constexpr float kSparseRatio = 0.5f;
 
-// A node with at most kGroupMax particles is "sparse" when its tight box is wider than
+// A node with at most gmax particles is "sparse" when its tight box is wider than
 // kSparseRatio times its distance from the system's centre of mass (root COM): its particles
 // are spread over a region comparable to its distance from the bulk of the mass, and one box
 // around all of them would make the walk open almost the whole tree.  The root is never
@@ -50,14 +50,14 @@ __device__ __forceinline__ bool node_sparse(const TreeArrays& t, int k, float cx
 }
 
 // A node is split (its particles do not all share one group) when it holds more than
-// kGroupMax particles, or when it is sparse and its parent is split.
-__device__ bool node_split(const TreeArrays& t, int k, float cx, float cy, float cz)
+// gmax particles, or when it is sparse and its parent is split.
+__device__ bool node_split(const TreeArrays& t, int k, int gmax, float cx, float cy, float cz)
 {
     // climb while the node is small: it is split only if every node up to the first large
     // ancestor is sparse
     int j = k;
     for (int guard = 0; guard <= kMaxLevels + 1; ++guard) {
-        if (t.count[j] > kGroupMax)
+        if (t.count[j] > gmax)
             return true;
         if (!node_sparse(t, j, cx, cy, cz))
             return false;
@@ -68,7 +68,8 @@ __device__ bool node_split(const TreeArrays& t, int k, float cx, float cy, float
     return false;
 }
 
-__global__ void __launch_bounds__(kThreads) k_group_flags(TreeArrays t, int n, int* __restrict__ flag)
+__global__ void __launch_bounds__(kThreads) k_group_flags(TreeArrays t, int n, int gmax,
+                                                           int* __restrict__ flag)
 {
     const int nodes = *t.n_nodes;
     const float4 com = t.mono[0];
@@ -76,15 +77,15 @@ __global__ void __launch_bounds__(kThreads) k_group_flags(TreeArrays t, int n, i
         const int cnt = t.count[k];
         const int st = t.start[k];
         const int nch = t.nchild[k];
-        if (k == 0 && cnt <= kGroupMax) {
+        if (k == 0 && cnt <= gmax) {
             flag[st] = 1;  // a small system is one group
             continue;
         }
-        if (!node_split(t, k, com.x, com.y, com.z))
+        if (!node_split(t, k, gmax, com.x, com.y, com.z))
             continue;
         if (nch == 0) {
-            // a split leaf: chunks of kGroupMax, or single particles when sparse
-            const int step = cnt > kGroupMax ? kGroupMax : 1;
+            // a split leaf: chunks of gmax, or single particles when sparse
+            const int step = cnt > gmax ? gmax : 1;
             for (int i = 0; i < cnt; i += step)
                 flag[st + i] = 1;
             continue;
@@ -93,11 +94,11 @@ __global__ void __launch_bounds__(kThreads) k_group_flags(TreeArrays t, int n, i
         int run = 0;
         for (int c = c0; c < c0 + nch; ++c) {
             const int cc = t.count[c];
-            if (cc > kGroupMax || node_sparse(t, c, com.x, com.y, com.z)) {
+            if (cc > gmax || node_sparse(t, c, com.x, com.y, com.z)) {
                 run = 0;  // the child cuts its own groups
                 continue;
             }
-            if (run == 0 || run + cc > kGroupMax) {
+            if (run == 0 || run + cc > gmax) {
                 flag[t.start[c]] = 1;
                 run = 0;
             }
@@ -209,14 +210,15 @@ int sms_now()
 
 int group_count_blocks(int n) { return (n + kChunk - 1) / kChunk > 0 ? (n + kChunk - 1) / kChunk : 1; }
 
-void launch_groups(const TreeArrays& t, int n, GroupTable& g, cudaStream_t s)
+void launch_groups(const TreeArrays& t, int n, int gmax, GroupTable& g, cudaStream_t s)
 {
+    gmax = gmax < 1 ? 1 : (gmax > kGroupMax ? kGroupMax : gmax);
     cudaMemsetAsync(g.flag, 0, sizeof(int) * static_cast<size_t>(n), s);
     const int sms = sms_now();
     int fb = (t.cap + kThreads - 1) / kThreads;
     fb = fb < 8 * sms ? fb : 8 * sms;
     count_launch();
-    k_group_flags<<<fb > 0 ? fb : 1, kThreads, 0, s>>>(t, n, g.flag);
+    k_group_flags<<<fb > 0 ? fb : 1, kThreads, 0, s>>>(t, n, gmax, g.flag);
     const int blocks = group_count_blocks(n);
     count_launch();
     k_flag_count<<<blocks, kThreads, 0, s>>>(g.flag, n, g.block_sums);

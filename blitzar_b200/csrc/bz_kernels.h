@@ -97,7 +97,7 @@ struct WalkParams {
     int want_pot;
 };
 // ---------------------------------------------------------------- target groups (bz_groups.cu)
-constexpr int kGroupMax = 32;  // particles per walk group (one warp)
+constexpr int kGroupMax = 32;  // largest walk group (one warp)
 struct GroupTable {
     int* flag;        // [n] group-start flags
     int* gstart;      // [n + 1] group start indices in sorted order, then the end sentinel
@@ -105,7 +105,7 @@ struct GroupTable {
     int* block_sums;  // [group_count_blocks(n)]
 };
 int group_count_blocks(int n);
-void launch_groups(const TreeArrays& t, int n, GroupTable& g, cudaStream_t s);
+void launch_groups(const TreeArrays& t, int n, int gmax, GroupTable& g, cudaStream_t s);
 
 struct WalkOutputs {
     float* ax;        // accumulated into (+=)

@@ -1,0 +1,173 @@
+// C++ host adapter over the libbzgrav C ABI with the calls of the reference's ParticleSystem
+// (engine/physics/core/particle/PhyParticleSystem.hpp:109-718): construction from a particle
+// list, the solver setters, update(dt) and the host-state export.  Header-only; links
+// against libbzgrav.so.  Errors follow the reference convention: calls return false and the
+// message is kept (lastError()), no exceptions on the stepping path.
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "bzgrav.h"
+
+namespace bzhost {
+
+// One particle as the reference's Particle carries it for gravity and export
+// (engine/physics/core/particle/PhyParticle.hpp:25-183: position, velocity, mass,
+// temperature).
+struct Particle {
+    float px = 0, py = 0, pz = 0;
+    float vx = 0, vy = 0, vz = 0;
+    float mass = 0;
+    float temperature = 0;
+};
+
+class GravitySystem {
+public:
+    enum class SolverMode { OctreeGpu, TreePm, OctreeReference };
+
+    explicit GravitySystem(std::vector<Particle> particles) : particles_(std::move(particles))
+    {
+        bz_config_init(&cfg_);
+    }
+    ~GravitySystem() { release(); }
+    GravitySystem(const GravitySystem&) = delete;
+    GravitySystem& operator=(const GravitySystem&) = delete;
+
+    // setters of PhyParticleSystem.hpp:187-252; they take effect at the next update()
+    void setSolverMode(SolverMode m)
+    {
+        cfg_.solver = m == SolverMode::TreePm ? BZ_SOLVER_TREEPM
+                      : m == SolverMode::OctreeReference ? BZ_SOLVER_OCTREE_REFERENCE
+                                                          : BZ_SOLVER_OCTREE;
+        invalidate();
+    }
+    void setOctreeTheta(float theta) { cfg_.octree_theta = theta; invalidate(); }
+    void setOctreeSoftening(float eps) { cfg_.octree_softening = eps; invalidate(); }
+    void setOctreeOpeningCriterion(int c) { cfg_.octree_opening_criterion = c; invalidate(); }
+    void setLinearOctreeLeafCapacity(int cap) { cfg_.linear_octree_leaf_capacity = cap; invalidate(); }
+    void setLeafCapacity(int cap) { cfg_.leaf_capacity = cap; invalidate(); }
+    void setMultipoleOrder(int order) { cfg_.multipole_order = order; invalidate(); }
+    void setPhysicsStabilityConstants(float max_acceleration, float min_softening,
+                                      float min_distance2, float min_theta)
+    {
+        cfg_.physics_max_acceleration = max_acceleration;
+        cfg_.physics_min_softening = min_softening;
+        cfg_.physics_min_distance2 = min_distance2;
+        cfg_.physics_min_theta = min_theta;
+        invalidate();
+    }
+    // the periodic TreePM subset of setTreePmParameters (PhyParticleSystem.hpp:204-208)
+    void setTreePmParameters(int grid_size, float r_split_cells, float r_cut_factor,
+                             int assignment, int gradient, double box_length)
+    {
+        cfg_.treepm_grid_size = grid_size;
+        cfg_.treepm_r_split_cells = r_split_cells;
+        cfg_.treepm_r_cut_factor = r_cut_factor;
+        cfg_.treepm_assignment = assignment;
+        cfg_.treepm_gradient = gradient;
+        cfg_.treepm_window_floor = gradient == 1 ? 0.0f : 0.08f;
+        cfg_.box_length = box_length;
+        invalidate();
+    }
+    void setTreePmNodeSizeFactor(float f) { cfg_.treepm_node_size_factor = f; invalidate(); }
+    void setDevice(int device) { cfg_.device = device; invalidate(); }
+    bz_config& config() { return cfg_; }
+
+    // ParticleSystem::update(dt): one leapfrog step (PhyParticleSystem.hpp:163)
+    bool update(float dt) { return step(dt, 1); }
+    bool step(double dt, uint32_t nsteps)
+    {
+        if (!ensure())
+            return false;
+        return check(bz_step(h_, dt, nsteps));
+    }
+    // syncHostState(): copy the device state into particles() (PhyParticleSystem.hpp:351)
+    bool syncHostState()
+    {
+        if (!h_)
+            return true;  // never uploaded: the host copy is current
+        const size_t n = particles_.size();
+        std::vector<float> p(3 * n), v(3 * n);
+        if (!check(bz_get_state(h_, p.data(), v.data())))
+            return false;
+        for (size_t i = 0; i < n; ++i) {
+            Particle& q = particles_[i];
+            q.px = p[i], q.py = p[n + i], q.pz = p[2 * n + i];
+            q.vx = v[i], q.vy = v[n + i], q.vz = v[2 * n + i];
+        }
+        return true;
+    }
+    const std::vector<Particle>& getParticles() const { return particles_; }
+    bool accelerations(std::vector<float>& acc_soa3)
+    {
+        if (!ensure())
+            return false;
+        acc_soa3.resize(3 * particles_.size());
+        return check(bz_accelerations(h_, acc_soa3.data(), nullptr));
+    }
+    bool energy(double& kinetic, double& potential, double momentum[3])
+    {
+        if (!ensure())
+            return false;
+        return check(bz_energy(h_, &kinetic, &potential, momentum));
+    }
+    const std::string& lastError() const { return err_; }
+
+private:
+    void invalidate()
+    {
+        if (h_) {
+            syncHostState();
+            release();
+        }
+    }
+    void release()
+    {
+        if (h_)
+            bz_destroy(h_);
+        h_ = nullptr;
+    }
+    bool ensure()
+    {
+        if (h_)
+            return true;
+        const size_t n = particles_.size();
+        if (n == 0)
+            return fail("no particles");
+        if (bz_create(&cfg_, n, &h_) != BZ_OK) {
+            h_ = nullptr;
+            return fail("[bz] engine creation failed (configuration or device memory)");
+        }
+        std::vector<float> p(3 * n), v(3 * n), m(n);
+        for (size_t i = 0; i < n; ++i) {
+            const Particle& q = particles_[i];
+            p[i] = q.px, p[n + i] = q.py, p[2 * n + i] = q.pz;
+            v[i] = q.vx, v[n + i] = q.vy, v[2 * n + i] = q.vz;
+            m[i] = q.mass;
+        }
+        return check(bz_set_state(h_, p.data(), v.data(), m.data(), n));
+    }
+    bool check(bz_status s)
+    {
+        if (s == BZ_OK)
+            return true;
+        char buf[1024] = {0};
+        if (h_)
+            bz_last_error(h_, buf, sizeof buf);
+        return fail(std::string("[bz] ") + bz_status_string(s) + (buf[0] ? ": " : "") + buf);
+    }
+    bool fail(const std::string& m)
+    {
+        err_ = m;
+        return false;
+    }
+
+    std::vector<Particle> particles_;
+    bz_config cfg_{};
+    bz_handle* h_ = nullptr;
+    std::string err_;
+};
+
+} // namespace bzhost

@@ -76,6 +76,7 @@ typedef struct bz_config {
     int32_t device;                /* CUDA device ordinal */
     uint64_t stream;               /* cudaStream_t to run on, or 0 for a private stream */
     int32_t use_graph;             /* capture bz_step's per-step work in a CUDA graph */
+    int32_t walk_group_size;       /* targets per walk group, 1..32 (default 32; bz_autotune) */
 } bz_config;
 
 typedef struct bz_handle bz_handle;
@@ -105,6 +106,13 @@ bz_status bz_set_state_f64(bz_handle* h, const double* pos_soa3, const double* v
  * CudOctreeGpuIntegrators.inl:121-195).  The force at the end of a step is reused at the
  * start of the next, so each step evaluates the force once. */
 bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps);
+
+/* Autotuner (no counterpart in the reference, whose leaf capacity and launch shapes are fixed
+ * settings): times `trials` force evaluations of the current state for each leaf capacity in
+ * {8, 12, 16, 24, 32, 48} and walk group size in {16, 24, 32}, keeps the fastest pair in the
+ * handle's configuration and reports it.  The state is not advanced.  Outputs may be NULL. */
+bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int32_t* group_size,
+                      float* ms_per_evaluation);
 
 /* Accelerations (and optionally potentials) of the current state, caller's particle order,
  * SoA 3n floats.  Replaces computeOctreeAccelerationKernel (engine/physics/octree/cuda/force/

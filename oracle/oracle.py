@@ -224,9 +224,10 @@ def tree_groups(tree, gmax=32):
 
 
 def walk(sorted_pos4, tree, theta=0.5, eps=0.01, rcut=0.0, box=0.0, rsplit=0.0,
-         min_dist2=1e-12, quadrupole=True, group=None, want_pot=False, max_node_size=0.0):
-    """Group walk.  group=None: groups cut from the tree (as the engine does); an integer:
-    fixed groups of that many consecutive sorted targets."""
+         min_dist2=1e-12, quadrupole=True, group=None, want_pot=False, max_node_size=0.0,
+         gmax=32):
+    """Group walk.  group=None: groups of at most gmax targets cut from the tree (as the
+    engine does); an integer: fixed groups of that many consecutive sorted targets."""
     n = len(sorted_pos4)
     prm = WalkParams(np.float32(theta) * np.float32(theta), np.float32(eps) * np.float32(eps),
                      np.float32(rcut) * np.float32(rcut), box, rsplit, min_dist2,
@@ -234,7 +235,7 @@ def walk(sorted_pos4, tree, theta=0.5, eps=0.01, rcut=0.0, box=0.0, rsplit=0.0,
     acc = np.zeros(3 * n, np.float64)
     pot = np.zeros(n, np.float64) if want_pot else None
     if group is None:
-        gstart = tree_groups(tree)
+        gstart = tree_groups(tree, gmax)
         ng = len(gstart) - 1
     else:
         gstart = np.arange(0, n + group, group, dtype=np.int64)

@@ -115,3 +115,33 @@ def test_energy_drift_is_small(gpu):
     e0, e1 = k0 + w0, k1 + w1
     assert abs(e1 - e0) < 5e-4 * abs(e0)
     assert np.abs(p1 - p0).max() < 1e-4 * np.sqrt(2 * k0 * m.sum())
+
+
+def test_headless_driver_matches_engine(gpu, tmp_path):
+    """The C++ headless driver (reference config + NBSIMBIN in, NBSIMBIN out) steps exactly as
+    the engine driven through ctypes does."""
+    import subprocess
+
+    from blitzar_b200 import build as b
+    from blitzar_b200 import ics, snapshot
+
+    n = 4096
+    pos, vel, m = ics.plummer(n, seed=8)
+    pos, vel, m = pos.astype(np.float32), vel.astype(np.float32), m.astype(np.float32)
+    snapshot.write_bin(tmp_path / "in.bin", pos, vel, m)
+    (tmp_path / "sim.ini").write_text(
+        "simulation(dt=0.001, solver=octree_gpu, integrator=leapfrog)\n"
+        "octree(theta=0.6, softening=0.02)\n"
+        f"input_file={tmp_path / 'in.bin'}\n")
+    r = subprocess.run([b.HEADLESS, "--config", str(tmp_path / "sim.ini"), "--run",
+                        "--target-steps", "10", "--export-format", "bin", "--export-path",
+                        str(tmp_path / "out.bin")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert "[headless] done steps=10" in r.stdout
+    p_h, v_h, m_h, _ = snapshot.read_bin(tmp_path / "out.bin")
+    with _engine(n, octree_theta=0.6, octree_softening=0.02) as e:
+        e.set_state(pos, vel, m)
+        e.step(1e-3, 10)
+        p_e, v_e = e.get_state()
+    assert np.array_equal(p_h, p_e.astype(np.float32)) and np.array_equal(v_h, v_e.astype(np.float32))
+    assert np.array_equal(m_h, m)

@@ -128,3 +128,41 @@ def test_reference_mode_forces_and_topology(gpu, oracle):
     oacc = oracle.ref_walk(pos, m, o, theta=0.5, softening=0.01)
     err = _rel(acc.astype(np.float64), oacc)
     assert err.max() < 1e-5, err.max()
+
+
+@pytest.mark.parametrize("gsize", [16, 24])
+def test_walk_group_size_matches_oracle(gpu, oracle, gsize):
+    """Smaller walk groups (an autotuner choice) follow the same tree-cut rule as the oracle."""
+    n = 20_000
+    pos = plummer(n, seed=23)
+    m = np.full(n, 1.0 / n, np.float32)
+    with _engine(n, octree_theta=0.5, octree_softening=0.01, walk_group_size=gsize) as e:
+        e.set_state(pos, None, m)
+        acc = e.accelerations()
+        npp, npn = e.interaction_counts()
+    sk, sp4, perm = _sorted_inputs(oracle, pos, m)
+    o = oracle.build_tree(sk, sp4, leaf_cap=16)
+    w = oracle.walk(sp4, o, theta=0.5, eps=0.01, gmax=gsize)
+    oacc = np.empty_like(w["acc"])
+    oacc[perm] = w["acc"]
+    assert _rel(acc.astype(np.float64), oacc).max() < 1e-5
+    assert w["group_sizes"].max() <= gsize
+    assert npp == int((w["n_pp"] * w["group_sizes"]).sum())
+    assert npn == int((w["n_pn"] * w["group_sizes"]).sum())
+
+
+def test_autotune_picks_a_candidate_and_keeps_accuracy(gpu, oracle):
+    n = 40_000
+    pos = plummer(n, seed=24)
+    m = np.full(n, 1.0 / n, np.float32)
+    with _engine(n, octree_theta=0.5, octree_softening=0.01) as e:
+        e.set_state(pos, None, m)
+        leaf, grp, ms = e.autotune(trials=2)
+        assert leaf in (8, 12, 16, 24, 32, 48) and grp in (16, 24, 32) and ms > 0
+        acc = e.accelerations()
+        e.step(1e-3, 3)  # the step graph is captured again with the tuned parameters
+        p, _ = e.get_state(f64=True)
+    assert np.isfinite(p).all()
+    tg = np.arange(0, n, 13)
+    ref = oracle.direct(oracle.pos4(pos, m), tg, eps=0.01)
+    assert np.median(_rel(acc[tg].astype(np.float64), ref)) < 2e-3

@@ -91,3 +91,60 @@ def test_ic_generators():
     assert r.max() <= 100.0
     pos, vel, m = ics.king(3000, 5, 6.0)
     assert np.isfinite(vel).all() and abs(m.sum() - 1.0) < 1e-12
+
+
+def _headless():
+    from blitzar_b200 import build as b
+
+    if not os.path.exists(b.HEADLESS):
+        b.build()
+    return b.HEADLESS
+
+
+def test_headless_resolves_reference_config(tmp_path):
+    """The C++ headless driver reads the reference's directive config (and flat keys) into the
+    engine configuration without touching a GPU."""
+    import json
+    import subprocess
+
+    cfg = tmp_path / "sim.ini"
+    cfg.write_text(
+        "# directive form\n"
+        "simulation(particle_count=3073, dt=0.002, solver=octree_gpu, integrator=leapfrog)\n"
+        "octree(theta=0.7, softening=0.05, criterion=com, leaf_capacity=256)\n"
+        "physics(max_acceleration=64, min_softening=0.0001, min_distance2=1e-12, min_theta=0.05)\n"
+        "treepm(enabled=true, assignment=pcs, grid_size=64, gradient=spectral)\n"
+        "input_file=state.bin\n")
+    out = subprocess.run([_headless(), "--config", str(cfg), "--dry-run"], capture_output=True,
+                         text=True, check=True).stdout
+    d = json.loads(out)
+    assert d["solver"] == 1 and d["treepm_grid_size"] == 64 and d["treepm_assignment"] == 2
+    assert d["treepm_gradient"] == 1 and d["dt"] == 0.002 and d["box_length"] == 1.0
+    assert abs(d["octree_theta"] - 0.7) < 1e-7 and abs(d["physics_max_acceleration"] - 64) < 1e-6
+    assert d["input"] == "state.bin"
+    bad = tmp_path / "bad.ini"
+    bad.write_text("simulation(solver=octree_gpu, integrator=euler)\n")
+    r = subprocess.run([_headless(), "--config", str(bad), "--dry-run"], capture_output=True, text=True)
+    assert r.returncode == 2 and "leapfrog" in r.stderr
+    bad.write_text("solver=pairwise_cuda\n")
+    r = subprocess.run([_headless(), "--config", str(bad), "--dry-run"], capture_output=True, text=True)
+    assert r.returncode == 2 and "not provided" in r.stderr
+
+
+def test_headless_snapshot_conversion_matches_python(tmp_path):
+    """C++ and Python writers agree byte for byte on .bin and .xyz."""
+    import subprocess
+
+    from blitzar_b200 import snapshot
+
+    rng = np.random.default_rng(3)
+    pos = (rng.standard_normal((257, 3)) * 10).astype(np.float32)
+    vel = rng.standard_normal((257, 3)).astype(np.float32)
+    m = rng.random(257).astype(np.float32)
+    src = tmp_path / "a.bin"
+    snapshot.write_bin(src, pos, vel, m)
+    subprocess.run([_headless(), "--convert", str(src), str(tmp_path / "b.bin")], check=True)
+    assert (tmp_path / "b.bin").read_bytes() == src.read_bytes()
+    subprocess.run([_headless(), "--convert", str(src), str(tmp_path / "c.xyz")], check=True)
+    snapshot.write_xyz(tmp_path / "d.xyz", pos, m, solver="octree_gpu", integrator="leapfrog", step=0)
+    assert (tmp_path / "c.xyz").read_text() == (tmp_path / "d.xyz").read_text()
