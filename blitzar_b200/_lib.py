@@ -25,7 +25,8 @@ EXPORTS = (
     "bz_reference_tree", "bz_interaction_counts", "bz_enable_phase_timing", "bz_phase_times",
     "bz_force_errors", "bz_pm_mesh", "bz_particle_count", "bz_device_bytes", "bz_last_error",
     "bz_status_string", "bz_version", "bz_kernel_launches", "bz_launches_per_step",
-    "bz_sort_pairs_noalloc", "bz_energy", "bz_autotune",
+    "bz_sort_pairs_noalloc", "bz_energy", "bz_autotune", "bz_learn_generate", "bz_learn_train",
+    "bz_learn_set", "bz_learn_get", "bz_learn_enable", "bz_learn_forward", "bz_learn_gradient",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -110,6 +111,14 @@ def load():
     L.bz_launches_per_step.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_energy.argtypes = [_vp, _vp, _vp, _vp]
     L.bz_autotune.argtypes = [_vp, C.c_int32, _vp, _vp, _vp]
+    L.bz_learn_generate.argtypes = [_vp, C.c_int64, C.c_uint64, _vp, _vp]
+    L.bz_learn_train.argtypes = [_vp, _vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_float,
+                                 C.c_uint64, _vp]
+    L.bz_learn_set.argtypes = [_vp, _vp, C.c_float]
+    L.bz_learn_get.argtypes = [_vp, _vp, _vp]
+    L.bz_learn_enable.argtypes = [_vp, C.c_int32]
+    L.bz_learn_forward.argtypes = [_vp, _vp, C.c_int64, _vp]
+    L.bz_learn_gradient.argtypes = [_vp, _vp, _vp, C.c_int64, _vp, _vp]
     L.bz_sort_pairs_noalloc.argtypes = [_vp, _vp, C.c_int64, C.c_int, C.c_uint64]
     _LIB = L
     return L
@@ -209,6 +218,51 @@ class Engine:
         self._check(self.L.bz_accelerations(self.h, _ptr(a), _ptr(p)), "bz_accelerations")
         acc = a.reshape(3, self.n).T.copy()
         return (acc, p) if want_pot else acc
+
+    # ---- learned pair correction
+    MLP_PARAMS = 1667
+
+    def learn_generate(self, nsamples, seed=1):
+        x = np.empty((nsamples, 6), np.float32)
+        y = np.empty((nsamples, 3), np.float32)
+        self._check(self.L.bz_learn_generate(self.h, nsamples, seed, _ptr(x), _ptr(y)), "bz_learn_generate")
+        return x, y
+
+    def learn_train(self, x, y, steps=3000, batch=4096, lr=3e-3, seed=1):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        loss = C.c_float(0.0)
+        self._check(self.L.bz_learn_train(self.h, _ptr(x), _ptr(y), len(x), steps, batch, lr, seed,
+                                          C.byref(loss)), "bz_learn_train")
+        return loss.value
+
+    def learn_set(self, params, scale):
+        p = np.ascontiguousarray(params, np.float32)
+        self._check(self.L.bz_learn_set(self.h, _ptr(p), scale), "bz_learn_set")
+
+    def learn_get(self):
+        p = np.empty(self.MLP_PARAMS, np.float32)
+        sc = C.c_float(0.0)
+        self._check(self.L.bz_learn_get(self.h, _ptr(p), C.byref(sc)), "bz_learn_get")
+        return p, sc.value
+
+    def learn_enable(self, on=True):
+        self._check(self.L.bz_learn_enable(self.h, 1 if on else 0), "bz_learn_enable")
+
+    def learn_forward(self, x):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.empty((len(x), 3), np.float32)
+        self._check(self.L.bz_learn_forward(self.h, _ptr(x), len(x), _ptr(y)), "bz_learn_forward")
+        return y
+
+    def learn_gradient(self, x, y):
+        x = np.ascontiguousarray(x, np.float32)
+        y = np.ascontiguousarray(y, np.float32)
+        g = np.empty(self.MLP_PARAMS, np.float32)
+        loss = C.c_float(0.0)
+        self._check(self.L.bz_learn_gradient(self.h, _ptr(x), _ptr(y), len(x), _ptr(g), C.byref(loss)),
+                    "bz_learn_gradient")
+        return g, loss.value
 
     def autotune(self, trials=3):
         """Pick the fastest (leaf capacity, walk group size) for the current state."""

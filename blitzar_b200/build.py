@@ -28,6 +28,7 @@ SOURCES = {
     "bz_sort.cu": [],
     "bz_tree.cu": ["--fmad=false"],
     "bz_groups.cu": [],
+    "bz_mlp.cu": [],
     "bz_walk.cu": [],
     "bz_pm.cu": [],
     "bz_state.cu": [],

@@ -87,6 +87,19 @@ struct bz_handle {
     double* h_dt = nullptr;  // pinned {dt, dt/2}
     unsigned long long last_pp = 0, last_pn = 0;
     bool ref_tree_valid = false;
+    // learned pair correction (TreePM)
+    struct {
+        float* params = nullptr;  // FP32 master weights [kMlpParams]
+        float* grad = nullptr;
+        float* adam_m = nullptr;
+        float* adam_v = nullptr;
+        float* loss = nullptr;
+        float scale = 0.0f;       // the network predicts residual / scale
+        bool trained = false;
+        bool enabled = false;
+        int* pair_src = nullptr;  // [capacity * kPairSlots]
+        int* pair_cnt = nullptr;  // [capacity]
+    } learn;
 };
 
 namespace {
@@ -197,8 +210,20 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
     o.az = d.acc[2];
     o.pot = want_pot ? d.pot : nullptr;
     o.totals = d.counters;
-    launch_walk(d.pos4, n, h->tree, h->groups, walk_params(h, want_pot), o, d.queue, d.spill,
-                d.err, h->stream);
+    WalkParams wp = walk_params(h, want_pot);
+    const bool learned = h->learn.enabled && h->learn.trained && h->cfg.solver == BZ_SOLVER_TREEPM;
+    if (learned) {
+        o.pair_src = h->learn.pair_src;
+        o.pair_cnt = h->learn.pair_cnt;
+        wp.rcorr2 = wp.rcut2;
+    }
+    launch_walk(d.pos4, n, h->tree, h->groups, wp, o, d.queue, d.spill, d.err, h->stream);
+    if (learned) {
+        const float hcell = static_cast<float>(h->cfg.box_length / h->cfg.treepm_grid_size);
+        launch_mlp_pairs(h->learn.params, d.pos4, n, h->learn.pair_src, h->learn.pair_cnt, hcell,
+                         static_cast<float>(h->cfg.box_length), h->learn.scale, d.acc[0], d.acc[1],
+                         d.acc[2], d.err, h->stream);
+    }
     record(h, kPhIntegrate);
     if (kick) {
         double* const* s = d.st[h->cur];
@@ -989,6 +1014,315 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     if (ms_per_evaluation)
         *ms_per_evaluation = best;
     return BZ_OK;
+}
+
+} // extern "C"
+
+namespace {
+
+bool learn_alloc(bz_handle* h)
+{
+    auto& L = h->learn;
+    if (L.params)
+        return true;
+    return dalloc(h, &L.params, kMlpParams) && dalloc(h, &L.grad, kMlpParams) &&
+           dalloc(h, &L.adam_m, kMlpParams) && dalloc(h, &L.adam_v, kMlpParams) &&
+           dalloc(h, &L.loss, 1);
+}
+
+bool learn_pairs_alloc(bz_handle* h)
+{
+    auto& L = h->learn;
+    if (L.pair_src)
+        return true;
+    return dalloc(h, &L.pair_src, h->capacity * static_cast<size_t>(kPairSlots)) &&
+           dalloc(h, &L.pair_cnt, h->capacity);
+}
+
+void drop_graphs(bz_handle* h)
+{
+    for (int i = 0; i < 2; ++i) {
+        if (h->graph[i])
+            cudaGraphExecDestroy(h->graph[i]);
+        h->graph[i] = nullptr;
+    }
+    h->forces_valid = false;
+}
+
+// Xavier-style uniform initialisation of the MLP parameters (seeded)
+std::vector<float> learn_init(uint64_t seed)
+{
+    std::vector<float> p(kMlpParams, 0.0f);
+    std::mt19937_64 rng(seed);
+    auto fill = [&](int off, int rows, int cols) {
+        const float a = std::sqrt(6.0f / static_cast<float>(rows + cols));
+        std::uniform_real_distribution<float> u(-a, a);
+        for (int i = 0; i < rows * cols; ++i)
+            p[off + i] = u(rng);
+    };
+    fill(kMlpOffW1, 32, 16);
+    for (int r = 0; r < 32; ++r)
+        p[kMlpOffW1 + r * 16 + 15] = 0.0f;  // b1
+    fill(kMlpOffW2, 32, 32);
+    fill(kMlpOffW3, 3, 32);
+    return p;
+}
+
+template <class T> struct DevBuf {
+    T* p = nullptr;
+    explicit DevBuf(size_t n) { cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)); }
+    ~DevBuf() { cudaFree(p); }
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+};
+
+} // namespace
+
+extern "C" {
+
+bz_status bz_learn_generate(bz_handle* h, int64_t nsamples, uint64_t seed, float* x6, float* y3)
+{
+    if (!h || nsamples <= 0 || !x6 || !y3)
+        return BZ_INVALID_ARGUMENT;
+    if (h->cfg.solver != BZ_SOLVER_TREEPM || !h->pm)
+        return fail(h, BZ_UNSUPPORTED, "bz_learn_generate: residuals are defined for the periodic TreePM solver");
+    cudaSetDevice(h->device);
+    const int M = h->cfg.treepm_grid_size;
+    const double L = h->cfg.box_length, hc = L / M;
+    const double rs = rsplit_len(h);
+    const double R = h->cfg.treepm_r_cut_factor * h->cfg.treepm_r_split_cells;  // cells
+    // sources on a coarse lattice, far enough apart that each probe's mesh error comes from
+    // its own source; probes uniformly in the ball of radius r_cut around each source
+    int sp = std::max(16, 2 * static_cast<int>(std::ceil(R)) + 8);
+    int per_axis = std::max(1, M / sp);
+    sp = M / per_axis;
+    const int S = per_axis * per_axis * per_axis;
+    const int P = static_cast<int>(std::min<int64_t>(256, (nsamples + S - 1) / S));
+    const int batch = S * P;
+    const int ntot = S + batch;
+    DevBuf<float4> dpos(ntot);
+    DevBuf<float> dacc(3 * static_cast<size_t>(ntot));
+    DevBuf<int> dtg(batch);
+    DevBuf<double> dlr(3 * static_cast<size_t>(batch));
+    const int kmax = 8;
+    DevBuf<double> dsk(5 * static_cast<size_t>(ewald_num_k(kmax)));
+    if (!dpos.p || !dacc.p || !dtg.p || !dlr.p || !dsk.p)
+        return fail(h, BZ_OUT_OF_MEMORY, "bz_learn_generate: temporary buffers");
+    std::vector<int> tg(batch);
+    for (int i = 0; i < batch; ++i)
+        tg[i] = S + i;
+    cudaMemcpyAsync(dtg.p, tg.data(), sizeof(int) * batch, cudaMemcpyHostToDevice, h->stream);
+    std::mt19937_64 rng(seed);
+    std::uniform_real_distribution<double> U(0.0, 1.0);
+    std::normal_distribution<double> G(0.0, 1.0);
+    std::vector<float4> pos(ntot);
+    std::vector<double> off(3 * static_cast<size_t>(S)), sep(3 * static_cast<size_t>(batch));
+    std::vector<float> acc(3 * static_cast<size_t>(ntot));
+    std::vector<double> lr(3 * static_cast<size_t>(batch));
+    int64_t done = 0;
+    while (done < nsamples) {
+        for (int a = 0; a < per_axis; ++a)
+            for (int b = 0; b < per_axis; ++b)
+                for (int c = 0; c < per_axis; ++c) {
+                    const int sidx = (a * per_axis + b) * per_axis + c;
+                    const int cell[3] = {a * sp + sp / 2, b * sp + sp / 2, c * sp + sp / 2};
+                    double q[3];
+                    for (int k = 0; k < 3; ++k) {
+                        off[3 * sidx + k] = U(rng);
+                        q[k] = (cell[k] + off[3 * sidx + k]) * hc;
+                    }
+                    pos[sidx] = make_float4(static_cast<float>(q[0]), static_cast<float>(q[1]),
+                                            static_cast<float>(q[2]), 1.0f);
+                }
+        for (int sidx = 0; sidx < S; ++sidx)
+            for (int j = 0; j < P; ++j) {
+                double u[3], nrm = 0.0;
+                for (int k = 0; k < 3; ++k) {
+                    u[k] = G(rng);
+                    nrm += u[k] * u[k];
+                }
+                nrm = std::sqrt(nrm);
+                const double r = std::max(0.02, R * std::cbrt(U(rng)));
+                const int pi = sidx * P + j;
+                double q[3];
+                const float4 sp4 = pos[sidx];
+                const double sq[3] = {sp4.x, sp4.y, sp4.z};
+                for (int k = 0; k < 3; ++k) {
+                    double v = sq[k] + u[k] / nrm * r * hc;
+                    v -= L * std::floor(v / L);
+                    q[k] = v;
+                }
+                pos[S + pi] = make_float4(static_cast<float>(q[0]), static_cast<float>(q[1]),
+                                          static_cast<float>(q[2]), 0.0f);
+                for (int k = 0; k < 3; ++k) {
+                    double d = static_cast<double>((k == 0 ? pos[S + pi].x : k == 1 ? pos[S + pi].y
+                                                                                     : pos[S + pi].z)) - sq[k];
+                    d -= L * std::nearbyint(d / L);
+                    sep[3 * static_cast<size_t>(pi) + k] = d / hc;
+                }
+            }
+        cudaMemcpyAsync(dpos.p, pos.data(), sizeof(float4) * ntot, cudaMemcpyHostToDevice, h->stream);
+        pm_forces(h->pm, dpos.p, ntot, dacc.p, dacc.p + ntot, dacc.p + 2 * static_cast<size_t>(ntot), h->stream);
+        launch_lr_ideal_f64(dpos.p, S, dtg.p, batch, L, 6.4 / L, kmax, rs, dsk.p, dlr.p, h->stream);
+        cudaMemcpyAsync(acc.data(), dacc.p, sizeof(float) * 3 * static_cast<size_t>(ntot),
+                        cudaMemcpyDeviceToHost, h->stream);
+        cudaMemcpyAsync(lr.data(), dlr.p, sizeof(double) * 3 * static_cast<size_t>(batch),
+                        cudaMemcpyDeviceToHost, h->stream);
+        const bz_status st = check_device(h, "bz_learn_generate");
+        if (st != BZ_OK)
+            return st;
+        const int64_t take = std::min<int64_t>(batch, nsamples - done);
+        for (int64_t i = 0; i < take; ++i) {
+            const int sidx = static_cast<int>(i / P);
+            const int64_t o = done + i;
+            for (int k = 0; k < 3; ++k) {
+                x6[6 * o + k] = static_cast<float>(sep[3 * i + k]);
+                x6[6 * o + 3 + k] = static_cast<float>(off[3 * sidx + k]);
+                const double fpm = acc[static_cast<size_t>(k) * ntot + S + i];
+                y3[3 * o + k] = static_cast<float>((fpm - lr[3 * i + k]) * hc * hc);
+            }
+        }
+        done += take;
+    }
+    return BZ_OK;
+}
+
+bz_status bz_learn_set(bz_handle* h, const float* params, float scale)
+{
+    if (!h || !params || !(scale > 0.0f))
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    if (!learn_alloc(h) || (h->cfg.solver == BZ_SOLVER_TREEPM && !learn_pairs_alloc(h)))
+        return fail(h, BZ_OUT_OF_MEMORY, "bz_learn_set");
+    cudaMemcpyAsync(h->learn.params, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice, h->stream);
+    h->learn.scale = scale;
+    h->learn.trained = true;
+    drop_graphs(h);
+    return check_device(h, "bz_learn_set");
+}
+
+bz_status bz_learn_get(bz_handle* h, float* params, float* scale)
+{
+    if (!h || !params || !h->learn.trained)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    cudaMemcpyAsync(params, h->learn.params, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, h->stream);
+    if (scale)
+        *scale = h->learn.scale;
+    return check_device(h, "bz_learn_get");
+}
+
+bz_status bz_learn_enable(bz_handle* h, int32_t enable)
+{
+    if (!h)
+        return BZ_INVALID_ARGUMENT;
+    if (enable && (!h->learn.trained || h->cfg.solver != BZ_SOLVER_TREEPM))
+        return fail(h, BZ_NOT_READY, "bz_learn_enable: no trained correction for a TreePM handle");
+    h->learn.enabled = enable != 0;
+    drop_graphs(h);
+    return BZ_OK;
+}
+
+bz_status bz_learn_train(bz_handle* h, const float* x6, const float* y3, int64_t n, int32_t steps,
+                         int32_t batch, float lr, uint64_t seed, float* final_loss)
+{
+    if (!h || !x6 || !y3 || n < batch || steps < 1 || batch < 128 || batch % 128 != 0 || !(lr > 0.0f))
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    if (!learn_alloc(h) || (h->cfg.solver == BZ_SOLVER_TREEPM && !learn_pairs_alloc(h)))
+        return fail(h, BZ_OUT_OF_MEMORY, "bz_learn_train");
+    double ss = 0.0;
+    for (int64_t i = 0; i < 3 * n; ++i)
+        ss += static_cast<double>(y3[i]) * y3[i];
+    const float scale = static_cast<float>(std::sqrt(ss / (3.0 * n)));
+    if (!(scale > 0.0f))
+        return fail(h, BZ_INVALID_ARGUMENT, "bz_learn_train: all targets are zero");
+    std::vector<float> yn(3 * static_cast<size_t>(n));
+    for (int64_t i = 0; i < 3 * n; ++i)
+        yn[i] = y3[i] / scale;
+    DevBuf<float> dx(6 * static_cast<size_t>(n)), dy(3 * static_cast<size_t>(n));
+    DevBuf<int> didx(n);
+    if (!dx.p || !dy.p || !didx.p)
+        return fail(h, BZ_OUT_OF_MEMORY, "bz_learn_train: sample buffers");
+    cudaMemcpyAsync(dx.p, x6, sizeof(float) * 6 * n, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(dy.p, yn.data(), sizeof(float) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+    const std::vector<float> p0 = learn_init(seed);
+    cudaMemcpyAsync(h->learn.params, p0.data(), sizeof(float) * kMlpParams, cudaMemcpyHostToDevice, h->stream);
+    cudaMemsetAsync(h->learn.grad, 0, sizeof(float) * kMlpParams, h->stream);
+    cudaMemsetAsync(h->learn.adam_m, 0, sizeof(float) * kMlpParams, h->stream);
+    cudaMemsetAsync(h->learn.adam_v, 0, sizeof(float) * kMlpParams, h->stream);
+    std::vector<int> perm(n);
+    for (int64_t i = 0; i < n; ++i)
+        perm[i] = static_cast<int>(i);
+    std::mt19937_64 rng(seed ^ 0x9e3779b97f4a7c15ull);
+    const int64_t per_epoch = n / batch;
+    const int tail = std::min(steps, 100);
+    for (int st = 0; st < steps; ++st) {
+        const int64_t k = st % per_epoch;
+        if (k == 0) {
+            std::shuffle(perm.begin(), perm.end(), rng);
+            cudaMemcpyAsync(didx.p, perm.data(), sizeof(int) * n, cudaMemcpyHostToDevice, h->stream);
+            // the host vector is reshuffled next epoch: wait for the upload first
+            cudaStreamSynchronize(h->stream);
+        }
+        if (st == steps - tail)
+            cudaMemsetAsync(h->learn.loss, 0, sizeof(float), h->stream);
+        launch_mlp_train_step(h->learn.params, dx.p, dy.p, didx.p + k * batch, batch, h->learn.grad,
+                              h->learn.loss, h->d.err, h->stream);
+        const float lr_t = 0.5f * lr * (1.0f + std::cos(3.14159265f * st / steps));
+        launch_mlp_adam(h->learn.params, h->learn.grad, h->learn.adam_m, h->learn.adam_v, st + 1, lr_t,
+                        h->stream);
+    }
+    float loss = 0.0f;
+    cudaMemcpyAsync(&loss, h->learn.loss, sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    const bz_status s = check_device(h, "bz_learn_train");
+    if (s != BZ_OK)
+        return s;
+    h->learn.scale = scale;
+    h->learn.trained = true;
+    drop_graphs(h);
+    if (final_loss)
+        *final_loss = loss / static_cast<float>(static_cast<int64_t>(tail) * batch * 3);
+    return BZ_OK;
+}
+
+bz_status bz_learn_forward(bz_handle* h, const float* x6, int64_t n, float* y3)
+{
+    if (!h || !x6 || !y3 || n <= 0 || !h->learn.trained)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    DevBuf<float> dx(6 * static_cast<size_t>(n)), dy(3 * static_cast<size_t>(n));
+    if (!dx.p || !dy.p)
+        return fail(h, BZ_OUT_OF_MEMORY, "bz_learn_forward");
+    cudaMemcpyAsync(dx.p, x6, sizeof(float) * 6 * n, cudaMemcpyHostToDevice, h->stream);
+    launch_mlp_forward(h->learn.params, dx.p, static_cast<int>(n), h->learn.scale, dy.p, h->d.err, h->stream);
+    cudaMemcpyAsync(y3, dy.p, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, h->stream);
+    return check_device(h, "bz_learn_forward");
+}
+
+bz_status bz_learn_gradient(bz_handle* h, const float* x6, const float* y3, int64_t n, float* grad,
+                            float* loss)
+{
+    if (!h || !x6 || !y3 || !grad || n <= 0 || !h->learn.trained)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    DevBuf<float> dx(6 * static_cast<size_t>(n)), dy(3 * static_cast<size_t>(n));
+    if (!dx.p || !dy.p)
+        return fail(h, BZ_OUT_OF_MEMORY, "bz_learn_gradient");
+    cudaMemcpyAsync(dx.p, x6, sizeof(float) * 6 * n, cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(dy.p, y3, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, h->stream);
+    cudaMemsetAsync(h->learn.grad, 0, sizeof(float) * kMlpParams, h->stream);
+    cudaMemsetAsync(h->learn.loss, 0, sizeof(float), h->stream);
+    launch_mlp_train_step(h->learn.params, dx.p, dy.p, nullptr, static_cast<int>(n), h->learn.grad,
+                          h->learn.loss, h->d.err, h->stream);
+    cudaMemcpyAsync(grad, h->learn.grad, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, h->stream);
+    float l = 0.0f;
+    cudaMemcpyAsync(&l, h->learn.loss, sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    const bz_status s = check_device(h, "bz_learn_gradient");
+    cudaMemsetAsync(h->learn.grad, 0, sizeof(float) * kMlpParams, h->stream);
+    if (loss)
+        *loss = l / static_cast<float>(n);
+    return s;
 }
 
 bz_status bz_morton_keys(bz_handle* h, uint64_t* sorted_keys, int32_t* perm)

@@ -145,7 +145,77 @@ __global__ void __launch_bounds__(kThreads) k_ewald_target(const float4* __restr
     }
 }
 
+// Ideal long-range (Gaussian-split) force of a periodic set of sources at one target: the
+// Ewald sum with the split's short-range part sum m w_split(r) r^-3 d removed, which leaves
+// the real-space weight w_alpha(r) - w_split(r) (both of the form erfc(r/2s) + r/(s sqrt(pi))
+// e^{-r^2/4s^2}).  Minimum image; the sources are the first n_src particles.
+__global__ void __launch_bounds__(kThreads) k_lr_ideal_target(const float4* __restrict__ pos4,
+                                                               int n_src,
+                                                               const int* __restrict__ targets,
+                                                               double box, double alpha,
+                                                               double rsplit, int nk,
+                                                               const double* __restrict__ sk,
+                                                               double* acc3)
+{
+    __shared__ double sh[kThreads / 32];
+    const int i = targets[blockIdx.x];
+    const float4 me = pos4[i];
+    const double c2 = 2.0 * alpha / sqrt(kPi);
+    const double u2 = 0.5 / rsplit, cs2 = 1.0 / (rsplit * sqrt(kPi));
+    const double inv_box = 1.0 / box;
+    double a[3] = {0, 0, 0};
+    for (int j = threadIdx.x; j < n_src; j += kThreads) {
+        if (j == i)
+            continue;
+        const float4 s = pos4[j];
+        double d[3] = {(double)s.x - me.x, (double)s.y - me.y, (double)s.z - me.z};
+        for (int c = 0; c < 3; ++c)
+            d[c] -= box * rint(d[c] * inv_box);
+        const double s2 = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+        if (s2 <= 0.0)
+            continue;
+        const double sr = sqrt(s2);
+        const double wa = erfc(alpha * sr) + c2 * sr * exp(-alpha * alpha * s2);
+        const double ws = erfc(u2 * sr) + cs2 * sr * exp(-u2 * u2 * s2);
+        const double f = (double)s.w * (wa - ws) / (s2 * sr);
+        a[0] += f * d[0];
+        a[1] += f * d[1];
+        a[2] += f * d[2];
+    }
+    const double V = box * box * box;
+    for (int q = threadIdx.x; q < nk; q += kThreads) {
+        const double kx = sk[5 * q], ky = sk[5 * q + 1], kz = sk[5 * q + 2];
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        const double coef = 2.0 * (4.0 * kPi / V) * exp(-k2 / (4.0 * alpha * alpha)) / k2;
+        double sn, cs;
+        sincos(kx * me.x + ky * me.y + kz * me.z, &sn, &cs);
+        const double im = cs * sk[5 * q + 4] - sn * sk[5 * q + 3];
+        a[0] += coef * im * kx;
+        a[1] += coef * im * ky;
+        a[2] += coef * im * kz;
+    }
+    for (int c = 0; c < 3; ++c) {
+        const double t = block_sum(a[c], sh);
+        if (threadIdx.x == 0)
+            acc3[3 * blockIdx.x + c] = t;
+    }
+}
+
 } // namespace
+
+void launch_lr_ideal_f64(const float4* pos4, int n_src, const int* targets, int nt, double box,
+                         double alpha, int kmax, double rsplit, double* sk_scratch, double* acc3,
+                         cudaStream_t s)
+{
+    const int nk = ewald_num_k(kmax);
+    count_launch();
+    k_ewald_sk<<<nk, kThreads, 0, s>>>(pos4, n_src, kmax, 2.0 * kPi / box, sk_scratch);
+    if (nt > 0) {
+        count_launch();
+        k_lr_ideal_target<<<nt, kThreads, 0, s>>>(pos4, n_src, targets, box, alpha, rsplit, nk,
+                                                   sk_scratch, acc3);
+    }
+}
 
 int ewald_num_k(int kmax)
 {

@@ -95,6 +95,7 @@ struct WalkParams {
     float max_node_size;  // > 0: nodes at least this large are never accepted as multipoles
     int quadrupole;
     int want_pot;
+    float rcorr2;     // > 0 with WalkOutputs.pair_src: record the pairs closer than this
 };
 // ---------------------------------------------------------------- target groups (bz_groups.cu)
 constexpr int kGroupMax = 32;  // largest walk group (one warp)
@@ -115,6 +116,8 @@ struct WalkOutputs {
     unsigned long long* n_pp;  // optional per-group counters
     unsigned long long* n_pn;
     unsigned long long* totals; // optional [2] sums of the above
+    int* pair_src;    // optional [n * kPairSlots]: sorted source index of each recorded pair
+    int* pair_cnt;    // [n]: recorded pairs per target (above kPairSlots raises kErrListCapacity)
 };
 void launch_walk(const float4* pos4, int n, const TreeArrays& t, const GroupTable& g,
                  const WalkParams& p, const WalkOutputs& o, unsigned* queue, int* spill, int* err,
@@ -170,6 +173,25 @@ void launch_scatter3(const float* ax, const float* ay, const float* az, const in
                      float* out_soa3, cudaStream_t s);
 void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s);
 
+// ---------------------------------------------------------------- learned correction (bz_mlp.cu)
+// Parameter block of the 6 -> 32 -> 32 -> 3 MLP (16 features incl. a constant 1 that carries
+// b1): W1[32][16], W2[32][32], b2[32], W3[3][32], b3[3].
+constexpr int kMlpOffW1 = 0;
+constexpr int kMlpOffW2 = kMlpOffW1 + 32 * 16;
+constexpr int kMlpOffB2 = kMlpOffW2 + 32 * 32;
+constexpr int kMlpOffW3 = kMlpOffB2 + 32;
+constexpr int kMlpOffB3 = kMlpOffW3 + 3 * 32;
+constexpr int kMlpParams = kMlpOffB3 + 3;
+constexpr int kPairSlots = 64;  // recorded pairs per target for the correction
+void launch_mlp_train_step(const float* params, const float* in6, const float* y3, const int* index,
+                           int n, float* grad, float* loss, int* err, cudaStream_t s);
+void launch_mlp_adam(float* params, float* grad, float* m, float* v, int step, float lr, cudaStream_t s);
+void launch_mlp_forward(const float* params, const float* in6, int n, float scale, float* out3,
+                        int* err, cudaStream_t s);
+void launch_mlp_pairs(const float* params, const float4* pos4, int n, const int* pair_src,
+                      const int* pair_cnt, float h, float box, float scale, float* ax, float* ay,
+                      float* az, int* err, cudaStream_t s);
+
 // ---------------------------------------------------------------- diagnostics (bz_diag.cu)
 // FP64 reference accelerations for the listed (sorted-order) targets: direct sum (open) or
 // Ewald (periodic).
@@ -179,5 +201,10 @@ void launch_ewald_f64(const float4* pos4, int n, const int* targets, int nt, dou
                       double box, double alpha, int kmax, double* sk_scratch, double* acc3,
                       cudaStream_t s);
 int ewald_num_k(int kmax);
+// Ideal Gaussian long-range force (Ewald with the real-space part of the split kernel removed)
+// at the listed targets from the first n_src particles, which also fill sk_scratch.
+void launch_lr_ideal_f64(const float4* pos4, int n_src, const int* targets, int nt, double box,
+                         double alpha, int kmax, double rsplit, double* sk_scratch, double* acc3,
+                         cudaStream_t s);
 
 } // namespace bz

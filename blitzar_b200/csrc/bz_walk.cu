@@ -47,6 +47,7 @@ struct __align__(16) WarpSmem {
         unsigned mask[kTile / 32][32];  // leaf flush: per-lane in-cutoff bits of the tile
     };
     float2 nd_qb[32];
+    int tidx[kTile];  // sorted index of each tile source (only when pairs are recorded)
     int stack[kStack];
     int nlist[kList];
     int lstart[kList];
@@ -284,8 +285,20 @@ template <bool PERIODIC, bool SPLIT, bool POT>
 __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* __restrict__ pos4,
                                              const TreeArrays& t, const WalkParams& p,
                                              float inv2rs, bool cut, float tx, float ty, float tz,
-                                             int self_index, Acc& acc, uint32_t& phase, int* err)
+                                             int self_index, Acc& acc, uint32_t& phase, int* err,
+                                             const WalkOutputs& o, int pair_row, int& npair)
 {
+    // pairs closer than rcorr are recorded for the learned correction (pair_row < 0: a lane
+    // without a target records nothing)
+    const bool rec = o.pair_src != nullptr && p.rcorr2 > 0.0f;
+    auto record = [&](float4 s4, int gidx) {
+        const float dx = s4.x - tx, dy = s4.y - ty, dz = s4.z - tz;
+        if (pair_row >= 0 && fmaf(dx, dx, fmaf(dy, dy, dz * dz)) <= p.rcorr2) {
+            if (npair < kPairSlots)
+                o.pair_src[static_cast<size_t>(pair_row) * kPairSlots + npair] = gidx;
+            ++npair;
+        }
+    };
     const int lane = threadIdx.x & 31;
     if (cut) {
         // Drop leaves that no target of this warp can reach: a leaf whose (shifted) box is
@@ -379,10 +392,16 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
         for (int j = lane; j < nl; j += 32) {
             const int lo = max(w.lpre[j], cbase);
             const int hi = min(w.lpre[j] + w.lcount[j], cend);
-            if (hi > lo)
+            if (hi > lo) {
                 bulk_g2s(&w.tile[lo - cbase], pos4 + (w.lstart[j] + (lo - w.lpre[j])),
                          static_cast<uint32_t>(hi - lo) * 16u, &w.bar);
+                if (rec)
+                    for (int q = lo; q < hi; ++q)
+                        w.tidx[q - cbase] = w.lstart[j] + (q - w.lpre[j]);
+            }
         }
+        if (rec)
+            __syncwarp();
         mbar_wait_bounded(&w.bar, phase, err);
         phase ^= 1u;
         // Periodic images: move the sources of each shifted leaf into the group's image in
@@ -453,8 +472,10 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                     break;
                 const int b = __ffs(m) - 1;
                 m &= m - 1u;
-                pair_fast<SPLIT>(w.tile[(wd << 5) + b], tx, ty, tz, p.eps2, p.rcut2, false, sk,
-                                 fx, fy, fz);
+                const float4 s4 = w.tile[(wd << 5) + b];
+                pair_fast<SPLIT>(s4, tx, ty, tz, p.eps2, p.rcut2, false, sk, fx, fy, fz);
+                if (rec)
+                    record(s4, w.tidx[(wd << 5) + b]);
             }
             __syncwarp();
             for (int j = jfirst; j < nl; ++j) {
@@ -485,6 +506,8 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                         s4.z = tz + (s4.z - tz - p.box * rintf((s4.z - tz) * inv_box));
                         pair_pp<SPLIT, POT>(s4, tx, ty, tz, p, inv2rs, cut,
                                             POT && gsrc0 + q == self_index, fx, fy, fz, fp);
+                        if (rec)
+                            record(s4, gsrc0 + q);
                     }
                     if (pre + w.lcount[j] <= cend)
                         jfirst = j + 1;
@@ -509,6 +532,9 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                         pair_pp<SPLIT, POT>(w.tile[off + q], tx, ty, tz, p, inv2rs, cut,
                                             POT && gsrc0 + q == self_index, fx, fy, fz, fp);
                 }
+                if (rec)
+                    for (int q2 = 0; q2 < cntp; ++q2)
+                        record(w.tile[off + q2], gsrc0 + q2);
                 if (pre + w.lcount[j] <= cend)
                     jfirst = j + 1;
             }
@@ -582,6 +608,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
         unsigned long long cnt_pp = 0, cnt_pn = 0;
         Acc acc;
         acc.zero();
+        int npair = 0;
         bool bail = false;
         while (top > 0 || gtop > 0) {
             if (top == 0) {  // refill from the spill area (uniform branch)
@@ -713,7 +740,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
             }
             if (nl >= 32 || lp >= kFlushParticles) {
                 flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, t, p, inv2rs, cut, me.x, me.y, me.z,
-                                                   ti, acc, phase, err);
+                                                   ti, acc, phase, err, o, valid ? ti : -1, npair);
                 nl = 0;
                 lp = 0;
             }
@@ -723,7 +750,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                 flush_nodes<PERIODIC, SPLIT, QUAD, POT>(w, nn, t, p, inv2rs, me.x, me.y, me.z, acc);
             if (nl > 0)
                 flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, t, p, inv2rs, cut, me.x, me.y, me.z,
-                                                   ti, acc, phase, err);
+                                                   ti, acc, phase, err, o, valid ? ti : -1, npair);
         }
         if (valid) {
             o.ax[ti] += acc.total(0);
@@ -731,6 +758,11 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
             o.az[ti] += acc.total(2);
             if (POT && o.pot)
                 o.pot[ti] += acc.total(3);
+            if (o.pair_cnt) {
+                o.pair_cnt[ti] = min(npair, kPairSlots);
+                if (npair > kPairSlots)
+                    raise_error(err, kErrListCapacity);
+            }
         }
         if (lane == 0) {
             if (o.n_pp)

@@ -183,6 +183,36 @@ bz_status bz_launches_per_step(bz_handle* h, uint64_t* launches);
 size_t bz_particle_count(const bz_handle* h);
 size_t bz_device_bytes(const bz_handle* h);
 
+/* ---- learned TreePM pair correction (no counterpart in the reference) -----------------
+ * A small MLP (6 -> 32 -> 32 -> 3, SiLU, BF16 weights and activations, FP32 accumulation on
+ * the tensor cores) maps a close pair's separation (target - source, in mesh cells) and the
+ * source's sub-cell offset to the residual of the mesh force of that pair against the ideal
+ * Gaussian long-range force (per unit source mass, times h^2).  With the correction enabled,
+ * every pair inside the short-range cutoff subtracts m_source / h^2 * prediction from its
+ * target's acceleration, which removes most of the mesh's anisotropy error near r_split.
+ *
+ * bz_learn_generate: residual samples produced by the engine itself for this handle's mesh,
+ *   split and assignment: sources on a coarse lattice with random sub-cell offsets, massless
+ *   probes around them, PM force minus the FP64 ideal long-range force (Ewald with the split's
+ *   real-space part removed).  x6 = {sep_x, sep_y, sep_z, off_x, off_y, off_z}, y3 = residual.
+ * bz_learn_train: Adam on the GPU with the library's own forward and backward kernels
+ *   (mean squared error of y3 / rms(y3)); keeps the weights in the handle.
+ * bz_learn_set / bz_learn_get: weights as kMlpParams = 1667 floats (W1[32][16] with b1 in
+ *   column 15, W2[32][32], b2[32], W3[3][32], b3[3]) and the target scale.
+ * bz_learn_enable: apply the correction in bz_step / bz_accelerations (TreePM only).
+ * bz_learn_forward: batch inference (scale applied); bz_learn_gradient: one backward pass
+ *   of the unscaled mean squared error against y3, no update (for gradient checks). */
+#define BZ_MLP_PARAMS 1667
+bz_status bz_learn_generate(bz_handle* h, int64_t nsamples, uint64_t seed, float* x6, float* y3);
+bz_status bz_learn_train(bz_handle* h, const float* x6, const float* y3, int64_t n, int32_t steps,
+                         int32_t batch, float lr, uint64_t seed, float* final_loss);
+bz_status bz_learn_set(bz_handle* h, const float* params, float scale);
+bz_status bz_learn_get(bz_handle* h, float* params, float* scale);
+bz_status bz_learn_enable(bz_handle* h, int32_t enable);
+bz_status bz_learn_forward(bz_handle* h, const float* x6, int64_t n, float* y3);
+bz_status bz_learn_gradient(bz_handle* h, const float* x6, const float* y3, int64_t n, float* grad,
+                            float* loss);
+
 /* Allocation-free stable radix sort of device-resident (key, value) pairs, in place, on the
  * calling thread's current device.  No counterpart in the reference (its sort,
  * thrust::sort_by_key, allocates temporary storage on every call).

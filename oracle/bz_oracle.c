@@ -1373,3 +1373,130 @@ int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rs
     free(sp);
     return 0;
 }
+
+/* ======================================================================================
+ * Learned pair correction: the MLP of blitzar_b200/csrc/bz_mlp.cu restated on the CPU with
+ * the same BF16 rounding points (features, weights, hidden activations and back-propagated
+ * errors are rounded to BF16 before each product; products accumulate in FP64 here, FP32 on
+ * the tensor cores).  Parameter block: W1[32][16] (column 15 = b1), W2[32][32], b2[32],
+ * W3[3][32], b3[3].
+ * ====================================================================================== */
+
+static float bf16_round(float x)
+{
+    uint32_t u;
+    memcpy(&u, &x, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u)
+        return x;
+    u += 0x7fffu + ((u >> 16) & 1u);
+    u &= 0xffff0000u;
+    memcpy(&x, &u, 4);
+    return x;
+}
+
+static void mlp_features(const float* in6, float* f)
+{
+    f[0] = in6[0];
+    f[1] = in6[1];
+    f[2] = in6[2];
+    for (int a = 0; a < 3; ++a) {
+        const double ps = 2.0 * M_PI * (double)in6[3 + a];
+        const double pt = 2.0 * M_PI * ((double)in6[3 + a] + (double)in6[a]);
+        f[3 + a] = (float)sin(ps);
+        f[6 + a] = (float)cos(ps);
+        f[9 + a] = (float)sin(pt);
+        f[12 + a] = (float)cos(pt);
+    }
+    f[15] = 1.0f;
+    for (int i = 0; i < 16; ++i)
+        f[i] = bf16_round(f[i]);
+}
+
+static double sigm(double z) { return 1.0 / (1.0 + exp(-z)); }
+
+/* forward of one sample; keeps the intermediate values for the backward pass */
+static void mlp_fwd1(const float* p, const float* in6, float* f, double* z1, float* h1, double* z2,
+                     float* h2, double* out)
+{
+    mlp_features(in6, f);
+    for (int n = 0; n < 32; ++n) {
+        double a = 0.0;
+        for (int k = 0; k < 16; ++k)
+            a += (double)bf16_round(p[n * 16 + k]) * f[k];
+        z1[n] = (float)a;
+        h1[n] = bf16_round((float)(z1[n] * sigm(z1[n])));
+    }
+    for (int n = 0; n < 32; ++n) {
+        double a = 0.0;
+        for (int k = 0; k < 32; ++k)
+            a += (double)bf16_round(p[512 + n * 32 + k]) * h1[k];
+        z2[n] = (float)a + p[1536 + n];
+        h2[n] = bf16_round((float)(z2[n] * sigm(z2[n])));
+    }
+    for (int o = 0; o < 3; ++o) {
+        double a = 0.0;
+        for (int k = 0; k < 32; ++k)
+            a += (double)bf16_round(p[1568 + o * 32 + k]) * h2[k];
+        out[o] = (float)a + p[1664 + o];
+    }
+}
+
+void or_mlp_forward(const float* params, const float* x6, int64_t n, float scale, float* out3)
+{
+    for (int64_t i = 0; i < n; ++i) {
+        float f[16], h1[32], h2[32];
+        double z1[32], z2[32], out[3];
+        mlp_fwd1(params, x6 + 6 * i, f, z1, h1, z2, h2, out);
+        for (int o = 0; o < 3; ++o)
+            out3[3 * i + o] = (float)(scale * out[o]);
+    }
+}
+
+/* gradient of (1/n) sum_i |out_i - y_i|^2 with respect to the parameter block */
+void or_mlp_grad(const float* params, const float* x6, const float* y3, int64_t n, double* grad,
+                 double* loss)
+{
+    const int np = 1667;
+    for (int i = 0; i < np; ++i)
+        grad[i] = 0.0;
+    double L = 0.0;
+    for (int64_t s = 0; s < n; ++s) {
+        float f[16], h1[32], h2[32];
+        double z1[32], z2[32], out[3];
+        mlp_fwd1(params, x6 + 6 * s, f, z1, h1, z2, h2, out);
+        float dout[3];
+        for (int o = 0; o < 3; ++o) {
+            const double e = (float)out[o] - y3[3 * s + o];
+            L += e * e;
+            dout[o] = bf16_round((float)(2.0 * e / (double)n));
+        }
+        float dz2[32], dz1[32];
+        for (int j = 0; j < 32; ++j) {
+            double a = 0.0;
+            for (int o = 0; o < 3; ++o)
+                a += (double)dout[o] * bf16_round(params[1568 + o * 32 + j]);
+            const double sg = sigm(z2[j]);
+            dz2[j] = bf16_round((float)((float)a * sg * (1.0 + z2[j] * (1.0 - sg))));
+        }
+        for (int j = 0; j < 32; ++j) {
+            double a = 0.0;
+            for (int k = 0; k < 32; ++k)
+                a += (double)dz2[k] * bf16_round(params[512 + k * 32 + j]);
+            const double sg = sigm(z1[j]);
+            dz1[j] = bf16_round((float)((float)a * sg * (1.0 + z1[j] * (1.0 - sg))));
+        }
+        for (int r = 0; r < 32; ++r) {
+            for (int k = 0; k < 16; ++k)
+                grad[r * 16 + k] += (double)dz1[r] * f[k];
+            for (int k = 0; k < 32; ++k)
+                grad[512 + r * 32 + k] += (double)dz2[r] * h1[k];
+            grad[1536 + r] += dz2[r];
+        }
+        for (int o = 0; o < 3; ++o) {
+            for (int k = 0; k < 32; ++k)
+                grad[1568 + o * 32 + k] += (double)dout[o] * h2[k];
+            grad[1664 + o] += dout[o];
+        }
+    }
+    *loss = L / (double)n;
+}

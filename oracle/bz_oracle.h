@@ -85,6 +85,11 @@ int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rs
 /* ---- split kernel helpers ---------------------------------------------------------------- */
 double or_split_weight(double s, double rsplit);
 
+/* ---- learned pair correction (MLP with the engine's BF16 rounding points) ---------- */
+void or_mlp_forward(const float* params, const float* x6, int64_t n, float scale, float* out3);
+void or_mlp_grad(const float* params, const float* x6, const float* y3, int64_t n, double* grad,
+                 double* loss);
+
 #ifdef __cplusplus
 }
 #endif

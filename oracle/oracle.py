@@ -61,6 +61,8 @@ def lib():
                                     _i32p, _i32p, _i32p, _i32p, _i32p, _i32p, _f32p, _f32p,
                                     _f32p, _f32p]
         L.or_build_tree.restype = C.c_int64
+        L.or_mlp_forward.argtypes = [_f32p, _f32p, C.c_int64, C.c_float, _f32p]
+        L.or_mlp_grad.argtypes = [_f32p, _f32p, _f32p, C.c_int64, _f64p, C.POINTER(C.c_double)]
         L.or_tree_groups.argtypes = [_i32p, _i32p, _i32p, _i32p, _f32p, _f32p, _f32p, C.c_int32,
                                      _i64p]
         L.or_tree_groups.restype = C.c_int64
@@ -312,3 +314,20 @@ def fft3d(cube_complex, inverse=False):
 
 def split_weight(s, rsplit):
     return lib().or_split_weight(float(s), float(rsplit))
+
+
+def mlp_forward(params, x6, scale=1.0):
+    """CPU restatement of the learned-correction MLP (same BF16 rounding points)."""
+    x = np.ascontiguousarray(x6, np.float32)
+    out = np.zeros((len(x), 3), np.float32)
+    lib().or_mlp_forward(np.ascontiguousarray(params, np.float32), x, len(x), scale, out)
+    return out
+
+
+def mlp_grad(params, x6, y3):
+    x = np.ascontiguousarray(x6, np.float32)
+    g = np.zeros(1667, np.float64)
+    loss = C.c_double(0.0)
+    lib().or_mlp_grad(np.ascontiguousarray(params, np.float32), x, np.ascontiguousarray(y3, np.float32),
+                      len(x), g, C.byref(loss))
+    return g, loss.value
