@@ -95,6 +95,7 @@ struct bz_handle {
         float* adam_v = nullptr;
         float* loss = nullptr;
         float scale = 0.0f;       // the network predicts residual / scale
+        float radius_cells = 0.0f;  // pairs closer than this (mesh cells) are corrected
         bool trained = false;
         bool enabled = false;
         int* pair_src = nullptr;  // [capacity * kPairSlots]
@@ -135,6 +136,18 @@ bool periodic(const bz_handle* h) { return h->cfg.solver == BZ_SOLVER_TREEPM && 
 float rsplit_len(const bz_handle* h)
 {
     return static_cast<float>(h->cfg.treepm_r_split_cells * h->cfg.box_length / h->cfg.treepm_grid_size);
+}
+
+// Correction radius in mesh cells: the short-range cutoff, capped so that the mean number of
+// neighbours inside it (at the handle's mean particle density) stays at 40 % of the recorded
+// pair slots per target.
+float learn_radius_cells(const bz_handle* h)
+{
+    const double M = h->cfg.treepm_grid_size;
+    const double rho = static_cast<double>(std::max<size_t>(h->n, 1)) / (M * M * M);
+    const double cap = std::cbrt(0.4 * kPairSlots / (4.18879020478639 * rho));
+    const double rc = h->cfg.treepm_r_cut_factor * h->cfg.treepm_r_split_cells;
+    return static_cast<float>(std::min(rc, cap));
 }
 
 void record(bz_handle* h, int i)
@@ -215,7 +228,9 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
     if (learned) {
         o.pair_src = h->learn.pair_src;
         o.pair_cnt = h->learn.pair_cnt;
-        wp.rcorr2 = wp.rcut2;
+        const float rc = (h->learn.radius_cells > 0.0f ? h->learn.radius_cells : learn_radius_cells(h)) *
+                         static_cast<float>(h->cfg.box_length / h->cfg.treepm_grid_size);
+        wp.rcorr2 = std::min(rc * rc, wp.rcut2);
     }
     launch_walk(d.pos4, n, h->tree, h->groups, wp, o, d.queue, d.spill, d.err, h->stream);
     if (learned) {
@@ -1090,7 +1105,8 @@ bz_status bz_learn_generate(bz_handle* h, int64_t nsamples, uint64_t seed, float
     const int M = h->cfg.treepm_grid_size;
     const double L = h->cfg.box_length, hc = L / M;
     const double rs = rsplit_len(h);
-    const double R = h->cfg.treepm_r_cut_factor * h->cfg.treepm_r_split_cells;  // cells
+    const double R = learn_radius_cells(h);  // probe ball radius in cells
+    h->learn.radius_cells = static_cast<float>(R);
     // sources on a coarse lattice, far enough apart that each probe's mesh error comes from
     // its own source; probes uniformly in the ball of radius r_cut around each source
     int sp = std::max(16, 2 * static_cast<int>(std::ceil(R)) + 8);

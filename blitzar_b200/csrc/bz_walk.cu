@@ -444,13 +444,13 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                 const int qb = wd << 5;
                 unsigned m = 0u;
                 if (qb + 32 <= nb) {
-#pragma unroll
-                    for (int b = 0; b < 32; ++b) {
+                    // highest source first, shifting the mask left (short loop body)
+#pragma unroll 8
+                    for (int b = 31; b >= 0; --b) {
                         const float4 s4 = w.tile[qb + b];
                         const float dx = s4.x - tx, dy = s4.y - ty, dz = s4.z - tz;
                         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        if (r2 <= p.rcut2)
-                            m |= 1u << b;
+                        m = (m << 1) | (r2 <= p.rcut2 ? 1u : 0u);
                     }
                 } else {
                     for (int b = 0; qb + b < nb; ++b) {
