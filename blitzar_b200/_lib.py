@@ -27,6 +27,7 @@ EXPORTS = (
     "bz_status_string", "bz_version", "bz_kernel_launches", "bz_launches_per_step",
     "bz_sort_pairs_noalloc", "bz_energy", "bz_autotune", "bz_learn_generate", "bz_learn_train",
     "bz_learn_set", "bz_learn_get", "bz_learn_enable", "bz_learn_forward", "bz_learn_gradient",
+    "bz_set_ensemble",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -111,6 +112,7 @@ def load():
     L.bz_launches_per_step.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_energy.argtypes = [_vp, _vp, _vp, _vp]
     L.bz_autotune.argtypes = [_vp, C.c_int32, _vp, _vp, _vp]
+    L.bz_set_ensemble.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_int32]
     L.bz_learn_generate.argtypes = [_vp, C.c_int64, C.c_uint64, _vp, _vp]
     L.bz_learn_train.argtypes = [_vp, _vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_float,
                                  C.c_uint64, _vp]
@@ -189,6 +191,23 @@ class Engine:
             m = np.ascontiguousarray(mass, np.float32)
             self._check(self.L.bz_set_state(self.h, _ptr(p), _ptr(v), _ptr(m), n), "bz_set_state")
         self.n = n
+
+    def set_ensemble(self, systems):
+        """systems: list of (pos[n,3], vel[n,3] or None, mass[n]) of independent systems."""
+        offs = np.zeros(len(systems) + 1, np.int64)
+        for i, (_, _, m) in enumerate(systems):
+            offs[i + 1] = offs[i] + len(m)
+        n = int(offs[-1])
+        pos = np.concatenate([np.asarray(p, np.float64) for p, _, _ in systems])
+        vel = np.concatenate([np.zeros((len(m), 3)) if v is None else np.asarray(v, np.float64)
+                              for _, v, m in systems])
+        mass = np.concatenate([np.asarray(m, np.float32) for _, _, m in systems])
+        ps = np.ascontiguousarray(pos.T.reshape(-1))
+        vs = np.ascontiguousarray(vel.T.reshape(-1))
+        self._check(self.L.bz_set_ensemble(self.h, _ptr(ps), _ptr(vs), _ptr(mass), _ptr(offs),
+                                           len(systems)), "bz_set_ensemble")
+        self.n = n
+        return offs
 
     def set_state_soa(self, pos_soa3, vel_soa3, mass):
         """Upload from caller-owned SoA float32 buffers (no copies on the Python side)."""

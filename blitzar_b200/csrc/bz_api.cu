@@ -87,6 +87,11 @@ struct bz_handle {
     double* h_dt = nullptr;  // pinned {dt, dt/2}
     unsigned long long last_pp = 0, last_pn = 0;
     bool ref_tree_valid = false;
+    // ensembles of independent systems (0 = one system)
+    int systems = 0;
+    long long* sys_offsets = nullptr;  // [kMaxSystems + 1] caller-index offsets
+    BoxF64* sys_boxes = nullptr;       // [kMaxSystems]
+    std::vector<long long> host_offsets;
     // learned pair correction (TreePM)
     struct {
         float* params = nullptr;  // FP32 master weights [kMlpParams]
@@ -184,10 +189,15 @@ void enqueue_order(bz_handle* h)
     DeviceBuffers& d = h->d;
     double* const* s = d.st[h->cur];
     record(h, kPhKeys);
-    if (!periodic(h))
-        launch_bbox_f64(s[0], s[1], s[2], n, d.box, h->stream);
-    launch_keys63(s[0], s[1], s[2], n, d.box, periodic(h) ? h->cfg.box_length : 0.0, d.keys,
-                  d.perm, h->stream);
+    if (h->systems > 0) {
+        launch_keys_ensemble(s[0], s[1], s[2], d.id[h->cur], n, h->sys_offsets, h->systems,
+                             h->sys_boxes, d.keys, d.perm, h->stream);
+    } else {
+        if (!periodic(h))
+            launch_bbox_f64(s[0], s[1], s[2], n, d.box, h->stream);
+        launch_keys63(s[0], s[1], s[2], n, d.box, periodic(h) ? h->cfg.box_length : 0.0, d.keys,
+                      d.perm, h->stream);
+    }
     record(h, kPhSort);
     launch_radix_sort(d.keys, d.perm, n, 64, h->sort, d.err, h->stream);
     record(h, kPhPermute);
@@ -203,9 +213,10 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
     const int n = static_cast<int>(h->n);
     DeviceBuffers& d = h->d;
     record(h, kPhTree);
+    const int root_level = h->systems > 0 ? kSystemLevels : 0;
     launch_tree_build(d.keys, d.pos4, n, h->cfg.leaf_capacity, kMaxLevels, h->tree, d.err,
-                      h->stream);
-    launch_groups(h->tree, n, h->cfg.walk_group_size, h->groups, h->stream);
+                      h->stream, root_level);
+    launch_groups(h->tree, n, h->cfg.walk_group_size, root_level, d.keys, h->groups, h->stream);
     record(h, kPhMesh);
     if (h->cfg.solver == BZ_SOLVER_TREEPM && h->pm) {
         pm_forces(h->pm, d.pos4, n, d.acc[0], d.acc[1], d.acc[2], h->stream);
@@ -561,6 +572,7 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
          dalloc(h, &t.mono, cap) && dalloc(h, &t.quadA, cap) && dalloc(h, &t.quadB, cap);
     GroupTable& gt = h->groups;
     ok = ok && dalloc(h, &gt.flag, n) && dalloc(h, &gt.gstart, n + 1) && dalloc(h, &gt.ngroups, 1) &&
+         dalloc(h, &gt.groot, n + 1) && dalloc(h, &gt.sysroot, kMaxSystems) &&
          dalloc(h, &gt.block_sums, static_cast<size_t>(group_count_blocks(static_cast<int>(n))));
     // walk spill area: one slot per warp the persistent walk grid can hold
     h->spill_slots = walk_spill_slots();
@@ -692,8 +704,14 @@ __global__ void k_f64_from_f64soa(const double* src, double* dst, int n)
 
 int blocks_for(size_t n) { return static_cast<int>(std::min<size_t>((n + 255) / 256, 148 * 8)); }
 
+void drop_graphs(bz_handle* h);
+
 bz_status upload_common(bz_handle* h, size_t n)
 {
+    if (h->systems > 0) {  // back to a single system: the captured step differs
+        h->systems = 0;
+        drop_graphs(h);
+    }
     h->n = n;
     h->cur = 0;
     h->forces_valid = false;
@@ -767,6 +785,35 @@ bz_status bz_set_state_f64(bz_handle* h, const double* pos, const double* vel, c
         ids[i] = static_cast<int>(i);
     cudaMemcpyAsync(d.id[0], ids.data(), n * sizeof(int), cudaMemcpyHostToDevice, h->stream);
     return check_device(h, "bz_set_state_f64");
+}
+
+bz_status bz_set_ensemble(bz_handle* h, const double* pos, const double* vel, const float* mass,
+                          const int64_t* offsets, int32_t systems)
+{
+    if (!h || !pos || !mass || !offsets || systems < 1 || systems > kMaxSystems)
+        return BZ_INVALID_ARGUMENT;
+    if (h->cfg.solver != BZ_SOLVER_OCTREE)
+        return fail(h, BZ_UNSUPPORTED, "bz_set_ensemble: ensembles run on the octree solver");
+    if (offsets[0] != 0)
+        return fail(h, BZ_INVALID_ARGUMENT, "bz_set_ensemble: offsets[0] must be 0");
+    for (int s = 0; s < systems; ++s)
+        if (offsets[s + 1] <= offsets[s])
+            return fail(h, BZ_INVALID_ARGUMENT, "bz_set_ensemble: every system needs a particle");
+    const size_t n = static_cast<size_t>(offsets[systems]);
+    if (n > h->capacity || n > static_cast<size_t>(INT32_MAX))
+        return BZ_INVALID_ARGUMENT;
+    bz_status st = bz_set_state_f64(h, pos, vel, mass, n);
+    if (st != BZ_OK)
+        return st;
+    if (!h->sys_offsets && (!dalloc(h, &h->sys_offsets, kMaxSystems + 1) ||
+                            !dalloc(h, &h->sys_boxes, kMaxSystems)))
+        return fail(h, BZ_OUT_OF_MEMORY, "bz_set_ensemble");
+    h->host_offsets.assign(offsets, offsets + systems + 1);
+    cudaMemcpyAsync(h->sys_offsets, h->host_offsets.data(), sizeof(long long) * (systems + 1),
+                    cudaMemcpyHostToDevice, h->stream);
+    h->systems = systems;
+    drop_graphs(h);
+    return check_device(h, "bz_set_ensemble");
 }
 
 bz_status bz_get_state(bz_handle* h, float* pos, float* vel)
@@ -1547,7 +1594,36 @@ bz_status bz_force_errors(bz_handle* h, int32_t nsample, uint64_t seed, float* e
     if (per)
         launch_ewald_f64(h->d.pos4, n, dslots, ns, eps, h->cfg.box_length, 6.4 / h->cfg.box_length,
                          kmax, sk, dref, h->stream);
-    else
+    else if (h->systems > 0) {
+        // each target sums over its own system only (systems are contiguous in sorted order)
+        std::vector<int> lo(ns), hi(ns), sys_first(h->systems, n), sys_last(h->systems, 0);
+        auto sys_of = [&](int caller) {
+            return static_cast<int>(std::upper_bound(h->host_offsets.begin(), h->host_offsets.end(),
+                                                     static_cast<long long>(caller)) -
+                                    h->host_offsets.begin()) - 1;
+        };
+        for (int i = 0; i < n; ++i) {
+            const int sy = sys_of(ids[i]);
+            sys_first[sy] = std::min(sys_first[sy], i);
+            sys_last[sy] = std::max(sys_last[sy], i + 1);
+        }
+        for (int i = 0; i < ns; ++i) {
+            const int sy = sys_of(all[i]);
+            lo[i] = sys_first[sy];
+            hi[i] = sys_last[sy];
+        }
+        int* drange = nullptr;
+        if (cudaMalloc(&drange, 2 * ns * sizeof(int)) != cudaSuccess) {
+            cudaFree(dslots);
+            cudaFree(dref);
+            return fail(h, BZ_OUT_OF_MEMORY, "bz_force_errors scratch");
+        }
+        cudaMemcpy(drange, lo.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
+        cudaMemcpy(drange + ns, hi.data(), ns * sizeof(int), cudaMemcpyHostToDevice);
+        launch_direct_f64(h->d.pos4, n, dslots, ns, eps, dref, h->stream, drange, drange + ns);
+        cudaStreamSynchronize(h->stream);
+        cudaFree(drange);
+    } else
         launch_direct_f64(h->d.pos4, n, dslots, ns, eps, dref, h->stream);
     std::vector<double> ref(3 * ns);
     std::vector<float> ax(n), ay(n), az(n);

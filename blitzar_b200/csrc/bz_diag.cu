@@ -30,13 +30,17 @@ __device__ double block_sum(double v, double* sh)
 
 __global__ void __launch_bounds__(kThreads) k_direct_f64(const float4* __restrict__ pos4, int n,
                                                           const int* __restrict__ targets,
+                                                          const int* __restrict__ src_lo,
+                                                          const int* __restrict__ src_hi,
                                                           double eps2, double* acc3)
 {
     __shared__ double sh[kThreads / 32];
     const int i = targets[blockIdx.x];
     const float4 me = pos4[i];
     double a[3] = {0, 0, 0};
-    for (int j = threadIdx.x; j < n; j += kThreads) {
+    const int j0 = src_lo ? src_lo[blockIdx.x] : 0;
+    const int j1 = src_hi ? src_hi[blockIdx.x] : n;
+    for (int j = j0 + threadIdx.x; j < j1; j += kThreads) {
         if (j == i)
             continue;
         const float4 s = pos4[j];
@@ -224,11 +228,11 @@ int ewald_num_k(int kmax)
 }
 
 void launch_direct_f64(const float4* pos4, int n, const int* targets, int nt, double eps,
-                       double* acc3, cudaStream_t s)
+                       double* acc3, cudaStream_t s, const int* src_lo, const int* src_hi)
 {
     if (nt > 0) {
         count_launch();
-        k_direct_f64<<<nt, kThreads, 0, s>>>(pos4, n, targets, eps * eps, acc3);
+        k_direct_f64<<<nt, kThreads, 0, s>>>(pos4, n, targets, src_lo, src_hi, eps * eps, acc3);
     }
 }
 

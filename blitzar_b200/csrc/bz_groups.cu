@@ -29,14 +29,23 @@ constexpr int kChunk = kThreads * kItems;  // flags per compaction block
 
 constexpr float kSparseRatio = 0.5f;
 
-// A node with at most gmax particles is "sparse" when its tight box is wider than
-// kSparseRatio times its distance from the system's centre of mass (root COM): its particles
-// are spread over a region comparable to its distance from the bulk of the mass, and one box
-// around all of them would make the walk open almost the whole tree.  The root is never
-// sparse.  Evaluated with round-to-nearest intrinsics (no contraction), as the oracle does.
-__device__ __forceinline__ bool node_sparse(const TreeArrays& t, int k, float cx, float cy, float cz)
+// The system root of node k: its ancestor at root_level (the tree root when root_level = 0).
+__device__ __forceinline__ int system_root(const TreeArrays& t, int k, int root_level)
 {
-    if (k == 0)
+    for (int guard = 0; guard <= kMaxLevels + 1 && t.level[k] > root_level; ++guard)
+        k = t.parent[k];
+    return k;
+}
+
+// A node with at most gmax particles is "sparse" when its tight box is wider than
+// kSparseRatio times its distance from its system's centre of mass: its particles are spread
+// over a region comparable to their distance from the bulk of the mass, and one box around all
+// of them would make the walk open almost the whole tree.  A system root is never sparse.
+// Evaluated with round-to-nearest intrinsics (no contraction), as the oracle does.
+__device__ __forceinline__ bool node_sparse(const TreeArrays& t, int k, int root_level, float cx,
+                                            float cy, float cz)
+{
+    if (t.level[k] <= root_level)
         return false;
     const float4 b0 = t.box0[k];
     const float4 b1 = t.box1[k];
@@ -49,17 +58,16 @@ __device__ __forceinline__ bool node_sparse(const TreeArrays& t, int k, float cx
     return e > __fmul_rn(kSparseRatio, d);
 }
 
-// A node is split (its particles do not all share one group) when it holds more than
-// gmax particles, or when it is sparse and its parent is split.
-__device__ bool node_split(const TreeArrays& t, int k, int gmax, float cx, float cy, float cz)
+// A node is split (its particles do not all share one group) when it holds more than gmax
+// particles, or when it is sparse and its parent is split.
+__device__ bool node_split(const TreeArrays& t, int k, int gmax, int root_level, float cx, float cy,
+                           float cz)
 {
-    // climb while the node is small: it is split only if every node up to the first large
-    // ancestor is sparse
     int j = k;
     for (int guard = 0; guard <= kMaxLevels + 1; ++guard) {
         if (t.count[j] > gmax)
             return true;
-        if (!node_sparse(t, j, cx, cy, cz))
+        if (!node_sparse(t, j, root_level, cx, cy, cz))
             return false;
         j = t.parent[j];
         if (j < 0)
@@ -69,19 +77,22 @@ __device__ bool node_split(const TreeArrays& t, int k, int gmax, float cx, float
 }
 
 __global__ void __launch_bounds__(kThreads) k_group_flags(TreeArrays t, int n, int gmax,
-                                                           int* __restrict__ flag)
+                                                           int root_level, int* __restrict__ flag)
 {
     const int nodes = *t.n_nodes;
-    const float4 com = t.mono[0];
     for (int k = blockIdx.x * kThreads + threadIdx.x; k < nodes; k += gridDim.x * kThreads) {
+        const int lev = t.level[k];
+        if (lev < root_level)
+            continue;  // above the systems: they cut their own groups
         const int cnt = t.count[k];
         const int st = t.start[k];
         const int nch = t.nchild[k];
-        if (k == 0 && cnt <= gmax) {
+        if (lev == root_level && cnt <= gmax) {
             flag[st] = 1;  // a small system is one group
             continue;
         }
-        if (!node_split(t, k, gmax, com.x, com.y, com.z))
+        const float4 com = t.mono[system_root(t, k, root_level)];
+        if (!node_split(t, k, gmax, root_level, com.x, com.y, com.z))
             continue;
         if (nch == 0) {
             // a split leaf: chunks of gmax, or single particles when sparse
@@ -94,7 +105,7 @@ __global__ void __launch_bounds__(kThreads) k_group_flags(TreeArrays t, int n, i
         int run = 0;
         for (int c = c0; c < c0 + nch; ++c) {
             const int cc = t.count[c];
-            if (cc > gmax || node_sparse(t, c, com.x, com.y, com.z)) {
+            if (cc > gmax || node_sparse(t, c, root_level, com.x, com.y, com.z)) {
                 run = 0;  // the child cuts its own groups
                 continue;
             }
@@ -105,6 +116,16 @@ __global__ void __launch_bounds__(kThreads) k_group_flags(TreeArrays t, int n, i
             run += cc;
         }
     }
+}
+
+// Ensembles: the node of each system's root, by system id (key bits 54..62).
+__global__ void k_system_roots(TreeArrays t, int root_level, const unsigned long long* __restrict__ keys,
+                               int* __restrict__ sysroot)
+{
+    const int nodes = *t.n_nodes;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < nodes; k += gridDim.x * blockDim.x)
+        if (t.level[k] == root_level && t.count[k] > 0)
+            sysroot[static_cast<int>(keys[t.start[k]] >> 54)] = k;
 }
 
 __global__ void __launch_bounds__(kThreads) k_flag_count(const int* __restrict__ flag, int n,
@@ -168,7 +189,10 @@ __global__ void __launch_bounds__(1024) k_flag_scan(int* __restrict__ block_sums
 __global__ void __launch_bounds__(kThreads) k_flag_emit(const int* __restrict__ flag, int n,
                                                          const int* __restrict__ block_offsets,
                                                          const int* __restrict__ ngroups,
-                                                         int* __restrict__ gstart)
+                                                         int* __restrict__ gstart,
+                                                         int* __restrict__ groot,
+                                                         const unsigned long long* __restrict__ keys,
+                                                         const int* __restrict__ sysroot)
 {
     const int base = blockIdx.x * kChunk;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -187,8 +211,10 @@ __global__ void __launch_bounds__(kThreads) k_flag_emit(const int* __restrict__ 
         int before = carry;
         for (int w = 0; w < warp; ++w)
             before += ws[w];
-        if (f)
+        if (f) {
             gstart[before + x - 1] = idx;
+            groot[before + x - 1] = sysroot ? sysroot[static_cast<int>(keys[idx] >> 54)] : 0;
+        }
         __syncthreads();
         if (threadIdx.x == kThreads - 1)
             carry = before + x;
@@ -210,7 +236,8 @@ int sms_now()
 
 int group_count_blocks(int n) { return (n + kChunk - 1) / kChunk > 0 ? (n + kChunk - 1) / kChunk : 1; }
 
-void launch_groups(const TreeArrays& t, int n, int gmax, GroupTable& g, cudaStream_t s)
+void launch_groups(const TreeArrays& t, int n, int gmax, int root_level,
+                   const unsigned long long* keys, GroupTable& g, cudaStream_t s)
 {
     gmax = gmax < 1 ? 1 : (gmax > kGroupMax ? kGroupMax : gmax);
     cudaMemsetAsync(g.flag, 0, sizeof(int) * static_cast<size_t>(n), s);
@@ -218,14 +245,19 @@ void launch_groups(const TreeArrays& t, int n, int gmax, GroupTable& g, cudaStre
     int fb = (t.cap + kThreads - 1) / kThreads;
     fb = fb < 8 * sms ? fb : 8 * sms;
     count_launch();
-    k_group_flags<<<fb > 0 ? fb : 1, kThreads, 0, s>>>(t, n, gmax, g.flag);
+    k_group_flags<<<fb > 0 ? fb : 1, kThreads, 0, s>>>(t, n, gmax, root_level, g.flag);
+    if (root_level > 0) {
+        count_launch();
+        k_system_roots<<<fb > 0 ? fb : 1, kThreads, 0, s>>>(t, root_level, keys, g.sysroot);
+    }
     const int blocks = group_count_blocks(n);
     count_launch();
     k_flag_count<<<blocks, kThreads, 0, s>>>(g.flag, n, g.block_sums);
     count_launch();
     k_flag_scan<<<1, 1024, 0, s>>>(g.block_sums, blocks, g.ngroups);
     count_launch();
-    k_flag_emit<<<blocks, kThreads, 0, s>>>(g.flag, n, g.block_sums, g.ngroups, g.gstart);
+    k_flag_emit<<<blocks, kThreads, 0, s>>>(g.flag, n, g.block_sums, g.ngroups, g.gstart, g.groot,
+                                            keys, root_level > 0 ? g.sysroot : nullptr);
 }
 
 } // namespace bz

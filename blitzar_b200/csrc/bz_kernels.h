@@ -24,6 +24,14 @@ void launch_bbox_f64(const double* x, const double* y, const double* z, int n, B
 void launch_keys63(const double* x, const double* y, const double* z, int n,
                    const BoxF64* box, double periodic_len, unsigned long long* keys,
                    uint32_t* perm, cudaStream_t s);
+// Ensembles: system s owns caller indices [offsets[s], offsets[s+1]); id[i] is the caller
+// index of slot i.  Keys carry the system in bits 54..62 (up to kMaxSystems systems) and 18
+// bits per axis of the system's own cube, so the top three octree levels split systems apart.
+constexpr int kMaxSystems = 512;
+constexpr int kSystemLevels = 3;
+void launch_keys_ensemble(const double* x, const double* y, const double* z, const int* id, int n,
+                          const long long* offsets, int systems, BoxF64* boxes,
+                          unsigned long long* keys, uint32_t* perm, cudaStream_t s);
 // Reference-compatible keys (FP32 bbox, the reference's quantisation and bit spread).
 void launch_keys_reference(const float* x, const float* y, const float* z, int n,
                            unsigned* bbox_ordered6, unsigned long long* keys, uint32_t* perm,
@@ -77,8 +85,10 @@ constexpr int kMaxLevels = 21;
 // Upper bound on device ordinals for per-device caches (function attributes, launch shapes).
 constexpr int kMaxDevices = 64;
 size_t tree_lookback_words(int cap);
+// min_split: nodes above this level split even when small (ensembles use kSystemLevels)
 void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
-                       int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s);
+                       int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s,
+                       int min_split = 0);
 
 // Reference-mode topology: the single leaf the reference builds for its own keys.
 void launch_reference_leaf(const float* x, const float* y, const float* z, const float* m,
@@ -104,9 +114,14 @@ struct GroupTable {
     int* gstart;      // [n + 1] group start indices in sorted order, then the end sentinel
     int* ngroups;     // [1]
     int* block_sums;  // [group_count_blocks(n)]
+    int* groot;       // [n]: node where each group's walk starts (its system's root)
+    int* sysroot;     // [kMaxSystems]: root node of each system (ensembles)
 };
 int group_count_blocks(int n);
-void launch_groups(const TreeArrays& t, int n, int gmax, GroupTable& g, cudaStream_t s);
+// root_level: level of the system roots (0 for one system, kSystemLevels for ensembles, whose
+// system id the sorted keys carry in bits 54..62)
+void launch_groups(const TreeArrays& t, int n, int gmax, int root_level,
+                   const unsigned long long* keys, GroupTable& g, cudaStream_t s);
 
 struct WalkOutputs {
     float* ax;        // accumulated into (+=)
@@ -195,8 +210,10 @@ void launch_mlp_pairs(const float* params, const float4* pos4, int n, const int*
 // ---------------------------------------------------------------- diagnostics (bz_diag.cu)
 // FP64 reference accelerations for the listed (sorted-order) targets: direct sum (open) or
 // Ewald (periodic).
+// src_lo/src_hi (optional, per target): sum only sources [src_lo, src_hi) (ensembles)
 void launch_direct_f64(const float4* pos4, int n, const int* targets, int nt, double eps,
-                       double* acc3, cudaStream_t s);
+                       double* acc3, cudaStream_t s, const int* src_lo = nullptr,
+                       const int* src_hi = nullptr);
 void launch_ewald_f64(const float4* pos4, int n, const int* targets, int nt, double eps,
                       double box, double alpha, int kmax, double* sk_scratch, double* acc3,
                       cudaStream_t s);

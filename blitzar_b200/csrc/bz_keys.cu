@@ -214,6 +214,109 @@ __global__ void __launch_bounds__(kThreads) k_keys_reference(const float* __rest
     }
 }
 
+// ---- ensembles: per-system boxes and keys (system id in the top 9 bits, 18 bits per axis)
+
+__device__ __forceinline__ int system_of(const long long* __restrict__ offsets, int systems, int id)
+{
+    int lo = 0, hi = systems;  // offsets[lo] <= id < offsets[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (offsets[mid] <= id)
+            lo = mid;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+__global__ void k_sys_box_init(BoxF64* boxes, int systems)
+{
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < systems; s += gridDim.x * blockDim.x)
+        for (int a = 0; a < 3; ++a) {
+            boxes[s].mn[a] = 0xffffffffffffffffull;
+            boxes[s].mx[a] = 0ull;
+        }
+}
+
+// Per-system FP64 min/max.  Particles of a system are contiguous in both the caller's and the
+// sorted order, so a warp usually holds one system: it then reduces by shuffles and issues one
+// atomic per axis; mixed warps fall back to per-lane atomics.  Exact either way.
+__global__ void __launch_bounds__(kThreads) k_sys_bbox(const double* __restrict__ x,
+                                                        const double* __restrict__ y,
+                                                        const double* __restrict__ z,
+                                                        const int* __restrict__ id, int n,
+                                                        const long long* __restrict__ offsets,
+                                                        int systems, BoxF64* boxes)
+{
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * kThreads; base < n; base += gridDim.x * kThreads) {
+        const int i = base + threadIdx.x;
+        const bool valid = i < n;
+        const int sys = valid ? system_of(offsets, systems, id[i]) : -1;
+        double p[3] = {0.0, 0.0, 0.0};
+        if (valid) {
+            p[0] = x[i];
+            p[1] = y[i];
+            p[2] = z[i];
+        }
+        const int s0 = __shfl_sync(kFullMask, sys, 0);
+        const bool uniform = __all_sync(kFullMask, !valid || sys == s0) && s0 >= 0;
+        if (uniform) {
+            for (int a = 0; a < 3; ++a) {
+                double mn = valid ? p[a] : 1e300, mx = valid ? p[a] : -1e300;
+                for (int o = 16; o > 0; o >>= 1) {
+                    mn = fmin(mn, __shfl_xor_sync(kFullMask, mn, o));
+                    mx = fmax(mx, __shfl_xor_sync(kFullMask, mx, o));
+                }
+                if (lane == 0) {
+                    atomicMin(&boxes[s0].mn[a], ordered_from_double(mn));
+                    atomicMax(&boxes[s0].mx[a], ordered_from_double(mx));
+                }
+            }
+        } else if (valid) {
+            for (int a = 0; a < 3; ++a) {
+                atomicMin(&boxes[sys].mn[a], ordered_from_double(p[a]));
+                atomicMax(&boxes[sys].mx[a], ordered_from_double(p[a]));
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) k_keys_ensemble(const double* __restrict__ x,
+                                                             const double* __restrict__ y,
+                                                             const double* __restrict__ z,
+                                                             const int* __restrict__ id, int n,
+                                                             const long long* __restrict__ offsets,
+                                                             int systems,
+                                                             const BoxF64* __restrict__ boxes,
+                                                             unsigned long long* __restrict__ keys,
+                                                             uint32_t* __restrict__ perm)
+{
+    for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+        const int sys = system_of(offsets, systems, id[i]);
+        const BoxF64 b = boxes[sys];
+        double o[3], mx[3];
+        for (int a = 0; a < 3; ++a) {
+            o[a] = double_from_ordered(b.mn[a]);
+            mx[a] = double_from_ordered(b.mx[a]);
+        }
+        double size = fmax(fmax(mx[0] - o[0], mx[1] - o[1]), mx[2] - o[2]);
+        if (!(size > 0.0))
+            size = 1.0;
+        const double scale = __ddiv_rn(262144.0, size);
+        const double p[3] = {x[i], y[i], z[i]};
+        unsigned long long q[3];
+        for (int a = 0; a < 3; ++a) {
+            double t = floor(__dmul_rn(__dsub_rn(p[a], o[a]), scale));
+            t = t >= 0.0 ? t : 0.0;
+            q[a] = static_cast<unsigned long long>(fmin(t, 262143.0));
+        }
+        keys[i] = (static_cast<unsigned long long>(sys) << 54) | (spread21(q[0]) << 2) |
+                  (spread21(q[1]) << 1) | spread21(q[2]);
+        perm[i] = static_cast<uint32_t>(i);
+    }
+}
+
 int grid_for(int n)
 {
     int dev = 0, sms = 148;
@@ -233,6 +336,18 @@ void launch_bbox_f64(const double* x, const double* y, const double* z, int n, B
     k_bbox_init<<<1, 32, 0, s>>>(box);
     count_launch();
     k_bbox_f64<<<grid_for(n), kThreads, 0, s>>>(x, y, z, n, box);
+}
+
+void launch_keys_ensemble(const double* x, const double* y, const double* z, const int* id, int n,
+                          const long long* offsets, int systems, BoxF64* boxes,
+                          unsigned long long* keys, uint32_t* perm, cudaStream_t s)
+{
+    count_launch();
+    k_sys_box_init<<<(systems + 255) / 256, 256, 0, s>>>(boxes, systems);
+    count_launch();
+    k_sys_bbox<<<grid_for(n), kThreads, 0, s>>>(x, y, z, id, n, offsets, systems, boxes);
+    count_launch();
+    k_keys_ensemble<<<grid_for(n), kThreads, 0, s>>>(x, y, z, id, n, offsets, systems, boxes, keys, perm);
 }
 
 void launch_keys63(const double* x, const double* y, const double* z, int n,

@@ -76,7 +76,7 @@ constexpr int kLookbackNodes = kThreads / 8;
 template <int TPN>
 __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long long* __restrict__ keys,
                                                           int l, int leaf_cap, int max_level,
-                                                          TreeArrays t, int* err)
+                                                          int min_split, TreeArrays t, int* err)
 {
     constexpr int kNodesPerTile = kThreads / TPN;
     __shared__ int s_tile;
@@ -108,7 +108,8 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
         if (k < next_first) {
             s0 = t.start[k];
             c0 = t.count[k];
-            split = c0 > leaf_cap && l < max_level;
+            // levels above min_split always split (ensembles: they separate the systems)
+            split = (c0 > leaf_cap || l < min_split) && l < max_level;
             if (TPN == 8) {
                 if (split && sub > 0)
                     bsub = lower_bound_digit(keys, s0, s0 + c0, shift, static_cast<unsigned>(sub));
@@ -359,7 +360,8 @@ __global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restr
 size_t tree_lookback_words(int cap) { return static_cast<size_t>(cap) / kLookbackNodes + 2 * kMaxLevels + 8; }
 
 void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
-                       int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s)
+                       int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s,
+                       int min_split)
 {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -382,10 +384,10 @@ void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4
         count_launch();
         if (wide)
             k_tree_level<8><<<static_cast<int>(blocks), kThreads, 0, s>>>(sorted_keys, l, leaf_cap,
-                                                                          max_level, t, err);
+                                                                          max_level, min_split, t, err);
         else
             k_tree_level<1><<<static_cast<int>(blocks), kThreads, 0, s>>>(sorted_keys, l, leaf_cap,
-                                                                          max_level, t, err);
+                                                                          max_level, min_split, t, err);
     }
     count_launch();
     k_tree_finish_last<<<sms, 256, 0, s>>>(t, max_level);

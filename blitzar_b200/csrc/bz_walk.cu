@@ -554,6 +554,7 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
 template <bool PERIODIC, bool SPLIT, bool QUAD, bool POT>
 __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__ pos4, int n,
                                                        TreeArrays t, const int* __restrict__ gstart,
+                                                       const int* __restrict__ groot,
                                                        const int* __restrict__ ngroups_ptr,
                                                        WalkParams p, float inv_box,
                                                        WalkOutputs o, unsigned* queue,
@@ -602,7 +603,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
         }
 
         if (lane == 0)
-            w.stack[0] = 0;
+            w.stack[0] = groot[g];  // the group's system root (node 0 for a single system)
         __syncwarp();
         int top = 1, gtop = 0, nn = 0, nl = 0, lp = 0;
         unsigned long long cnt_pp = 0, cnt_pn = 0;
@@ -824,7 +825,7 @@ void launch_variant(const float4* pos4, int n, const TreeArrays& t, const GroupT
     k_zero_u32<<<1, 1, 0, s>>>(queue);
     count_launch();
     k_walk<PERIODIC, SPLIT, QUAD, POT><<<l.blocks, kWarps * 32, l.smem, s>>>(
-        pos4, n, t, g.gstart, g.ngroups, p, inv_box, o, queue, spill, err);
+        pos4, n, t, g.gstart, g.groot, g.ngroups, p, inv_box, o, queue, spill, err);
 }
 
 template <bool PERIODIC, bool SPLIT>

@@ -101,6 +101,16 @@ bz_status bz_set_state(bz_handle* h, const float* pos_soa3, const float* vel_soa
 bz_status bz_set_state_f64(bz_handle* h, const double* pos_soa3, const double* vel_soa3,
                            const float* mass, size_t n);
 
+/* Ensembles of independent systems in one handle (no counterpart in the reference, which
+ * steps one system per process): system s owns caller indices [offsets[s], offsets[s+1]),
+ * offsets[0] = 0, num_systems <= 512, each with at least one particle; FP64 SoA state as in
+ * bz_set_state_f64.  Systems never interact: keys carry the system in their top 9 bits, the
+ * top three octree levels separate the systems, and every walk group starts at its own
+ * system's root.  All systems share one launch per phase and one captured step.  Octree
+ * solver only.  A later bz_set_state returns the handle to a single system. */
+bz_status bz_set_ensemble(bz_handle* h, const double* pos_soa3, const double* vel_soa3,
+                          const float* mass, const int64_t* offsets, int32_t num_systems);
+
 /* Advance nsteps leapfrog (KDK) steps of size dt.  Replaces ParticleSystem::update
  * (PhyParticleSystem.hpp:163; octree_gpu leapfrog in engine/physics/core/cuda/integration/
  * CudOctreeGpuIntegrators.inl:121-195).  The force at the end of a step is reused at the
