@@ -58,6 +58,8 @@ WORKLOADS = {
     "plummer65k": dict(kind="octree", ic="plummer", n=65536, theta=0.5, eps=0.01, dt=1e-3, seed=1),
     "hernquist4m": dict(kind="octree", ic="hernquist", n=4194304, theta=0.4, eps=0.005, dt=2e-4,
                         seed=3),
+    "ensemble256": dict(kind="ensemble", clusters=256, n_min=1024, n_max=65536, w0_min=3.0,
+                        w0_max=9.0, theta=0.5, eps=0.01, dt=1e-3, seed=5),
 }
 
 
@@ -101,9 +103,29 @@ def init_dist(world, local, backend="nccl"):
     return dist
 
 
+def make_ensemble(w, rank):
+    """King clusters with N log-uniform in [n_min, n_max] and W0 uniform in [w0_min, w0_max]."""
+    from blitzar_b200 import ics
+
+    rng = np.random.default_rng(w["seed"] + rank)
+    sizes = np.rint(np.exp(rng.uniform(np.log(w["n_min"]), np.log(w["n_max"]), w["clusters"])))
+    w0 = rng.uniform(w["w0_min"], w["w0_max"], w["clusters"])
+    systems = []
+    for i, (n, W0) in enumerate(zip(sizes.astype(int), w0)):
+        p, v, m = ics.king(int(n), 1000 * (w["seed"] + rank) + i, float(W0))
+        systems.append((p, v, m.astype(np.float32)))
+    return systems
+
+
 def make_ics(w, rank):
     from blitzar_b200 import ics
 
+    if w["kind"] == "ensemble":
+        systems = make_ensemble(w, rank)
+        pos = np.concatenate([p for p, _, _ in systems])
+        vel = np.concatenate([v for _, v, _ in systems])
+        mass = np.concatenate([m for _, _, m in systems])
+        return pos, vel, mass
     if w["kind"] == "treepm":
         pos, vel, mass = ics.grf_grid(w["n_side"], seed=w["seed"] + rank, rms_cells=w["rms_cells"])
     elif w["ic"] == "hernquist":
@@ -124,7 +146,7 @@ def engine_config(w):
                     treepm_node_size_factor=w["node_size_factor"],
                     octree_theta=w["theta"], octree_softening=w["eps_lattice"] / w["n_side"],
                     multipole_order=2)
-    return dict(solver=0, octree_theta=w["theta"], octree_softening=w["eps"], multipole_order=2)
+    return dict(solver=0, octree_theta=w["theta"], octree_softening=w["eps"], multipole_order=2)  # octree, ensemble
 
 
 class ClockSampler:
@@ -242,6 +264,32 @@ def cpu_baseline(w, pos, mass, sample, seed=7):
             kind = "port"
             text = "oracle port: FP64 PM + FP64 direct short range on a target sample, scaled to N"
         t_step = t_pm + t_tree * n / len(targets)
+    elif w["kind"] == "ensemble":
+        if R is None:
+            return None
+        # the reference steps one system per process: time its octree_cpu (build + walk of
+        # every particle) on a few clusters spread in size and scale by particle count
+        systems = make_ensemble(w, 0)
+        order = np.argsort([len(m) for _, _, m in systems])
+        pick = order[np.linspace(0, len(order) - 1, 5).astype(int)]
+        t_s, n_s = 0.0, 0
+        for i in pick:
+            p, _, mm = systems[i]
+            q = p.astype(np.float32)
+            cx, cy, cz = [np.ascontiguousarray(q[:, a]) for a in range(3)]
+            mm = np.ascontiguousarray(mm, np.float32)
+            k = len(mm)
+            bx, by, bz = [np.zeros(k, np.float32) for _ in range(3)]
+            t0 = time.perf_counter()
+            R.ref_octree_cpu_accel(cx, cy, cz, mm, k, w["theta"], w["eps"], 1e-12, 1e30, 0, 0.0, 0.0,
+                                   None, 0, bx, by, bz)
+            t_s += time.perf_counter() - t0
+            n_s += k
+        t_step = t_s * n / n_s
+        cores = int(R.ref_omp_threads())
+        kind = "reference"
+        text = (f"reference octree_cpu (build + walk of every particle) on {len(pick)} of "
+                f"{len(systems)} clusters ({n_s} particles, spread in size), scaled to all {n}")
     else:
         if R is None:
             return None
@@ -360,13 +408,18 @@ def run_ours(args, w, rank, world, local):
     stream = torch.cuda.Stream()
     cfg = engine_config(w)
     eng = Engine(n, stream=stream.cuda_stream, device=local, **cfg)
-    eng.set_state(pos, vel, mass, f64=True)
+    systems = None
+    if w["kind"] == "ensemble":
+        systems = make_ensemble(w, rank)
+        offsets = eng.set_ensemble(systems)
+    else:
+        eng.set_state(pos, vel, mass, f64=True)
     dt = w["dt"]
     with torch.cuda.stream(stream):
         for _ in range(max(3, args.warmup)):
             eng.step(dt, 1)
     torch.cuda.synchronize()
-    energy0 = eng.energy() if w["kind"] == "octree" else None
+    energy0 = eng.energy() if w["kind"] in ("octree", "ensemble") else None
 
     clocks = ClockSampler(local)
     if dist:
@@ -445,7 +498,40 @@ def run_ours(args, w, rank, world, local):
 
     # end to end through the C ABI with pinned host buffers: upload state, one step, download
     e2e = None
-    if args.e2e_steps > 0:
+    if args.e2e_steps > 0 and systems is not None:
+        # ensembles: FP64 SoA state and the system offsets through bz_set_ensemble
+        import ctypes as C
+
+        hp = torch.empty(3 * n, dtype=torch.float64, pin_memory=True).numpy()
+        hv = torch.empty(3 * n, dtype=torch.float64, pin_memory=True).numpy()
+        hm = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
+        hm[:] = mass
+        offs = np.ascontiguousarray(offsets, np.int64)
+
+        def up():
+            eng._check(eng.L.bz_set_ensemble(eng.h, hp.ctypes.data, hv.ctypes.data, hm.ctypes.data,
+                                              offs.ctypes.data, len(systems)), "bz_set_ensemble")
+
+        def down():
+            eng._check(eng.L.bz_get_state_f64(eng.h, hp.ctypes.data, hv.ctypes.data), "bz_get_state_f64")
+
+        down()
+        up()
+        eng.step(dt, 1)
+        down()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            up()
+            eng.step(dt, 1)
+            down()
+        torch.cuda.synchronize()
+        sec = time.perf_counter() - t0
+        e2e = {"value": n * world * args.e2e_steps / sec, "unit": "particle-steps/s",
+               "h2d_bytes_per_step": 6 * 8 * n + 4 * n + 8 * len(offs), "d2h_bytes_per_step": 6 * 8 * n,
+               "note": "each step uploads the full FP64 ensemble state, which forces a fresh force "
+                       "evaluation before the leapfrog step (two evaluations per step)"}
+    elif args.e2e_steps > 0:
         hp = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
         hv = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
         hm = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
@@ -487,10 +573,12 @@ def run_ours(args, w, rank, world, local):
         "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": ms / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": ("synthetic (seeded GRF-displaced grid)" if w["kind"] == "treepm"
+                 else "synthetic (seeded King clusters)" if w["kind"] == "ensemble"
                  else f"synthetic (seeded {w['ic'].capitalize()} sphere)"),
         "config": config_dict(w, args, n),
         "force_error": {"median": errs["median"], "p99": errs["p99"], "sample": args.error_sample,
-                        "reference": "FP64 Ewald" if w["kind"] == "treepm" else "FP64 direct sum"},
+                        "reference": "FP64 Ewald" if w["kind"] == "treepm" else
+                        "FP64 direct sum within each system" if w["kind"] == "ensemble" else "FP64 direct sum"},
         "roofline": roofline, "roofline_secondary": secondary,
         "phase_ms": ph, "gpu_launches": launches_step * args.steps, "launches_per_step": launches_step,
         "clocks": clk, "e2e": e2e, "cpu_baseline": cpu,
