@@ -27,7 +27,7 @@ EXPORTS = (
     "bz_status_string", "bz_version", "bz_kernel_launches", "bz_launches_per_step",
     "bz_sort_pairs_noalloc", "bz_energy", "bz_autotune", "bz_learn_generate", "bz_learn_train",
     "bz_learn_set", "bz_learn_get", "bz_learn_enable", "bz_learn_forward", "bz_learn_gradient",
-    "bz_set_ensemble",
+    "bz_set_ensemble", "bz_adaptive_levels", "bz_adaptive_updates",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -60,6 +60,8 @@ class BzConfig(C.Structure):
         ("stream", C.c_uint64),
         ("use_graph", C.c_int32),
         ("walk_group_size", C.c_int32),
+        ("adaptive_max_level", C.c_int32),
+        ("adaptive_eta", C.c_float),
     ]
 
 
@@ -112,6 +114,8 @@ def load():
     L.bz_launches_per_step.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_energy.argtypes = [_vp, _vp, _vp, _vp]
     L.bz_autotune.argtypes = [_vp, C.c_int32, _vp, _vp, _vp]
+    L.bz_adaptive_levels.argtypes = [_vp, _vp]
+    L.bz_adaptive_updates.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_set_ensemble.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_int32]
     L.bz_learn_generate.argtypes = [_vp, C.c_int64, C.c_uint64, _vp, _vp]
     L.bz_learn_train.argtypes = [_vp, _vp, _vp, C.c_int64, C.c_int32, C.c_int32, C.c_float,
@@ -191,6 +195,16 @@ class Engine:
             m = np.ascontiguousarray(mass, np.float32)
             self._check(self.L.bz_set_state(self.h, _ptr(p), _ptr(v), _ptr(m), n), "bz_set_state")
         self.n = n
+
+    def adaptive_levels(self):
+        lv = np.empty(self.n, np.uint8)
+        self._check(self.L.bz_adaptive_levels(self.h, _ptr(lv)), "bz_adaptive_levels")
+        return lv
+
+    def adaptive_updates(self):
+        u = C.c_uint64(0)
+        self._check(self.L.bz_adaptive_updates(self.h, C.byref(u)), "bz_adaptive_updates")
+        return u.value
 
     def set_ensemble(self, systems):
         """systems: list of (pos[n,3], vel[n,3] or None, mass[n]) of independent systems."""

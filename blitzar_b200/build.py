@@ -29,6 +29,7 @@ SOURCES = {
     "bz_tree.cu": ["--fmad=false"],
     "bz_groups.cu": [],
     "bz_mlp.cu": [],
+    "bz_adaptive.cu": [],
     "bz_walk.cu": [],
     "bz_pm.cu": [],
     "bz_state.cu": [],

@@ -87,6 +87,14 @@ struct bz_handle {
     double* h_dt = nullptr;  // pinned {dt, dt/2}
     unsigned long long last_pp = 0, last_pn = 0;
     bool ref_tree_valid = false;
+    // adaptive block steps
+    struct {
+        AdaptiveState st{};
+        unsigned char* active = nullptr;  // [capacity] sorted-slot flags of the current substep
+        int* lmax = nullptr;
+        bool ready = false;               // levels and cached accelerations match the state
+    } ad;
+    const unsigned char* walk_active = nullptr;  // mask handed to the walk (adaptive substeps)
     // ensembles of independent systems (0 = one system)
     int systems = 0;
     long long* sys_offsets = nullptr;  // [kMaxSystems + 1] caller-index offsets
@@ -235,6 +243,7 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
     o.pot = want_pot ? d.pot : nullptr;
     o.totals = d.counters;
     WalkParams wp = walk_params(h, want_pot);
+    wp.active = h->walk_active;
     const bool learned = h->learn.enabled && h->learn.trained && h->cfg.solver == BZ_SOLVER_TREEPM;
     if (learned) {
         o.pair_src = h->learn.pair_src;
@@ -457,6 +466,8 @@ bz_status bz_config_init(bz_config* c)
     c->stream = 0;
     c->use_graph = 1;
     c->walk_group_size = kGroupMax;
+    c->adaptive_max_level = 0;
+    c->adaptive_eta = 0.02f;
     return BZ_OK;
 }
 
@@ -516,7 +527,8 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
         }
     }
     if (cfg->leaf_capacity < 1 || cfg->octree_theta <= 0.0f || cfg->walk_group_size < 1 ||
-        cfg->walk_group_size > kGroupMax) {
+        cfg->walk_group_size > kGroupMax || cfg->adaptive_max_level < 0 || cfg->adaptive_max_level > 12 ||
+        (cfg->adaptive_max_level > 0 && (cfg->solver != BZ_SOLVER_OCTREE || !(cfg->adaptive_eta > 0.0f)))) {
         delete h;
         return BZ_INVALID_ARGUMENT;
     }
@@ -573,6 +585,10 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     GroupTable& gt = h->groups;
     ok = ok && dalloc(h, &gt.flag, n) && dalloc(h, &gt.gstart, n + 1) && dalloc(h, &gt.ngroups, 1) &&
          dalloc(h, &gt.groot, n + 1) && dalloc(h, &gt.sysroot, kMaxSystems) &&
+         (cfg->adaptive_max_level == 0 ||
+          (dalloc(h, &h->ad.st.level, n) && dalloc(h, &h->ad.st.ax, n) && dalloc(h, &h->ad.st.ay, n) &&
+           dalloc(h, &h->ad.st.az, n) && dalloc(h, &h->ad.st.updates, 1) && dalloc(h, &h->ad.active, n) &&
+           dalloc(h, &h->ad.lmax, 1))) &&
          dalloc(h, &gt.block_sums, static_cast<size_t>(group_count_blocks(static_cast<int>(n))));
     // walk spill area: one slot per warp the persistent walk grid can hold
     h->spill_slots = walk_spill_slots();
@@ -715,6 +731,7 @@ bz_status upload_common(bz_handle* h, size_t n)
     h->n = n;
     h->cur = 0;
     h->forces_valid = false;
+    h->ad.ready = false;
     h->ref_tree_valid = false;
     return BZ_OK;
 }
@@ -969,6 +986,90 @@ bz_status bz_energy(bz_handle* h, double* kinetic, double* potential, double* mo
     return BZ_OK;
 }
 
+} // extern "C"
+
+namespace {
+
+AdaptiveParams adaptive_params(const bz_handle* h, double dt)
+{
+    AdaptiveParams p{};
+    p.dt_max = dt;
+    p.eta = h->cfg.adaptive_eta;
+    p.eps = std::max(h->cfg.octree_softening, h->cfg.physics_min_softening);
+    p.max_level = h->cfg.adaptive_max_level;
+    return p;
+}
+
+// Block steps with power-of-two levels (the kernels in bz_adaptive.cu describe the scheme).
+// The forces of the current state are valid on entry (ensure_forces).
+bz_status adaptive_steps(bz_handle* h, double dt, uint32_t nsteps)
+{
+    const int n = static_cast<int>(h->n);
+    DeviceBuffers& d = h->d;
+    const AdaptiveParams p = adaptive_params(h, dt);
+    if (!h->ad.ready) {
+        double* const* st = d.st[h->cur];
+        cudaMemsetAsync(h->ad.st.updates, 0, sizeof(unsigned long long), h->stream);
+        launch_adaptive_init(d.acc[0], d.acc[1], d.acc[2], st[3], st[4], st[5], d.id[h->cur], n, p,
+                             h->ad.st, h->stream);
+        h->ad.ready = true;
+    }
+    for (uint32_t b = 0; b < nsteps; ++b) {
+        launch_level_max(h->ad.st.level, n, h->ad.lmax, h->stream);
+        int L = 0;
+        cudaMemcpyAsync(&L, h->ad.lmax, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+        if (cudaStreamSynchronize(h->stream) != cudaSuccess)
+            return check_device(h, "bz_step (adaptive)");
+        L = std::min(std::max(L, 0), h->cfg.adaptive_max_level);
+        for (int sub = 0; sub < (1 << L); ++sub) {
+            double* const* st = d.st[h->cur];
+            launch_adaptive_open_drift(st[0], st[1], st[2], st[3], st[4], st[5], d.id[h->cur], n, p,
+                                       h->ad.st, sub, L, h->stream);
+            enqueue_order(h);
+            launch_adaptive_active(d.id[h->cur], n, h->ad.st, sub, L, h->ad.active, h->stream);
+            h->walk_active = h->ad.active;
+            enqueue_forces(h, false, false);
+            h->walk_active = nullptr;
+            double* const* st2 = d.st[h->cur];
+            launch_adaptive_close(d.acc[0], d.acc[1], d.acc[2], st2[3], st2[4], st2[5], d.id[h->cur],
+                                  h->ad.active, n, p, h->ad.st, sub, L, h->stream);
+        }
+    }
+    // d.acc holds only the closing particles of the last substep: re-evaluate before a plain step
+    h->forces_valid = false;
+    const bz_status s = check_device(h, "bz_step (adaptive)");
+    if (s != BZ_OK)
+        return s;
+    read_counters(h);
+    return BZ_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+bz_status bz_adaptive_levels(bz_handle* h, uint8_t* levels)
+{
+    if (!h || !levels || h->cfg.adaptive_max_level <= 0 || !h->ad.ready)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    cudaMemcpyAsync(levels, h->ad.st.level, h->n, cudaMemcpyDeviceToHost, h->stream);
+    return check_device(h, "bz_adaptive_levels");
+}
+
+bz_status bz_adaptive_updates(bz_handle* h, uint64_t* updates)
+{
+    if (!h || !updates || h->cfg.adaptive_max_level <= 0)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    unsigned long long u = 0;
+    if (h->ad.ready)
+        cudaMemcpyAsync(&u, h->ad.st.updates, sizeof(u), cudaMemcpyDeviceToHost, h->stream);
+    const bz_status s = check_device(h, "bz_adaptive_updates");
+    *updates = u;
+    return s;
+}
+
 bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps)
 {
     if (!h || h->n == 0)
@@ -981,10 +1082,13 @@ bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps)
     h->h_dt[0] = dt;
     h->h_dt[1] = 0.5 * dt;
     cudaMemcpyAsync(h->d.dt, h->h_dt, 2 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
-    bz_status s = ensure_forces(h);
+    // adaptive block steps carry their own cached accelerations once started
+    bz_status s = (h->cfg.adaptive_max_level > 0 && h->ad.ready) ? BZ_OK : ensure_forces(h);
     if (s != BZ_OK)
         return s;
     h->stepping = true;
+    if (h->cfg.adaptive_max_level > 0)
+        return adaptive_steps(h, dt, nsteps);
     uint32_t done = 0;
     if (h->cfg.use_graph && !h->timing) {
         build_graphs(h);

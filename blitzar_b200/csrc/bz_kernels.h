@@ -106,6 +106,7 @@ struct WalkParams {
     int quadrupole;
     int want_pot;
     float rcorr2;     // > 0 with WalkOutputs.pair_src: record the pairs closer than this
+    const unsigned char* active;  // optional [n]: walk only groups with an active target
 };
 // ---------------------------------------------------------------- target groups (bz_groups.cu)
 constexpr int kGroupMax = 32;  // largest walk group (one warp)
@@ -187,6 +188,34 @@ void launch_energy(const double* vx, const double* vy, const double* vz, const f
 void launch_scatter3(const float* ax, const float* ay, const float* az, const int* id, int n,
                      float* out_soa3, cudaStream_t s);
 void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s);
+
+// ---------------------------------------------------------------- adaptive steps (bz_adaptive.cu)
+struct AdaptiveParams {
+    double dt_max;
+    float eta;
+    float eps;
+    int max_level;
+};
+struct AdaptiveState {        // indexed by caller index
+    unsigned char* level;
+    float* ax;
+    float* ay;
+    float* az;
+    unsigned long long* updates;  // [1] particle steps closed so far
+};
+void launch_adaptive_init(const float* ax, const float* ay, const float* az, const double* vx,
+                          const double* vy, const double* vz, const int* id, int n,
+                          const AdaptiveParams& p, const AdaptiveState& a, cudaStream_t s);
+void launch_level_max(const unsigned char* level, int n, int* out, cudaStream_t s);
+void launch_adaptive_open_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
+                                const int* id, int n, const AdaptiveParams& p, const AdaptiveState& a,
+                                int sub, int L, cudaStream_t s);
+void launch_adaptive_active(const int* id, int n, const AdaptiveState& a, int sub, int L,
+                            unsigned char* active, cudaStream_t s);
+void launch_adaptive_close(const float* ax, const float* ay, const float* az, double* vx, double* vy,
+                           double* vz, const int* id, const unsigned char* active, int n,
+                           const AdaptiveParams& p, const AdaptiveState& a, int sub, int L,
+                           cudaStream_t s);
 
 // ---------------------------------------------------------------- learned correction (bz_mlp.cu)
 // Parameter block of the 6 -> 32 -> 32 -> 3 MLP (16 features incl. a constant 1 that carries

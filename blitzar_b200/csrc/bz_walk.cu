@@ -588,6 +588,9 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
         const int ti = g0 + lane;
         const bool valid = lane < gn;
         const float4 me = pos4[valid ? ti : g0];
+        // adaptive steps: only groups holding a target that closes its step are walked
+        if (p.active != nullptr && !__any_sync(kFullMask, valid && p.active[ti] != 0))
+            continue;
         float gmin[3] = {me.x, me.y, me.z}, gmax[3] = {me.x, me.y, me.z};
 #pragma unroll
         for (int a = 0; a < 3; ++a)

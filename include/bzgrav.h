@@ -77,6 +77,9 @@ typedef struct bz_config {
     uint64_t stream;               /* cudaStream_t to run on, or 0 for a private stream */
     int32_t use_graph;             /* capture bz_step's per-step work in a CUDA graph */
     int32_t walk_group_size;       /* targets per walk group, 1..32 (default 32; bz_autotune) */
+    int32_t adaptive_max_level;    /* adaptive(max_level): 0 = fixed steps; k > 0: power-of-two
+                                      block steps dt / 2^l, l <= k (octree solver) */
+    float adaptive_eta;            /* adaptive(eta): stable dt = eta * min(sqrt(eps/|a|), eps/|v|) */
 } bz_config;
 
 typedef struct bz_handle bz_handle;
@@ -116,6 +119,14 @@ bz_status bz_set_ensemble(bz_handle* h, const double* pos_soa3, const double* ve
  * CudOctreeGpuIntegrators.inl:121-195).  The force at the end of a step is reused at the
  * start of the next, so each step evaluates the force once. */
 bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps);
+
+/* Adaptive block steps (adaptive_max_level > 0): each bz_step step is one block of dt split
+ * into 2^L substeps (L = finest level present at its start); the per-particle level follows
+ * engine/physics/core/cuda/integration/CudAdaptive.inl:42-71.  bz_adaptive_levels writes
+ * each particle's level (caller order); bz_adaptive_updates the particle steps closed so far
+ * (each is one force evaluation and one kick of one particle). */
+bz_status bz_adaptive_levels(bz_handle* h, uint8_t* levels);
+bz_status bz_adaptive_updates(bz_handle* h, uint64_t* updates);
 
 /* Autotuner (no counterpart in the reference, whose leaf capacity and launch shapes are fixed
  * settings): times `trials` force evaluations of the current state for each leaf capacity in
