@@ -59,7 +59,8 @@ WORKLOADS = {
     "hernquist4m": dict(kind="octree", ic="hernquist", n=4194304, theta=0.4, eps=0.005, dt=2e-4,
                         seed=3),
     "ensemble256": dict(kind="ensemble", clusters=256, n_min=1024, n_max=65536, w0_min=3.0,
-                        w0_max=9.0, theta=0.5, eps=0.01, dt=1e-3, seed=5),
+                        w0_max=9.0, theta=0.5, eps=0.01, dt=1e-3, seed=5, adaptive_levels=7,
+                        adaptive_eta=0.02),
 }
 
 
@@ -146,7 +147,10 @@ def engine_config(w):
                     treepm_node_size_factor=w["node_size_factor"],
                     octree_theta=w["theta"], octree_softening=w["eps_lattice"] / w["n_side"],
                     multipole_order=2)
-    return dict(solver=0, octree_theta=w["theta"], octree_softening=w["eps"], multipole_order=2)  # octree, ensemble
+    cfg = dict(solver=0, octree_theta=w["theta"], octree_softening=w["eps"], multipole_order=2)
+    if w.get("adaptive_levels"):
+        cfg.update(adaptive_max_level=w["adaptive_levels"], adaptive_eta=w["adaptive_eta"])
+    return cfg
 
 
 class ClockSampler:
@@ -429,10 +433,13 @@ def run_ours(args, w, rank, world, local):
     time.sleep(0.3)
     start = torch.cuda.Event(enable_timing=True)
     end = torch.cuda.Event(enable_timing=True)
+    adaptive = bool(w.get("adaptive_levels"))
+    upd0 = eng.adaptive_updates() if adaptive else 0
     start.record(stream)
     eng.step(dt, args.steps)
     end.record(stream)
     torch.cuda.synchronize()
+    updates = (eng.adaptive_updates() - upd0) if adaptive else n * args.steps
     if dist:
         dist.barrier()
     clk = clocks.stop()
@@ -441,7 +448,9 @@ def run_ours(args, w, rank, world, local):
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = n * world * args.steps / (ms / 1e3)
+    # particle-steps: with adaptive block steps, every closed step of every particle (one force
+    # evaluation and one kick each); otherwise N per step
+    value = updates * world / (ms / 1e3)
     drift = None
     if energy0 is not None:
         k1, w1, p1 = eng.energy()
@@ -460,7 +469,7 @@ def run_ours(args, w, rank, world, local):
     split = w["kind"] == "treepm"
     flops = pp * FLOP_PP[split] + pn * FLOP_PN[(split, True)]
     walk_ms = ph["walk"]
-    achieved_tf = flops / (walk_ms * 1e-3) / 1e12
+    achieved_tf = flops / (walk_ms * 1e-3) / 1e12 if walk_ms > 0 else 0.0
     peak_tf = SMS * FP32_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
     traffic = load_traffic(f"walk_{args.workload}")
     roofline = {
@@ -520,14 +529,16 @@ def run_ours(args, w, rank, world, local):
         eng.step(dt, 1)
         down()
         torch.cuda.synchronize()
+        steps_done = 0
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
             up()
             eng.step(dt, 1)
+            steps_done += eng.adaptive_updates() if adaptive else n  # counter restarts per upload
             down()
         torch.cuda.synchronize()
         sec = time.perf_counter() - t0
-        e2e = {"value": n * world * args.e2e_steps / sec, "unit": "particle-steps/s",
+        e2e = {"value": steps_done * world / sec, "unit": "particle-steps/s",
                "h2d_bytes_per_step": 6 * 8 * n + 4 * n + 8 * len(offs), "d2h_bytes_per_step": 6 * 8 * n,
                "note": "each step uploads the full FP64 ensemble state, which forces a fresh force "
                        "evaluation before the leapfrog step (two evaluations per step)"}
@@ -587,6 +598,12 @@ def run_ours(args, w, rank, world, local):
         line["energy"] = drift
     if learned is not None:
         line["learned"] = learned
+    if adaptive:
+        line["adaptive"] = {"max_level": w["adaptive_levels"], "eta": w["adaptive_eta"],
+                            "block_steps": args.steps, "particle_steps": int(updates),
+                            "mean_steps_per_particle_per_block": updates / (n * args.steps),
+                            "note": "ms_per_step is per block step of dt_max; phase_ms covers "
+                                    "one substep"}
     eng.close()
     if rank == 0:
         print(json.dumps(line))

@@ -1022,6 +1022,7 @@ bz_status adaptive_steps(bz_handle* h, double dt, uint32_t nsteps)
             return check_device(h, "bz_step (adaptive)");
         L = std::min(std::max(L, 0), h->cfg.adaptive_max_level);
         for (int sub = 0; sub < (1 << L); ++sub) {
+            record(h, kEvStepStart);
             double* const* st = d.st[h->cur];
             launch_adaptive_open_drift(st[0], st[1], st[2], st[3], st[4], st[5], d.id[h->cur], n, p,
                                        h->ad.st, sub, L, h->stream);
@@ -1037,9 +1038,12 @@ bz_status adaptive_steps(bz_handle* h, double dt, uint32_t nsteps)
     }
     // d.acc holds only the closing particles of the last substep: re-evaluate before a plain step
     h->forces_valid = false;
+    if (h->timing)
+        record(h, kNumPhases);
     const bz_status s = check_device(h, "bz_step (adaptive)");
     if (s != BZ_OK)
         return s;
+    collect_timing(h);  // phases of the last substep
     read_counters(h);
     return BZ_OK;
 }
