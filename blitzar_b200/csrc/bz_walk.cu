@@ -300,9 +300,13 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
         }
     };
     const int lane = threadIdx.x & 31;
-    if (cut) {
+    // Force-only evaluation above the minimum-distance floor runs the per-lane cutoff filter
+    const bool fast = !POT && p.eps2 > p.min_dist2;
+    if (cut && !fast) {
         // Drop leaves that no target of this warp can reach: a leaf whose (shifted) box is
         // farther than the cutoff from every lane's target holds no pair inside the cutoff.
+        // (With the per-lane filter this costs more than it saves: the filter drops the same
+        // sources exactly.)
         // Lane j loads the boxes of list entries j and j + 32 in one round (no serial chain
         // of loads); each box is then broadcast by shuffle and tested against every target.
         float4 lo[2], hi[2];
@@ -374,7 +378,6 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
     if (lane + 32 < nl)
         w.lpre[lane + 32] = i1 - c1;
     __syncwarp();
-    const bool fast = !POT && p.eps2 > p.min_dist2;
     SplitK sk;
     sk.inv2rs = inv2rs;
     sk.cexp = -1.4426950408889634f * inv2rs * inv2rs;
