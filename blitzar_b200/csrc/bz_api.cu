@@ -39,6 +39,7 @@ struct DeviceBuffers {
     int* id[2] = {};
     float4* pos4 = nullptr;
     float* acc[3] = {};
+    float* acc_pm[3] = {};  // mesh-leg accelerations when it runs on the second stream
     float* pot = nullptr;
     unsigned long long* keys = nullptr;
     uint32_t* perm = nullptr;
@@ -63,6 +64,8 @@ struct bz_handle {
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
+    cudaStream_t pm_stream = nullptr;  // TreePM: the mesh leg overlaps the tree build and walk
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     size_t capacity = 0;
     size_t n = 0;
     int cur = 0;
@@ -220,13 +223,22 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
 {
     const int n = static_cast<int>(h->n);
     DeviceBuffers& d = h->d;
+    // TreePM: the mesh leg needs only the ordered positions, so (outside phase timing) it runs
+    // on a second stream while this one builds the tree and walks; joined before the kick
+    const bool overlap = h->cfg.solver == BZ_SOLVER_TREEPM && h->pm && h->pm_stream && !h->timing;
+    if (overlap) {
+        cudaEventRecord(h->ev_fork, h->stream);
+        cudaStreamWaitEvent(h->pm_stream, h->ev_fork, 0);
+        pm_forces(h->pm, d.pos4, n, d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], h->pm_stream);
+        cudaEventRecord(h->ev_join, h->pm_stream);
+    }
     record(h, kPhTree);
     const int root_level = h->systems > 0 ? kSystemLevels : 0;
     launch_tree_build(d.keys, d.pos4, n, h->cfg.leaf_capacity, kMaxLevels, h->tree, d.err,
                       h->stream, root_level);
     launch_groups(h->tree, n, h->cfg.walk_group_size, root_level, d.keys, h->groups, h->stream);
     record(h, kPhMesh);
-    if (h->cfg.solver == BZ_SOLVER_TREEPM && h->pm) {
+    if (h->cfg.solver == BZ_SOLVER_TREEPM && h->pm && !overlap) {
         pm_forces(h->pm, d.pos4, n, d.acc[0], d.acc[1], d.acc[2], h->stream);
     } else {
         for (int a = 0; a < 3; ++a)
@@ -253,6 +265,10 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
         wp.rcorr2 = std::min(rc * rc, wp.rcut2);
     }
     launch_walk(d.pos4, n, h->tree, h->groups, wp, o, d.queue, d.spill, d.err, h->stream);
+    if (overlap) {
+        cudaStreamWaitEvent(h->stream, h->ev_join, 0);
+        launch_add3(d.acc[0], d.acc[1], d.acc[2], d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], n, h->stream);
+    }
     if (learned) {
         const float hcell = static_cast<float>(h->cfg.box_length / h->cfg.treepm_grid_size);
         launch_mlp_pairs(h->learn.params, d.pos4, n, h->learn.pair_src, h->learn.pair_cnt, hcell,
@@ -495,7 +511,15 @@ bz_status bz_destroy(bz_handle* h)
     for (int i = 0; i <= kEvStepStart; ++i)
         if (h->ev[i])
             cudaEventDestroy(h->ev[i]);
+    if (h->pm_stream)
+        cudaStreamSynchronize(h->pm_stream);
     pm_destroy(h->pm);
+    if (h->ev_fork)
+        cudaEventDestroy(h->ev_fork);
+    if (h->ev_join)
+        cudaEventDestroy(h->ev_join);
+    if (h->pm_stream)
+        cudaStreamDestroy(h->pm_stream);
     for (void* p : h->allocations)
         cudaFree(p);
     if (h->h_dt)
@@ -610,6 +634,20 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
             return BZ_OUT_OF_MEMORY;
         }
         h->bytes += pm_bytes(h->pm);
+        // second stream and fork/join events for the concurrent mesh leg (best effort: without
+        // them the mesh leg runs in line)
+        if (!dalloc(h, &h->d.acc_pm[0], n) || !dalloc(h, &h->d.acc_pm[1], n) || !dalloc(h, &h->d.acc_pm[2], n)) {
+            bz_destroy(h);
+            return BZ_OUT_OF_MEMORY;
+        }
+        if (cudaStreamCreateWithFlags(&h->pm_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            if (h->pm_stream)
+                cudaStreamDestroy(h->pm_stream);
+            h->pm_stream = nullptr;
+        }
     }
     for (int i = 0; i <= kEvStepStart; ++i)
         cudaEventCreate(&h->ev[i]);

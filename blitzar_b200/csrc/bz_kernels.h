@@ -188,6 +188,9 @@ void launch_energy(const double* vx, const double* vy, const double* vz, const f
 void launch_scatter3(const float* ax, const float* ay, const float* az, const int* id, int n,
                      float* out_soa3, cudaStream_t s);
 void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s);
+// a += b, three components
+void launch_add3(float* ax, float* ay, float* az, const float* bx, const float* by, const float* bz,
+                 int n, cudaStream_t s);
 
 // ---------------------------------------------------------------- adaptive steps (bz_adaptive.cu)
 struct AdaptiveParams {

@@ -473,6 +473,10 @@ int pm_solve(PmPlan* p, cudaStream_t s)
     const int M = p->mesh;
     const size_t half = static_cast<size_t>(M) * M * (M / 2 + 1);
     const int sms = sm_count();
+    // the transforms run on the caller's stream (the force pass may run the mesh leg on a
+    // second stream, concurrently with the tree build and walk)
+    cufftSetStream(p->r2c, s);
+    cufftSetStream(p->c2r, s);
     if (cufftExecR2C(p->r2c, p->rho, p->spec) != CUFFT_SUCCESS)
         return 1;
     if (p->gradient) {

@@ -201,6 +201,27 @@ void launch_scatter3(const float* ax, const float* ay, const float* az, const in
     k_scatter3<<<grid_for(n), kThreads, 0, s>>>(ax, ay, az, id, n, out_soa3);
 }
 
+namespace {
+__global__ void __launch_bounds__(kThreads) k_add3(float* __restrict__ ax, float* __restrict__ ay,
+                                                   float* __restrict__ az, const float* __restrict__ bx,
+                                                   const float* __restrict__ by,
+                                                   const float* __restrict__ bz, int n)
+{
+    for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
+        ax[i] += bx[i];
+        ay[i] += by[i];
+        az[i] += bz[i];
+    }
+}
+} // namespace
+
+void launch_add3(float* ax, float* ay, float* az, const float* bx, const float* by, const float* bz,
+                 int n, cudaStream_t s)
+{
+    count_launch();
+    k_add3<<<grid_for(n), kThreads, 0, s>>>(ax, ay, az, bx, by, bz, n);
+}
+
 void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s)
 {
     count_launch();
