@@ -49,6 +49,9 @@ WORKLOADS = {
     "treepm128": dict(kind="treepm", n_side=128, mesh=256, r_split_cells=1.0, r_cut_factor=5.0,
                       theta=0.5, eps_lattice=0.02, dt=5e-4, seed=2, rms_cells=0.2,
                       assignment="pcs", gradient="spectral", node_size_factor=0.5),
+    "treepm256": dict(kind="treepm", n_side=256, mesh=512, r_split_cells=1.0, r_cut_factor=5.0,
+                      theta=0.5, eps_lattice=0.02, dt=5e-4, seed=4, rms_cells=0.2,
+                      assignment="pcs", gradient="spectral", node_size_factor=0.5),
     "treepm128_cic": dict(kind="treepm", n_side=128, mesh=128, r_split_cells=1.25, r_cut_factor=4.5,
                           theta=0.5, eps_lattice=0.02, dt=5e-4, seed=2, rms_cells=0.2,
                           assignment="cic", gradient="centred-difference", node_size_factor=0.0),
@@ -75,6 +78,8 @@ def parse():
     ap.add_argument("--error-sample", type=int, default=2048)
     ap.add_argument("--cpu-sample", type=int, default=16384)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default leaf capacity, group size and mesh overlap")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-correction comparison (TreePM workloads)")
     return ap.parse_args()
@@ -430,6 +435,10 @@ def run_ours(args, w, rank, world, local):
     else:
         eng.set_state(pos, vel, mass, f64=True)
     dt = w["dt"]
+    tuned = None
+    if not args.no_autotune and not w.get("adaptive_levels"):
+        eng.autotune(trials=2)  # untimed: picks leaf capacity, group size, mesh overlap
+        tuned = eng.last_tune
     with torch.cuda.stream(stream):
         for _ in range(max(3, args.warmup)):
             eng.step(dt, 1)
@@ -615,6 +624,8 @@ def run_ours(args, w, rank, world, local):
         line["energy"] = drift
     if learned is not None:
         line["learned"] = learned
+    if tuned is not None:
+        line["autotune"] = tuned
     if adaptive:
         line["adaptive"] = {"max_level": w["adaptive_levels"], "eta": w["adaptive_eta"],
                             "block_steps": args.steps, "particle_steps": int(updates),

@@ -113,7 +113,7 @@ def load():
     L.bz_kernel_launches.restype = C.c_uint64
     L.bz_launches_per_step.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_energy.argtypes = [_vp, _vp, _vp, _vp]
-    L.bz_autotune.argtypes = [_vp, C.c_int32, _vp, _vp, _vp]
+    L.bz_autotune.argtypes = [_vp, C.c_int32, _vp, _vp, _vp, _vp]
     L.bz_adaptive_levels.argtypes = [_vp, _vp]
     L.bz_adaptive_updates.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_set_ensemble.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_int32]
@@ -302,8 +302,11 @@ class Engine:
         leaf = C.c_int32(0)
         grp = C.c_int32(0)
         ms = C.c_float(0.0)
-        self._check(self.L.bz_autotune(self.h, trials, C.byref(leaf), C.byref(grp), C.byref(ms)),
-                    "bz_autotune")
+        ov = C.c_int32(0)
+        self._check(self.L.bz_autotune(self.h, trials, C.byref(leaf), C.byref(grp), C.byref(ms),
+                                       C.byref(ov)), "bz_autotune")
+        self.last_tune = dict(leaf_capacity=leaf.value, walk_group_size=grp.value,
+                              mesh_overlap=bool(ov.value), ms_per_evaluation=ms.value)
         return leaf.value, grp.value, ms.value
 
     def energy(self, potential=True):

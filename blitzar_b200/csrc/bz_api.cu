@@ -65,6 +65,7 @@ struct bz_handle {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t pm_stream = nullptr;  // TreePM: the mesh leg overlaps the tree build and walk
+    bool mesh_overlap = true;          // use it (bz_autotune decides)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     size_t capacity = 0;
     size_t n = 0;
@@ -225,7 +226,8 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
     DeviceBuffers& d = h->d;
     // TreePM: the mesh leg needs only the ordered positions, so (outside phase timing) it runs
     // on a second stream while this one builds the tree and walks; joined before the kick
-    const bool overlap = h->cfg.solver == BZ_SOLVER_TREEPM && h->pm && h->pm_stream && !h->timing;
+    const bool overlap = h->cfg.solver == BZ_SOLVER_TREEPM && h->pm && h->pm_stream && h->mesh_overlap &&
+                         !h->timing;
     if (overlap) {
         cudaEventRecord(h->ev_fork, h->stream);
         cudaStreamWaitEvent(h->pm_stream, h->ev_fork, 0);
@@ -1155,7 +1157,7 @@ bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps)
 }
 
 bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int32_t* group_size,
-                      float* ms_per_evaluation)
+                      float* ms_per_evaluation, int32_t* mesh_overlap)
 {
     if (!h || h->n == 0 || trials < 1)
         return BZ_INVALID_ARGUMENT;
@@ -1165,6 +1167,8 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     static const int kLeaf[] = {8, 12, 16, 24, 32, 48};
     static const int kGroup[] = {16, 24, 32};
     const int leaf0 = h->cfg.leaf_capacity, group0 = h->cfg.walk_group_size;
+    const bool overlap0 = h->mesh_overlap;
+    const int n_overlap = h->pm_stream ? 2 : 1;  // TreePM: mesh leg concurrent or in line
     const bool timing0 = h->timing;
     h->timing = false;
     h->stepping = false;
@@ -1173,39 +1177,45 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     cudaEventCreate(&e1);
     float best = -1.0f;
     int best_leaf = leaf0, best_group = group0;
+    bool best_overlap = overlap0;
     bz_status st = BZ_OK;
-    for (int leaf : kLeaf) {
-        for (int group : kGroup) {
-            h->cfg.leaf_capacity = leaf;
-            h->cfg.walk_group_size = group;
-            enqueue_order(h);  // warm-up evaluation with these parameters
-            enqueue_forces(h, false, false);
-            cudaEventRecord(e0, h->stream);
-            for (int r = 0; r < trials; ++r) {
-                enqueue_order(h);
+    for (int ov = 0; ov < n_overlap && st == BZ_OK; ++ov) {
+        for (int leaf : kLeaf) {
+            for (int group : kGroup) {
+                h->mesh_overlap = ov == 0;
+                h->cfg.leaf_capacity = leaf;
+                h->cfg.walk_group_size = group;
+                enqueue_order(h);  // warm-up evaluation with these parameters
                 enqueue_forces(h, false, false);
+                cudaEventRecord(e0, h->stream);
+                for (int r = 0; r < trials; ++r) {
+                    enqueue_order(h);
+                    enqueue_forces(h, false, false);
+                }
+                cudaEventRecord(e1, h->stream);
+                st = check_device(h, "bz_autotune");
+                if (st != BZ_OK)
+                    break;
+                float ms = 0.0f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                ms /= static_cast<float>(trials);
+                if (best < 0.0f || ms < best) {
+                    best = ms;
+                    best_leaf = leaf;
+                    best_group = group;
+                    best_overlap = h->mesh_overlap;
+                }
             }
-            cudaEventRecord(e1, h->stream);
-            st = check_device(h, "bz_autotune");
             if (st != BZ_OK)
                 break;
-            float ms = 0.0f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            ms /= static_cast<float>(trials);
-            if (best < 0.0f || ms < best) {
-                best = ms;
-                best_leaf = leaf;
-                best_group = group;
-            }
         }
-        if (st != BZ_OK)
-            break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     h->timing = timing0;
     h->cfg.leaf_capacity = st == BZ_OK ? best_leaf : leaf0;
     h->cfg.walk_group_size = st == BZ_OK ? best_group : group0;
+    h->mesh_overlap = st == BZ_OK ? best_overlap : overlap0;
     // the captured step holds the old parameters: capture again on the next bz_step
     for (int i = 0; i < 2; ++i) {
         if (h->graph[i])
@@ -1221,6 +1231,8 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
         *group_size = best_group;
     if (ms_per_evaluation)
         *ms_per_evaluation = best;
+    if (mesh_overlap)
+        *mesh_overlap = best_overlap ? 1 : 0;
     return BZ_OK;
 }
 

@@ -130,10 +130,11 @@ bz_status bz_adaptive_updates(bz_handle* h, uint64_t* updates);
 
 /* Autotuner (no counterpart in the reference, whose leaf capacity and launch shapes are fixed
  * settings): times `trials` force evaluations of the current state for each leaf capacity in
- * {8, 12, 16, 24, 32, 48} and walk group size in {16, 24, 32}, keeps the fastest pair in the
- * handle's configuration and reports it.  The state is not advanced.  Outputs may be NULL. */
+ * {8, 12, 16, 24, 32, 48}, walk group size in {16, 24, 32} and, for TreePM, the mesh leg run
+ * concurrently with the tree build and walk or in line; keeps the fastest choice in the handle
+ * and reports it.  The state is not advanced.  Outputs may be NULL. */
 bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int32_t* group_size,
-                      float* ms_per_evaluation);
+                      float* ms_per_evaluation, int32_t* mesh_overlap);
 
 /* Accelerations (and optionally potentials) of the current state, caller's particle order,
  * SoA 3n floats.  Replaces computeOctreeAccelerationKernel (engine/physics/octree/cuda/force/
