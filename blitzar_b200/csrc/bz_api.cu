@@ -1061,18 +1061,51 @@ bz_status adaptive_steps(bz_handle* h, double dt, uint32_t nsteps)
         if (cudaStreamSynchronize(h->stream) != cudaSuccess)
             return check_device(h, "bz_step (adaptive)");
         L = std::min(std::max(L, 0), h->cfg.adaptive_max_level);
+        // The first substep of a block drifts, sorts and builds the tree as a plain step does;
+        // later substeps keep that topology, drift the particles inside it and refit every
+        // node's box and moments bottom-up (the walk needs correct ranges, boxes and moments,
+        // not Morton-consistent cells).
+        const int root_level = h->systems > 0 ? kSystemLevels : 0;
         for (int sub = 0; sub < (1 << L); ++sub) {
             record(h, kEvStepStart);
+            {
+                double* const* st = d.st[h->cur];
+                launch_adaptive_open_drift(st[0], st[1], st[2], st[3], st[4], st[5], d.id[h->cur], n,
+                                           p, h->ad.st, sub, L, h->stream);
+            }
+            if (sub == 0) {
+                enqueue_order(h);
+                record(h, kPhTree);
+                launch_tree_build(d.keys, d.pos4, n, h->cfg.leaf_capacity, kMaxLevels, h->tree, d.err,
+                                  h->stream, root_level);
+                launch_groups(h->tree, n, h->cfg.walk_group_size, root_level, d.keys, h->groups,
+                              h->stream);
+            } else {
+                double* const* st = d.st[h->cur];
+                record(h, kPhKeys);
+                record(h, kPhSort);
+                record(h, kPhPermute);
+                launch_refresh_pos4(st[0], st[1], st[2], d.mass[h->cur], n, d.pos4, h->stream);
+                record(h, kPhTree);
+                launch_tree_refit(d.pos4, h->tree, h->stream);
+            }
             double* const* st = d.st[h->cur];
-            launch_adaptive_open_drift(st[0], st[1], st[2], st[3], st[4], st[5], d.id[h->cur], n, p,
-                                       h->ad.st, sub, L, h->stream);
-            enqueue_order(h);
             launch_adaptive_active(d.id[h->cur], n, h->ad.st, sub, L, h->ad.active, h->stream);
-            h->walk_active = h->ad.active;
-            enqueue_forces(h, false, false);
-            h->walk_active = nullptr;
-            double* const* st2 = d.st[h->cur];
-            launch_adaptive_close(d.acc[0], d.acc[1], d.acc[2], st2[3], st2[4], st2[5], d.id[h->cur],
+            record(h, kPhMesh);
+            for (int a = 0; a < 3; ++a)
+                cudaMemsetAsync(d.acc[a], 0, sizeof(float) * n, h->stream);
+            record(h, kPhWalk);
+            cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), h->stream);
+            WalkOutputs o{};
+            o.ax = d.acc[0];
+            o.ay = d.acc[1];
+            o.az = d.acc[2];
+            o.totals = d.counters;
+            WalkParams wp = walk_params(h, false);
+            wp.active = h->ad.active;
+            launch_walk(d.pos4, n, h->tree, h->groups, wp, o, d.queue, d.spill, d.err, h->stream);
+            record(h, kPhIntegrate);
+            launch_adaptive_close(d.acc[0], d.acc[1], d.acc[2], st[3], st[4], st[5], d.id[h->cur],
                                   h->ad.active, n, p, h->ad.st, sub, L, h->stream);
         }
     }

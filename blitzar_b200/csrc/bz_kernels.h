@@ -90,6 +90,10 @@ void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4
                        int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s,
                        int min_split = 0);
 
+// Keep the topology, recompute every node's tight box and moments from the current pos4
+// (particles drifted inside their nodes: adaptive substeps).
+void launch_tree_refit(const float4* pos4, TreeArrays& t, cudaStream_t s);
+
 // Reference-mode topology: the single leaf the reference builds for its own keys.
 void launch_reference_leaf(const float* x, const float* y, const float* z, const float* m,
                            const uint32_t* sorted_index, int n, float* hot8, cudaStream_t s);
@@ -189,6 +193,9 @@ void launch_scatter3(const float* ax, const float* ay, const float* az, const in
                      float* out_soa3, cudaStream_t s);
 void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s);
 // a += b, three components
+// pos4[i] = {x, y, z, m} in FP32 from the FP64 state (same order)
+void launch_refresh_pos4(const double* x, const double* y, const double* z, const float* m, int n,
+                         float4* pos4, cudaStream_t s);
 void launch_add3(float* ax, float* ay, float* az, const float* bx, const float* by, const float* bz,
                  int n, cudaStream_t s);
 

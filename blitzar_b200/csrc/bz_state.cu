@@ -215,6 +215,26 @@ __global__ void __launch_bounds__(kThreads) k_add3(float* __restrict__ ax, float
 }
 } // namespace
 
+namespace {
+__global__ void __launch_bounds__(kThreads) k_refresh_pos4(const double* __restrict__ x,
+                                                           const double* __restrict__ y,
+                                                           const double* __restrict__ z,
+                                                           const float* __restrict__ m, int n,
+                                                           float4* __restrict__ pos4)
+{
+    for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads)
+        pos4[i] = make_float4(static_cast<float>(x[i]), static_cast<float>(y[i]),
+                              static_cast<float>(z[i]), m[i]);
+}
+} // namespace
+
+void launch_refresh_pos4(const double* x, const double* y, const double* z, const float* m, int n,
+                         float4* pos4, cudaStream_t s)
+{
+    count_launch();
+    k_refresh_pos4<<<grid_for(n), kThreads, 0, s>>>(x, y, z, m, n, pos4);
+}
+
 void launch_add3(float* ax, float* ay, float* az, const float* bx, const float* by, const float* bz,
                  int n, cudaStream_t s)
 {

@@ -357,6 +357,19 @@ __global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restr
 
 } // namespace
 
+void launch_tree_refit(const float4* pos4, TreeArrays& t, cudaStream_t s)
+{
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaMemsetAsync(t.arrive, 0, sizeof(int) * static_cast<size_t>(t.cap), s);
+    long long mb = (static_cast<long long>(t.cap) + kThreads - 1) / kThreads;
+    if (mb > 16LL * sms)
+        mb = 16LL * sms;
+    count_launch();
+    k_tree_moments<<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+}
+
 size_t tree_lookback_words(int cap) { return static_cast<size_t>(cap) / kLookbackNodes + 2 * kMaxLevels + 8; }
 
 void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
