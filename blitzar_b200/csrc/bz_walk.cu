@@ -47,6 +47,7 @@ struct __align__(16) WarpSmem {
         unsigned mask[kTile / 32][32];  // leaf flush: per-lane in-cutoff bits of the tile
     };
     float2 nd_qb[32];
+    float nd_tr[32];  // -tr(Q) eps^2 / 3 of each node (traceless Newtonian form only)
     int tidx[kTile];  // sorted index of each tile source (only when pairs are recorded)
     int stack[kStack];
     int nlist[kList];
@@ -218,6 +219,33 @@ __device__ __forceinline__ void pair_pn(const float4 mo, const float4 qa, const 
     }
 }
 
+// Force-only Newtonian quadrupole interaction with the traceless second moment
+// Q' = Q - tr(Q)/3 I.  With softening the trace does not drop out of the expansion; written with
+// Q' the acceleration is (m/s^3 + 15/2 (dQ'd + trm)/s^7) d - 3 Q'd/s^5 with s^2 = r^2 + eps^2 and
+// trm = -tr(Q) eps^2/3, algebraically the same as the traceful form (the m/s^3 + (15/2 dQd/s^7 -
+// 3/2 tr/s^5)) d - 3 Qd/s^5 of pair_pn).  Used only when eps^2 exceeds the minimum distance^2,
+// so the minimum-distance guard of pair_pn can never trigger.
+__device__ __forceinline__ void pair_pn_newton(const float4 mo, const float4 qa, const float2 qb,
+                                               float trm, float tx, float ty, float tz, float eps2,
+                                               float& fx, float& fy, float& fz)
+{
+    const float dx = mo.x - tx, dy = mo.y - ty, dz = mo.z - tz;
+    const float s2 = fmaf(dx, dx, fmaf(dy, dy, fmaf(dz, dz, eps2)));
+    const float rinv = rsqrt_approx(s2);
+    const float a = rinv * rinv;       // 1/r^2
+    const float b = rinv * a;          // 1/r^3
+    const float t5 = b * a;            // 1/r^5
+    const float qdx = fmaf(qa.x, dx, fmaf(qa.y, dy, qa.z * dz));
+    const float qdy = fmaf(qa.y, dx, fmaf(qa.w, dy, qb.x * dz));
+    const float qdz = fmaf(qa.z, dx, fmaf(qb.x, dy, qb.y * dz));
+    const float dqd = fmaf(dx, qdx, fmaf(dy, qdy, fmaf(dz, qdz, trm)));
+    const float c0 = fmaf(7.5f * t5, a * dqd, mo.w * b);
+    const float n2 = -3.0f * t5;
+    fx = fmaf(c0, dx, fmaf(n2, qdx, fx));
+    fy = fmaf(c0, dy, fmaf(n2, qdy, fy));
+    fz = fmaf(c0, dz, fmaf(n2, qdz, fz));
+}
+
 struct Acc {
     float s[4];
     float e[4];
@@ -247,6 +275,8 @@ __device__ __forceinline__ void flush_nodes(WarpSmem& w, int nn, const TreeArray
                                             float ty, float tz, Acc& acc)
 {
     const int lane = threadIdx.x & 31;
+    // Newtonian force-only quadrupoles take the traceless form; it needs eps^2 > min distance^2
+    const bool newton = !SPLIT && QUAD && !POT && p.eps2 > p.min_dist2;
     for (int base = 0; base < nn; base += 32) {
         const int m = min(32, nn - base);
         if (lane < m) {
@@ -261,16 +291,39 @@ __device__ __forceinline__ void flush_nodes(WarpSmem& w, int nn, const TreeArray
             }
             w.nd_mono[lane] = mo;
             if (QUAD) {
-                w.nd_qa[lane] = t.quadA[k];
-                w.nd_qb[lane] = t.quadB[k];
+                float4 qa = t.quadA[k];
+                float2 qb = t.quadB[k];
+                if (newton) {
+                    const float tr = qa.x + qa.w + qb.y;
+                    const float tr3 = tr * (1.0f / 3.0f);
+                    qa.x -= tr3;
+                    qa.w -= tr3;
+                    qb.y -= tr3;
+                    w.nd_tr[lane] = -tr3 * p.eps2;
+                }
+                w.nd_qa[lane] = qa;
+                w.nd_qb[lane] = qb;
             }
         }
         __syncwarp();
         float fx = 0.0f, fy = 0.0f, fz = 0.0f, fp = 0.0f;
-        for (int j = 0; j < m; ++j) {
-            const float4 qa = QUAD ? w.nd_qa[j] : make_float4(0, 0, 0, 0);
-            const float2 qb = QUAD ? w.nd_qb[j] : make_float2(0, 0);
-            pair_pn<SPLIT, QUAD, POT>(w.nd_mono[j], qa, qb, tx, ty, tz, p, inv2rs, fx, fy, fz, fp);
+        if (newton) {
+            int j = 0;
+            for (; j + 1 < m; j += 2) {
+                pair_pn_newton(w.nd_mono[j], w.nd_qa[j], w.nd_qb[j], w.nd_tr[j], tx, ty, tz, p.eps2,
+                               fx, fy, fz);
+                pair_pn_newton(w.nd_mono[j + 1], w.nd_qa[j + 1], w.nd_qb[j + 1], w.nd_tr[j + 1], tx,
+                               ty, tz, p.eps2, fx, fy, fz);
+            }
+            if (j < m)
+                pair_pn_newton(w.nd_mono[j], w.nd_qa[j], w.nd_qb[j], w.nd_tr[j], tx, ty, tz, p.eps2,
+                               fx, fy, fz);
+        } else {
+            for (int j = 0; j < m; ++j) {
+                const float4 qa = QUAD ? w.nd_qa[j] : make_float4(0, 0, 0, 0);
+                const float2 qb = QUAD ? w.nd_qb[j] : make_float2(0, 0);
+                pair_pn<SPLIT, QUAD, POT>(w.nd_mono[j], qa, qb, tx, ty, tz, p, inv2rs, fx, fy, fz, fp);
+            }
         }
         acc.add(0, fx);
         acc.add(1, fy);
