@@ -27,7 +27,7 @@ EXPORTS = (
     "bz_status_string", "bz_version", "bz_kernel_launches", "bz_launches_per_step",
     "bz_sort_pairs_noalloc", "bz_energy", "bz_autotune", "bz_learn_generate", "bz_learn_train",
     "bz_learn_set", "bz_learn_get", "bz_learn_enable", "bz_learn_forward", "bz_learn_gradient",
-    "bz_set_ensemble", "bz_adaptive_levels", "bz_adaptive_updates",
+    "bz_set_ensemble", "bz_adaptive_levels", "bz_adaptive_updates", "bz_set_mesh_schedule",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -114,6 +114,7 @@ def load():
     L.bz_launches_per_step.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_energy.argtypes = [_vp, _vp, _vp, _vp]
     L.bz_autotune.argtypes = [_vp, C.c_int32, _vp, _vp, _vp, _vp]
+    L.bz_set_mesh_schedule.argtypes = [_vp, C.c_int32]
     L.bz_adaptive_levels.argtypes = [_vp, _vp]
     L.bz_adaptive_updates.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_set_ensemble.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_int32]
@@ -298,7 +299,9 @@ class Engine:
         return g, loss.value
 
     def autotune(self, trials=3):
-        """Pick the fastest (leaf capacity, walk group size) for the current state."""
+        """Pick the fastest (leaf capacity, walk group size, TreePM mesh schedule) for the current
+        state; the schedule is 0 in line, 1 concurrent with the tree build and walk, 2 also
+        concurrent with the sort."""
         leaf = C.c_int32(0)
         grp = C.c_int32(0)
         ms = C.c_float(0.0)
@@ -306,8 +309,13 @@ class Engine:
         self._check(self.L.bz_autotune(self.h, trials, C.byref(leaf), C.byref(grp), C.byref(ms),
                                        C.byref(ov)), "bz_autotune")
         self.last_tune = dict(leaf_capacity=leaf.value, walk_group_size=grp.value,
-                              mesh_overlap=bool(ov.value), ms_per_evaluation=ms.value)
+                              mesh_schedule=ov.value, ms_per_evaluation=ms.value)
         return leaf.value, grp.value, ms.value
+
+    def set_mesh_schedule(self, schedule):
+        """Pin the TreePM mesh-leg schedule (0 in line, 1 concurrent with the tree build and
+        walk, 2 also concurrent with the sort)."""
+        self._check(self.L.bz_set_mesh_schedule(self.h, int(schedule)), "bz_set_mesh_schedule")
 
     def energy(self, potential=True):
         """FP64 (kinetic, potential or None, momentum[3]) of the current state."""

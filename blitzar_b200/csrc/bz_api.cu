@@ -40,6 +40,7 @@ struct DeviceBuffers {
     float4* pos4 = nullptr;
     float* acc[3] = {};
     float* acc_pm[3] = {};  // mesh-leg accelerations when it runs on the second stream
+    float4* pos4_drift = nullptr;  // drifted FP32 positions in the pre-sort order (mesh mode 2)
     float* pot = nullptr;
     unsigned long long* keys = nullptr;
     uint32_t* perm = nullptr;
@@ -65,8 +66,13 @@ struct bz_handle {
     cudaStream_t stream = nullptr;
     bool own_stream = false;
     cudaStream_t pm_stream = nullptr;  // TreePM: the mesh leg overlaps the tree build and walk
-    bool mesh_overlap = true;          // use it (bz_autotune decides)
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // TreePM mesh-leg schedule (bz_autotune decides): 0 in line on the main stream; 1 on
+    // pm_stream, forked after the sort, concurrent with the tree build and walk; 2 as 1, but in a
+    // step the deposit and field solve are forked right after the drift (they take the particles
+    // in any order), so they also run concurrently with the keys, sort and permutation; only the
+    // interpolation waits for the new order
+    int mesh_overlap = 1;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_sorted = nullptr;
     size_t capacity = 0;
     size_t n = 0;
     int cur = 0;
@@ -219,19 +225,33 @@ void enqueue_order(bz_handle* h)
     h->cur = nxt;
 }
 
-// Forces of the (already ordered) state into d.acc; optional closing kick.
-void enqueue_forces(bz_handle* h, bool kick, bool want_pot)
+// TreePM with the mesh leg on the second stream (outside phase timing).
+bool mesh_concurrent(const bz_handle* h)
+{
+    return h->cfg.solver == BZ_SOLVER_TREEPM && h->pm && h->pm_stream && h->mesh_overlap > 0 &&
+           !h->timing;
+}
+
+// Forces of the (already ordered) state into d.acc; optional closing kick.  `mesh_forked`: the
+// step already forked the deposit and field solve onto pm_stream (mesh mode 2).
+void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = false)
 {
     const int n = static_cast<int>(h->n);
     DeviceBuffers& d = h->d;
-    // TreePM: the mesh leg needs only the ordered positions, so (outside phase timing) it runs
-    // on a second stream while this one builds the tree and walks; joined before the kick
-    const bool overlap = h->cfg.solver == BZ_SOLVER_TREEPM && h->pm && h->pm_stream && h->mesh_overlap &&
-                         !h->timing;
+    // TreePM: the mesh leg needs only the ordered positions, so it runs on a second stream
+    // while this one builds the tree and walks; joined before the kick
+    const bool overlap = mesh_concurrent(h);
     if (overlap) {
-        cudaEventRecord(h->ev_fork, h->stream);
-        cudaStreamWaitEvent(h->pm_stream, h->ev_fork, 0);
-        pm_forces(h->pm, d.pos4, n, d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], h->pm_stream);
+        if (mesh_forked) {
+            // deposit and solve are under way; the interpolation needs the new order
+            cudaEventRecord(h->ev_sorted, h->stream);
+            cudaStreamWaitEvent(h->pm_stream, h->ev_sorted, 0);
+            pm_interp(h->pm, d.pos4, n, d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], h->pm_stream);
+        } else {
+            cudaEventRecord(h->ev_fork, h->stream);
+            cudaStreamWaitEvent(h->pm_stream, h->ev_fork, 0);
+            pm_forces(h->pm, d.pos4, n, d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], h->pm_stream);
+        }
         cudaEventRecord(h->ev_join, h->pm_stream);
     }
     record(h, kPhTree);
@@ -289,10 +309,20 @@ void enqueue_step(bz_handle* h)
     const int n = static_cast<int>(h->n);
     DeviceBuffers& d = h->d;
     double* const* s = d.st[h->cur];
+    const bool early = mesh_concurrent(h) && h->mesh_overlap == 2;
     launch_kick_drift(s[0], s[1], s[2], s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt,
-                      periodic(h) ? h->cfg.box_length : 0.0, nullptr, h->stream);
+                      periodic(h) ? h->cfg.box_length : 0.0, nullptr, h->stream,
+                      early ? d.mass[h->cur] : nullptr, early ? d.pos4_drift : nullptr);
+    if (early) {
+        // the mass deposit is a sum over particles in any order: start it and the field solve
+        // now, concurrently with the keys, sort and permutation of this stream
+        cudaEventRecord(h->ev_fork, h->stream);
+        cudaStreamWaitEvent(h->pm_stream, h->ev_fork, 0);
+        pm_deposit(h->pm, d.pos4_drift, n, h->pm_stream);
+        pm_solve(h->pm, h->pm_stream);
+    }
     enqueue_order(h);
-    enqueue_forces(h, true, false);
+    enqueue_forces(h, true, false, early);
 }
 
 bz_status check_device(bz_handle* h, const char* what)
@@ -520,6 +550,8 @@ bz_status bz_destroy(bz_handle* h)
         cudaEventDestroy(h->ev_fork);
     if (h->ev_join)
         cudaEventDestroy(h->ev_join);
+    if (h->ev_sorted)
+        cudaEventDestroy(h->ev_sorted);
     if (h->pm_stream)
         cudaStreamDestroy(h->pm_stream);
     for (void* p : h->allocations)
@@ -638,13 +670,15 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
         h->bytes += pm_bytes(h->pm);
         // second stream and fork/join events for the concurrent mesh leg (best effort: without
         // them the mesh leg runs in line)
-        if (!dalloc(h, &h->d.acc_pm[0], n) || !dalloc(h, &h->d.acc_pm[1], n) || !dalloc(h, &h->d.acc_pm[2], n)) {
+        if (!dalloc(h, &h->d.acc_pm[0], n) || !dalloc(h, &h->d.acc_pm[1], n) || !dalloc(h, &h->d.acc_pm[2], n) ||
+            !dalloc(h, &h->d.pos4_drift, n)) {
             bz_destroy(h);
             return BZ_OUT_OF_MEMORY;
         }
         if (cudaStreamCreateWithFlags(&h->pm_stream, cudaStreamNonBlocking) != cudaSuccess ||
             cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
-            cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+            cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_sorted, cudaEventDisableTiming) != cudaSuccess) {
             cudaGetLastError();
             if (h->pm_stream)
                 cudaStreamDestroy(h->pm_stream);
@@ -1189,6 +1223,21 @@ bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps)
     return BZ_OK;
 }
 
+bz_status bz_set_mesh_schedule(bz_handle* h, int32_t schedule)
+{
+    if (!h || schedule < 0 || schedule > 2)
+        return BZ_INVALID_ARGUMENT;
+    if (h->mesh_overlap != schedule) {
+        h->mesh_overlap = schedule;
+        for (int i = 0; i < 2; ++i) {  // captured steps hold the old schedule
+            if (h->graph[i])
+                cudaGraphExecDestroy(h->graph[i]);
+            h->graph[i] = nullptr;
+        }
+    }
+    return BZ_OK;
+}
+
 bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int32_t* group_size,
                       float* ms_per_evaluation, int32_t* mesh_overlap)
 {
@@ -1200,31 +1249,34 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     static const int kLeaf[] = {8, 12, 16, 24, 32, 48};
     static const int kGroup[] = {16, 24, 32};
     const int leaf0 = h->cfg.leaf_capacity, group0 = h->cfg.walk_group_size;
-    const bool overlap0 = h->mesh_overlap;
-    const int n_overlap = h->pm_stream ? 2 : 1;  // TreePM: mesh leg concurrent or in line
+    const int overlap0 = h->mesh_overlap;
+    const int n_overlap = h->pm_stream ? 3 : 1;  // TreePM: the three mesh-leg schedules
     const bool timing0 = h->timing;
     h->timing = false;
     h->stepping = false;
+    // The timed unit is a step of zero length (drift, order, forces, kick): it leaves positions
+    // and velocities unchanged (x + 0 v, v + 0 a with finite forces of the current state), and
+    // it is the unit in which the mesh schedules differ.
+    bz_status st = ensure_forces(h);
+    if (st != BZ_OK)
+        return st;
+    cudaMemsetAsync(h->d.dt, 0, 2 * sizeof(double), h->stream);
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     float best = -1.0f;
     int best_leaf = leaf0, best_group = group0;
-    bool best_overlap = overlap0;
-    bz_status st = BZ_OK;
+    int best_overlap = overlap0;
     for (int ov = 0; ov < n_overlap && st == BZ_OK; ++ov) {
         for (int leaf : kLeaf) {
             for (int group : kGroup) {
-                h->mesh_overlap = ov == 0;
+                h->mesh_overlap = n_overlap > 1 ? ov : overlap0;
                 h->cfg.leaf_capacity = leaf;
                 h->cfg.walk_group_size = group;
-                enqueue_order(h);  // warm-up evaluation with these parameters
-                enqueue_forces(h, false, false);
+                enqueue_step(h);  // warm-up step with these parameters
                 cudaEventRecord(e0, h->stream);
-                for (int r = 0; r < trials; ++r) {
-                    enqueue_order(h);
-                    enqueue_forces(h, false, false);
-                }
+                for (int r = 0; r < trials; ++r)
+                    enqueue_step(h);
                 cudaEventRecord(e1, h->stream);
                 st = check_device(h, "bz_autotune");
                 if (st != BZ_OK)
@@ -1265,7 +1317,7 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     if (ms_per_evaluation)
         *ms_per_evaluation = best;
     if (mesh_overlap)
-        *mesh_overlap = best_overlap ? 1 : 0;
+        *mesh_overlap = best_overlap;
     return BZ_OK;
 }
 

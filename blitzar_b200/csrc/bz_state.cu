@@ -90,7 +90,9 @@ __global__ void __launch_bounds__(kThreads) k_kick_drift(double* __restrict__ x,
                                                           const float* __restrict__ ay,
                                                           const float* __restrict__ az, int n,
                                                           const double* __restrict__ dtp,
-                                                          double L, BoxF64* box)
+                                                          double L, BoxF64* box,
+                                                          const float* __restrict__ mass,
+                                                          float4* __restrict__ pos4)
 {
     const double dt = *dtp;
     const double h = 0.5 * dt;
@@ -107,6 +109,9 @@ __global__ void __launch_bounds__(kThreads) k_kick_drift(double* __restrict__ x,
         x[i] = p[0];
         y[i] = p[1];
         z[i] = p[2];
+        if (pos4)  // FP32 copy in the current (pre-sort) order, as k_permute converts it
+            pos4[i] = make_float4(static_cast<float>(p[0]), static_cast<float>(p[1]),
+                                  static_cast<float>(p[2]), mass[i]);
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             mn[a] = fmin(mn[a], p[a]);
@@ -183,7 +188,8 @@ void launch_kick(double* vx, double* vy, double* vz, const float* ax, const floa
 
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
                        const float* ax, const float* ay, const float* az, int n,
-                       const double* dt, double periodic_len, BoxF64* box, cudaStream_t s)
+                       const double* dt, double periodic_len, BoxF64* box, cudaStream_t s,
+                       const float* mass, float4* pos4)
 {
     if (box) {
         count_launch();
@@ -191,7 +197,7 @@ void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, 
     }
     count_launch();
     k_kick_drift<<<grid_for(n), kThreads, 0, s>>>(x, y, z, vx, vy, vz, ax, ay, az, n, dt,
-                                                  periodic_len, box);
+                                                  periodic_len, box, mass, pos4);
 }
 
 void launch_scatter3(const float* ax, const float* ay, const float* az, const int* id, int n,

@@ -129,12 +129,20 @@ bz_status bz_adaptive_levels(bz_handle* h, uint8_t* levels);
 bz_status bz_adaptive_updates(bz_handle* h, uint64_t* updates);
 
 /* Autotuner (no counterpart in the reference, whose leaf capacity and launch shapes are fixed
- * settings): times `trials` force evaluations of the current state for each leaf capacity in
- * {8, 12, 16, 24, 32, 48}, walk group size in {16, 24, 32} and, for TreePM, the mesh leg run
- * concurrently with the tree build and walk or in line; keeps the fastest choice in the handle
- * and reports it.  The state is not advanced.  Outputs may be NULL. */
+ * settings): times `trials` steps of zero length (drift, keys, sort, forces, kick; positions and
+ * velocities come out unchanged) of the current state for each leaf capacity in
+ * {8, 12, 16, 24, 32, 48}, walk group size in {16, 24, 32} and, for TreePM, each mesh-leg
+ * schedule: *mesh_overlap = 0 in line; 1 on a second stream concurrent with the tree build and
+ * walk; 2 as 1 with the deposit and field solve also concurrent with the keys, sort and
+ * permutation of a step.  Keeps the fastest choice in the handle and reports it, with the time
+ * of one such step in *ms_per_evaluation.  Outputs may be NULL. */
 bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int32_t* group_size,
                       float* ms_per_evaluation, int32_t* mesh_overlap);
+
+/* Pins the TreePM mesh-leg schedule (0, 1 or 2 as reported by bz_autotune; the default is 1).
+ * Schedules 1 and 2 need the second stream, created with the handle; without it every schedule
+ * runs in line.  The results of the schedules differ only in the order of the float mass sums. */
+bz_status bz_set_mesh_schedule(bz_handle* h, int32_t schedule);
 
 /* Accelerations (and optionally potentials) of the current state, caller's particle order,
  * SoA 3n floats.  Replaces computeOctreeAccelerationKernel (engine/physics/octree/cuda/force/

@@ -137,3 +137,49 @@ def test_node_size_cap_matches_oracle(gpu, oracle):
     sizes = w["group_sizes"]
     assert npp == int((w["n_pp"] * sizes).sum())
     assert npn == int((w["n_pn"] * sizes).sum())
+
+
+def _treepm_run(schedule, pos, vel, m, steps, use_graph=1, tune=False):
+    n = len(m)
+    with _engine(n, solver=1, box_length=1.0, treepm_grid_size=64, treepm_assignment=2,
+                 treepm_gradient=1, treepm_window_floor=0.0, treepm_r_cut_factor=5.0,
+                 treepm_node_size_factor=0.5, octree_softening=0.02 / 64, use_graph=use_graph) as e:
+        e.set_state(pos, vel, m, f64=True)
+        if tune:
+            before = e.get_state(f64=True)
+            e.autotune(trials=1)
+            after = e.get_state(f64=True)
+            return before, after, e.last_tune
+        e.set_mesh_schedule(schedule)
+        e.step(1e-3, steps)
+        return e.get_state(f64=True)
+
+
+@pytest.mark.parametrize("use_graph", [0, 1])
+def test_mesh_schedules_agree(gpu, use_graph):
+    """The three mesh-leg schedules (in line; concurrent with the tree build and walk; deposit and
+    field solve forked at the drift) compute the same step: they differ only in the order of the
+    float mass sums of the deposit."""
+    n = 32 ** 3
+    rng = np.random.default_rng(41)
+    g = (np.indices((32, 32, 32)).reshape(3, -1).T + 0.5) / 32.0
+    pos = (g + 0.2 / 32 * rng.standard_normal(g.shape)) % 1.0
+    vel = 0.05 * rng.standard_normal(g.shape)
+    m = np.full(n, 1.0 / n, np.float32)
+    runs = [_treepm_run(s, pos, vel, m, 6, use_graph) for s in (0, 1, 2)]
+    for p, v in runs[1:]:
+        assert np.abs(p - runs[0][0]).max() < 1e-9
+        assert np.abs(v - runs[0][1]).max() < 1e-6 * np.abs(runs[0][1]).max()
+
+
+def test_autotune_leaves_state_unchanged(gpu):
+    """The autotuner times zero-length steps: positions and velocities come out bit for bit."""
+    n = 16 ** 3
+    rng = np.random.default_rng(42)
+    pos = rng.random((n, 3))
+    vel = 0.1 * rng.standard_normal((n, 3))
+    m = np.full(n, 1.0 / n, np.float32)
+    before, after, tune = _treepm_run(None, pos, vel, m, 0, tune=True)
+    assert tune["mesh_schedule"] in (0, 1, 2)
+    for a, b in zip(before, after):  # caller order
+        assert np.array_equal(a, b)
