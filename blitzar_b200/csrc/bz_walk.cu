@@ -496,6 +496,9 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
             // result is bit-identical to summing every listed source in tile order.
             const int nb = cend - cbase;
             const int nw = (nb + 31) >> 5;
+            // r2 <= rcut2 exactly when r2 - next_float(rcut2) is negative (a float difference
+            // has the exact sign), so the sign bit is the mask bit: one funnel shift appends it
+            const float rc2n = __uint_as_float(__float_as_uint(p.rcut2) + 1u);
             for (int wd = 0; wd < nw; ++wd) {
                 const int qb = wd << 5;
                 unsigned m = 0u;
@@ -506,7 +509,7 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                         const float4 s4 = w.tile[qb + b];
                         const float dx = s4.x - tx, dy = s4.y - ty, dz = s4.z - tz;
                         const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-                        m = (m << 1) | (r2 <= p.rcut2 ? 1u : 0u);
+                        m = __funnelshift_l(__float_as_uint(__fsub_rn(r2, rc2n)), m, 1);
                     }
                 } else {
                     for (int b = 0; qb + b < nb; ++b) {
