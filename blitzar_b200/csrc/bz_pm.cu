@@ -107,6 +107,20 @@ __device__ __forceinline__ int wrapm(int i, int m)
     return i < 0 ? i + m : i;
 }
 
+// Index i + d, d in [-m, m], wrapped into [0, m).
+__device__ __forceinline__ int wrap1(int i, int m) { return i < 0 ? i + m : (i >= m ? i - m : i); }
+
+// Weight of stencil column q (a lane's own column) without indexing a register array.
+template <int P>
+__device__ __forceinline__ float column_weight(const float* w, int q)
+{
+    float r = 0.0f;
+#pragma unroll
+    for (int a = 0; a < P; ++a)
+        r = q == a ? w[a] : r;
+    return r;
+}
+
 template <int P>
 __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __restrict__ pos4, int n,
                                                              int chunk, int mesh, float inv_h,
@@ -316,9 +330,12 @@ __global__ void __launch_bounds__(kThreads) k_pack_force(const float* __restrict
         force[i] = make_float4(f3[i], f3[total + i], f3[2 * total + i], 0.0f);
 }
 
-// Interpolation: the same order-p stencil gathers the interleaved force mesh at each
-// particle (Morton order keeps neighbouring threads on neighbouring cells, so the gathers hit
-// L1/L2).
+// Interpolation with four lanes per particle: lane q of a quad gathers stencil column
+// x = bx + q of every (y, z) row of the order-p stencil from the interleaved force mesh, and the
+// quad adds its partial sums.  A quad thus reads whole 64-byte rows, and the eight
+// Morton-consecutive particles of a warp share most of their rows, so one load instruction
+// touches a few cache lines instead of one per lane (the one-lane-per-particle form is bound
+// by L1 wavefronts).
 template <int P>
 __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ pos4, int n, int mesh,
                                                       float inv_h, const float4* __restrict__ force,
@@ -326,37 +343,45 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
                                                       float* __restrict__ az)
 {
     const size_t M = static_cast<size_t>(mesh);
-    for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
-        const float4 p = pos4[i];
-        float wx[P], wy[P], wz[P];
-        const int bx = stencil<P>(p.x, inv_h, mesh, wx);
-        const int by = stencil<P>(p.y, inv_h, mesh, wy);
-        const int bz = stencil<P>(p.z, inv_h, mesh, wz);
-        int xs[P];
-#pragma unroll
-        for (int a = 0; a < P; ++a)
-            xs[a] = wrapm(bx + a, mesh);
+    const int q = threadIdx.x & 3;
+    const int warps = gridDim.x * (kThreads / 32);
+    const int gw = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
+    for (int i0 = gw * 8; i0 < n; i0 += warps * 8) {
+        const int i = i0 + ((threadIdx.x & 31) >> 2);
         float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+        if (i < n && q < P) {
+            const float4 p = pos4[i];
+            float wx[P], wy[P], wz[P];
+            const int bx = stencil<P>(p.x, inv_h, mesh, wx);
+            const int by = stencil<P>(p.y, inv_h, mesh, wy);
+            const int bz = stencil<P>(p.z, inv_h, mesh, wz);
+            const float wq = column_weight<P>(wx, q);
+            const int xs = wrap1(bx + q, mesh);
 #pragma unroll
-        for (int c = 0; c < P; ++c) {
-            const size_t zrow = static_cast<size_t>(wrapm(bz + c, mesh)) * M;
+            for (int c = 0; c < P; ++c) {
+                const size_t zrow = static_cast<size_t>(wrap1(bz + c, mesh)) * M;
+                const float wzq = wz[c] * wq;
 #pragma unroll
-            for (int b = 0; b < P; ++b) {
-                const size_t row = (zrow + wrapm(by + b, mesh)) * M;
-                const float wzy = wz[c] * wy[b];
-#pragma unroll
-                for (int a = 0; a < P; ++a) {
-                    const float4 f = __ldg(&force[row + xs[a]]);
-                    const float w = wzy * wx[a];
+                for (int b = 0; b < P; ++b) {
+                    const float4 f = __ldg(&force[(zrow + wrap1(by + b, mesh)) * M + xs]);
+                    const float w = wzq * wy[b];
                     gx = fmaf(w, f.x, gx);
                     gy = fmaf(w, f.y, gy);
                     gz = fmaf(w, f.z, gz);
                 }
             }
         }
-        ax[i] = gx;
-        ay[i] = gy;
-        az[i] = gz;
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+            gx += __shfl_xor_sync(kFullMask, gx, o);
+            gy += __shfl_xor_sync(kFullMask, gy, o);
+            gz += __shfl_xor_sync(kFullMask, gz, o);
+        }
+        if (i < n && q == 0) {
+            ax[i] = gx;
+            ay[i] = gy;
+            az[i] = gz;
+        }
     }
 }
 
@@ -504,7 +529,7 @@ void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float
 {
     const int M = p->mesh;
     const float inv_h = static_cast<float>(M / p->box);
-    int b = (n + kThreads - 1) / kThreads;
+    int b = (n + kThreads / 4 - 1) / (kThreads / 4);  // four lanes per particle
     b = b < sm_count() * 8 ? b : sm_count() * 8;
     count_launch();
     if (p->order == 2)
