@@ -79,6 +79,7 @@ struct bz_handle {
     bool forces_valid = false;
     DeviceBuffers d;
     SortWorkspace sort{};
+    AdaptiveSortWorkspace asort{};  // the per-step re-sort of nearly sorted keys
     TreeArrays tree{};
     GroupTable groups{};
     PmPlan* pm = nullptr;
@@ -217,7 +218,8 @@ void enqueue_order(bz_handle* h)
                       d.perm, h->stream);
     }
     record(h, kPhSort);
-    launch_radix_sort(d.keys, d.perm, n, 64, h->sort, d.err, h->stream);
+    // the keys arrive in the previous sorted order (perm = identity): nearly sorted after a step
+    launch_radix_sort_adaptive(d.keys, d.perm, n, 64, h->sort, h->asort, d.err, h->stream);
     record(h, kPhPermute);
     const int nxt = h->cur ^ 1;
     launch_permute(d.perm, n, d.st[h->cur], d.st[nxt], 6, d.mass[h->cur], d.mass[nxt],
@@ -628,6 +630,16 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
          dalloc(h, &sw.base, 8 * 256) && dalloc(h, &sw.ticket, 8) && dalloc(h, &sw.epoch, 1) &&
          dalloc(h, &sw.trivial, 8) && dalloc(h, &sw.state, words);
     sw.max_tiles = static_cast<int>(words / 256);
+    AdaptiveSortWorkspace& aw = h->asort;
+    aw.cap = adaptive_sort_cap(static_cast<int>(n));
+    SortWorkspace& fw = aw.fsort;
+    const size_t fwords = sort_state_words(aw.cap);
+    ok = ok && dalloc(h, &aw.fkeys, aw.cap) && dalloc(h, &aw.fvals, aw.cap) && dalloc(h, &aw.flag, n) &&
+         dalloc(h, &aw.block_sums, adaptive_sort_blocks(static_cast<int>(n))) && dalloc(h, &aw.ctl, 4) &&
+         dalloc(h, &fw.keys_alt, aw.cap) && dalloc(h, &fw.vals_alt, aw.cap) && dalloc(h, &fw.hist, 8 * 256) &&
+         dalloc(h, &fw.base, 8 * 256) && dalloc(h, &fw.ticket, 8) && dalloc(h, &fw.epoch, 1) &&
+         dalloc(h, &fw.trivial, 8) && dalloc(h, &fw.state, fwords);
+    fw.max_tiles = static_cast<int>(fwords / 256);
     // tree
     TreeArrays& t = h->tree;
     t.cap = static_cast<int>(2 * n + 1024);
@@ -657,6 +669,8 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     }
     cudaMemsetAsync(sw.state, 0, words * sizeof(unsigned long long), h->stream);
     cudaMemsetAsync(sw.epoch, 0, sizeof(uint32_t), h->stream);
+    cudaMemsetAsync(h->asort.fsort.epoch, 0, sizeof(uint32_t), h->stream);
+    cudaMemsetAsync(h->asort.fsort.state, 0, fwords * sizeof(unsigned long long), h->stream);
     cudaMemsetAsync(d.err, 0, sizeof(int), h->stream);
     if (cfg->solver == BZ_SOLVER_TREEPM) {
         int perr = 0;
@@ -1654,7 +1668,7 @@ bz_status bz_morton_keys(bz_handle* h, uint64_t* sorted_keys, int32_t* perm)
             launch_bbox_f64(tmp, tmp + n, tmp + 2 * n, n, d.box, h->stream);
         launch_keys63(tmp, tmp + n, tmp + 2 * n, n, d.box, periodic(h) ? h->cfg.box_length : 0.0,
                       d.keys, d.perm, h->stream);
-        launch_radix_sort(d.keys, d.perm, n, 64, h->sort, d.err, h->stream);
+        launch_radix_sort_adaptive(d.keys, d.perm, n, 64, h->sort, h->asort, d.err, h->stream);
         cudaStreamSynchronize(h->stream);
         cudaFree(tmp);
         h->allocations.pop_back();

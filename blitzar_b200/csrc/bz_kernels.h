@@ -55,6 +55,27 @@ int sort_tile_items();
 // sorted result lands back in (keys, vals).
 void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits,
                        SortWorkspace& ws, int* err, cudaStream_t s);
+// Workspace of launch_radix_sort_adaptive: the locally out-of-order pairs F (at most cap of
+// them) with their own sort workspace, compaction block sums and four control words
+// (out-of-order count, U-not-sorted flag, pairs for the small sort, pairs for the full sort).
+struct AdaptiveSortWorkspace {
+    unsigned long long* fkeys;  // [cap]
+    uint32_t* fvals;            // [cap]
+    SortWorkspace fsort;        // alt buffers and look-back state sized for cap
+    unsigned char* flag;        // [n] out-of-order flags
+    int* block_sums;            // [adaptive_sort_blocks(n)]
+    int* ctl;                   // [4]
+    int cap;
+};
+int adaptive_sort_blocks(int n);
+int adaptive_sort_cap(int n);
+// The same stable sort as launch_radix_sort for vals = 0..n-1 on entry (the original
+// positions), fast when the keys are nearly sorted (a step's re-sort of the previous order):
+// only the locally out-of-order pairs are radix-sorted and merged back; other inputs take the
+// full sort, decided on the device.  Uses ws.keys_alt / ws.vals_alt for the in-order pairs.
+void launch_radix_sort_adaptive(unsigned long long* keys, uint32_t* vals, int n, int bits,
+                                SortWorkspace& ws, AdaptiveSortWorkspace& aws, int* err,
+                                cudaStream_t s);
 
 // ---------------------------------------------------------------- tree (bz_tree.cu)
 struct TreeArrays {

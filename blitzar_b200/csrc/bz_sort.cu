@@ -32,9 +32,14 @@ __global__ void k_sort_init(SortWorkspace ws)
         ws.epoch[0] += 1;
 }
 
+// `n_dev` (optional) holds the key count on the device; `n` is then only the capacity the
+// grid was sized for.
 __global__ void __launch_bounds__(kThreads) k_histogram(const unsigned long long* __restrict__ keys,
-                                                         int n, int passes, SortWorkspace ws)
+                                                         int n, int passes, SortWorkspace ws,
+                                                         const int* __restrict__ n_dev)
 {
+    if (n_dev)
+        n = *n_dev;
     __shared__ uint32_t h[8][256];
     for (int i = threadIdx.x; i < 8 * 256; i += kThreads)
         (&h[0][0])[i] = 0;
@@ -54,8 +59,10 @@ __global__ void __launch_bounds__(kThreads) k_histogram(const unsigned long long
 
 // One block per digit position: exclusive scan of its 256 counts; flags passes in which a
 // single digit holds every key (such a pass is the identity and is skipped).
-__global__ void k_scan_hist(int n, SortWorkspace ws)
+__global__ void k_scan_hist(int n, SortWorkspace ws, const int* __restrict__ n_dev)
 {
+    if (n_dev)
+        n = *n_dev;
     __shared__ uint32_t s[256];
     const int p = blockIdx.x, d = threadIdx.x;
     const uint32_t c = ws.hist[p * 256 + d];
@@ -97,10 +104,13 @@ struct PassSmem {
 __global__ void __launch_bounds__(kThreads) k_onesweep(unsigned long long* keys_a, uint32_t* vals_a,
                                                         unsigned long long* keys_b,
                                                         uint32_t* vals_b, int n, int pass,
-                                                        SortWorkspace ws, int* err)
+                                                        SortWorkspace ws, int* err,
+                                                        const int* __restrict__ n_dev)
 {
     if (ws.trivial[pass])
         return;
+    if (n_dev)
+        n = *n_dev;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PassSmem& sm = *reinterpret_cast<PassSmem*>(smem_raw);
     int np = 0;
@@ -119,6 +129,8 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(unsigned long long* keys_
     __syncthreads();
     const int tile = sm.tile;
     const long long base = static_cast<long long>(tile) * kTile;
+    if (base >= n)
+        return;  // a grid sized for a larger capacity: no later tile waits for this one
     const int shift = 8 * pass;
     const unsigned lt = lanemask_lt();
 
@@ -221,8 +233,10 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(unsigned long long* keys_
 // copy it back so callers always find it in (keys, vals).
 __global__ void k_fixup(unsigned long long* keys_a, uint32_t* vals_a,
                         const unsigned long long* keys_b, const uint32_t* vals_b, int n,
-                        int passes, SortWorkspace ws)
+                        int passes, SortWorkspace ws, const int* __restrict__ n_dev)
 {
+    if (n_dev)
+        n = *n_dev;
     int np = 0;
     for (int p = 0; p < passes; ++p)
         np += ws.trivial[p] ? 0 : 1;
@@ -244,11 +258,12 @@ size_t sort_state_words(int n)
     return (tiles < 1 ? 1 : tiles) * 256;
 }
 
-void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits,
-                       SortWorkspace& ws, int* err, cudaStream_t s)
+namespace {
+
+// The passes for a grid of capacity n; with n_dev the device-held count decides the work.
+void enqueue_sort(unsigned long long* keys, uint32_t* vals, int n, int bits, SortWorkspace& ws,
+                  int* err, cudaStream_t s, const int* n_dev)
 {
-    if (n <= 1)
-        return;
     const int passes = (bits + 7) / 8;
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -258,9 +273,9 @@ void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits
     int hb = (n + kThreads - 1) / kThreads;
     hb = hb < 2 * sms ? hb : 2 * sms;
     count_launch();
-    k_histogram<<<hb, kThreads, 0, s>>>(keys, n, passes, ws);
+    k_histogram<<<hb, kThreads, 0, s>>>(keys, n, passes, ws, n_dev);
     count_launch();
-    k_scan_hist<<<passes, 256, 0, s>>>(n, ws);
+    k_scan_hist<<<passes, 256, 0, s>>>(n, ws, n_dev);
     const int tiles = (n + kTile - 1) / kTile;
     const size_t smem = sizeof(PassSmem);
     // function attributes belong to the device's context: set once per device
@@ -274,12 +289,280 @@ void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits
     for (int p = 0; p < passes; ++p) {
         count_launch();
         k_onesweep<<<tiles, kThreads, smem, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, p, ws,
-                                                 err);
+                                                 err, n_dev);
     }
     int fb = (n + 255) / 256;
     fb = fb < 4 * sms ? fb : 4 * sms;
     count_launch();
-    k_fixup<<<fb, 256, 0, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, passes, ws);
+    k_fixup<<<fb, 256, 0, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, passes, ws, n_dev);
+}
+
+} // namespace
+
+void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits,
+                       SortWorkspace& ws, int* err, cudaStream_t s)
+{
+    if (n <= 1)
+        return;
+    enqueue_sort(keys, vals, n, bits, ws, err, s, nullptr);
+}
+
+// ---- nearly sorted inputs -------------------------------------------------------------------
+// Between two steps of a simulation the particles move little, so the keys arrive (in the
+// previous step's sorted order) almost sorted.  The adaptive sort splits the positions into
+// U, those not locally out of order (key neither below any of the kWindow keys before it nor
+// above any of the kWindow keys after it), and F, the rest; checks that U is sorted (a window
+// of one misses runs of particles that moved past a run of others together); sorts F (small)
+// with the radix sort;
+// and merges the two by (key, original position).  Because the values are the original
+// positions 0..n-1, that order is exactly the stable order of the full sort.  When U is not
+// sorted or F exceeds its capacity, the full radix sort runs instead.  The choice is made on
+// the device: every kernel is always launched (the step stays one captured graph), and the
+// kernels of the path not taken return at once.
+namespace {
+
+constexpr int kInvItems = 16;
+constexpr int kInvChunk = kThreads * kInvItems;  // positions per flag/compaction block
+constexpr int kMergeSeg = 256;                  // in-order positions per merge segment
+constexpr int kWindow = 8;                      // neighbours compared on each side
+
+// Flags the out-of-order positions of a chunk (staged with its halo in shared memory) and
+// counts them per block.
+__global__ void __launch_bounds__(kThreads) k_inv_flag(const unsigned long long* __restrict__ keys, int n,
+                                                        unsigned char* __restrict__ flag,
+                                                        int* __restrict__ block_sums)
+{
+    __shared__ unsigned long long sk[kInvChunk + 2 * kWindow];
+    const int base = blockIdx.x * kInvChunk;
+    for (int j = threadIdx.x; j < kInvChunk + 2 * kWindow; j += kThreads) {
+        const int i = base - kWindow + j;
+        // outside [0, n) the halo can neither be below a key before it nor above one after it
+        sk[j] = i < 0 ? 0ull : (i >= n ? ~0ull : keys[i]);
+    }
+    __syncthreads();
+    int c = 0;
+    for (int it = 0; it < kInvItems; ++it) {
+        const int j = it * kThreads + threadIdx.x;
+        const int i = base + j;
+        if (i >= n)
+            break;
+        const unsigned long long v = sk[j + kWindow];
+        bool f = false;
+#pragma unroll
+        for (int w = 1; w <= kWindow; ++w)
+            f = f || v < sk[j + kWindow - w] || v > sk[j + kWindow + w];
+        flag[i] = f ? 1 : 0;
+        c += f ? 1 : 0;
+    }
+    for (int o = 16; o > 0; o >>= 1)
+        c += __shfl_xor_sync(kFullMask, c, o);
+    __shared__ int ws[kWarps];
+    if ((threadIdx.x & 31) == 0)
+        ws[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < kWarps; ++w)
+            t += ws[w];
+        block_sums[blockIdx.x] = t;
+    }
+}
+
+// Exclusive scan of the block counts in one block; ctl[0] = out-of-order count, ctl[1] = 0.
+__global__ void __launch_bounds__(1024) k_inv_scan(int* __restrict__ block_sums, int blocks,
+                                                   int* __restrict__ ctl)
+{
+    __shared__ int carry;
+    __shared__ int ws[32];
+    if (threadIdx.x == 0)
+        carry = 0;
+    __syncthreads();
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int base = 0; base < blocks; base += 1024) {
+        const int i = base + threadIdx.x;
+        const int v = i < blocks ? block_sums[i] : 0;
+        const int x = warp_incl_scan(v);
+        if (lane == 31)
+            ws[warp] = x;
+        __syncthreads();
+        if (warp == 0)
+            ws[lane] = warp_incl_scan(ws[lane]);
+        __syncthreads();
+        const int before = (warp > 0 ? ws[warp - 1] : 0) + carry;
+        if (i < blocks)
+            block_sums[i] = before + x - v;
+        __syncthreads();
+        if (threadIdx.x == 1023)
+            carry = before + x;
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        ctl[0] = carry;
+        ctl[1] = 0;
+    }
+}
+
+// Stable split into U (ukeys/uvals, in order) and F (fkeys/fvals, the first `cap` of them).
+__global__ void __launch_bounds__(kThreads) k_inv_emit(const unsigned long long* __restrict__ keys,
+                                                        const uint32_t* __restrict__ vals,
+                                                        const unsigned char* __restrict__ flag, int n,
+                                                        const int* __restrict__ block_offsets, int cap,
+                                                        unsigned long long* __restrict__ ukeys,
+                                                        uint32_t* __restrict__ uvals,
+                                                        unsigned long long* __restrict__ fkeys,
+                                                        uint32_t* __restrict__ fvals)
+{
+    const int base = blockIdx.x * kInvChunk;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ int ws[kWarps];
+    __shared__ int carry;
+    if (threadIdx.x == 0)
+        carry = block_offsets[blockIdx.x];
+    __syncthreads();
+    for (int it = 0; it < kInvItems; ++it) {
+        const int i = base + it * kThreads + threadIdx.x;
+        const int f = i < n ? flag[i] : 0;
+        const int x = warp_incl_scan(f);
+        if (lane == 31)
+            ws[warp] = x;
+        __syncthreads();
+        int before = carry;
+        for (int w = 0; w < warp; ++w)
+            before += ws[w];
+        if (i < n) {
+            const int fb = before + x - f;  // out-of-order positions before i
+            if (f) {
+                if (fb < cap) {
+                    fkeys[fb] = keys[i];
+                    fvals[fb] = vals[i];
+                }
+            } else {
+                ukeys[i - fb] = keys[i];
+                uvals[i - fb] = vals[i];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == kThreads - 1)
+            carry = before + x;
+        __syncthreads();
+    }
+}
+
+// ctl[1] |= 1 when U is not sorted.
+__global__ void __launch_bounds__(kThreads) k_inv_verify(const unsigned long long* __restrict__ ukeys,
+                                                          int n, int* __restrict__ ctl)
+{
+    const int m = n - ctl[0];
+    bool bad = false;
+    for (int j = blockIdx.x * kThreads + threadIdx.x; j + 1 < m; j += gridDim.x * kThreads)
+        bad = bad || ukeys[j] > ukeys[j + 1];
+    if (__any_sync(kFullMask, bad) && (threadIdx.x & 31) == 0)
+        atomicOr(&ctl[1], 1);
+}
+
+// ctl[2] = pairs for the small sort (fast path) and ctl[3] = pairs for the full sort.
+__global__ void k_inv_mode(int n, int cap, int* __restrict__ ctl)
+{
+    const bool fast = ctl[1] == 0 && ctl[0] <= cap;
+    ctl[2] = fast ? ctl[0] : 0;
+    ctl[3] = fast ? 0 : n;
+}
+
+// Entries of the sorted (k, v)[lo, hi) ordered before (key, val) by (key, value), plus lo.
+__device__ __forceinline__ int rank_in(const unsigned long long* __restrict__ k,
+                                       const uint32_t* __restrict__ v, int lo, int hi,
+                                       unsigned long long key, uint32_t val)
+{
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        const unsigned long long km = k[mid];
+        if (km < key || (km == key && v[mid] < val))
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    return lo;
+}
+
+// Fast path: an in-order pair at U index j lands at j + (F pairs before it); an out-of-order
+// pair at F index q lands at q + (U pairs before it).  A segment of kMergeSeg U pairs first
+// bounds the F range that can fall inside it (usually empty).
+__global__ void __launch_bounds__(kThreads) k_inv_merge(const unsigned long long* __restrict__ ukeys,
+                                                         const uint32_t* __restrict__ uvals,
+                                                         const unsigned long long* __restrict__ fkeys,
+                                                         const uint32_t* __restrict__ fvals, int n,
+                                                         const int* __restrict__ ctl,
+                                                         unsigned long long* __restrict__ keys,
+                                                         uint32_t* __restrict__ vals)
+{
+    if (ctl[3] != 0)
+        return;  // the full sort ran
+    const int nf = ctl[2], m = n - nf;
+    const int useg = (m + kMergeSeg - 1) / kMergeSeg;
+    const int fseg = (nf + kThreads - 1) / kThreads;
+    __shared__ int s_lo, s_hi;
+    for (int sgi = blockIdx.x; sgi < useg + fseg; sgi += gridDim.x) {
+        if (sgi < useg) {
+            const int j0 = sgi * kMergeSeg;
+            const int j1 = min(j0 + kMergeSeg, m) - 1;
+            if (threadIdx.x == 0) {
+                s_lo = nf ? rank_in(fkeys, fvals, 0, nf, ukeys[j0], uvals[j0]) : 0;
+                s_hi = nf ? rank_in(fkeys, fvals, 0, nf, ukeys[j1], uvals[j1]) : 0;
+            }
+            __syncthreads();
+            const int lo = s_lo, hi = s_hi;
+            for (int j = j0 + threadIdx.x; j <= j1; j += kThreads) {
+                const unsigned long long key = ukeys[j];
+                const uint32_t val = uvals[j];
+                const int before = lo == hi ? lo : rank_in(fkeys, fvals, lo, hi, key, val);
+                keys[j + before] = key;
+                vals[j + before] = val;
+            }
+            __syncthreads();
+        } else {
+            const int q = (sgi - useg) * kThreads + threadIdx.x;
+            if (q < nf) {
+                const unsigned long long key = fkeys[q];
+                const uint32_t val = fvals[q];
+                const int pos = q + rank_in(ukeys, uvals, 0, m, key, val);
+                keys[pos] = key;
+                vals[pos] = val;
+            }
+        }
+    }
+}
+
+} // namespace
+
+int adaptive_sort_blocks(int n) { return n > 0 ? (n + kInvChunk - 1) / kInvChunk : 1; }
+int adaptive_sort_cap(int n) { return n / 8 > 4096 ? n / 8 : 4096; }
+
+void launch_radix_sort_adaptive(unsigned long long* keys, uint32_t* vals, int n, int bits,
+                                SortWorkspace& ws, AdaptiveSortWorkspace& aws, int* err,
+                                cudaStream_t s)
+{
+    if (n <= 1)
+        return;
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int blocks = adaptive_sort_blocks(n);
+    count_launch(3);
+    k_inv_flag<<<blocks, kThreads, 0, s>>>(keys, n, aws.flag, aws.block_sums);
+    k_inv_scan<<<1, 1024, 0, s>>>(aws.block_sums, blocks, aws.ctl);
+    k_inv_emit<<<blocks, kThreads, 0, s>>>(keys, vals, aws.flag, n, aws.block_sums, aws.cap,
+                                           ws.keys_alt, ws.vals_alt, aws.fkeys, aws.fvals);
+    int vb = (n + kThreads - 1) / kThreads;
+    vb = vb < 4 * sms ? vb : 4 * sms;
+    count_launch(2);
+    k_inv_verify<<<vb, kThreads, 0, s>>>(ws.keys_alt, n, aws.ctl);
+    k_inv_mode<<<1, 1, 0, s>>>(n, aws.cap, aws.ctl);
+    // fast path: sort F in place (its own workspace); otherwise the full sort of (keys, vals)
+    enqueue_sort(aws.fkeys, aws.fvals, aws.cap, bits, aws.fsort, err, s, aws.ctl + 2);
+    enqueue_sort(keys, vals, n, bits, ws, err, s, aws.ctl + 3);
+    count_launch();
+    k_inv_merge<<<8 * sms, kThreads, 0, s>>>(ws.keys_alt, ws.vals_alt, aws.fkeys, aws.fvals, n,
+                                             aws.ctl, keys, vals);
 }
 
 } // namespace bz
