@@ -632,14 +632,10 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     sw.max_tiles = static_cast<int>(words / 256);
     AdaptiveSortWorkspace& aw = h->asort;
     aw.cap = adaptive_sort_cap(static_cast<int>(n));
-    SortWorkspace& fw = aw.fsort;
-    const size_t fwords = sort_state_words(aw.cap);
-    ok = ok && dalloc(h, &aw.fkeys, aw.cap) && dalloc(h, &aw.fvals, aw.cap) && dalloc(h, &aw.flag, n) &&
+    ok = ok && dalloc(h, &aw.fkeys, aw.cap) && dalloc(h, &aw.fvals, aw.cap) && dalloc(h, &aw.falt_keys, aw.cap) &&
+         dalloc(h, &aw.falt_vals, aw.cap) && dalloc(h, &aw.flag, n) &&
          dalloc(h, &aw.block_sums, adaptive_sort_blocks(static_cast<int>(n))) && dalloc(h, &aw.ctl, 4) &&
-         dalloc(h, &fw.keys_alt, aw.cap) && dalloc(h, &fw.vals_alt, aw.cap) && dalloc(h, &fw.hist, 8 * 256) &&
-         dalloc(h, &fw.base, 8 * 256) && dalloc(h, &fw.ticket, 8) && dalloc(h, &fw.epoch, 1) &&
-         dalloc(h, &fw.trivial, 8) && dalloc(h, &fw.state, fwords);
-    fw.max_tiles = static_cast<int>(fwords / 256);
+         dalloc(h, &aw.job, 1);
     // tree
     TreeArrays& t = h->tree;
     t.cap = static_cast<int>(2 * n + 1024);
@@ -669,8 +665,6 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     }
     cudaMemsetAsync(sw.state, 0, words * sizeof(unsigned long long), h->stream);
     cudaMemsetAsync(sw.epoch, 0, sizeof(uint32_t), h->stream);
-    cudaMemsetAsync(h->asort.fsort.epoch, 0, sizeof(uint32_t), h->stream);
-    cudaMemsetAsync(h->asort.fsort.state, 0, fwords * sizeof(unsigned long long), h->stream);
     cudaMemsetAsync(d.err, 0, sizeof(int), h->stream);
     if (cfg->solver == BZ_SOLVER_TREEPM) {
         int perr = 0;

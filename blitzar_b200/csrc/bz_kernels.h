@@ -55,16 +55,27 @@ int sort_tile_items();
 // sorted result lands back in (keys, vals).
 void launch_radix_sort(unsigned long long* keys, uint32_t* vals, int n, int bits,
                        SortWorkspace& ws, int* err, cudaStream_t s);
+// Arrays and count of one radix sort, read by the sort kernels from device memory.
+struct SortJob {
+    unsigned long long* ka;
+    uint32_t* va;
+    unsigned long long* kb;  // alternate buffers
+    uint32_t* vb;
+    int n;
+};
 // Workspace of launch_radix_sort_adaptive: the locally out-of-order pairs F (at most cap of
-// them) with their own sort workspace, compaction block sums and four control words
-// (out-of-order count, U-not-sorted flag, pairs for the small sort, pairs for the full sort).
+// them) and alternate buffers to sort them, flags, compaction block sums, four control words
+// (out-of-order count, in-order-part-not-sorted flag, fast-path count, full-sort count) and
+// the radix sort's job.
 struct AdaptiveSortWorkspace {
-    unsigned long long* fkeys;  // [cap]
-    uint32_t* fvals;            // [cap]
-    SortWorkspace fsort;        // alt buffers and look-back state sized for cap
-    unsigned char* flag;        // [n] out-of-order flags
-    int* block_sums;            // [adaptive_sort_blocks(n)]
-    int* ctl;                   // [4]
+    unsigned long long* fkeys;      // [cap]
+    uint32_t* fvals;                // [cap]
+    unsigned long long* falt_keys;  // [cap]
+    uint32_t* falt_vals;            // [cap]
+    unsigned char* flag;            // [n] out-of-order flags
+    int* block_sums;                // [adaptive_sort_blocks(n)]
+    int* ctl;                       // [4]
+    SortJob* job;                   // [1]
     int cap;
 };
 int adaptive_sort_blocks(int n);

@@ -32,14 +32,16 @@ __global__ void k_sort_init(SortWorkspace ws)
         ws.epoch[0] += 1;
 }
 
-// `n_dev` (optional) holds the key count on the device; `n` is then only the capacity the
-// grid was sized for.
+// `job` (optional) names the arrays and the count on the device; the host-side arguments are
+// then only the capacity the grid was sized for.
 __global__ void __launch_bounds__(kThreads) k_histogram(const unsigned long long* __restrict__ keys,
                                                          int n, int passes, SortWorkspace ws,
-                                                         const int* __restrict__ n_dev)
+                                                         const SortJob* __restrict__ job)
 {
-    if (n_dev)
-        n = *n_dev;
+    if (job) {
+        keys = job->ka;
+        n = job->n;
+    }
     __shared__ uint32_t h[8][256];
     for (int i = threadIdx.x; i < 8 * 256; i += kThreads)
         (&h[0][0])[i] = 0;
@@ -59,10 +61,10 @@ __global__ void __launch_bounds__(kThreads) k_histogram(const unsigned long long
 
 // One block per digit position: exclusive scan of its 256 counts; flags passes in which a
 // single digit holds every key (such a pass is the identity and is skipped).
-__global__ void k_scan_hist(int n, SortWorkspace ws, const int* __restrict__ n_dev)
+__global__ void k_scan_hist(int n, SortWorkspace ws, const SortJob* __restrict__ job)
 {
-    if (n_dev)
-        n = *n_dev;
+    if (job)
+        n = job->n;
     __shared__ uint32_t s[256];
     const int p = blockIdx.x, d = threadIdx.x;
     const uint32_t c = ws.hist[p * 256 + d];
@@ -105,12 +107,17 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(unsigned long long* keys_
                                                         unsigned long long* keys_b,
                                                         uint32_t* vals_b, int n, int pass,
                                                         SortWorkspace ws, int* err,
-                                                        const int* __restrict__ n_dev)
+                                                        const SortJob* __restrict__ job)
 {
     if (ws.trivial[pass])
         return;
-    if (n_dev)
-        n = *n_dev;
+    if (job) {
+        keys_a = job->ka;
+        vals_a = job->va;
+        keys_b = job->kb;
+        vals_b = job->vb;
+        n = job->n;
+    }
     extern __shared__ __align__(16) unsigned char smem_raw[];
     PassSmem& sm = *reinterpret_cast<PassSmem*>(smem_raw);
     int np = 0;
@@ -233,10 +240,15 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(unsigned long long* keys_
 // copy it back so callers always find it in (keys, vals).
 __global__ void k_fixup(unsigned long long* keys_a, uint32_t* vals_a,
                         const unsigned long long* keys_b, const uint32_t* vals_b, int n,
-                        int passes, SortWorkspace ws, const int* __restrict__ n_dev)
+                        int passes, SortWorkspace ws, const SortJob* __restrict__ job)
 {
-    if (n_dev)
-        n = *n_dev;
+    if (job) {
+        keys_a = job->ka;
+        vals_a = job->va;
+        keys_b = job->kb;
+        vals_b = job->vb;
+        n = job->n;
+    }
     int np = 0;
     for (int p = 0; p < passes; ++p)
         np += ws.trivial[p] ? 0 : 1;
@@ -260,9 +272,10 @@ size_t sort_state_words(int n)
 
 namespace {
 
-// The passes for a grid of capacity n; with n_dev the device-held count decides the work.
+// The passes for a grid of capacity n; with `job` the device-held arrays and count decide the
+// work.
 void enqueue_sort(unsigned long long* keys, uint32_t* vals, int n, int bits, SortWorkspace& ws,
-                  int* err, cudaStream_t s, const int* n_dev)
+                  int* err, cudaStream_t s, const SortJob* job)
 {
     const int passes = (bits + 7) / 8;
     int dev = 0, sms = 148;
@@ -273,9 +286,9 @@ void enqueue_sort(unsigned long long* keys, uint32_t* vals, int n, int bits, Sor
     int hb = (n + kThreads - 1) / kThreads;
     hb = hb < 2 * sms ? hb : 2 * sms;
     count_launch();
-    k_histogram<<<hb, kThreads, 0, s>>>(keys, n, passes, ws, n_dev);
+    k_histogram<<<hb, kThreads, 0, s>>>(keys, n, passes, ws, job);
     count_launch();
-    k_scan_hist<<<passes, 256, 0, s>>>(n, ws, n_dev);
+    k_scan_hist<<<passes, 256, 0, s>>>(n, ws, job);
     const int tiles = (n + kTile - 1) / kTile;
     const size_t smem = sizeof(PassSmem);
     // function attributes belong to the device's context: set once per device
@@ -289,12 +302,12 @@ void enqueue_sort(unsigned long long* keys, uint32_t* vals, int n, int bits, Sor
     for (int p = 0; p < passes; ++p) {
         count_launch();
         k_onesweep<<<tiles, kThreads, smem, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, p, ws,
-                                                 err, n_dev);
+                                                 err, job);
     }
     int fb = (n + 255) / 256;
     fb = fb < 4 * sms ? fb : 4 * sms;
     count_launch();
-    k_fixup<<<fb, 256, 0, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, passes, ws, n_dev);
+    k_fixup<<<fb, 256, 0, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, passes, ws, job);
 }
 
 } // namespace
@@ -340,6 +353,18 @@ __global__ void __launch_bounds__(kThreads) k_inv_flag(const unsigned long long*
         sk[j] = i < 0 ? 0ull : (i >= n ? ~0ull : keys[i]);
     }
     __syncthreads();
+    // a chunk sorted together with its halo has nothing out of order
+    bool unsorted = false;
+    for (int j = threadIdx.x; j + 1 < kInvChunk + 2 * kWindow; j += kThreads)
+        unsorted = unsorted || sk[j] > sk[j + 1];
+    if (!__syncthreads_or(unsorted)) {
+        for (int j = threadIdx.x; j < kInvChunk; j += kThreads)
+            if (base + j < n)
+                flag[base + j] = 0;
+        if (threadIdx.x == 0)
+            block_sums[blockIdx.x] = 0;
+        return;
+    }
     int c = 0;
     for (int it = 0; it < kInvItems; ++it) {
         const int j = it * kThreads + threadIdx.x;
@@ -407,12 +432,22 @@ __global__ void __launch_bounds__(kThreads) k_inv_emit(const unsigned long long*
                                                         const uint32_t* __restrict__ vals,
                                                         const unsigned char* __restrict__ flag, int n,
                                                         const int* __restrict__ block_offsets, int cap,
+                                                        const int* __restrict__ ctl,
                                                         unsigned long long* __restrict__ ukeys,
                                                         uint32_t* __restrict__ uvals,
                                                         unsigned long long* __restrict__ fkeys,
                                                         uint32_t* __restrict__ fvals)
 {
     const int base = blockIdx.x * kInvChunk;
+    const int fb0 = block_offsets[blockIdx.x];
+    const int fb1 = blockIdx.x + 1 < gridDim.x ? block_offsets[blockIdx.x + 1] : ctl[0];
+    if (fb0 == fb1) {  // nothing out of order here: a shifted copy into U
+        for (int i = base + threadIdx.x; i < min(base + kInvChunk, n); i += kThreads) {
+            ukeys[i - fb0] = keys[i];
+            uvals[i - fb0] = vals[i];
+        }
+        return;
+    }
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __shared__ int ws[kWarps];
     __shared__ int carry;
@@ -460,12 +495,16 @@ __global__ void __launch_bounds__(kThreads) k_inv_verify(const unsigned long lon
         atomicOr(&ctl[1], 1);
 }
 
-// ctl[2] = pairs for the small sort (fast path) and ctl[3] = pairs for the full sort.
-__global__ void k_inv_mode(int n, int cap, int* __restrict__ ctl)
+// Picks the radix sort's job: the out-of-order pairs (fast path; ctl[3] = 0) or all pairs
+// (ctl[3] = n).  ctl[2] = the fast path's out-of-order count.
+__global__ void k_inv_mode(int n, int cap, int* __restrict__ ctl, SortJob* __restrict__ job,
+                           SortJob fast_job, SortJob full_job)
 {
     const bool fast = ctl[1] == 0 && ctl[0] <= cap;
     ctl[2] = fast ? ctl[0] : 0;
     ctl[3] = fast ? 0 : n;
+    fast_job.n = ctl[0];
+    *job = fast ? fast_job : full_job;
 }
 
 // Entries of the sorted (k, v)[lo, hi) ordered before (key, val) by (key, value), plus lo.
@@ -551,15 +590,16 @@ void launch_radix_sort_adaptive(unsigned long long* keys, uint32_t* vals, int n,
     k_inv_flag<<<blocks, kThreads, 0, s>>>(keys, n, aws.flag, aws.block_sums);
     k_inv_scan<<<1, 1024, 0, s>>>(aws.block_sums, blocks, aws.ctl);
     k_inv_emit<<<blocks, kThreads, 0, s>>>(keys, vals, aws.flag, n, aws.block_sums, aws.cap,
-                                           ws.keys_alt, ws.vals_alt, aws.fkeys, aws.fvals);
+                                           aws.ctl, ws.keys_alt, ws.vals_alt, aws.fkeys, aws.fvals);
     int vb = (n + kThreads - 1) / kThreads;
     vb = vb < 4 * sms ? vb : 4 * sms;
     count_launch(2);
     k_inv_verify<<<vb, kThreads, 0, s>>>(ws.keys_alt, n, aws.ctl);
-    k_inv_mode<<<1, 1, 0, s>>>(n, aws.cap, aws.ctl);
-    // fast path: sort F in place (its own workspace); otherwise the full sort of (keys, vals)
-    enqueue_sort(aws.fkeys, aws.fvals, aws.cap, bits, aws.fsort, err, s, aws.ctl + 2);
-    enqueue_sort(keys, vals, n, bits, ws, err, s, aws.ctl + 3);
+    const SortJob fast_job{aws.fkeys, aws.fvals, aws.falt_keys, aws.falt_vals, 0};
+    const SortJob full_job{keys, vals, ws.keys_alt, ws.vals_alt, n};
+    k_inv_mode<<<1, 1, 0, s>>>(n, aws.cap, aws.ctl, aws.job, fast_job, full_job);
+    // one radix sort: of F in place on the fast path, else of all of (keys, vals)
+    enqueue_sort(keys, vals, n, bits, ws, err, s, aws.job);
     count_launch();
     k_inv_merge<<<8 * sms, kThreads, 0, s>>>(ws.keys_alt, ws.vals_alt, aws.fkeys, aws.fvals, n,
                                              aws.ctl, keys, vals);
