@@ -114,10 +114,34 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
                 if (split && sub > 0)
                     bsub = lower_bound_digit(keys, s0, s0 + c0, shift, static_cast<unsigned>(sub));
             } else if (split) {
-                b[0] = s0;
+                // the seven searches advance in lockstep, so each step's seven loads are in
+                // flight together (one memory round trip per step, not one per search step)
+                int lo[8], hi[8];
+#pragma unroll
+                for (int d = 1; d < 8; ++d) {
+                    lo[d] = s0;
+                    hi[d] = s0 + c0;
+                }
+                for (int step = 0; step < 32; ++step) {
+                    bool open = false;
+#pragma unroll
+                    for (int d = 1; d < 8; ++d) {
+                        if (lo[d] < hi[d]) {
+                            const int mid = (lo[d] + hi[d]) >> 1;
+                            const unsigned dm = static_cast<unsigned>((keys[mid] >> shift) & 7u);
+                            if (dm < static_cast<unsigned>(d))
+                                lo[d] = mid + 1;
+                            else
+                                hi[d] = mid;
+                            open = true;
+                        }
+                    }
+                    if (!open)
+                        break;
+                }
 #pragma unroll
                 for (int d = 1; d < 8; ++d)
-                    b[d] = lower_bound_digit(keys, b[d - 1], s0 + c0, shift, static_cast<unsigned>(d));
+                    b[d] = lo[d];
             }
         }
         if (TPN == 8) {
