@@ -28,6 +28,7 @@ EXPORTS = (
     "bz_sort_pairs_noalloc", "bz_energy", "bz_autotune", "bz_learn_generate", "bz_learn_train",
     "bz_learn_set", "bz_learn_get", "bz_learn_enable", "bz_learn_forward", "bz_learn_gradient",
     "bz_set_ensemble", "bz_adaptive_levels", "bz_adaptive_updates", "bz_set_mesh_schedule",
+    "bz_walk_blocks_per_sm",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -115,6 +116,7 @@ def load():
     L.bz_energy.argtypes = [_vp, _vp, _vp, _vp]
     L.bz_autotune.argtypes = [_vp, C.c_int32, _vp, _vp, _vp, _vp]
     L.bz_set_mesh_schedule.argtypes = [_vp, C.c_int32]
+    L.bz_walk_blocks_per_sm.argtypes = [_vp, C.c_int32, _vp]
     L.bz_adaptive_levels.argtypes = [_vp, _vp]
     L.bz_adaptive_updates.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_set_ensemble.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_int32]
@@ -309,8 +311,16 @@ class Engine:
         self._check(self.L.bz_autotune(self.h, trials, C.byref(leaf), C.byref(grp), C.byref(ms),
                                        C.byref(ov)), "bz_autotune")
         self.last_tune = dict(leaf_capacity=leaf.value, walk_group_size=grp.value,
-                              mesh_schedule=ov.value, ms_per_evaluation=ms.value)
+                              mesh_schedule=ov.value, walk_blocks_per_sm=self.walk_blocks_per_sm(),
+                              ms_per_evaluation=ms.value)
         return leaf.value, grp.value, ms.value
+
+    def walk_blocks_per_sm(self, value=-1):
+        """Cap on resident walk blocks per SM (0: as many as fit); value < 0 only queries."""
+        cur = C.c_int32(0)
+        self._check(self.L.bz_walk_blocks_per_sm(self.h, int(value), C.byref(cur)),
+                    "bz_walk_blocks_per_sm")
+        return cur.value
 
     def set_mesh_schedule(self, schedule):
         """Pin the TreePM mesh-leg schedule (0 in line, 1 concurrent with the tree build and

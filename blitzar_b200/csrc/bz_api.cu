@@ -72,6 +72,7 @@ struct bz_handle {
     // in any order), so they also run concurrently with the keys, sort and permutation; only the
     // interpolation waits for the new order
     int mesh_overlap = 1;
+    int walk_blocks_per_sm = 0;  // cap on resident walk blocks per SM (0: as many as fit)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_sorted = nullptr;
     size_t capacity = 0;
     size_t n = 0;
@@ -280,6 +281,7 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
     o.totals = d.counters;
     WalkParams wp = walk_params(h, want_pot);
     wp.active = h->walk_active;
+    wp.blocks_per_sm = h->walk_blocks_per_sm;
     const bool learned = h->learn.enabled && h->learn.trained && h->cfg.solver == BZ_SOLVER_TREEPM;
     if (learned) {
         o.pair_src = h->learn.pair_src;
@@ -1231,6 +1233,23 @@ bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps)
     return BZ_OK;
 }
 
+bz_status bz_walk_blocks_per_sm(bz_handle* h, int32_t set_value, int32_t* current)
+{
+    if (!h || set_value > 64)
+        return BZ_INVALID_ARGUMENT;
+    if (set_value >= 0 && set_value != h->walk_blocks_per_sm) {
+        h->walk_blocks_per_sm = set_value;
+        for (int i = 0; i < 2; ++i) {  // captured steps hold the old grid
+            if (h->graph[i])
+                cudaGraphExecDestroy(h->graph[i]);
+            h->graph[i] = nullptr;
+        }
+    }
+    if (current)
+        *current = h->walk_blocks_per_sm;
+    return BZ_OK;
+}
+
 bz_status bz_set_mesh_schedule(bz_handle* h, int32_t schedule)
 {
     if (!h || schedule < 0 || schedule > 2)
@@ -1257,7 +1276,7 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     static const int kLeaf[] = {8, 12, 16, 24, 32, 48};
     static const int kGroup[] = {16, 24, 32};
     const int leaf0 = h->cfg.leaf_capacity, group0 = h->cfg.walk_group_size;
-    const int overlap0 = h->mesh_overlap;
+    const int overlap0 = h->mesh_overlap, bps0 = h->walk_blocks_per_sm;
     const int n_overlap = h->pm_stream ? 3 : 1;  // TreePM: the three mesh-leg schedules
     const bool timing0 = h->timing;
     h->timing = false;
@@ -1272,35 +1291,63 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
+    // ms per zero-length step with the handle's current parameters
+    auto time_steps = [&](float* ms) -> bz_status {
+        enqueue_step(h);  // warm-up step with these parameters
+        cudaEventRecord(e0, h->stream);
+        for (int r = 0; r < trials; ++r)
+            enqueue_step(h);
+        cudaEventRecord(e1, h->stream);
+        const bz_status rc = check_device(h, "bz_autotune");
+        if (rc != BZ_OK)
+            return rc;
+        cudaEventElapsedTime(ms, e0, e1);
+        *ms /= static_cast<float>(trials);
+        return BZ_OK;
+    };
     float best = -1.0f;
     int best_leaf = leaf0, best_group = group0;
-    int best_overlap = overlap0;
-    for (int ov = 0; ov < n_overlap && st == BZ_OK; ++ov) {
-        for (int leaf : kLeaf) {
-            for (int group : kGroup) {
-                h->mesh_overlap = n_overlap > 1 ? ov : overlap0;
-                h->cfg.leaf_capacity = leaf;
-                h->cfg.walk_group_size = group;
-                enqueue_step(h);  // warm-up step with these parameters
-                cudaEventRecord(e0, h->stream);
-                for (int r = 0; r < trials; ++r)
-                    enqueue_step(h);
-                cudaEventRecord(e1, h->stream);
-                st = check_device(h, "bz_autotune");
-                if (st != BZ_OK)
-                    break;
-                float ms = 0.0f;
-                cudaEventElapsedTime(&ms, e0, e1);
-                ms /= static_cast<float>(trials);
-                if (best < 0.0f || ms < best) {
-                    best = ms;
-                    best_leaf = leaf;
-                    best_group = group;
-                    best_overlap = h->mesh_overlap;
-                }
-            }
+    int best_overlap = overlap0, best_bps = bps0;
+    // stage 1: leaf capacity x walk group size
+    for (int leaf : kLeaf) {
+        for (int group : kGroup) {
+            h->cfg.leaf_capacity = leaf;
+            h->cfg.walk_group_size = group;
+            float ms = 0.0f;
+            st = time_steps(&ms);
             if (st != BZ_OK)
                 break;
+            if (best < 0.0f || ms < best) {
+                best = ms;
+                best_leaf = leaf;
+                best_group = group;
+            }
+        }
+        if (st != BZ_OK)
+            break;
+    }
+    // stage 2 (TreePM with the second stream): mesh schedule x cap on resident walk blocks per
+    // SM (the walk holds every SM's registers; a lower cap lets the mesh kernels co-run)
+    if (st == BZ_OK && n_overlap > 1) {
+        static const int kBps[] = {0, 6, 5};
+        h->cfg.leaf_capacity = best_leaf;
+        h->cfg.walk_group_size = best_group;
+        for (int ov = 0; ov < n_overlap && st == BZ_OK; ++ov) {
+            for (int bps : kBps) {
+                if (ov == 0 && bps != 0)
+                    continue;  // in line: nothing runs beside the walk
+                h->mesh_overlap = ov;
+                h->walk_blocks_per_sm = bps;
+                float ms = 0.0f;
+                st = time_steps(&ms);
+                if (st != BZ_OK)
+                    break;
+                if (ms < best) {
+                    best = ms;
+                    best_overlap = ov;
+                    best_bps = bps;
+                }
+            }
         }
     }
     cudaEventDestroy(e0);
@@ -1309,6 +1356,7 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     h->cfg.leaf_capacity = st == BZ_OK ? best_leaf : leaf0;
     h->cfg.walk_group_size = st == BZ_OK ? best_group : group0;
     h->mesh_overlap = st == BZ_OK ? best_overlap : overlap0;
+    h->walk_blocks_per_sm = st == BZ_OK ? best_bps : bps0;
     // the captured step holds the old parameters: capture again on the next bz_step
     for (int i = 0; i < 2; ++i) {
         if (h->graph[i])

@@ -143,6 +143,8 @@ struct WalkParams {
     int want_pot;
     float rcorr2;     // > 0 with WalkOutputs.pair_src: record the pairs closer than this
     const unsigned char* active;  // optional [n]: walk only groups with an active target
+    int blocks_per_sm;            // > 0: at most this many resident walk blocks per SM (room
+                                  // for kernels of a concurrent stream); 0 = as many as fit
 };
 // ---------------------------------------------------------------- target groups (bz_groups.cu)
 constexpr int kGroupMax = 32;  // largest walk group (one warp)

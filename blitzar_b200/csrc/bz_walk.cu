@@ -846,11 +846,12 @@ __global__ void k_zero_u32(unsigned* p) { *p = 0u; }
 
 struct WalkLaunch {
     int blocks = 0;
+    int sms = 0;
     size_t smem = 0;
 };
 
 template <bool PERIODIC, bool SPLIT, bool QUAD, bool POT>
-WalkLaunch walk_shape(int n)
+WalkLaunch walk_shape(int n, int blocks_per_sm)
 {
     // function attributes and occupancy belong to the device: one cached shape per device
     static WalkLaunch cached[kMaxDevices];
@@ -867,9 +868,12 @@ WalkLaunch walk_shape(int n)
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_walk<PERIODIC, SPLIT, QUAD, POT>,
                                                       kWarps * 32, smem);
         c.smem = smem;
+        c.sms = sms;
         c.blocks = sms * (per_sm > 0 ? per_sm : 1);
     }
     WalkLaunch l = c;
+    if (blocks_per_sm > 0 && l.sms * blocks_per_sm < l.blocks)
+        l.blocks = l.sms * blocks_per_sm;
     const int need = (n + kWarps - 1) / kWarps;  // groups <= n
     if (l.blocks > need)
         l.blocks = need < 1 ? 1 : need;
@@ -881,7 +885,7 @@ void launch_variant(const float4* pos4, int n, const TreeArrays& t, const GroupT
                     const WalkParams& p, const WalkOutputs& o, unsigned* queue, int* spill,
                     int* err, cudaStream_t s)
 {
-    const WalkLaunch l = walk_shape<PERIODIC, SPLIT, QUAD, POT>(n);
+    const WalkLaunch l = walk_shape<PERIODIC, SPLIT, QUAD, POT>(n, p.blocks_per_sm);
     const float inv_box = p.box > 0.0f ? 1.0f / p.box : 0.0f;
     count_launch();
     k_zero_u32<<<1, 1, 0, s>>>(queue);

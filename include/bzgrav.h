@@ -130,12 +130,14 @@ bz_status bz_adaptive_updates(bz_handle* h, uint64_t* updates);
 
 /* Autotuner (no counterpart in the reference, whose leaf capacity and launch shapes are fixed
  * settings): times `trials` steps of zero length (drift, keys, sort, forces, kick; positions and
- * velocities come out unchanged) of the current state for each leaf capacity in
- * {8, 12, 16, 24, 32, 48}, walk group size in {16, 24, 32} and, for TreePM, each mesh-leg
- * schedule: *mesh_overlap = 0 in line; 1 on a second stream concurrent with the tree build and
- * walk; 2 as 1 with the deposit and field solve also concurrent with the keys, sort and
- * permutation of a step.  Keeps the fastest choice in the handle and reports it, with the time
- * of one such step in *ms_per_evaluation.  Outputs may be NULL. */
+ * velocities come out unchanged) of the current state, first for each leaf capacity in
+ * {8, 12, 16, 24, 32, 48} x walk group size in {16, 24, 32}, then, for TreePM, with the best of
+ * those, for each mesh-leg schedule x walk blocks per SM in {as many as fit, 6, 5}
+ * (bz_walk_blocks_per_sm).  Schedules: *mesh_overlap = 0 in line; 1 on a second stream
+ * concurrent with the tree build and walk; 2 as 1 with the deposit and field solve also
+ * concurrent with the keys, sort and permutation of a step.  Keeps the fastest choice in the
+ * handle and reports it, with the time of one such step in *ms_per_evaluation.  Outputs may be
+ * NULL. */
 bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int32_t* group_size,
                       float* ms_per_evaluation, int32_t* mesh_overlap);
 
@@ -143,6 +145,13 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
  * Schedules 1 and 2 need the second stream, created with the handle; without it every schedule
  * runs in line.  The results of the schedules differ only in the order of the float mass sums. */
 bz_status bz_set_mesh_schedule(bz_handle* h, int32_t schedule);
+
+/* Cap on the resident blocks per SM of the walk kernel (0: as many as fit, the default).  The
+ * walk is a persistent kernel that otherwise holds every SM's registers; a lower cap lets the
+ * TreePM mesh leg's kernels co-run with it.  bz_autotune picks it with the mesh schedule.
+ * set_value < 0 only queries; *current (may be NULL) receives the value in force.  Results do
+ * not depend on it. */
+bz_status bz_walk_blocks_per_sm(bz_handle* h, int32_t set_value, int32_t* current);
 
 /* Accelerations (and optionally potentials) of the current state, caller's particle order,
  * SoA 3n floats.  Replaces computeOctreeAccelerationKernel (engine/physics/octree/cuda/force/

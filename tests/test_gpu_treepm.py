@@ -183,3 +183,29 @@ def test_autotune_leaves_state_unchanged(gpu):
     assert tune["mesh_schedule"] in (0, 1, 2)
     for a, b in zip(before, after):  # caller order
         assert np.array_equal(a, b)
+
+
+def test_walk_block_cap_does_not_change_results(gpu):
+    """Capping the persistent walk's resident blocks per SM (room for the concurrent mesh leg)
+    changes only the grid: every group is still walked by one warp in the same way (bit for bit
+    in the tree-only solver; TreePM adds mesh forces whose float atomics sum in any order)."""
+    n = 24 ** 3
+    rng = np.random.default_rng(43)
+    pos = rng.random((n, 3))
+    m = np.full(n, 1.0 / n, np.float32)
+    for treepm in (False, True):
+        kw = dict(solver=1, box_length=1.0, treepm_grid_size=32, treepm_assignment=2,
+                  treepm_gradient=1, treepm_window_floor=0.0, treepm_r_cut_factor=5.0,
+                  treepm_node_size_factor=0.5, octree_softening=0.02 / 32) if treepm else {}
+        out = []
+        for cap in (0, 2, 5):
+            with _engine(n, **kw) as e:
+                e.set_state(pos, None, m, f64=True)
+                assert e.walk_blocks_per_sm(cap) == cap
+                out.append(e.accelerations().astype(np.float64))
+        for a in out[1:]:
+            if treepm:
+                scale = np.linalg.norm(out[0], axis=1).max()
+                assert np.abs(a - out[0]).max() < 1e-5 * scale
+            else:
+                assert np.array_equal(a, out[0])
