@@ -437,7 +437,7 @@ def run_ours(args, w, rank, world, local):
     dt = w["dt"]
     tuned = None
     if not args.no_autotune and not w.get("adaptive_levels"):
-        eng.autotune(trials=2)  # untimed: picks leaf capacity, group size, mesh overlap
+        eng.autotune(trials=5)  # untimed: picks leaf capacity, group size, mesh schedule
         tuned = eng.last_tune
     with torch.cuda.stream(stream):
         for _ in range(max(3, args.warmup)):

@@ -71,7 +71,7 @@ struct bz_handle {
     // step the deposit and field solve are forked right after the drift (they take the particles
     // in any order), so they also run concurrently with the keys, sort and permutation; only the
     // interpolation waits for the new order
-    int mesh_overlap = 1;
+    int mesh_overlap = 2;
     int walk_blocks_per_sm = 0;  // cap on resident walk blocks per SM (0: as many as fit)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_sorted = nullptr;
     size_t capacity = 0;
@@ -1291,18 +1291,52 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
-    // ms per zero-length step with the handle's current parameters
+    // ms per zero-length step with the handle's current parameters, launched the way bz_step
+    // launches them: as a captured graph (two steps, so the state buffers end where they began)
+    // unless the handle steps eagerly
     auto time_steps = [&](float* ms) -> bz_status {
-        enqueue_step(h);  // warm-up step with these parameters
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t ex = nullptr;
+        bool graph = h->cfg.use_graph && !h->graph_failed;
+        if (graph) {
+            if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                enqueue_step(h);
+                enqueue_step(h);
+                if (cudaStreamEndCapture(h->stream, &g) != cudaSuccess || !g ||
+                    cudaGraphInstantiate(&ex, g, 0) != cudaSuccess)
+                    graph = false;
+            } else {
+                graph = false;
+            }
+            if (!graph) {
+                if (g)
+                    cudaGraphDestroy(g);
+                g = nullptr;
+                cudaGetLastError();
+            }
+        }
+        auto run = [&]() {
+            if (graph) {
+                cudaGraphLaunch(ex, h->stream);
+            } else {
+                enqueue_step(h);
+                enqueue_step(h);
+            }
+        };
+        run();  // warm-up with these parameters
         cudaEventRecord(e0, h->stream);
         for (int r = 0; r < trials; ++r)
-            enqueue_step(h);
+            run();
         cudaEventRecord(e1, h->stream);
         const bz_status rc = check_device(h, "bz_autotune");
+        if (ex)
+            cudaGraphExecDestroy(ex);
+        if (g)
+            cudaGraphDestroy(g);
         if (rc != BZ_OK)
             return rc;
         cudaEventElapsedTime(ms, e0, e1);
-        *ms /= static_cast<float>(trials);
+        *ms /= static_cast<float>(2 * trials);
         return BZ_OK;
     };
     float best = -1.0f;

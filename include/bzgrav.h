@@ -129,8 +129,9 @@ bz_status bz_adaptive_levels(bz_handle* h, uint8_t* levels);
 bz_status bz_adaptive_updates(bz_handle* h, uint64_t* updates);
 
 /* Autotuner (no counterpart in the reference, whose leaf capacity and launch shapes are fixed
- * settings): times `trials` steps of zero length (drift, keys, sort, forces, kick; positions and
- * velocities come out unchanged) of the current state, first for each leaf capacity in
+ * settings): times 2 x `trials` steps of zero length (drift, keys, sort, forces, kick; positions
+ * and velocities come out unchanged) of the current state, launched as bz_step launches them (a
+ * captured graph unless use_graph is 0), first for each leaf capacity in
  * {8, 12, 16, 24, 32, 48} x walk group size in {16, 24, 32}, then, for TreePM, with the best of
  * those, for each mesh-leg schedule x walk blocks per SM in {as many as fit, 6, 5}
  * (bz_walk_blocks_per_sm).  Schedules: *mesh_overlap = 0 in line; 1 on a second stream
@@ -141,7 +142,7 @@ bz_status bz_adaptive_updates(bz_handle* h, uint64_t* updates);
 bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int32_t* group_size,
                       float* ms_per_evaluation, int32_t* mesh_overlap);
 
-/* Pins the TreePM mesh-leg schedule (0, 1 or 2 as reported by bz_autotune; the default is 1).
+/* Pins the TreePM mesh-leg schedule (0, 1 or 2 as reported by bz_autotune; the default is 2).
  * Schedules 1 and 2 need the second stream, created with the handle; without it every schedule
  * runs in line.  The results of the schedules differ only in the order of the float mass sums. */
 bz_status bz_set_mesh_schedule(bz_handle* h, int32_t schedule);
