@@ -126,16 +126,27 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
                                                              int chunk, int mesh, float inv_h,
                                                              float inv_h3, float* __restrict__ rho)
 {
-    __shared__ float tile[kTileCells];
+    // The tile accumulates in 32-bit fixed point: integer shared-memory atomics are native and
+    // about three times the rate of float ones, and integer sums are exact and independent of
+    // the order of the additions.  The block's scale 2^k keeps any cell sum below 2^31 / 1.01: a
+    // cell receives at most (largest 1-D weight)^3 x sum |m| / h^3 from the chunk, and the
+    // rounding of at most chunk x P^3 contributions adds less than 2^15.  One unit is then
+    // below 2 x 1.01 x (largest weight)^3 x sum |m| / h^3 / 2^31: with at most 512 particles a
+    // chunk, a few 1e-7 of a mean cell.
+    __shared__ int tile[kTileCells];
     __shared__ int s_lo[3], s_hi[3];
+    __shared__ float s_mass, s_scale, s_unscale;
     const int base = blockIdx.x * chunk;
     const int end = min(base + chunk, n);
     if (threadIdx.x < 3) {
         s_lo[threadIdx.x] = 1 << 30;
         s_hi[threadIdx.x] = -(1 << 30);
     }
+    if (threadIdx.x == 0)
+        s_mass = 0.0f;
     __syncthreads();
     int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
+    float msum = 0.0f;
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
         float w[P];
@@ -145,19 +156,37 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
             lo[a] = min(lo[a], b[a]);
             hi[a] = max(hi[a], b[a] + P - 1);
         }
+        msum += fabsf(p.w);
     }
     for (int a = 0; a < 3; ++a) {
         atomicMin(&s_lo[a], lo[a]);
         atomicMax(&s_hi[a], hi[a]);
     }
+    for (int o = 16; o > 0; o >>= 1)
+        msum += __shfl_xor_sync(kFullMask, msum, o);
+    if ((threadIdx.x & 31) == 0)
+        atomicAdd(&s_mass, msum);
     __syncthreads();
+    if (threadIdx.x == 0) {
+        constexpr float kWmax3 = P == 2 ? 1.0f : (P == 3 ? 0.421875f : 0.2962963f);
+        const float bound = s_mass * inv_h3 * kWmax3 * 1.01f;  // margin for float rounding
+        int k = 0;
+        if (bound > 0.0f) {
+            int e = 0;
+            frexpf(bound, &e);  // bound < 2^e
+            k = min(max(31 - e, -120), 120);
+        }
+        s_scale = ldexpf(1.0f, k);
+        s_unscale = ldexpf(1.0f, -k);
+    }
     const int ex = s_hi[0] - s_lo[0] + 1, ey = s_hi[1] - s_lo[1] + 1, ez = s_hi[2] - s_lo[2] + 1;
     const bool tiled = ex > 0 && ey > 0 && ez > 0 && static_cast<long long>(ex) * ey * ez <= kTileCells;
     const int ox = s_lo[0], oy = s_lo[1], oz = s_lo[2];
     if (tiled)
         for (int c = threadIdx.x; c < ex * ey * ez; c += kThreads)
-            tile[c] = 0.0f;
+            tile[c] = 0;
     __syncthreads();
+    const float scale = s_scale, unscale = s_unscale;
     const size_t M = static_cast<size_t>(mesh);
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
@@ -175,7 +204,8 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
                 for (int a = 0; a < P; ++a) {
                     const float v = wzy * wx[a];
                     if (tiled) {
-                        atomicAdd(&tile[((bz + c - oz) * ey + (by + b - oy)) * ex + (bx + a - ox)], v);
+                        atomicAdd(&tile[((bz + c - oz) * ey + (by + b - oy)) * ex + (bx + a - ox)],
+                                  __float2int_rn(v * scale));
                     } else {
                         const size_t g = (static_cast<size_t>(wrapm(bz + c, mesh)) * M + wrapm(by + b, mesh)) * M +
                                          wrapm(bx + a, mesh);
@@ -201,7 +231,7 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int tx = xa + j - ox;
-            v[j] = (tx >= 0 && tx < ex) ? tile[(z * ey + y) * ex + tx] : 0.0f;
+            v[j] = (tx >= 0 && tx < ex) ? static_cast<float>(tile[(z * ey + y) * ex + tx]) * unscale : 0.0f;
             any = any || v[j] != 0.0f;
         }
         if (!any)
@@ -483,7 +513,7 @@ int pm_deposit_chunk(const PmPlan* p, int n)
     // A chunk of c Morton-consecutive particles spans about c / (n / M^3) cells of a roughly
     // uniform distribution; keep (cbrt(cells) + p)^3 within the tile with margin.
     const double cells_per_particle = static_cast<double>(p->mesh) * p->mesh * p->mesh / (n > 0 ? n : 1);
-    int chunk = 4096;
+    int chunk = 512;  // also bounds the fixed-point unit of the tile (see k_deposit_tiled)
     while (chunk > 128) {
         const double side = std::cbrt(chunk * cells_per_particle) + p->order + 1.0;
         if (side * side * side <= 0.6 * kTileCells)
