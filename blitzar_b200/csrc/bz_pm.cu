@@ -374,12 +374,16 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
 {
     const size_t M = static_cast<size_t>(mesh);
     const int q = threadIdx.x & 3;
-    const int warps = gridDim.x * (kThreads / 32);
-    const int gw = blockIdx.x * (kThreads / 32) + (threadIdx.x >> 5);
-    for (int i0 = gw * 8; i0 < n; i0 += warps * 8) {
+    // each block walks one contiguous (Morton-ordered) range, 64 particles at a time, so that
+    // consecutive rounds reuse the stencil rows they share in L1
+    constexpr int kRound = (kThreads / 32) * 8;
+    const int per_block = ((n + gridDim.x - 1) / gridDim.x + kRound - 1) / kRound * kRound;
+    const int start = blockIdx.x * per_block;
+    const int stop = min(start + per_block, n);
+    for (int i0 = start + (threadIdx.x >> 5) * 8; i0 < stop; i0 += kRound) {
         const int i = i0 + ((threadIdx.x & 31) >> 2);
         float gx = 0.0f, gy = 0.0f, gz = 0.0f;
-        if (i < n && q < P) {
+        if (i < stop && q < P) {
             const float4 p = pos4[i];
             float wx[P], wy[P], wz[P];
             const int bx = stencil<P>(p.x, inv_h, mesh, wx);
@@ -407,7 +411,7 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
             gy += __shfl_xor_sync(kFullMask, gy, o);
             gz += __shfl_xor_sync(kFullMask, gz, o);
         }
-        if (i < n && q == 0) {
+        if (i < stop && q == 0) {
             ax[i] = gx;
             ay[i] = gy;
             az[i] = gz;
