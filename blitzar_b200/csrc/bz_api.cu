@@ -291,9 +291,12 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
         wp.rcorr2 = std::min(rc * rc, wp.rcut2);
     }
     launch_walk(d.pos4, n, h->tree, h->groups, wp, o, d.queue, d.spill, d.err, h->stream);
+    // the mesh leg's accelerations complete d.acc here, or inside the closing kick
+    const bool add_in_kick = overlap && kick && !learned;
     if (overlap) {
         cudaStreamWaitEvent(h->stream, h->ev_join, 0);
-        launch_add3(d.acc[0], d.acc[1], d.acc[2], d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], n, h->stream);
+        if (!add_in_kick)
+            launch_add3(d.acc[0], d.acc[1], d.acc[2], d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], n, h->stream);
     }
     if (learned) {
         const float hcell = static_cast<float>(h->cfg.box_length / h->cfg.treepm_grid_size);
@@ -304,7 +307,11 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
     record(h, kPhIntegrate);
     if (kick) {
         double* const* s = d.st[h->cur];
-        launch_kick(s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt + 1, h->stream);
+        if (add_in_kick)
+            launch_kick(s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt + 1, h->stream,
+                        d.acc_pm[0], d.acc_pm[1], d.acc_pm[2]);
+        else
+            launch_kick(s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt + 1, h->stream);
     }
 }
 

@@ -213,8 +213,10 @@ const float4* pm_force_mesh(PmPlan* p);  // interleaved {ax, ay, az, 0}
 void launch_permute(const uint32_t* perm, int n, const double* const* src, double* const* dst,
                     int ndouble, const float* msrc, float* mdst, const int* idsrc, int* iddst,
                     float4* pos4, double periodic_len, cudaStream_t s);
-void launch_kick(double* vx, double* vy, double* vz, const float* ax, const float* ay,
-                 const float* az, int n, const double* dt_half, cudaStream_t s);
+// Closing half kick; with b (may be NULL) the accelerations are first completed, a += b.
+void launch_kick(double* vx, double* vy, double* vz, float* ax, float* ay, float* az, int n,
+                 const double* dt_half, cudaStream_t s, const float* bx = nullptr,
+                 const float* by = nullptr, const float* bz = nullptr);
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
                        const float* ax, const float* ay, const float* az, int n,
                        const double* dt, double periodic_len, BoxF64* box, cudaStream_t s,

@@ -55,18 +55,32 @@ __global__ void __launch_bounds__(kThreads) k_permute(const uint32_t* __restrict
     }
 }
 
+// Closing half kick.  With (bx, by, bz) (the mesh leg's accelerations from the second stream)
+// the accelerations are first completed in place, a += b, as k_add3 would.
 __global__ void __launch_bounds__(kThreads) k_kick(double* __restrict__ vx, double* __restrict__ vy,
                                                     double* __restrict__ vz,
-                                                    const float* __restrict__ ax,
-                                                    const float* __restrict__ ay,
-                                                    const float* __restrict__ az, int n,
-                                                    const double* __restrict__ dt_half)
+                                                    float* __restrict__ ax,
+                                                    float* __restrict__ ay,
+                                                    float* __restrict__ az, int n,
+                                                    const double* __restrict__ dt_half,
+                                                    const float* __restrict__ bx,
+                                                    const float* __restrict__ by,
+                                                    const float* __restrict__ bz)
 {
     const double h = *dt_half;
     for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
-        vx[i] += static_cast<double>(ax[i]) * h;
-        vy[i] += static_cast<double>(ay[i]) * h;
-        vz[i] += static_cast<double>(az[i]) * h;
+        float a[3] = {ax[i], ay[i], az[i]};
+        if (bx) {
+            a[0] += bx[i];
+            a[1] += by[i];
+            a[2] += bz[i];
+            ax[i] = a[0];
+            ay[i] = a[1];
+            az[i] = a[2];
+        }
+        vx[i] += static_cast<double>(a[0]) * h;
+        vy[i] += static_cast<double>(a[1]) * h;
+        vz[i] += static_cast<double>(a[2]) * h;
     }
 }
 
@@ -179,11 +193,12 @@ void launch_permute(const uint32_t* perm, int n, const double* const* src, doubl
     k_permute<<<grid_for(n), kThreads, 0, s>>>(perm, n, a, ndouble, msrc, mdst, idsrc, iddst, pos4);
 }
 
-void launch_kick(double* vx, double* vy, double* vz, const float* ax, const float* ay,
-                 const float* az, int n, const double* dt_half, cudaStream_t s)
+void launch_kick(double* vx, double* vy, double* vz, float* ax, float* ay, float* az, int n,
+                 const double* dt_half, cudaStream_t s, const float* bx, const float* by,
+                 const float* bz)
 {
     count_launch();
-    k_kick<<<grid_for(n), kThreads, 0, s>>>(vx, vy, vz, ax, ay, az, n, dt_half);
+    k_kick<<<grid_for(n), kThreads, 0, s>>>(vx, vy, vz, ax, ay, az, n, dt_half, bx, by, bz);
 }
 
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
