@@ -501,8 +501,9 @@ def run_ours(args, w, rank, world, local):
         "kernel": "k_walk (group tree walk + pair/multipole arithmetic)",
         "bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
         "frac": achieved_tf / peak_tf,
-        "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak is provided",
+        "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak is provided. The walk is issue-bound (ncu_issue_active_pct of the warp-issue slots busy): its filter, traversal and list work are not counted as flops",
         "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
+        "ncu_issue_active_pct": None if traffic is None else traffic.get("issue_active_pct"),
         "interactions_per_launch": {"particle_particle": pp, "particle_node": pn},
         "flops_per_interaction": {"pp": FLOP_PP[split], "pn": FLOP_PN[(split, True)]},
         "launch_ms": walk_ms,
