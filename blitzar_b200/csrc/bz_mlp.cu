@@ -60,6 +60,37 @@ struct __align__(1024) MlpSmem {
     uint32_t tmem;
 };
 
+// Inference needs only the forward operands: one hidden buffer serves both layers (H2 is
+// written after the second product has consumed H1), and tensor memory holds D1 / D3 in
+// columns 0.. and D2 in 32.. (D3 is written after D1 has been read out).  17 KB of shared
+// memory and 64 TMEM columns a block, so eight blocks share an SM (512 columns).
+constexpr uint32_t kInferCols = 64;
+constexpr uint32_t kInferD1 = 0, kInferD2 = 32, kInferD3 = 0;
+constexpr int kInferBlocksPerSm = 8;
+
+struct __align__(1024) MlpInferSmem {
+    __nv_bfloat16 x[kRows * kFeat];      // A  X       LBO 128 SBO 256
+    __nv_bfloat16 h1[kRows * kHid];      // A  H1, then H2
+    __nv_bfloat16 w1[kHid * kFeat];      // B  W1
+    __nv_bfloat16 w2[kHid * kHid];       // B  W2
+    __nv_bfloat16 w3[kOutPad * kHid];    // B  W3 (rows 3..15 zero)
+    float b2[kHid];
+    float b3[4];
+    float red[2][3];
+    unsigned long long bar;
+    uint32_t tmem;
+};
+
+template <class S> struct MlpCols;
+template <> struct MlpCols<MlpSmem> {
+    static constexpr uint32_t d1 = kColD1, d2 = kColD2, d3 = kColD3, alloc = kTmemCols;
+    __device__ static __nv_bfloat16* h2(MlpSmem& sm) { return sm.h2; }
+};
+template <> struct MlpCols<MlpInferSmem> {
+    static constexpr uint32_t d1 = kInferD1, d2 = kInferD2, d3 = kInferD3, alloc = kInferCols;
+    __device__ static __nv_bfloat16* h2(MlpInferSmem& sm) { return sm.h1; }
+};
+
 __device__ __forceinline__ uint32_t kmaj(int row, int k, int lbo, int sbo)
 {
     return static_cast<uint32_t>((row & 7) * 16 + (k & 7) * 2 + (k >> 3) * lbo + (row >> 3) * sbo);
@@ -154,7 +185,9 @@ __device__ __forceinline__ void put_col(__nv_bfloat16* base, int row0, int col, 
         *reinterpret_cast<__nv_bfloat16*>(b + kmaj(row0 + r, col, lbo, sbo)) = __float2bfloat16_rn(v[r]);
 }
 
-__device__ __forceinline__ float sigmoidf_(float z) { return 1.0f / (1.0f + __expf(-z)); }
+// Fast reciprocal: the activations are rounded to BF16 right after (__fdividef returns 0 for a
+// denominator above 2^126, where the sigmoid is 0 to BF16 precision anyway).
+__device__ __forceinline__ float sigmoidf_(float z) { return __fdividef(1.0f, 1.0f + __expf(-z)); }
 
 __device__ __forceinline__ void features(const float* in6, float* f)
 {
@@ -174,7 +207,8 @@ __device__ __forceinline__ void features(const float* in6, float* f)
     f[15] = 1.0f;
 }
 
-__device__ void load_weights(MlpSmem& sm, const float* __restrict__ p)
+template <class S>
+__device__ void load_forward_weights(S& sm, const float* __restrict__ p)
 {
     const float* W1 = p + kMlpOffW1;
     const float* W2 = p + kMlpOffW2;
@@ -182,8 +216,6 @@ __device__ void load_weights(MlpSmem& sm, const float* __restrict__ p)
     unsigned char* w1 = reinterpret_cast<unsigned char*>(sm.w1);
     unsigned char* w2 = reinterpret_cast<unsigned char*>(sm.w2);
     unsigned char* w3 = reinterpret_cast<unsigned char*>(sm.w3);
-    unsigned char* w2t = reinterpret_cast<unsigned char*>(sm.w2t);
-    unsigned char* w3t = reinterpret_cast<unsigned char*>(sm.w3t);
     for (int i = threadIdx.x; i < kHid * kFeat; i += blockDim.x) {
         const int n = i / kFeat, k = i % kFeat;
         *reinterpret_cast<__nv_bfloat16*>(w1 + kmaj(n, k, 128, 256)) = __float2bfloat16_rn(W1[i]);
@@ -191,17 +223,11 @@ __device__ void load_weights(MlpSmem& sm, const float* __restrict__ p)
     for (int i = threadIdx.x; i < kHid * kHid; i += blockDim.x) {
         const int n = i / kHid, k = i % kHid;
         *reinterpret_cast<__nv_bfloat16*>(w2 + kmaj(n, k, 128, 512)) = __float2bfloat16_rn(W2[n * kHid + k]);
-        *reinterpret_cast<__nv_bfloat16*>(w2t + kmaj(n, k, 128, 512)) = __float2bfloat16_rn(W2[k * kHid + n]);
     }
     for (int i = threadIdx.x; i < kOutPad * kHid; i += blockDim.x) {
         const int n = i / kHid, k = i % kHid;
         *reinterpret_cast<__nv_bfloat16*>(w3 + kmaj(n, k, 128, 512)) =
             __float2bfloat16_rn(n < 3 ? W3[n * kHid + k] : 0.0f);
-    }
-    for (int i = threadIdx.x; i < kHid * kOutPad; i += blockDim.x) {
-        const int n = i / kOutPad, k = i % kOutPad;
-        *reinterpret_cast<__nv_bfloat16*>(w3t + kmaj(n, k, 128, 256)) =
-            __float2bfloat16_rn(k < 3 ? W3[k * kHid + n] : 0.0f);
     }
     for (int i = threadIdx.x; i < kHid; i += blockDim.x)
         sm.b2[i] = p[kMlpOffB2 + i];
@@ -209,12 +235,32 @@ __device__ void load_weights(MlpSmem& sm, const float* __restrict__ p)
         sm.b3[threadIdx.x] = threadIdx.x < 3 ? p[kMlpOffB3 + threadIdx.x] : 0.0f;
 }
 
-__device__ __forceinline__ void tmem_setup(MlpSmem& sm)
+// Training also needs the transposed W2 and W3 for back-propagation.
+__device__ void load_weights(MlpSmem& sm, const float* __restrict__ p)
+{
+    load_forward_weights(sm, p);
+    const float* W2 = p + kMlpOffW2;
+    const float* W3 = p + kMlpOffW3;
+    unsigned char* w2t = reinterpret_cast<unsigned char*>(sm.w2t);
+    unsigned char* w3t = reinterpret_cast<unsigned char*>(sm.w3t);
+    for (int i = threadIdx.x; i < kHid * kHid; i += blockDim.x) {
+        const int n = i / kHid, k = i % kHid;
+        *reinterpret_cast<__nv_bfloat16*>(w2t + kmaj(n, k, 128, 512)) = __float2bfloat16_rn(W2[k * kHid + n]);
+    }
+    for (int i = threadIdx.x; i < kHid * kOutPad; i += blockDim.x) {
+        const int n = i / kOutPad, k = i % kOutPad;
+        *reinterpret_cast<__nv_bfloat16*>(w3t + kmaj(n, k, 128, 256)) =
+            __float2bfloat16_rn(k < 3 ? W3[k * kHid + n] : 0.0f);
+    }
+}
+
+template <class S>
+__device__ __forceinline__ void tmem_setup(S& sm)
 {
     if (threadIdx.x < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&sm.tmem)),
-                     "r"(kTmemCols));
+                     "r"(MlpCols<S>::alloc));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (threadIdx.x == 0)
@@ -225,20 +271,21 @@ __device__ __forceinline__ void tmem_setup(MlpSmem& sm)
     tc_fence_after();
 }
 
-__device__ __forceinline__ void tmem_release(MlpSmem& sm)
+template <class S>
+__device__ __forceinline__ void tmem_release(S& sm)
 {
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
     if (threadIdx.x < 32)
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sm.tmem),
-                     "r"(kTmemCols));
+                     "r"(MlpCols<S>::alloc));
 }
 
 // Make the operands written by all threads visible to the tensor core, issue `body` from one
 // thread, and wait (bounded) for the products to land in tensor memory.
-template <class F>
-__device__ __forceinline__ void mma_step(MlpSmem& sm, uint32_t& phase, int* err, F body)
+template <class S, class F>
+__device__ __forceinline__ void mma_step(S& sm, uint32_t& phase, int* err, F body)
 {
     proxy_fence();
     tc_fence_before();
@@ -254,46 +301,50 @@ __device__ __forceinline__ void mma_step(MlpSmem& sm, uint32_t& phase, int* err,
 }
 
 // Forward pass of the tile already in sm.x: leaves Z1 (D1), Z2 (D2) and the network output
-// (D3) in tensor memory and returns this row's pre-activations and output.
-__device__ void forward(MlpSmem& sm, uint32_t tm, uint32_t& phase, int* err, float* z1, float* z2,
-                        float* out, bool keep_bwg)
+// (D3) in tensor memory and returns this row's pre-activations and output.  KEEP_BWG (training)
+// also stores the activations transposed for the weight-gradient product.
+template <bool KEEP_BWG, class S>
+__device__ void forward(S& sm, uint32_t tm, uint32_t& phase, int* err, float* z1, float* z2,
+                        float* out)
 {
+    using C = MlpCols<S>;
     const int r = threadIdx.x;
     const uint32_t lane = static_cast<uint32_t>((r & ~31)) << 16;
     mma_step(sm, phase, err, [&] {
-        umma(tm + kColD1, sdesc(sm.x, 128, 256), sdesc(sm.w1, 128, 256), idesc_bf16(128, 32), 0);
+        umma(tm + C::d1, sdesc(sm.x, 128, 256), sdesc(sm.w1, 128, 256), idesc_bf16(128, 32), 0);
     });
     float h[32];
-    tmem_ld32(tm + lane + kColD1, z1);
+    tmem_ld32(tm + lane + C::d1, z1);
 #pragma unroll
     for (int i = 0; i < 32; ++i)
         h[i] = z1[i] * sigmoidf_(z1[i]);
     put_row(sm.h1, r, h, 32, 128, 512);
-    if (keep_bwg)
+    if constexpr (KEEP_BWG)
         put_col(sm.bwg, 0, r, h, 32, 128, 2048);
     mma_step(sm, phase, err, [&] {
         for (int j = 0; j < 2; ++j)
-            umma(tm + kColD2, sdesc(reinterpret_cast<unsigned char*>(sm.h1) + 256 * j, 128, 512),
+            umma(tm + C::d2, sdesc(reinterpret_cast<unsigned char*>(sm.h1) + 256 * j, 128, 512),
                  sdesc(reinterpret_cast<unsigned char*>(sm.w2) + 256 * j, 128, 512),
                  idesc_bf16(128, 32), j);
     });
-    tmem_ld32(tm + lane + kColD2, z2);
+    tmem_ld32(tm + lane + C::d2, z2);
 #pragma unroll
     for (int i = 0; i < 32; ++i) {
         z2[i] += sm.b2[i];
         h[i] = z2[i] * sigmoidf_(z2[i]);
     }
-    put_row(sm.h2, r, h, 32, 128, 512);
-    if (keep_bwg)
+    __nv_bfloat16* h2 = C::h2(sm);
+    put_row(h2, r, h, 32, 128, 512);
+    if constexpr (KEEP_BWG)
         put_col(sm.bwg, 48, r, h, 32, 128, 2048);
     mma_step(sm, phase, err, [&] {
         for (int j = 0; j < 2; ++j)
-            umma(tm + kColD3, sdesc(reinterpret_cast<unsigned char*>(sm.h2) + 256 * j, 128, 512),
+            umma(tm + C::d3, sdesc(reinterpret_cast<unsigned char*>(h2) + 256 * j, 128, 512),
                  sdesc(reinterpret_cast<unsigned char*>(sm.w3) + 256 * j, 128, 512),
                  idesc_bf16(128, 16), j);
     });
     float o[16];
-    tmem_ld16(tm + lane + kColD3, o);
+    tmem_ld16(tm + lane + C::d3, o);
     out[0] = o[0] + sm.b3[0];
     out[1] = o[1] + sm.b3[1];
     out[2] = o[2] + sm.b3[2];
@@ -337,7 +388,7 @@ __global__ void __launch_bounds__(kThreadsMlp) k_mlp_train(const float* __restri
     put_col(sm.bwg, 32, r, f, 16, 128, 2048);
 
     float z1[32], z2[32], out[3];
-    forward(sm, tm, phase, err, z1, z2, out, true);
+    forward<true>(sm, tm, phase, err, z1, z2, out);
 
     // dL/dout for L = sum (out - y)^2 / batch
     float d[16];
@@ -412,16 +463,15 @@ __global__ void __launch_bounds__(kThreadsMlp) k_mlp_train(const float* __restri
 }
 
 // Batch inference: out3 = scale * network(in6) (per sample).
-__global__ void __launch_bounds__(kThreadsMlp) k_mlp_forward(const float* __restrict__ params,
-                                                              const float* __restrict__ in6, int n,
-                                                              float scale, float* __restrict__ out3,
-                                                              int* err)
+__global__ void __launch_bounds__(kThreadsMlp, kInferBlocksPerSm) k_mlp_forward(
+    const float* __restrict__ params, const float* __restrict__ in6, int n, float scale,
+    float* __restrict__ out3, int* err)
 {
     extern __shared__ __align__(1024) unsigned char smraw[];
-    MlpSmem& sm = *reinterpret_cast<MlpSmem*>(
+    MlpInferSmem& sm = *reinterpret_cast<MlpInferSmem*>(
         (reinterpret_cast<uintptr_t>(smraw) + 1023) & ~static_cast<uintptr_t>(1023));
     const int r = threadIdx.x;
-    load_weights(sm, params);
+    load_forward_weights(sm, params);
     tmem_setup(sm);
     const uint32_t tm = sm.tmem;
     uint32_t phase = 0;
@@ -435,7 +485,7 @@ __global__ void __launch_bounds__(kThreadsMlp) k_mlp_forward(const float* __rest
         features(in, f);
         put_row(sm.x, r, f, 16, 128, 256);
         float z1[32], z2[32], out[3];
-        forward(sm, tm, phase, err, z1, z2, out, false);
+        forward<false>(sm, tm, phase, err, z1, z2, out);
         if (valid)
             for (int i = 0; i < 3; ++i)
                 out3[3 * static_cast<size_t>(s) + i] = scale * out[i];
@@ -446,20 +496,16 @@ __global__ void __launch_bounds__(kThreadsMlp) k_mlp_forward(const float* __rest
 // Pair correction: rows of a tile are (target, pair slot) for 2 targets x kPairSlots slots.
 // Each listed pair subtracts m_source / h^2 * scale * network(separation, source offset)
 // from its target's acceleration.
-__global__ void __launch_bounds__(kThreadsMlp) k_mlp_pairs(const float* __restrict__ params,
-                                                            const float4* __restrict__ pos4, int n,
-                                                            const int* __restrict__ pair_src,
-                                                            const int* __restrict__ pair_cnt,
-                                                            float inv_h, float box, float coef,
-                                                            float* __restrict__ ax,
-                                                            float* __restrict__ ay,
-                                                            float* __restrict__ az, int* err)
+__global__ void __launch_bounds__(kThreadsMlp, kInferBlocksPerSm) k_mlp_pairs(
+    const float* __restrict__ params, const float4* __restrict__ pos4, int n,
+    const int* __restrict__ pair_src, const int* __restrict__ pair_cnt, float inv_h, float box,
+    float coef, float* __restrict__ ax, float* __restrict__ ay, float* __restrict__ az, int* err)
 {
     extern __shared__ __align__(1024) unsigned char smraw[];
-    MlpSmem& sm = *reinterpret_cast<MlpSmem*>(
+    MlpInferSmem& sm = *reinterpret_cast<MlpInferSmem*>(
         (reinterpret_cast<uintptr_t>(smraw) + 1023) & ~static_cast<uintptr_t>(1023));
     const int r = threadIdx.x;
-    load_weights(sm, params);
+    load_forward_weights(sm, params);
     tmem_setup(sm);
     const uint32_t tm = sm.tmem;
     uint32_t phase = 0;
@@ -495,7 +541,7 @@ __global__ void __launch_bounds__(kThreadsMlp) k_mlp_pairs(const float* __restri
         features(in, f);
         put_row(sm.x, r, f, 16, 128, 256);
         float z1[32], z2[32], out[3];
-        forward(sm, tm, phase, err, z1, z2, out, false);
+        forward<false>(sm, tm, phase, err, z1, z2, out);
         float c[3];
         for (int i = 0; i < 3; ++i) {
             c[i] = valid ? coef * ms * out[i] : 0.0f;
@@ -534,6 +580,15 @@ __global__ void k_adam(float* __restrict__ p, float* __restrict__ g, float* __re
 }
 
 size_t mlp_smem() { return sizeof(MlpSmem) + 1024; }
+// Inference blocks request at least 1/7 of an SM's shared memory so that no more than
+// kInferBlocksPerSm of them (whose TMEM columns add up to the SM's 512) are ever co-resident:
+// a ninth block's tcgen05.alloc would otherwise wait for a column range to be freed.
+size_t mlp_infer_smem()
+{
+    const size_t need = sizeof(MlpInferSmem) + 1024;
+    const size_t floor = 228 * 1024 / (kInferBlocksPerSm + 1) + 1024;
+    return need > floor ? need : floor;
+}
 
 void set_mlp_attrs()
 {
@@ -543,8 +598,8 @@ void set_mlp_attrs()
     if (dev >= 0 && dev < kMaxDevices && done[dev])
         return;
     cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(mlp_smem()));
-    cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(mlp_smem()));
-    cudaFuncSetAttribute(k_mlp_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(mlp_smem()));
+    cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(mlp_infer_smem()));
+    cudaFuncSetAttribute(k_mlp_pairs, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(mlp_infer_smem()));
     if (dev >= 0 && dev < kMaxDevices)
         done[dev] = true;
 }
@@ -583,10 +638,11 @@ void launch_mlp_forward(const float* params, const float* in6, int n, float scal
 {
     set_mlp_attrs();
     int blocks = (n + kRows - 1) / kRows;
-    const int cap = 2 * sm_count();
+    const int cap = kInferBlocksPerSm * sm_count();
     blocks = blocks < cap ? blocks : cap;
     count_launch();
-    k_mlp_forward<<<blocks > 0 ? blocks : 1, kThreadsMlp, mlp_smem(), s>>>(params, in6, n, scale, out3, err);
+    k_mlp_forward<<<blocks > 0 ? blocks : 1, kThreadsMlp, mlp_infer_smem(), s>>>(params, in6, n, scale,
+                                                                                 out3, err);
 }
 
 void launch_mlp_pairs(const float* params, const float4* pos4, int n, const int* pair_src,
@@ -595,10 +651,10 @@ void launch_mlp_pairs(const float* params, const float4* pos4, int n, const int*
 {
     set_mlp_attrs();
     int blocks = (n + 1) / 2;
-    const int cap = 2 * sm_count();
+    const int cap = kInferBlocksPerSm * sm_count();
     blocks = blocks < cap ? blocks : cap;
     count_launch();
-    k_mlp_pairs<<<blocks > 0 ? blocks : 1, kThreadsMlp, mlp_smem(), s>>>(
+    k_mlp_pairs<<<blocks > 0 ? blocks : 1, kThreadsMlp, mlp_infer_smem(), s>>>(
         params, pos4, n, pair_src, pair_cnt, 1.0f / h, box, scale / (h * h), ax, ay, az, err);
 }
 
