@@ -28,7 +28,7 @@ EXPORTS = (
     "bz_sort_pairs_noalloc", "bz_energy", "bz_autotune", "bz_learn_generate", "bz_learn_train",
     "bz_learn_set", "bz_learn_get", "bz_learn_enable", "bz_learn_forward", "bz_learn_gradient",
     "bz_set_ensemble", "bz_adaptive_levels", "bz_adaptive_updates", "bz_set_mesh_schedule",
-    "bz_walk_blocks_per_sm",
+    "bz_walk_blocks_per_sm", "bz_set_state_acc", "bz_get_state_acc",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -117,6 +117,8 @@ def load():
     L.bz_autotune.argtypes = [_vp, C.c_int32, _vp, _vp, _vp, _vp]
     L.bz_set_mesh_schedule.argtypes = [_vp, C.c_int32]
     L.bz_walk_blocks_per_sm.argtypes = [_vp, C.c_int32, _vp]
+    L.bz_set_state_acc.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_size_t]
+    L.bz_get_state_acc.argtypes = [_vp, _vp, _vp, _vp]
     L.bz_adaptive_levels.argtypes = [_vp, _vp]
     L.bz_adaptive_updates.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_set_ensemble.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_int32]
@@ -241,6 +243,19 @@ class Engine:
         fn = self.L.bz_get_state_f64 if f64 else self.L.bz_get_state
         self._check(fn(self.h, _ptr(p), _ptr(v)), "bz_get_state")
         return p.reshape(3, n).T.copy(), (None if v is None else v.reshape(3, n).T.copy())
+
+    def set_state_acc_soa(self, pos_soa3, vel_soa3, mass, acc_soa3):
+        """Upload a leapfrog state with the accelerations of its positions (caller-owned SoA
+        float32 buffers): the next step needs no set-up force evaluation."""
+        n = mass.shape[0]
+        self._check(self.L.bz_set_state_acc(self.h, _ptr(pos_soa3), _ptr(vel_soa3), _ptr(mass),
+                                            _ptr(acc_soa3), n), "bz_set_state_acc")
+        self.n = n
+
+    def get_state_acc_soa(self, pos_soa3, vel_soa3, acc_soa3):
+        """Download positions, velocities and the accelerations of the positions (SoA)."""
+        self._check(self.L.bz_get_state_acc(self.h, _ptr(pos_soa3), _ptr(vel_soa3), _ptr(acc_soa3)),
+                    "bz_get_state_acc")
 
     def get_state_soa(self, pos_soa3, vel_soa3):
         self._check(self.L.bz_get_state(self.h, _ptr(pos_soa3), _ptr(vel_soa3)), "bz_get_state")

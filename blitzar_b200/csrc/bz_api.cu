@@ -870,6 +870,25 @@ bz_status bz_set_state(bz_handle* h, const float* pos, const float* vel, const f
     return check_device(h, "bz_set_state");
 }
 
+bz_status bz_set_state_acc(bz_handle* h, const float* pos, const float* vel, const float* mass,
+                           const float* acc, size_t n)
+{
+    if (!h || !acc)
+        return BZ_INVALID_ARGUMENT;
+    if (h->cfg.adaptive_max_level > 0)
+        return fail(h, BZ_UNSUPPORTED, "adaptive steps keep per-particle accelerations of their own");
+    const bz_status st = bz_set_state(h, pos, vel, mass, n);
+    if (st != BZ_OK)
+        return st;
+    // the state sits in caller order now (buffer 0, identity ids): so do the accelerations
+    for (int a = 0; a < 3; ++a)
+        cudaMemcpyAsync(h->d.acc[a], acc + a * n, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    const bz_status st2 = check_device(h, "bz_set_state_acc");
+    if (st2 == BZ_OK)
+        h->forces_valid = true;
+    return st2;
+}
+
 bz_status bz_set_state_f64(bz_handle* h, const double* pos, const double* vel, const float* mass,
                            size_t n)
 {
@@ -939,6 +958,31 @@ bz_status bz_get_state(bz_handle* h, float* pos, float* vel)
     if (vel)
         cudaMemcpyAsync(vel, d.stage + 3 * n, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
     return check_device(h, "bz_get_state");
+}
+
+bz_status bz_get_state_acc(bz_handle* h, float* pos, float* vel, float* acc)
+{
+    if (!h || !pos || !acc || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    if (h->cfg.adaptive_max_level > 0)
+        return fail(h, BZ_UNSUPPORTED, "adaptive steps keep per-particle accelerations of their own");
+    bz_status st = ensure_forces(h);
+    if (st != BZ_OK)
+        return st;
+    const size_t n = h->n;
+    DeviceBuffers& d = h->d;
+    double* const* s = d.st[h->cur];
+    count_launch();
+    k_pack_state<<<blocks_for(n), 256, 0, h->stream>>>(s[0], s[1], s[2], s[3], s[4], s[5], d.id[h->cur],
+                                                       static_cast<int>(n), d.stage, vel ? 1 : 0);
+    cudaMemcpyAsync(pos, d.stage, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    if (vel)
+        cudaMemcpyAsync(vel, d.stage + 3 * n, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    // the stage is reused after the copies above (stream order)
+    launch_scatter3(d.acc[0], d.acc[1], d.acc[2], d.id[h->cur], static_cast<int>(n), d.stage, h->stream);
+    cudaMemcpyAsync(acc, d.stage, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    return check_device(h, "bz_get_state_acc");
 }
 
 bz_status bz_get_state_f64(bz_handle* h, double* pos, double* vel)

@@ -172,6 +172,18 @@ bz_status bz_energy(bz_handle* h, double* kinetic, double* potential, double* mo
 bz_status bz_get_state(bz_handle* h, float* pos_soa3, float* vel_soa3);
 bz_status bz_get_state_f64(bz_handle* h, double* pos_soa3, double* vel_soa3);
 
+/* Leapfrog (kick-drift-kick) state with its accelerations, for hosts that keep the state in
+ * their own memory between steps.  bz_get_state_acc returns positions, velocities (may be
+ * NULL) and the accelerations of those positions (SoA 3n floats each, caller order; computed
+ * first if the handle has none).  bz_set_state_acc uploads a state together with its
+ * accelerations, which must be the forces at these positions (as bz_get_state_acc or
+ * bz_accelerations returned them): the next bz_step then needs no set-up force evaluation,
+ * as a step of a resident state needs none.  Neither applies to adaptive block steps
+ * (BZ_UNSUPPORTED). */
+bz_status bz_set_state_acc(bz_handle* h, const float* pos3n, const float* vel3n, const float* mass,
+                           const float* acc3n, size_t n);
+bz_status bz_get_state_acc(bz_handle* h, float* pos3n, float* vel3n, float* acc3n);
+
 /* Morton keys of the current state, sorted, with the stable sort permutation (sorted
  * position -> caller index): buildMortonCodesKernel + thrust::sort_by_key
  * (engine/physics/octree/cuda/linear/OctKeyKernels.inl:22-46, OctBuild.inl:96). */

@@ -145,3 +145,33 @@ def test_headless_driver_matches_engine(gpu, tmp_path):
         p_e, v_e = e.get_state()
     assert np.array_equal(p_h, p_e.astype(np.float32)) and np.array_equal(v_h, v_e.astype(np.float32))
     assert np.array_equal(m_h, m)
+
+
+def test_state_with_accelerations(gpu):
+    """A state uploaded with the accelerations of its positions steps exactly like the same
+    state uploaded alone (whose set-up evaluation computes those forces), and the accelerations
+    returned with a state are the forces at its positions."""
+    n = 20_000
+    pos = plummer(n, seed=8)
+    rng = np.random.default_rng(8)
+    vel = (0.1 * rng.standard_normal((n, 3))).astype(np.float32)
+    m = np.full(n, 1.0 / n, np.float32)
+    with _engine(n) as e:
+        e.set_state(pos, vel, m)
+        acc = e.accelerations()
+    with _engine(n) as e:
+        e.set_state(pos, vel, m)
+        e.step(1e-3, 3)
+        pa, va = e.get_state(f64=True)
+    ps = np.ascontiguousarray(pos.T, np.float32).ravel()
+    vs = np.ascontiguousarray(vel.T, np.float32).ravel()
+    acs = np.ascontiguousarray(acc.T, np.float32).ravel()
+    with _engine(n) as e:
+        e.set_state_acc_soa(ps, vs, m, acs)
+        e.step(1e-3, 3)
+        pb, vb = e.get_state(f64=True)
+        p3, v3, a3 = (np.empty(3 * n, np.float32) for _ in range(3))
+        e.get_state_acc_soa(p3, v3, a3)
+        again = e.accelerations()
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+    assert np.array_equal(a3.reshape(3, n).T, again)
