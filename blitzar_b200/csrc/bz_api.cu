@@ -52,7 +52,7 @@ struct DeviceBuffers {
     unsigned* queue = nullptr;
     int* spill = nullptr;
     unsigned long long* counters = nullptr;  // [2] pp, pn
-    float* stage = nullptr;                  // 7n floats for host transfers
+    float* stage = nullptr;                  // 10n floats for host transfers
     float* ref_xyzm = nullptr;               // 4n floats, caller order, reference mode
     float4* ref_orig = nullptr;              // n float4, caller order
     float* ref_hot8 = nullptr;               // 8 floats
@@ -630,7 +630,7 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
          dalloc(h, &d.box, 1) && dalloc(h, &d.bbox32, 8) && dalloc(h, &d.err, 1) &&
          dalloc(h, &d.dt, 2) && dalloc(h, &d.energy, energy_scratch_doubles()) &&
          dalloc(h, &d.queue, 1) && dalloc(h, &d.counters, 2) &&
-         dalloc(h, &d.stage, 7 * n) && dalloc(h, &d.ref_xyzm, 4 * n) && dalloc(h, &d.ref_orig, n) &&
+         dalloc(h, &d.stage, 10 * n) && dalloc(h, &d.ref_xyzm, 4 * n) && dalloc(h, &d.ref_orig, n) &&
          dalloc(h, &d.ref_hot8, 8);
     // sort workspace
     SortWorkspace& sw = h->sort;
@@ -744,6 +744,36 @@ __global__ void k_unpack_state(const float* __restrict__ st, int n, int have_vel
     }
 }
 
+// As k_unpack_state, into the device's current particle order: slot i takes caller particle
+// id[i] (ids kept), with the accelerations staged after the state (caller order).
+__global__ void k_unpack_state_kept(const float* __restrict__ st, int n, int have_vel, double* x,
+                                    double* y, double* z, double* vx, double* vy, double* vz,
+                                    float* m, const int* __restrict__ id, double box,
+                                    float* ax, float* ay, float* az)
+{
+    const float* acc = st + 7 * static_cast<size_t>(n);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int c = id[i];
+        double p[3] = {st[c], st[n + c], st[2 * n + c]};
+        if (box > 0.0)
+            for (int a = 0; a < 3; ++a) {
+                p[a] -= box * floor(p[a] / box);
+                if (p[a] >= box)
+                    p[a] = 0.0;
+            }
+        x[i] = p[0];
+        y[i] = p[1];
+        z[i] = p[2];
+        vx[i] = have_vel ? st[3 * n + c] : 0.0;
+        vy[i] = have_vel ? st[4 * n + c] : 0.0;
+        vz[i] = have_vel ? st[5 * n + c] : 0.0;
+        m[i] = st[6 * n + c];
+        ax[i] = acc[c];
+        ay[i] = acc[n + c];
+        az[i] = acc[2 * n + c];
+    }
+}
+
 __global__ void k_pack_state(const double* x, const double* y, const double* z,
                              const double* vx, const double* vy, const double* vz,
                              const int* __restrict__ id, int n, float* out, int want_vel)
@@ -849,12 +879,10 @@ void enqueue_reference_order(bz_handle* h)
 
 extern "C" {
 
-bz_status bz_set_state(bz_handle* h, const float* pos, const float* vel, const float* mass,
-                       size_t n)
+// Uploads and unpacks an FP32 state (caller order, buffer 0) on the handle's stream.
+static void enqueue_set_state(bz_handle* h, const float* pos, const float* vel, const float* mass,
+                              size_t n)
 {
-    if (!h || !pos || !mass || n == 0 || n > h->capacity)
-        return BZ_INVALID_ARGUMENT;
-    cudaSetDevice(h->device);
     DeviceBuffers& d = h->d;
     cudaMemcpyAsync(d.stage, pos, 3 * n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
     if (vel)
@@ -867,26 +895,56 @@ bz_status bz_set_state(bz_handle* h, const float* pos, const float* vel, const f
                                                          s[0], s[1], s[2], s[3], s[4], s[5],
                                                          d.mass[0], d.id[0],
                                                          periodic(h) ? h->cfg.box_length : 0.0);
+}
+
+bz_status bz_set_state(bz_handle* h, const float* pos, const float* vel, const float* mass,
+                       size_t n)
+{
+    if (!h || !pos || !mass || n == 0 || n > h->capacity)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    enqueue_set_state(h, pos, vel, mass, n);
     return check_device(h, "bz_set_state");
 }
 
 bz_status bz_set_state_acc(bz_handle* h, const float* pos, const float* vel, const float* mass,
                            const float* acc, size_t n)
 {
-    if (!h || !acc)
+    if (!h || !pos || !mass || !acc || n == 0 || n > h->capacity)
         return BZ_INVALID_ARGUMENT;
     if (h->cfg.adaptive_max_level > 0)
         return fail(h, BZ_UNSUPPORTED, "adaptive steps keep per-particle accelerations of their own");
-    const bz_status st = bz_set_state(h, pos, vel, mass, n);
-    if (st != BZ_OK)
-        return st;
-    // the state sits in caller order now (buffer 0, identity ids): so do the accelerations
-    for (int a = 0; a < 3; ++a)
-        cudaMemcpyAsync(h->d.acc[a], acc + a * n, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
-    const bz_status st2 = check_device(h, "bz_set_state_acc");
-    if (st2 == BZ_OK)
+    cudaSetDevice(h->device);
+    DeviceBuffers& d = h->d;
+    if (h->n == n && h->systems == 0) {
+        // A state of the same size replaces the held one in the device's current particle order
+        // (the last sort's): a host round trip of the state then leaves it nearly sorted, and
+        // the next step's re-sort and mesh deposit stay on their fast paths.  The result is
+        // that of a caller-order upload (the step sorts either way), up to the order of
+        // particles with equal keys.
+        cudaMemcpyAsync(d.stage, pos, 3 * n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+        if (vel)
+            cudaMemcpyAsync(d.stage + 3 * n, vel, 3 * n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+        cudaMemcpyAsync(d.stage + 6 * n, mass, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+        cudaMemcpyAsync(d.stage + 7 * n, acc, 3 * n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+        h->ad.ready = false;
+        h->ref_tree_valid = false;
+        double* const* s = d.st[h->cur];
+        count_launch();
+        k_unpack_state_kept<<<blocks_for(n), 256, 0, h->stream>>>(
+            d.stage, static_cast<int>(n), vel ? 1 : 0, s[0], s[1], s[2], s[3], s[4], s[5],
+            d.mass[h->cur], d.id[h->cur], periodic(h) ? h->cfg.box_length : 0.0, d.acc[0], d.acc[1],
+            d.acc[2]);
+    } else {
+        enqueue_set_state(h, pos, vel, mass, n);
+        // the state sits in caller order now (buffer 0, identity ids): so do the accelerations
+        for (int a = 0; a < 3; ++a)
+            cudaMemcpyAsync(d.acc[a], acc + a * n, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    }
+    const bz_status st = check_device(h, "bz_set_state_acc");
+    if (st == BZ_OK)
         h->forces_valid = true;
-    return st2;
+    return st;
 }
 
 bz_status bz_set_state_f64(bz_handle* h, const double* pos, const double* vel, const float* mass,

@@ -178,8 +178,10 @@ bz_status bz_get_state_f64(bz_handle* h, double* pos_soa3, double* vel_soa3);
  * first if the handle has none).  bz_set_state_acc uploads a state together with its
  * accelerations, which must be the forces at these positions (as bz_get_state_acc or
  * bz_accelerations returned them): the next bz_step then needs no set-up force evaluation,
- * as a step of a resident state needs none.  Neither applies to adaptive block steps
- * (BZ_UNSUPPORTED). */
+ * as a step of a resident state needs none.  A state of the size the handle already holds
+ * replaces it in the device's current particle order, so that a round trip through the host
+ * keeps the next re-sort cheap; results are those of a fresh upload up to the order of
+ * particles with identical keys.  Neither applies to adaptive block steps (BZ_UNSUPPORTED). */
 bz_status bz_set_state_acc(bz_handle* h, const float* pos3n, const float* vel3n, const float* mass,
                            const float* acc3n, size_t n);
 bz_status bz_get_state_acc(bz_handle* h, float* pos3n, float* vel3n, float* acc3n);

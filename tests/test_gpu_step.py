@@ -175,3 +175,26 @@ def test_state_with_accelerations(gpu):
         again = e.accelerations()
     assert np.array_equal(pa, pb) and np.array_equal(va, vb)
     assert np.array_equal(a3.reshape(3, n).T, again)
+
+
+def test_state_round_trip_keeps_order(gpu):
+    """Uploading a held state back (same size) keeps the device's particle order; the steps that
+    follow match those of a fresh engine given the same state and accelerations."""
+    n = 20_000
+    pos = plummer(n, seed=9)
+    rng = np.random.default_rng(9)
+    vel = (0.1 * rng.standard_normal((n, 3))).astype(np.float32)
+    m = np.full(n, 1.0 / n, np.float32)
+    p3, v3, a3 = (np.empty(3 * n, np.float32) for _ in range(3))
+    with _engine(n) as e:
+        e.set_state(pos, vel, m)
+        e.step(1e-3, 2)
+        e.get_state_acc_soa(p3, v3, a3)
+        e.set_state_acc_soa(p3, v3, m, a3)  # same size: kept in the sorted order
+        e.step(1e-3, 2)
+        pa, va = e.get_state(f64=True)
+    with _engine(n) as e:
+        e.set_state_acc_soa(p3, v3, m, a3)
+        e.step(1e-3, 2)
+        pb, vb = e.get_state(f64=True)
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
