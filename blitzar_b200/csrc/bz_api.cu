@@ -1034,12 +1034,13 @@ bz_status bz_get_state_acc(bz_handle* h, float* pos, float* vel, float* acc)
     count_launch();
     k_pack_state<<<blocks_for(n), 256, 0, h->stream>>>(s[0], s[1], s[2], s[3], s[4], s[5], d.id[h->cur],
                                                        static_cast<int>(n), d.stage, vel ? 1 : 0);
+    launch_scatter3(d.acc[0], d.acc[1], d.acc[2], d.id[h->cur], static_cast<int>(n), d.stage + 6 * n,
+                    h->stream);
+    // the three copies follow each other without a kernel between them
     cudaMemcpyAsync(pos, d.stage, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
     if (vel)
         cudaMemcpyAsync(vel, d.stage + 3 * n, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
-    // the stage is reused after the copies above (stream order)
-    launch_scatter3(d.acc[0], d.acc[1], d.acc[2], d.id[h->cur], static_cast<int>(n), d.stage, h->stream);
-    cudaMemcpyAsync(acc, d.stage, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(acc, d.stage + 6 * n, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
     return check_device(h, "bz_get_state_acc");
 }
 
