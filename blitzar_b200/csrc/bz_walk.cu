@@ -307,15 +307,7 @@ __device__ __forceinline__ void flush_nodes(WarpSmem& w, int nn, const TreeArray
         }
         __syncwarp();
         float fx = 0.0f, fy = 0.0f, fz = 0.0f, fp = 0.0f;
-        if (newton && m == 32) {
-            // a full batch: a fixed trip count unrolled by four (shared-memory operands at constant
-            // offsets within each group of four); same summation order.  Unrolling all 32 was
-            // slower (code size), by four the fastest of 2 / 4 / 8 / 32 on the octree workloads
-#pragma unroll 4
-            for (int j = 0; j < 32; ++j)
-                pair_pn_newton(w.nd_mono[j], w.nd_qa[j], w.nd_qb[j], w.nd_tr[j], tx, ty, tz, p.eps2,
-                               fx, fy, fz);
-        } else if (newton) {
+        if (newton) {
             int j = 0;
             for (; j + 1 < m; j += 2) {
                 pair_pn_newton(w.nd_mono[j], w.nd_qa[j], w.nd_qb[j], w.nd_tr[j], tx, ty, tz, p.eps2,
@@ -545,24 +537,6 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                     record(s4, w.tidx[(wd << 5) + b]);
             }
             __syncwarp();
-            for (int j = jfirst; j < nl; ++j) {
-                if (w.lpre[j] >= cend)
-                    break;
-                if (w.lpre[j] + w.lcount[j] <= cend)
-                    jfirst = j + 1;
-            }
-        } else if (fast && !cut && !per_pair && !rec) {
-            // no cutoff, no per-pair images, nothing recorded: the tile's sources in tile order,
-            // one loop unrolled by four instead of one short loop per leaf (same summation order)
-            const int nb = cend - cbase;
-            int q = 0;
-            for (; q + 4 <= nb; q += 4) {
-#pragma unroll
-                for (int u = 0; u < 4; ++u)
-                    pair_fast<SPLIT>(w.tile[q + u], tx, ty, tz, p.eps2, p.rcut2, false, sk, fx, fy, fz);
-            }
-            for (; q < nb; ++q)
-                pair_fast<SPLIT>(w.tile[q], tx, ty, tz, p.eps2, p.rcut2, false, sk, fx, fy, fz);
             for (int j = jfirst; j < nl; ++j) {
                 if (w.lpre[j] >= cend)
                     break;
