@@ -151,7 +151,10 @@ def engine_config(w):
                     treepm_window_floor=0.0 if spectral else 0.08,
                     treepm_node_size_factor=w["node_size_factor"],
                     octree_theta=w["theta"], octree_softening=w["eps_lattice"] / w["n_side"],
-                    multipole_order=2)
+                    # with the node-size cap no node is accepted inside the cutoff on these
+                    # boxes (particle_node = 0 in the counters), so the walk needs no multipoles
+                    # and the tree no second moments; the cic workload (no cap) keeps them
+                    multipole_order=1 if w["node_size_factor"] > 0 else 2)
     cfg = dict(solver=0, octree_theta=w["theta"], octree_softening=w["eps"], multipole_order=2)
     if w.get("adaptive_levels"):
         cfg.update(adaptive_max_level=w["adaptive_levels"], adaptive_eta=w["adaptive_eta"])

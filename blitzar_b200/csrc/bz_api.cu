@@ -260,7 +260,7 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
     record(h, kPhTree);
     const int root_level = h->systems > 0 ? kSystemLevels : 0;
     launch_tree_build(d.keys, d.pos4, n, h->cfg.leaf_capacity, kMaxLevels, h->tree, d.err,
-                      h->stream, root_level);
+                      h->stream, root_level, h->cfg.multipole_order >= 2);
     launch_groups(h->tree, n, h->cfg.walk_group_size, root_level, d.keys, h->groups, h->stream);
     record(h, kPhMesh);
     if (h->cfg.solver == BZ_SOLVER_TREEPM && h->pm && !overlap) {
@@ -1231,7 +1231,7 @@ bz_status adaptive_steps(bz_handle* h, double dt, uint32_t nsteps)
                 enqueue_order(h);
                 record(h, kPhTree);
                 launch_tree_build(d.keys, d.pos4, n, h->cfg.leaf_capacity, kMaxLevels, h->tree, d.err,
-                                  h->stream, root_level);
+                                  h->stream, root_level, h->cfg.multipole_order >= 2);
                 launch_groups(h->tree, n, h->cfg.walk_group_size, root_level, d.keys, h->groups,
                               h->stream);
             } else {
@@ -1241,7 +1241,7 @@ bz_status adaptive_steps(bz_handle* h, double dt, uint32_t nsteps)
                 record(h, kPhPermute);
                 launch_refresh_pos4(st[0], st[1], st[2], d.mass[h->cur], n, d.pos4, h->stream);
                 record(h, kPhTree);
-                launch_tree_refit(d.pos4, h->tree, h->stream);
+                launch_tree_refit(d.pos4, h->tree, h->stream, h->cfg.multipole_order >= 2);
             }
             double* const* st = d.st[h->cur];
             launch_adaptive_active(d.id[h->cur], n, h->ad.st, sub, L, h->ad.active, h->stream);

@@ -118,13 +118,14 @@ constexpr int kMaxLevels = 21;
 constexpr int kMaxDevices = 64;
 size_t tree_lookback_words(int cap);
 // min_split: nodes above this level split even when small (ensembles use kSystemLevels)
+// quad = false: second moments left zero (walks without quadrupoles)
 void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
                        int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s,
-                       int min_split = 0);
+                       int min_split = 0, bool quad = true);
 
 // Keep the topology, recompute every node's tight box and moments from the current pos4
 // (particles drifted inside their nodes: adaptive substeps).
-void launch_tree_refit(const float4* pos4, TreeArrays& t, cudaStream_t s);
+void launch_tree_refit(const float4* pos4, TreeArrays& t, cudaStream_t s, bool quad = true);
 
 // Reference-mode topology: the single leaf the reference builds for its own keys.
 void launch_reference_leaf(const float* x, const float* y, const float* z, const float* m,

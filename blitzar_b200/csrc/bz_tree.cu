@@ -240,6 +240,8 @@ __global__ void k_tree_finish_last(TreeArrays t, int max_level)
     }
 }
 
+// QUAD = false (monopole walks): the second moments are left zero, without their pass.
+template <bool QUAD>
 __device__ void leaf_moments(const float4* __restrict__ pos4, int k, TreeArrays& t)
 {
     const int s = t.start[k], e = s + t.count[k];
@@ -263,7 +265,7 @@ __device__ void leaf_moments(const float4* __restrict__ pos4, int k, TreeArrays&
     const double cy = tm > 0.0 ? sy / tm : 0.5 * ((double)mn[1] + (double)mx[1]);
     const double cz = tm > 0.0 ? sz / tm : 0.5 * ((double)mn[2] + (double)mx[2]);
     double q[6] = {0, 0, 0, 0, 0, 0};
-    for (int i = s; i < e; ++i) {
+    for (int i = s; QUAD && i < e; ++i) {
         const float4 p = pos4[i];
         const double dx = (double)p.x - cx, dy = (double)p.y - cy, dz = (double)p.z - cz;
         const double w = (double)p.w;
@@ -290,6 +292,7 @@ __device__ void leaf_moments(const float4* __restrict__ pos4, int k, TreeArrays&
     t.quadB[k] = make_float2((float)q[4], (float)q[5]);
 }
 
+template <bool QUAD>
 __device__ void internal_moments(int k, TreeArrays& t)
 {
     const int c0 = t.child[k], nc = t.nchild[k];
@@ -323,7 +326,7 @@ __device__ void internal_moments(int k, TreeArrays& t)
     double q[6] = {0, 0, 0, 0, 0, 0};
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
-        if (j < nc) {
+        if (QUAD && j < nc) {
             const int c = c0 + j;
             const double dx = __ldcg(&t.c64[3 * c]) - cx;
             const double dy = __ldcg(&t.c64[3 * c + 1]) - cy;
@@ -355,6 +358,7 @@ __device__ void internal_moments(int k, TreeArrays& t)
 
 // One thread per leaf computes its moments, then climbs: the child that arrives last at a
 // parent (atomic counter) computes the parent from all children in octant order.
+template <bool QUAD>
 __global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restrict__ pos4,
                                                             TreeArrays t)
 {
@@ -362,7 +366,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restr
     for (int k = blockIdx.x * kThreads + threadIdx.x; k < nn; k += gridDim.x * kThreads) {
         if (t.nchild[k] != 0)
             continue;
-        leaf_moments(pos4, k, t);
+        leaf_moments<QUAD>(pos4, k, t);
         int node = k;
         for (;;) {
             const int p = t.parent[node];
@@ -373,7 +377,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restr
             if (old != t.nchild[p] - 1)
                 break;
             __threadfence();
-            internal_moments(p, t);
+            internal_moments<QUAD>(p, t);
             node = p;
         }
     }
@@ -381,7 +385,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restr
 
 } // namespace
 
-void launch_tree_refit(const float4* pos4, TreeArrays& t, cudaStream_t s)
+void launch_tree_refit(const float4* pos4, TreeArrays& t, cudaStream_t s, bool quad)
 {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -391,14 +395,17 @@ void launch_tree_refit(const float4* pos4, TreeArrays& t, cudaStream_t s)
     if (mb > 16LL * sms)
         mb = 16LL * sms;
     count_launch();
-    k_tree_moments<<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+    if (quad)
+        k_tree_moments<true><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+    else
+        k_tree_moments<false><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
 }
 
 size_t tree_lookback_words(int cap) { return static_cast<size_t>(cap) / kLookbackNodes + 2 * kMaxLevels + 8; }
 
 void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4, int n,
                        int leaf_cap, int max_level, TreeArrays& t, int* err, cudaStream_t s,
-                       int min_split)
+                       int min_split, bool quad)
 {
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
@@ -432,7 +439,10 @@ void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4
     if (mb > 16LL * sms)
         mb = 16LL * sms;
     count_launch();
-    k_tree_moments<<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+    if (quad)
+        k_tree_moments<true><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+    else
+        k_tree_moments<false><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
 }
 
 } // namespace bz

@@ -209,3 +209,26 @@ def test_walk_block_cap_does_not_change_results(gpu):
                 assert np.abs(a - out[0]).max() < 1e-5 * scale
             else:
                 assert np.array_equal(a, out[0])
+
+
+def test_node_cap_walk_needs_no_multipoles(gpu):
+    """With the node-size cap no node is accepted inside the cutoff on a near-uniform box, so the
+    monopole walk (which also skips the tree's second moments) gives the quadrupole walk's
+    forces; only the mesh's float reductions may order differently."""
+    n = 32 ** 3
+    rng = np.random.default_rng(44)
+    g = (np.indices((32, 32, 32)).reshape(3, -1).T + 0.5) / 32.0
+    pos = (g + 0.2 / 32 * rng.standard_normal(g.shape)) % 1.0
+    m = np.full(n, 1.0 / n, np.float32)
+    out = []
+    for order in (2, 1):
+        with _engine(n, solver=1, box_length=1.0, treepm_grid_size=64, treepm_assignment=2,
+                     treepm_gradient=1, treepm_window_floor=0.0, treepm_r_cut_factor=5.0,
+                     treepm_node_size_factor=0.5, octree_softening=0.02 / 32,
+                     multipole_order=order) as e:
+            e.set_state(pos, None, m, f64=True)
+            out.append(e.accelerations().astype(np.float64))
+            pp, pn = e.interaction_counts()
+            assert pn == 0 and pp > 0
+    scale = np.linalg.norm(out[0], axis=1).max()
+    assert np.abs(out[1] - out[0]).max() < 1e-6 * scale
