@@ -173,7 +173,8 @@ bz_status bz_get_state(bz_handle* h, float* pos_soa3, float* vel_soa3);
 bz_status bz_get_state_f64(bz_handle* h, double* pos_soa3, double* vel_soa3);
 
 /* Leapfrog (kick-drift-kick) state with its accelerations, for hosts that keep the state in
- * their own memory between steps.  bz_get_state_acc returns positions, velocities (may be
+ * their own memory between steps (no counterpart in the reference, whose state stays on its
+ * device between ParticleSystem::update calls).  bz_get_state_acc returns positions, velocities (may be
  * NULL) and the accelerations of those positions (SoA 3n floats each, caller order; computed
  * first if the handle has none).  bz_set_state_acc uploads a state together with its
  * accelerations, which must be the forces at these positions (as bz_get_state_acc or
