@@ -191,6 +191,7 @@ WalkParams walk_params(const bz_handle* h, bool want_pot)
     p.min_dist2 = h->cfg.physics_min_distance2;
     p.quadrupole = h->cfg.multipole_order >= 2 ? 1 : 0;
     p.want_pot = want_pot ? 1 : 0;
+    p.max_acc = h->cfg.physics_max_acceleration;
     if (h->cfg.solver == BZ_SOLVER_TREEPM) {
         const float rs = rsplit_len(h);
         const float rc = h->cfg.treepm_r_cut_factor * rs;
@@ -282,6 +283,8 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
     WalkParams wp = walk_params(h, want_pot);
     wp.active = h->walk_active;
     wp.blocks_per_sm = h->walk_blocks_per_sm;
+    // the mesh force computed in line is already in d.acc: the walk clamps the sum
+    wp.clamp_total = h->cfg.solver == BZ_SOLVER_TREEPM && h->pm && !overlap ? 1 : 0;
     const bool learned = h->learn.enabled && h->learn.trained && h->cfg.solver == BZ_SOLVER_TREEPM;
     if (learned) {
         o.pair_src = h->learn.pair_src;
@@ -296,7 +299,8 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
     if (overlap) {
         cudaStreamWaitEvent(h->stream, h->ev_join, 0);
         if (!add_in_kick)
-            launch_add3(d.acc[0], d.acc[1], d.acc[2], d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], n, h->stream);
+            launch_add3(d.acc[0], d.acc[1], d.acc[2], d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], n,
+                        h->cfg.physics_max_acceleration, h->stream);
     }
     if (learned) {
         const float hcell = static_cast<float>(h->cfg.box_length / h->cfg.treepm_grid_size);
@@ -309,7 +313,7 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
         double* const* s = d.st[h->cur];
         if (add_in_kick)
             launch_kick(s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt + 1, h->stream,
-                        d.acc_pm[0], d.acc_pm[1], d.acc_pm[2]);
+                        d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], h->cfg.physics_max_acceleration);
         else
             launch_kick(s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt + 1, h->stream);
     }
@@ -508,7 +512,7 @@ bz_status bz_config_init(bz_config* c)
     c->linear_octree_leaf_capacity = 256;
     c->leaf_capacity = 16;
     c->multipole_order = 2;
-    c->physics_max_acceleration = 1e30f;
+    c->physics_max_acceleration = 64.0f;  // kPhysicsMaxAccelerationDefault (FndConstants.hpp:21)
     c->physics_min_softening = 0.0f;
     c->physics_min_distance2 = 1.0e-12f;
     c->physics_min_theta = 0.05f;
@@ -595,7 +599,10 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
             return BZ_INVALID_ARGUMENT;
         }
     }
+    // physics_max_acceleration: the reference's validator rejects values <= 0
+    // (engine/config/validation/physics/CfgPhysics.cpp:20-24)
     if (cfg->leaf_capacity < 1 || cfg->octree_theta <= 0.0f || cfg->walk_group_size < 1 ||
+        !(cfg->physics_max_acceleration > 0.0f) ||
         cfg->walk_group_size > kGroupMax || cfg->adaptive_max_level < 0 || cfg->adaptive_max_level > 12 ||
         (cfg->adaptive_max_level > 0 && (cfg->solver != BZ_SOLVER_OCTREE || !(cfg->adaptive_eta > 0.0f)))) {
         delete h;

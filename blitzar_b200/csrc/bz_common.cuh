@@ -42,6 +42,19 @@ __device__ __forceinline__ int warp_incl_scan(int v)
     return v;
 }
 
+// The acceleration clamp of the reference (clampAcceleration, engine/physics/core/cuda/
+// prelude/CudForceKernels.inl:7-14): a vector longer than max_acc is scaled to that length.
+__device__ __forceinline__ void clamp_acceleration(float& x, float& y, float& z, float max_acc)
+{
+    const float norm = sqrtf(x * x + y * y + z * z);
+    if (norm > max_acc && norm > 1e-12f) {
+        const float s = max_acc / norm;
+        x *= s;
+        y *= s;
+        z *= s;
+    }
+}
+
 // Ordered-integer images of doubles so that atomicMin/atomicMax on unsigned long long give
 // the IEEE order (used for the FP64 bounding box).
 __device__ __forceinline__ unsigned long long ordered_from_double(double d)

@@ -146,6 +146,8 @@ struct WalkParams {
     const unsigned char* active;  // optional [n]: walk only groups with an active target
     int blocks_per_sm;            // > 0: at most this many resident walk blocks per SM (room
                                   // for kernels of a concurrent stream); 0 = as many as fit
+    float max_acc;                // acceleration clamp of the walk's sum (and of the total)
+    int clamp_total;              // the output already holds the mesh force: clamp the sum
 };
 // ---------------------------------------------------------------- target groups (bz_groups.cu)
 constexpr int kGroupMax = 32;  // largest walk group (one warp)
@@ -214,10 +216,11 @@ const float4* pm_force_mesh(PmPlan* p);  // interleaved {ax, ay, az, 0}
 void launch_permute(const uint32_t* perm, int n, const double* const* src, double* const* dst,
                     int ndouble, const float* msrc, float* mdst, const int* idsrc, int* iddst,
                     float4* pos4, double periodic_len, cudaStream_t s);
-// Closing half kick; with b (may be NULL) the accelerations are first completed, a += b.
+// Closing half kick; with b (may be NULL) the accelerations are first completed,
+// a = clamp(a + b, max_acc).
 void launch_kick(double* vx, double* vy, double* vz, float* ax, float* ay, float* az, int n,
                  const double* dt_half, cudaStream_t s, const float* bx = nullptr,
-                 const float* by = nullptr, const float* bz = nullptr);
+                 const float* by = nullptr, const float* bz = nullptr, float max_acc = 0.0f);
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
                        const float* ax, const float* ay, const float* az, int n,
                        const double* dt, double periodic_len, BoxF64* box, cudaStream_t s,
@@ -230,12 +233,12 @@ void launch_energy(const double* vx, const double* vy, const double* vz, const f
 void launch_scatter3(const float* ax, const float* ay, const float* az, const int* id, int n,
                      float* out_soa3, cudaStream_t s);
 void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s);
-// a += b, three components
 // pos4[i] = {x, y, z, m} in FP32 from the FP64 state (same order)
 void launch_refresh_pos4(const double* x, const double* y, const double* z, const float* m, int n,
                          float4* pos4, cudaStream_t s);
+// a = clamp(a + b, max_acc), three components (the reference's clamp of the TreePM sum)
 void launch_add3(float* ax, float* ay, float* az, const float* bx, const float* by, const float* bz,
-                 int n, cudaStream_t s);
+                 int n, float max_acc, cudaStream_t s);
 
 // ---------------------------------------------------------------- adaptive steps (bz_adaptive.cu)
 struct AdaptiveParams {

@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kThreads) k_permute(const uint32_t* __restrict
 }
 
 // Closing half kick.  With (bx, by, bz) (the mesh leg's accelerations from the second stream)
-// the accelerations are first completed in place, a += b, as k_add3 would.
+// the accelerations are first completed in place, a = clamp(a + b), as k_add3 would.
 __global__ void __launch_bounds__(kThreads) k_kick(double* __restrict__ vx, double* __restrict__ vy,
                                                     double* __restrict__ vz,
                                                     float* __restrict__ ax,
@@ -65,7 +65,7 @@ __global__ void __launch_bounds__(kThreads) k_kick(double* __restrict__ vx, doub
                                                     const double* __restrict__ dt_half,
                                                     const float* __restrict__ bx,
                                                     const float* __restrict__ by,
-                                                    const float* __restrict__ bz)
+                                                    const float* __restrict__ bz, float max_acc)
 {
     const double h = *dt_half;
     for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
@@ -74,6 +74,7 @@ __global__ void __launch_bounds__(kThreads) k_kick(double* __restrict__ vx, doub
             a[0] += bx[i];
             a[1] += by[i];
             a[2] += bz[i];
+            clamp_acceleration(a[0], a[1], a[2], max_acc);
             ax[i] = a[0];
             ay[i] = a[1];
             az[i] = a[2];
@@ -195,10 +196,11 @@ void launch_permute(const uint32_t* perm, int n, const double* const* src, doubl
 
 void launch_kick(double* vx, double* vy, double* vz, float* ax, float* ay, float* az, int n,
                  const double* dt_half, cudaStream_t s, const float* bx, const float* by,
-                 const float* bz)
+                 const float* bz, float max_acc)
 {
     count_launch();
-    k_kick<<<grid_for(n), kThreads, 0, s>>>(vx, vy, vz, ax, ay, az, n, dt_half, bx, by, bz);
+    k_kick<<<grid_for(n), kThreads, 0, s>>>(vx, vy, vz, ax, ay, az, n, dt_half, bx, by, bz,
+                                            max_acc);
 }
 
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
@@ -226,12 +228,15 @@ namespace {
 __global__ void __launch_bounds__(kThreads) k_add3(float* __restrict__ ax, float* __restrict__ ay,
                                                    float* __restrict__ az, const float* __restrict__ bx,
                                                    const float* __restrict__ by,
-                                                   const float* __restrict__ bz, int n)
+                                                   const float* __restrict__ bz, int n,
+                                                   float max_acc)
 {
     for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
-        ax[i] += bx[i];
-        ay[i] += by[i];
-        az[i] += bz[i];
+        float x = ax[i] + bx[i], y = ay[i] + by[i], z = az[i] + bz[i];
+        clamp_acceleration(x, y, z, max_acc);
+        ax[i] = x;
+        ay[i] = y;
+        az[i] = z;
     }
 }
 } // namespace
@@ -257,10 +262,10 @@ void launch_refresh_pos4(const double* x, const double* y, const double* z, cons
 }
 
 void launch_add3(float* ax, float* ay, float* az, const float* bx, const float* by, const float* bz,
-                 int n, cudaStream_t s)
+                 int n, float max_acc, cudaStream_t s)
 {
     count_launch();
-    k_add3<<<grid_for(n), kThreads, 0, s>>>(ax, ay, az, bx, by, bz, n);
+    k_add3<<<grid_for(n), kThreads, 0, s>>>(ax, ay, az, bx, by, bz, n, max_acc);
 }
 
 void launch_f64_to_f32(const double* src, float* dst, int n, cudaStream_t s)

@@ -816,9 +816,18 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                                                    ti, acc, phase, err, o, valid ? ti : -1, npair);
         }
         if (valid) {
-            o.ax[ti] += acc.total(0);
-            o.ay[ti] += acc.total(1);
-            o.az[ti] += acc.total(2);
+            // the walk's sum is clamped, and so is its sum with a mesh force already in the
+            // output (treePmComputeAcceleration, TpmTreeForce.inl:9-25; OctGpu.inl:227)
+            float fx = acc.total(0), fy = acc.total(1), fz = acc.total(2);
+            clamp_acceleration(fx, fy, fz, p.max_acc);
+            fx += o.ax[ti];
+            fy += o.ay[ti];
+            fz += o.az[ti];
+            if (p.clamp_total)
+                clamp_acceleration(fx, fy, fz, p.max_acc);
+            o.ax[ti] = fx;
+            o.ay[ti] = fy;
+            o.az[ti] = fz;
             if (POT && o.pot)
                 o.pot[ti] += acc.total(3);
             if (o.pair_cnt) {

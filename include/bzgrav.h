@@ -58,7 +58,10 @@ typedef struct bz_config {
     int32_t linear_octree_leaf_capacity; /* reference-mode leaf rule (default 256) */
     int32_t leaf_capacity;         /* production adaptive octree: particles per leaf */
     int32_t multipole_order;       /* 1 monopole, 2 monopole + quadrupole */
-    float physics_max_acceleration;/* physics_max_acceleration (clamp; 1e30 disables) */
+    float physics_max_acceleration;/* physics_max_acceleration: every particle's acceleration is
+                                      clamped to this length, the walk's sum first and then its
+                                      sum with the mesh force (reference default 64; must be
+                                      > 0; 1e30 leaves physical forces unclamped) */
     float physics_min_softening;   /* physics_min_softening */
     float physics_min_distance2;   /* physics_min_distance2 */
     float physics_min_theta;       /* physics_min_theta */
@@ -85,7 +88,7 @@ typedef struct bz_config {
 typedef struct bz_handle bz_handle;
 
 /* Default configuration (reference defaults: theta 0.5, softening 0.01, leaf capacity 256,
- * TreePM grid 128, split 1.25 cells, cutoff 4.5 r_s, quadrupole on). */
+ * max acceleration 64, TreePM grid 128, split 1.25 cells, cutoff 4.5 r_s, quadrupole on). */
 bz_status bz_config_init(bz_config* cfg);
 
 /* Create an engine for up to `capacity` particles.  Replaces ParticleSystem construction +

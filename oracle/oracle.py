@@ -32,9 +32,25 @@ class WalkParams(C.Structure):
                 ("quadrupole", C.c_int), ("group", C.c_int), ("max_node_size", C.c_float)]
 
 
+def reference_dir() -> str | None:
+    """Root of a BLITZAR checkout to compile the reference shim from: $BZ_REFERENCE_DIR, else a
+    checkout named ``reference`` beside this repository; None when neither exists."""
+    env = os.environ.get("BZ_REFERENCE_DIR")
+    cand = env if env else os.path.join(os.path.dirname(HERE), os.pardir, "reference")
+    cand = os.path.abspath(cand)
+    return cand if os.path.isdir(os.path.join(cand, "engine")) else None
+
+
 def build(ref: bool = False) -> None:
-    """Compile the restatement (and, with ref=True, the reference shim) in place."""
-    target = ["all", "ref"] if ref else ["all"]
+    """Compile the restatement (and, with ref=True, the reference shim from reference_dir())
+    in place."""
+    target = ["all"]
+    if ref:
+        root = reference_dir()
+        if root is None:
+            raise RuntimeError("reference shim requested but no BLITZAR checkout was found: "
+                               "set BZ_REFERENCE_DIR to its root")
+        target += ["ref", f"REF={root}"]
     subprocess.run(["make", "-s", "-C", HERE] + target, check=True)
 
 
@@ -310,6 +326,18 @@ def fft3d(cube_complex, inverse=False):
     lib().or_fft3d(a, cube_complex.shape[0], 1 if inverse else 0)
     a = a.reshape(-1, 2)
     return (a[:, 0] + 1j * a[:, 1]).reshape(cube_complex.shape)
+
+
+def clamp_acceleration(acc, max_acc):
+    """The reference's acceleration clamp (clampAcceleration, engine/physics/core/cuda/prelude/
+    CudForceKernels.inl:7-14) on an (n, 3) array: FP32 norm, vectors longer than max_acc
+    scaled to that length."""
+    a = np.asarray(acc, np.float32)
+    norm = np.sqrt((a * a).sum(axis=1, dtype=np.float32)).astype(np.float32)
+    m = np.float32(max_acc)
+    scale = np.where((norm > m) & (norm > np.float32(1e-12)), m / np.maximum(norm, np.float32(1e-30)),
+                     np.float32(1.0)).astype(np.float32)
+    return (np.asarray(acc, np.float64) * scale[:, None]).astype(np.float64)
 
 
 def split_weight(s, rsplit):

@@ -23,7 +23,7 @@ def test_ensemble_forces_are_per_system(gpu, oracle):
 
     systems = _systems([1500, 40, 7000, 1, 3200, 33], seed=3)
     n = sum(len(m) for _, _, m in systems)
-    with Engine(n, octree_theta=0.4, octree_softening=0.01) as e:
+    with Engine(n, octree_theta=0.4, octree_softening=0.01, physics_max_acceleration=1e30) as e:
         offs = e.set_ensemble(systems)
         acc = e.accelerations().astype(np.float64)
         errs = e.force_errors(nsample=min(2000, n), seed=4)
@@ -46,14 +46,15 @@ def test_ensemble_steps_like_separate_runs(gpu):
 
     systems = _systems([3000, 800, 5000], seed=9)
     n = sum(len(m) for _, _, m in systems)
-    with Engine(n, octree_theta=0.3, octree_softening=0.01) as e:
+    with Engine(n, octree_theta=0.3, octree_softening=0.01, physics_max_acceleration=1e30) as e:
         offs = e.set_ensemble(systems)
         e.step(1e-3, 20)
         pe, ve = e.get_state(f64=True)
         k, w, _ = e.energy()
     ke_sum = w_sum = 0.0
     for i, (p, v, m) in enumerate(systems):
-        with Engine(len(m), octree_theta=0.3, octree_softening=0.01) as s:
+        with Engine(len(m), octree_theta=0.3, octree_softening=0.01,
+                    physics_max_acceleration=1e30) as s:
             s.set_state(p, v, m, f64=True)
             k0, w0, _ = s.energy()
             s.step(1e-3, 20)

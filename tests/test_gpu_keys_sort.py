@@ -10,6 +10,7 @@ pytestmark = pytest.mark.gpu
 
 def _engine(n, **kw):
     from blitzar_b200._lib import Engine
+    kw.setdefault("physics_max_acceleration", 1e30)  # parity with the unclamped oracle
     return Engine(n, **kw)
 
 

@@ -30,7 +30,7 @@ def _inputs(n, seed):
 
 def _engine(n=4096, **kw):
     from blitzar_b200._lib import Engine
-
+    kw.setdefault("physics_max_acceleration", 1e30)  # parity with the unclamped oracle
     cfg = dict(solver=1, box_length=1.0, treepm_grid_size=32, treepm_assignment=2, treepm_gradient=1,
                treepm_window_floor=0.0, octree_softening=1e-3)
     cfg.update(kw)
@@ -79,7 +79,8 @@ def test_learned_correction_reduces_mesh_error(gpu):
     pos, _, m = ics.grf_grid(ns, seed=2, rms_cells=0.2)
     cfg = dict(solver=1, box_length=1.0, treepm_grid_size=mesh, treepm_r_split_cells=0.8,
                treepm_r_cut_factor=5.0, treepm_assignment=2, treepm_gradient=1,
-               treepm_window_floor=0.0, treepm_node_size_factor=0.5, octree_softening=0.02 / ns)
+               treepm_window_floor=0.0, treepm_node_size_factor=0.5, octree_softening=0.02 / ns,
+               physics_max_acceleration=1e30)
     with Engine(len(m), **cfg) as e:
         e.set_state(pos, None, m.astype(np.float32), f64=True)
         plain = e.force_errors(nsample=1024, seed=3)

@@ -10,6 +10,7 @@ pytestmark = pytest.mark.gpu
 
 def _engine(n, **kw):
     from blitzar_b200._lib import Engine
+    kw.setdefault("physics_max_acceleration", 1e30)  # parity with the unclamped oracle
     return Engine(n, **kw)
 
 
@@ -139,7 +140,8 @@ def test_headless_driver_matches_engine(gpu, tmp_path):
     assert r.returncode == 0, r.stderr
     assert "[headless] done steps=10" in r.stdout
     p_h, v_h, m_h, _ = snapshot.read_bin(tmp_path / "out.bin")
-    with _engine(n, octree_theta=0.6, octree_softening=0.02) as e:
+    # the headless run keeps the reference's default clamp (64); so does this handle
+    with _engine(n, octree_theta=0.6, octree_softening=0.02, physics_max_acceleration=64.0) as e:
         e.set_state(pos, vel, m)
         e.step(1e-3, 10)
         p_e, v_e = e.get_state()

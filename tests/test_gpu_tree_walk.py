@@ -10,6 +10,7 @@ pytestmark = pytest.mark.gpu
 
 def _engine(n, **kw):
     from blitzar_b200._lib import Engine
+    kw.setdefault("physics_max_acceleration", 1e30)  # parity with the unclamped oracle
     return Engine(n, **kw)
 
 
@@ -85,6 +86,33 @@ def test_walk_matches_oracle_open(gpu, oracle, quad, theta):
     sizes = w["group_sizes"]
     assert npp == int((w["n_pp"] * sizes).sum())
     assert npn == int((w["n_pn"] * sizes).sum())
+
+
+def test_acceleration_clamp_matches_reference_rule(gpu, oracle):
+    """physics_max_acceleration (reference default 64) clamps every particle's walk sum, as
+    clampAcceleration does at the end of the reference walk (OctGpu.inl:227).  Close pairs
+    planted in a Plummer sphere exceed the limit; the clamped forces equal the oracle's walk
+    passed through the reference's clamp rule, and unclamped particles are untouched."""
+    n = 20_000
+    pos = plummer(n, seed=31)
+    rng = np.random.default_rng(32)
+    pick = rng.choice(n, 40, replace=False)
+    pos[pick[20:]] = pos[pick[:20]] + np.float32(2e-4) * rng.standard_normal((20, 3)).astype(np.float32)
+    m = np.full(n, 1.0 / n, np.float32)
+    eps = 1e-4
+    with _engine(n, octree_theta=0.5, octree_softening=eps, physics_max_acceleration=64.0) as e:
+        e.set_state(pos, None, m)
+        acc = e.accelerations().astype(np.float64)
+    sk, sp4, perm = _sorted_inputs(oracle, pos, m)
+    o = oracle.build_tree(sk, sp4, leaf_cap=16)
+    w = oracle.walk(sp4, o, theta=0.5, eps=eps, quadrupole=True)
+    raw = np.empty_like(w["acc"])
+    raw[perm] = w["acc"]
+    assert (np.linalg.norm(raw, axis=1) > 64.0).sum() >= 10  # the planted pairs exceed the limit
+    ref = oracle.clamp_acceleration(raw, 64.0)
+    err = _rel(acc, ref)
+    assert err.max() < 1e-5, err.max()
+    assert np.linalg.norm(acc, axis=1).max() <= 64.0 * (1 + 1e-6)
 
 
 def test_walk_accuracy_vs_fp64_direct(gpu, oracle):

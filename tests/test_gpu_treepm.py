@@ -9,6 +9,7 @@ pytestmark = pytest.mark.gpu
 
 def _engine(n, **kw):
     from blitzar_b200._lib import Engine
+    kw.setdefault("physics_max_acceleration", 1e30)  # parity with the unclamped oracle
     return Engine(n, **kw)
 
 
@@ -82,6 +83,44 @@ def test_treepm_forces_match_oracle(gpu, oracle, variant):
     ref = apm + asr
     err = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
     assert np.median(err) < 1e-5 and err.max() < 1e-3, (np.median(err), err.max())
+
+
+@pytest.mark.parametrize("schedule", [0, 2])
+def test_treepm_acceleration_clamp(gpu, oracle, schedule):
+    """TreePM with the reference's default clamp (64): the walk's sum is clamped, then its sum
+    with the mesh force (treePmComputeAcceleration, TpmTreeForce.inl:9-25), whether the mesh
+    force is computed in line (schedule 0: the walk clamps the total) or concurrently (schedule
+    2: the sum is completed and clamped after the join)."""
+    n, mesh = 16_384, 32
+    pos = _box_particles(n, 33)
+    rng = np.random.default_rng(34)
+    pick = rng.choice(n, 40, replace=False)
+    pos[pick[20:]] = (pos[pick[:20]] + np.float32(2e-4) * rng.standard_normal((20, 3)).astype(np.float32)) % 1.0
+    m = np.full(n, 1.0 / n, np.float32)
+    rs = 1.25 / mesh
+    rc = 5.5 * rs
+    eps = 2e-4
+    with _engine(n, solver=1, box_length=1.0, treepm_grid_size=mesh, octree_softening=eps,
+                 treepm_r_cut_factor=5.5, treepm_assignment=2, treepm_gradient=1,
+                 treepm_window_floor=0.0, physics_max_acceleration=64.0) as e:
+        e.set_state(pos, None, m)
+        e.set_mesh_schedule(schedule)
+        acc = e.accelerations().astype(np.float64)
+    p4 = oracle.pos4(pos, m)
+    apm = oracle.pm_periodic(p4, mesh, 1.0, rs, assignment="pcs", spectral=True, window_floor=0.0)
+    keys = oracle.morton63(pos.astype(np.float64), [0, 0, 0], 1.0)
+    perm = oracle.stable_sort(keys)
+    t = oracle.build_tree(keys[perm], p4[perm], leaf_cap=16)
+    w = oracle.walk(p4[perm], t, theta=0.5, eps=eps, rcut=rc, box=1.0, rsplit=rs)
+    asr = np.empty_like(w["acc"])
+    asr[perm] = w["acc"]
+    assert (np.linalg.norm(asr, axis=1) > 64.0).sum() >= 10
+    ref = oracle.clamp_acceleration(apm + oracle.clamp_acceleration(asr, 64.0), 64.0)
+    clamped = np.linalg.norm(asr, axis=1) > 64.0
+    err = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    assert err[clamped].max() < 1e-5, err[clamped].max()
+    assert np.median(err) < 1e-5
+    assert np.linalg.norm(acc, axis=1).max() <= 64.0 * (1 + 1e-6)
 
 
 @pytest.mark.parametrize("variant", ["reference", "production"])
