@@ -76,7 +76,8 @@ def parse():
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="treepm128")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--error-sample", type=int, default=2048)
-    ap.add_argument("--cpu-sample", type=int, default=16384)
+    ap.add_argument("--cpu-budget", type=float, default=20.0,
+                    help="seconds of reference CPU work for the cpu_baseline object")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default leaf capacity, group size and mesh overlap")
@@ -231,61 +232,32 @@ def load_traffic(name):
 
 # --------------------------------------------------------------------------- CPU baseline
 
-def cpu_baseline(w, pos, mass, sample, seed=7):
-    """Reference CPU path on a bounded sample: returns (particle-steps/s, cores, kind, text)."""
+def cpu_reference_step(w, pos, mass, budget_s, seed=7, chunk=65536):
+    """One force evaluation of the reference's CPU code on the box's host cores, measured, not
+    modelled, as far as `budget_s` seconds allow.
+
+    TreePM: the reference's periodic PM templates (TpmAssignment/TpmField, FP32, CIC) over all
+    N particles, then its octree_cpu build over all N (Octree::build, serial in the reference),
+    then its cutoff/erfc-split walk (Octree::computeForceOn, OpenMP) over the targets in seeded
+    random chunks.  Octree: the build, then the walk over the targets.  Ensembles: build and
+    walk of whole clusters, one after another.  The PM and the build always run in full; only
+    walk chunks (or clusters) left when the budget runs out are extrapolated, by target (or
+    particle) count, and the result says so.  Returns a dict or None without the reference
+    library."""
     from oracle import oracle as O
 
     n = len(mass)
     rng = np.random.default_rng(seed)
-    targets = np.sort(rng.choice(n, size=min(sample, n), replace=False)).astype(np.int32)
-    p32 = pos.astype(np.float32)
-    x, y, z = [np.ascontiguousarray(p32[:, a]) for a in range(3)]
-    m = np.ascontiguousarray(mass, np.float32)
     R = O.ref() if O.ref_available() else None
-    if w["kind"] == "treepm":
-        M = w["mesh"]
-        rs = w["r_split_cells"] / M
-        rc = w["r_cut_factor"] * rs
-        eps = w["eps_lattice"] / w["n_side"]
-        if R is not None:
-            ax, ay, az = [np.zeros(n, np.float32) for _ in range(3)]
-            t0 = time.perf_counter()
-            R.ref_pm_periodic(x, y, z, m, n, M, 1.0, rs, 0, b"cic", ax, ay, az, None, None)
-            t_pm = time.perf_counter() - t0
-            bx, by, bz = [np.zeros(len(targets), np.float32) for _ in range(3)]
-            t0 = time.perf_counter()
-            R.ref_octree_cpu_accel(x, y, z, m, n, w["theta"], eps, 1e-12, 1e30, 0, rs, rc * rc,
-                                   targets.ctypes.data, len(targets), bx, by, bz)
-            t_tree = time.perf_counter() - t0
-            cores = int(R.ref_omp_threads())
-            kind = "reference"
-            text = (f"reference CPU TreePM pieces built from the reference sources: periodic PM "
-                    f"(templates TpmAssignment/TpmField, FP32, mesh {M}^3) over all {n} particles "
-                    f"+ octree_cpu build over all {n} and its cutoff/erfc-split walk for "
-                    f"{len(targets)} seeded targets, walk time scaled to N (open-boundary short "
-                    f"range: the reference has no periodic split)")
-        else:
-            p4 = O.pos4(p32, m)
-            t0 = time.perf_counter()
-            O.pm_periodic(p4, M, 1.0, rs)
-            t_pm = time.perf_counter() - t0
-            t0 = time.perf_counter()
-            O.direct(p4, targets[:1024].astype(np.int64), eps=eps, box=1.0, rsplit=rs, rcut=rc)
-            t_tree = (time.perf_counter() - t0) * len(targets) / 1024
-            cores = os.cpu_count() or 1
-            kind = "port"
-            text = "oracle port: FP64 PM + FP64 direct short range on a target sample, scaled to N"
-        t_step = t_pm + t_tree * n / len(targets)
-    elif w["kind"] == "ensemble":
+    t_start = time.perf_counter()
+    pieces = {}
+    if w["kind"] == "ensemble":
         if R is None:
             return None
-        # the reference steps one system per process: time its octree_cpu (build + walk of
-        # every particle) on a few clusters spread in size and scale by particle count
         systems = make_ensemble(w, 0)
-        order = np.argsort([len(m) for _, _, m in systems])
-        pick = order[np.linspace(0, len(order) - 1, 5).astype(int)]
-        t_s, n_s = 0.0, 0
-        for i in pick:
+        order = rng.permutation(len(systems))
+        t_s, n_s, done = 0.0, 0, 0
+        for i in order:
             p, _, mm = systems[i]
             q = p.astype(np.float32)
             cx, cy, cz = [np.ascontiguousarray(q[:, a]) for a in range(3)]
@@ -293,56 +265,135 @@ def cpu_baseline(w, pos, mass, sample, seed=7):
             k = len(mm)
             bx, by, bz = [np.zeros(k, np.float32) for _ in range(3)]
             t0 = time.perf_counter()
-            R.ref_octree_cpu_accel(cx, cy, cz, mm, k, w["theta"], w["eps"], 1e-12, 1e30, 0, 0.0, 0.0,
-                                   None, 0, bx, by, bz)
+            R.ref_octree_cpu_accel(cx, cy, cz, mm, k, w["theta"], w["eps"], 1e-12, 1e30, 0, 0.0,
+                                   0.0, None, 0, bx, by, bz)
             t_s += time.perf_counter() - t0
             n_s += k
+            done += 1
+            if time.perf_counter() - t_start > budget_s:
+                break
         t_step = t_s * n / n_s
-        cores = int(R.ref_omp_threads())
-        kind = "reference"
-        text = (f"reference octree_cpu (build + walk of every particle) on {len(pick)} of "
-                f"{len(systems)} clusters ({n_s} particles, spread in size), scaled to all {n}")
+        pieces["clusters_s"] = t_s
+        text = (f"reference octree_cpu (build + walk of every particle of a cluster) on {done} of "
+                f"{len(systems)} clusters in seeded random order ({n_s} of {n} particles)")
+        extrapolated = n_s < n
+        cores, kind = int(R.ref_omp_threads()), "reference"
     else:
-        if R is None:
-            return None
-        ax, ay, az = [np.zeros(len(targets), np.float32) for _ in range(3)]
-        t0 = time.perf_counter()
-        R.ref_octree_cpu_accel(x, y, z, m, n, w["theta"], w["eps"], 1e-12, 1e30, 0, 0.0, 0.0,
-                               targets.ctypes.data, len(targets), ax, ay, az)
-        t_tree = time.perf_counter() - t0
-        t_step = t_tree * n / len(targets)
-        cores = int(R.ref_omp_threads())
-        kind = "reference"
-        text = f"reference octree_cpu build over all {n} + walk for {len(targets)} targets, scaled to N"
-    return n / t_step, cores, kind, text
+        p32 = pos.astype(np.float32)
+        x, y, z = [np.ascontiguousarray(p32[:, a]) for a in range(3)]
+        m = np.ascontiguousarray(mass, np.float32)
+        targets = rng.permutation(n).astype(np.int32)
+        treepm = w["kind"] == "treepm"
+        if treepm:
+            M = w["mesh"]
+            rs = w["r_split_cells"] / M
+            rc = w["r_cut_factor"] * rs
+            eps = w["eps_lattice"] / w["n_side"]
+            theta = w["theta"]
+        else:
+            rs = rc = 0.0
+            eps, theta = w["eps"], w["theta"]
+        if R is not None:
+            if treepm:
+                ax, ay, az = [np.zeros(n, np.float32) for _ in range(3)]
+                t0 = time.perf_counter()
+                R.ref_pm_periodic(x, y, z, m, n, M, 1.0, rs, 0, b"cic", ax, ay, az, None, None)
+                pieces["pm_s"] = time.perf_counter() - t0
+            t0 = time.perf_counter()
+            tree = R.ref_octree_cpu_build(x, y, z, m, n, theta, eps, 1e-12, 1e30, 0, rs, rc * rc)
+            pieces["build_s"] = time.perf_counter() - t0
+            t_walk, walked = 0.0, 0
+            try:
+                while walked < n:
+                    tg = np.ascontiguousarray(np.sort(targets[walked:walked + chunk]))
+                    bx, by, bz = [np.zeros(len(tg), np.float32) for _ in range(3)]
+                    t0 = time.perf_counter()
+                    R.ref_octree_cpu_walk(tree, tg.ctypes.data, len(tg), bx, by, bz)
+                    t_walk += time.perf_counter() - t0
+                    walked += len(tg)
+                    if time.perf_counter() - t_start > budget_s:
+                        break
+            finally:
+                R.ref_octree_cpu_free(tree)
+            pieces["walk_s"] = t_walk
+            pieces["walk_targets"] = walked
+            t_step = pieces.get("pm_s", 0.0) + pieces["build_s"] + t_walk * n / walked
+            cores, kind = int(R.ref_omp_threads()), "reference"
+            text = ("reference CPU code built from its sources: " +
+                    (f"periodic PM templates (TpmAssignment/TpmField, FP32 CIC, mesh {M}^3) over all "
+                     f"{n} particles, " if treepm else "") +
+                    f"octree_cpu build over all {n} (Octree::build) and its "
+                    + ("cutoff/erfc-split " if treepm else "") +
+                    f"walk (Octree::computeForceOn) for {walked} seeded targets"
+                    + (f", walk time scaled to all {n}" if walked < n else "")
+                    + (" (open-boundary short range: the reference has no periodic split)"
+                       if treepm else ""))
+        else:
+            p4 = O.pos4(p32, m)
+            if treepm:
+                t0 = time.perf_counter()
+                O.pm_periodic(p4, M, 1.0, rs)
+                pieces["pm_s"] = time.perf_counter() - t0
+            t_walk, walked = 0.0, 0
+            while walked < n:
+                tg = np.sort(targets[walked:walked + 1024]).astype(np.int64)
+                t0 = time.perf_counter()
+                O.direct(p4, tg, eps=eps, box=1.0 if treepm else 0.0, rsplit=rs, rcut=rc)
+                t_walk += time.perf_counter() - t0
+                walked += len(tg)
+                if time.perf_counter() - t_start > budget_s:
+                    break
+            pieces["direct_s"] = t_walk
+            pieces["direct_targets"] = walked
+            t_step = pieces.get("pm_s", 0.0) + t_walk * n / walked
+            cores, kind = os.cpu_count() or 1, "port"
+            text = (f"oracle port: " + ("FP64 PM over all particles + " if treepm else "") +
+                    f"FP64 direct sum for {walked} seeded targets"
+                    + (f", scaled to all {n}" if walked < n else ""))
+        extrapolated = pieces.get("walk_targets", pieces.get("direct_targets", n)) < n
+    return {"value": n / t_step, "unit": "particle-steps/s", "cores": cores, "kind": kind,
+            "sample": text, "step_s": t_step, "measured_s": time.perf_counter() - t_start,
+            "extrapolated": bool(extrapolated), "pieces": pieces}
 
 
 # --------------------------------------------------------------------------- arms
 
 def run_reference(args, w, rank, world):
+    """The reference's own CPU implementation of the path on this box's host cores: whole
+    force evaluations (cpu_reference_step) repeated while they fit in a few minutes; rank 0
+    only.  "steps" is the number actually timed; a step whose walk did not finish within the
+    budget is extrapolated and marked so."""
     if rank != 0:
         return 0
     pos, vel, mass = make_ics(w, 0)
     n = len(mass)
-    for _ in range(args.warmup if args.warmup < 1 else 1):
-        pass
-    vals = []
-    res = None
-    for _ in range(max(1, min(args.steps, 3))):
-        res = cpu_baseline(w, pos, mass, args.cpu_sample)
+    budget = float(os.environ.get("BZ_REFERENCE_BUDGET_S", "240"))
+    results = []
+    t0 = time.perf_counter()
+    while len(results) < max(1, args.steps):
+        res = cpu_reference_step(w, pos, mass, budget)
         if res is None:
-            print(json.dumps({"impl": "reference", "unavailable": "reference CPU library not built"}))
+            print(json.dumps({"impl": "reference", "unavailable": "reference CPU library not built "
+                              "(oracle/_ref/libbzref.so needs a BLITZAR checkout at build time)"}))
             return 0
-        vals.append(res[0])
-    value = float(np.median(vals))
+        results.append(res)
+        # another step only if it surely fits in the budget too
+        if res["extrapolated"] or (time.perf_counter() - t0) + res["measured_s"] > budget:
+            break
+    step_s = float(np.median([r["step_s"] for r in results]))
+    value = n / step_s
+    last = results[-1]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "particle-steps/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * n / value, "higher_is_better": True, "scaling": "weak",
+        "n_gpus": args.gpus, "steps": len(results), "steps_requested": args.steps, "warmup": 0,
+        "ms_per_step": 1e3 * step_s, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "extrapolated": any(r["extrapolated"] for r in results),
+        "measured_s": time.perf_counter() - t0,
         "config": config_dict(w, args, n),
-        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": res[1], "kind": res[2],
-                         "sample": res[3]},
+        "cpu_baseline": {"value": value, "unit": "particle-steps/s", "cores": last["cores"],
+                         "kind": last["kind"], "sample": last["sample"],
+                         "extrapolated": last["extrapolated"], "pieces": last["pieces"]},
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -492,22 +543,37 @@ def run_ours(args, w, rank, world, local):
     eng.enable_timing(True)
     eng.step(dt, 3)
     ph = eng.phase_times()
-    pp, pn = eng.interaction_counts()
+    listed, evaluated, nodes = eng.walk_counts()
     eng.enable_timing(False)
     split = w["kind"] == "treepm"
-    flops = pp * FLOP_PP[split] + pn * FLOP_PN[(split, True)]
+    # algorithmic flops: pairs that went through the pair law (inside the cutoff) and
+    # multipole terms; the distance tests of listed pairs outside the cutoff are not counted
+    flops = evaluated * FLOP_PP[split] + nodes * FLOP_PN[(split, True)]
     walk_ms = ph["walk"]
     achieved_tf = flops / (walk_ms * 1e-3) / 1e12 if walk_ms > 0 else 0.0
     peak_tf = SMS * FP32_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
-    traffic = load_traffic(f"walk_{args.workload}")
+    # DRAM traffic and issue utilisation come from an ncu capture committed under profiles/;
+    # they are quoted only when that capture used this run's walk settings
+    prof = load_traffic(f"walk_{args.workload}")
+    leaf_now = tuned["leaf_capacity"] if tuned else cfg.get("leaf_capacity", 16)
+    group_now = tuned["walk_group_size"] if tuned else 32
+    prof_ok = (prof is not None and prof.get("leaf_capacity") == leaf_now
+               and prof.get("walk_group_size") == group_now)
     roofline = {
         "kernel": "k_walk (group tree walk + pair/multipole arithmetic)",
         "bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
         "frac": achieved_tf / peak_tf,
-        "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak is provided. The walk is issue-bound (ncu_issue_active_pct of the warp-issue slots busy): its filter, traversal and list work are not counted as flops",
-        "traffic": None if traffic is None else traffic.get("dram_bytes_per_launch"),
-        "ncu_issue_active_pct": None if traffic is None else traffic.get("issue_active_pct"),
-        "interactions_per_launch": {"particle_particle": pp, "particle_node": pn},
+        "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak is provided",
+        "traffic": prof.get("dram_bytes_per_launch") if prof_ok else None,
+        "ncu_issue_active_pct": prof.get("issue_active_pct") if prof_ok else None,
+        "traffic_source": (f"profiles/walk_{args.workload}.json: one ncu capture at leaf "
+                           f"{prof.get('leaf_capacity')}, group {prof.get('walk_group_size')}"
+                           if prof_ok else
+                           "none: no committed ncu capture of this workload at this run's leaf "
+                           "capacity and group size"),
+        "interactions_per_launch": {"listed_pairs": listed, "evaluated_pairs": evaluated,
+                                    "particle_node": nodes},
+        "listed_per_evaluated": (listed / evaluated) if evaluated else None,
         "flops_per_interaction": {"pp": FLOP_PP[split], "pn": FLOP_PN[(split, True)]},
         "launch_ms": walk_ms,
     }
@@ -577,23 +643,24 @@ def run_ours(args, w, rank, world, local):
                "note": "each step uploads the full FP64 ensemble state, which forces a fresh force "
                        "evaluation before the leapfrog step (two evaluations per step)"}
     elif args.e2e_steps > 0:
-        # the host keeps the leapfrog state (positions, velocities, masses and the accelerations
-        # of the positions) in pinned memory and round-trips it through the C ABI every step
-        hp = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
-        hv = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
+        # the host keeps the FP64 leapfrog state (positions, velocities, masses and the FP32
+        # accelerations of the positions) in pinned memory and round-trips it through the C ABI
+        # every step
+        hp = torch.empty(3 * n, dtype=torch.float64, pin_memory=True).numpy()
+        hv = torch.empty(3 * n, dtype=torch.float64, pin_memory=True).numpy()
         ha = torch.empty(3 * n, dtype=torch.float32, pin_memory=True).numpy()
         hm = torch.empty(n, dtype=torch.float32, pin_memory=True).numpy()
         hm[:] = mass
-        eng.get_state_acc_soa(hp, hv, ha)
-        eng.set_state_acc_soa(hp, hv, hm, ha)
+        eng.get_state_acc_f64_soa(hp, hv, ha)
+        eng.set_state_acc_f64_soa(hp, hv, hm, ha)
         eng.step(dt, 1)
-        eng.get_state_acc_soa(hp, hv, ha)
+        eng.get_state_acc_f64_soa(hp, hv, ha)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            eng.set_state_acc_soa(hp, hv, hm, ha)
+            eng.set_state_acc_f64_soa(hp, hv, hm, ha)
             eng.step(dt, 1)
-            eng.get_state_acc_soa(hp, hv, ha)
+            eng.get_state_acc_f64_soa(hp, hv, ha)
         torch.cuda.synchronize()
         sec = time.perf_counter() - t0
         if dist:
@@ -601,22 +668,19 @@ def run_ours(args, w, rank, world, local):
             dist.all_reduce(t, op=dist.ReduceOp.MAX)
             sec = float(t.item())
         e2e = {"value": n * world * args.e2e_steps / sec, "unit": "particle-steps/s",
-               "h2d_bytes_per_step": 10 * 4 * n, "d2h_bytes_per_step": 9 * 4 * n,
-               "note": "each step uploads the FP32 leapfrog state with the accelerations of its "
-                       "positions (bz_set_state_acc), steps once (one force evaluation, as for a "
-                       "resident state) and downloads state and accelerations (bz_get_state_acc); "
-                       "wall clock over the steps"}
+               "h2d_bytes_per_step": (6 * 8 + 4 + 3 * 4) * n, "d2h_bytes_per_step": (6 * 8 + 3 * 4) * n,
+               "note": "each step uploads the FP64 leapfrog state with the FP32 accelerations of "
+                       "its positions (bz_set_state_acc_f64), steps once (one force evaluation, "
+                       "as for a resident state) and downloads state and accelerations "
+                       "(bz_get_state_acc_f64); wall clock over the steps"}
 
     learned = None
     if w["kind"] == "treepm" and not args.no_learned:
         learned = learned_comparison(w, pos, vel, mass, stream, local, dt, args.error_sample)
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
-        res = cpu_baseline(w, pos, mass, args.cpu_sample)
-        if res is not None:
-            cpu = {"value": res[0], "unit": "particle-steps/s", "cores": res[1], "kind": res[2],
-                   "sample": res[3]}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_reference_step(w, pos, mass, args.cpu_budget)
 
     line = {
         "metric": METRIC, "value": value, "unit": "particle-steps/s", "n_gpus": world,

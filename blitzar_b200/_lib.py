@@ -28,7 +28,8 @@ EXPORTS = (
     "bz_sort_pairs_noalloc", "bz_energy", "bz_autotune", "bz_learn_generate", "bz_learn_train",
     "bz_learn_set", "bz_learn_get", "bz_learn_enable", "bz_learn_forward", "bz_learn_gradient",
     "bz_set_ensemble", "bz_adaptive_levels", "bz_adaptive_updates", "bz_set_mesh_schedule",
-    "bz_walk_blocks_per_sm", "bz_set_state_acc", "bz_get_state_acc",
+    "bz_walk_blocks_per_sm", "bz_set_state_acc", "bz_get_state_acc", "bz_set_state_acc_f64",
+    "bz_get_state_acc_f64", "bz_walk_counts",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -97,6 +98,7 @@ def load():
     L.bz_tree_topology.argtypes = [_vp, C.POINTER(C.c_int64)] + [_vp] * 8
     L.bz_reference_tree.argtypes = [_vp, C.POINTER(C.c_int64)] + [_vp] * 6
     L.bz_interaction_counts.argtypes = [_vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+    L.bz_walk_counts.argtypes = [_vp] + [C.POINTER(C.c_uint64)] * 3
     L.bz_enable_phase_timing.argtypes = [_vp, C.c_int]
     L.bz_phase_times.argtypes = [_vp, _vp, C.c_int]
     L.bz_force_errors.argtypes = [_vp, C.c_int32, C.c_uint64, _vp, _vp, C.POINTER(C.c_double),
@@ -119,6 +121,8 @@ def load():
     L.bz_walk_blocks_per_sm.argtypes = [_vp, C.c_int32, _vp]
     L.bz_set_state_acc.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_size_t]
     L.bz_get_state_acc.argtypes = [_vp, _vp, _vp, _vp]
+    L.bz_set_state_acc_f64.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_size_t]
+    L.bz_get_state_acc_f64.argtypes = [_vp, _vp, _vp, _vp]
     L.bz_adaptive_levels.argtypes = [_vp, _vp]
     L.bz_adaptive_updates.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_set_ensemble.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_int32]
@@ -257,6 +261,18 @@ class Engine:
         self._check(self.L.bz_get_state_acc(self.h, _ptr(pos_soa3), _ptr(vel_soa3), _ptr(acc_soa3)),
                     "bz_get_state_acc")
 
+    def set_state_acc_f64_soa(self, pos_soa3, vel_soa3, mass, acc_soa3):
+        """As set_state_acc_soa with FP64 positions and velocities (accelerations FP32)."""
+        n = mass.shape[0]
+        self._check(self.L.bz_set_state_acc_f64(self.h, _ptr(pos_soa3), _ptr(vel_soa3), _ptr(mass),
+                                                _ptr(acc_soa3), n), "bz_set_state_acc_f64")
+        self.n = n
+
+    def get_state_acc_f64_soa(self, pos_soa3, vel_soa3, acc_soa3):
+        """FP64 positions and velocities with the FP32 accelerations of the positions (SoA)."""
+        self._check(self.L.bz_get_state_acc_f64(self.h, _ptr(pos_soa3), _ptr(vel_soa3),
+                                                _ptr(acc_soa3)), "bz_get_state_acc_f64")
+
     def get_state_soa(self, pos_soa3, vel_soa3):
         self._check(self.L.bz_get_state(self.h, _ptr(pos_soa3), _ptr(vel_soa3)), "bz_get_state")
 
@@ -386,6 +402,12 @@ class Engine:
         a, b = C.c_uint64(0), C.c_uint64(0)
         self._check(self.L.bz_interaction_counts(self.h, C.byref(a), C.byref(b)), "bz_interaction_counts")
         return a.value, b.value
+
+    def walk_counts(self):
+        """(listed pairs, pairs through the pair law, multipole terms) of the last walk."""
+        a, b, c = C.c_uint64(0), C.c_uint64(0), C.c_uint64(0)
+        self._check(self.L.bz_walk_counts(self.h, C.byref(a), C.byref(b), C.byref(c)), "bz_walk_counts")
+        return a.value, b.value, c.value
 
     def enable_timing(self, on=True):
         self._check(self.L.bz_enable_phase_timing(self.h, 1 if on else 0), "bz_enable_phase_timing")

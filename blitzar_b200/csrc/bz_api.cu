@@ -51,7 +51,7 @@ struct DeviceBuffers {
     double* energy = nullptr;  // energy/momentum reduction scratch + results
     unsigned* queue = nullptr;
     int* spill = nullptr;
-    unsigned long long* counters = nullptr;  // [2] pp, pn
+    unsigned long long* counters = nullptr;  // [3] listed pp, pn, evaluated pp
     float* stage = nullptr;                  // 10n floats for host transfers
     float* ref_xyzm = nullptr;               // 4n floats, caller order, reference mode
     float4* ref_orig = nullptr;              // n float4, caller order
@@ -97,7 +97,7 @@ struct bz_handle {
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graph_failed = false;
     double* h_dt = nullptr;  // pinned {dt, dt/2}
-    unsigned long long last_pp = 0, last_pn = 0;
+    unsigned long long last_pp = 0, last_pn = 0, last_eval = 0;
     bool ref_tree_valid = false;
     // adaptive block steps
     struct {
@@ -273,7 +273,7 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
     if (want_pot)
         cudaMemsetAsync(d.pot, 0, sizeof(float) * n, h->stream);
     record(h, kPhWalk);
-    cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), h->stream);
+    cudaMemsetAsync(d.counters, 0, 3 * sizeof(unsigned long long), h->stream);
     WalkOutputs o{};
     o.ax = d.acc[0];
     o.ay = d.acc[1];
@@ -396,10 +396,11 @@ void collect_timing(bz_handle* h)
 
 void read_counters(bz_handle* h)
 {
-    unsigned long long c[2] = {0, 0};
+    unsigned long long c[3] = {0, 0, 0};
     cudaMemcpy(c, h->d.counters, sizeof(c), cudaMemcpyDeviceToHost);
     h->last_pp = c[0];
     h->last_pn = c[1];
+    h->last_eval = c[2];
 }
 
 bz_status ensure_forces(bz_handle* h)
@@ -636,7 +637,7 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     ok = ok && dalloc(h, &d.pot, n) && dalloc(h, &d.keys, n) && dalloc(h, &d.perm, n) &&
          dalloc(h, &d.box, 1) && dalloc(h, &d.bbox32, 8) && dalloc(h, &d.err, 1) &&
          dalloc(h, &d.dt, 2) && dalloc(h, &d.energy, energy_scratch_doubles()) &&
-         dalloc(h, &d.queue, 1) && dalloc(h, &d.counters, 2) &&
+         dalloc(h, &d.queue, 1) && dalloc(h, &d.counters, 3) &&
          dalloc(h, &d.stage, 10 * n) && dalloc(h, &d.ref_xyzm, 4 * n) && dalloc(h, &d.ref_orig, n) &&
          dalloc(h, &d.ref_hot8, 8);
     // sort workspace
@@ -816,6 +817,60 @@ __global__ void k_gather_f64(const double* const* __restrict__ src_unused, const
     }
 }
 
+// Six FP64 arrays (x, y, z, vx, vy, vz) by value.
+struct Soa6 {
+    double* a[6];
+};
+
+// FP64 state into caller order, one output array per component (the alternate state buffers
+// serve as the staging area between steps: nothing reads them until the next permutation).
+__global__ void k_gather_f64_soa(const double* x, const double* y, const double* z,
+                                 const double* vx, const double* vy, const double* vz,
+                                 const int* __restrict__ id, int n, Soa6 out, int want_vel)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int o = id[i];
+        out.a[0][o] = x[i];
+        out.a[1][o] = y[i];
+        out.a[2][o] = z[i];
+        if (want_vel) {
+            out.a[3][o] = vx[i];
+            out.a[4][o] = vy[i];
+            out.a[5][o] = vz[i];
+        }
+    }
+}
+
+// As k_unpack_state_kept for an FP64 state staged in caller order in `in` (slot i takes caller
+// particle id[i]); masses and accelerations staged as FP32 in st (mass at 6n, acc at 7n).
+__global__ void k_unpack_state_kept_f64(Soa6 in, const float* __restrict__ st, int n, int have_vel,
+                                        double* x, double* y, double* z, double* vx, double* vy,
+                                        double* vz, float* m, const int* __restrict__ id,
+                                        double box, float* ax, float* ay, float* az)
+{
+    const float* acc = st + 7 * static_cast<size_t>(n);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int c = id[i];
+        double p[3] = {in.a[0][c], in.a[1][c], in.a[2][c]};
+        if (box > 0.0)
+            for (int a = 0; a < 3; ++a) {
+                p[a] -= box * floor(p[a] / box);
+                if (p[a] >= box)
+                    p[a] = 0.0;
+            }
+        x[i] = p[0];
+        y[i] = p[1];
+        z[i] = p[2];
+        vx[i] = have_vel ? in.a[3][c] : 0.0;
+        vy[i] = have_vel ? in.a[4][c] : 0.0;
+        vz[i] = have_vel ? in.a[5][c] : 0.0;
+        m[i] = st[6 * n + c];
+        ax[i] = acc[c];
+        ay[i] = acc[n + c];
+        az[i] = acc[2 * n + c];
+    }
+}
+
 // caller-order FP32 positions + mass (reference mode / key parity)
 __global__ void k_caller_xyzm(const double* x, const double* y, const double* z,
                               const float* m, const int* __restrict__ id, int n, float* xyzm,
@@ -885,6 +940,28 @@ void enqueue_reference_order(bz_handle* h)
 } // namespace
 
 extern "C" {
+
+// Downloads the FP64 state in caller order through the alternate state buffers.
+static void enqueue_get_f64(bz_handle* h, double* pos, double* vel)
+{
+    const size_t n = h->n;
+    DeviceBuffers& d = h->d;
+    double* const* s = d.st[h->cur];
+    double* const* alt = d.st[h->cur ^ 1];
+    Soa6 out;
+    for (int a = 0; a < 6; ++a)
+        out.a[a] = alt[a];
+    count_launch();
+    k_gather_f64_soa<<<blocks_for(n), 256, 0, h->stream>>>(s[0], s[1], s[2], s[3], s[4], s[5],
+                                                           d.id[h->cur], static_cast<int>(n), out,
+                                                           vel ? 1 : 0);
+    for (int a = 0; a < 3; ++a)
+        cudaMemcpyAsync(pos + a * n, alt[a], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (vel)
+        for (int a = 0; a < 3; ++a)
+            cudaMemcpyAsync(vel + a * n, alt[3 + a], n * sizeof(double), cudaMemcpyDeviceToHost,
+                            h->stream);
+}
 
 // Uploads and unpacks an FP32 state (caller order, buffer 0) on the handle's stream.
 static void enqueue_set_state(bz_handle* h, const float* pos, const float* vel, const float* mass,
@@ -1056,24 +1133,72 @@ bz_status bz_get_state_f64(bz_handle* h, double* pos, double* vel)
     if (!h || !pos || h->n == 0)
         return BZ_INVALID_ARGUMENT;
     cudaSetDevice(h->device);
+    enqueue_get_f64(h, pos, vel);
+    return check_device(h, "bz_get_state_f64");
+}
+
+bz_status bz_get_state_acc_f64(bz_handle* h, double* pos, double* vel, float* acc)
+{
+    if (!h || !pos || !acc || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    cudaSetDevice(h->device);
+    if (h->cfg.adaptive_max_level > 0)
+        return fail(h, BZ_UNSUPPORTED, "adaptive steps keep per-particle accelerations of their own");
+    bz_status st = ensure_forces(h);
+    if (st != BZ_OK)
+        return st;
     const size_t n = h->n;
     DeviceBuffers& d = h->d;
-    double* const* s = d.st[h->cur];
-    // reuse the alternate state buffers as a 6n-double staging area
-    double* tmp = nullptr;
-    if (!dalloc(h, &tmp, 6 * n))
-        return fail(h, BZ_OUT_OF_MEMORY, "bz_get_state_f64 staging");
-    count_launch();
-    k_gather_f64<<<blocks_for(n), 256, 0, h->stream>>>(nullptr, s[0], s[1], s[2], s[3], s[4], s[5],
-                                                       d.id[h->cur], static_cast<int>(n), tmp,
-                                                       vel ? 1 : 0);
-    cudaMemcpyAsync(pos, tmp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-    if (vel)
-        cudaMemcpyAsync(vel, tmp + 3 * n, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-    const bz_status st = check_device(h, "bz_get_state_f64");
-    cudaFree(tmp);
-    h->allocations.pop_back();
-    h->bytes -= 6 * n * sizeof(double);
+    launch_scatter3(d.acc[0], d.acc[1], d.acc[2], d.id[h->cur], static_cast<int>(n), d.stage + 6 * n,
+                    h->stream);
+    enqueue_get_f64(h, pos, vel);
+    cudaMemcpyAsync(acc, d.stage + 6 * n, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    return check_device(h, "bz_get_state_acc_f64");
+}
+
+bz_status bz_set_state_acc_f64(bz_handle* h, const double* pos, const double* vel, const float* mass,
+                               const float* acc, size_t n)
+{
+    if (!h || !pos || !mass || !acc || n == 0 || n > h->capacity)
+        return BZ_INVALID_ARGUMENT;
+    if (h->cfg.adaptive_max_level > 0)
+        return fail(h, BZ_UNSUPPORTED, "adaptive steps keep per-particle accelerations of their own");
+    cudaSetDevice(h->device);
+    DeviceBuffers& d = h->d;
+    if (h->n == n && h->systems == 0) {
+        // as bz_set_state_acc: a state of the same size keeps the device's particle order; the
+        // FP64 arrays are staged in caller order in the alternate state buffers
+        double* const* alt = d.st[h->cur ^ 1];
+        Soa6 in;
+        for (int a = 0; a < 3; ++a) {
+            in.a[a] = alt[a];
+            in.a[3 + a] = alt[3 + a];
+            cudaMemcpyAsync(alt[a], pos + a * n, n * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+            if (vel)
+                cudaMemcpyAsync(alt[3 + a], vel + a * n, n * sizeof(double), cudaMemcpyHostToDevice,
+                                h->stream);
+        }
+        cudaMemcpyAsync(d.stage + 6 * n, mass, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+        cudaMemcpyAsync(d.stage + 7 * n, acc, 3 * n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+        h->ad.ready = false;
+        h->ref_tree_valid = false;
+        double* const* s = d.st[h->cur];
+        count_launch();
+        k_unpack_state_kept_f64<<<blocks_for(n), 256, 0, h->stream>>>(
+            in, d.stage, static_cast<int>(n), vel ? 1 : 0, s[0], s[1], s[2], s[3], s[4], s[5],
+            d.mass[h->cur], d.id[h->cur], periodic(h) ? h->cfg.box_length : 0.0, d.acc[0], d.acc[1],
+            d.acc[2]);
+    } else {
+        const bz_status st0 = bz_set_state_f64(h, pos, vel, mass, n);
+        if (st0 != BZ_OK)
+            return st0;
+        // caller order now (buffer 0, identity ids): so are the accelerations
+        for (int a = 0; a < 3; ++a)
+            cudaMemcpyAsync(d.acc[a], acc + a * n, n * sizeof(float), cudaMemcpyHostToDevice, h->stream);
+    }
+    const bz_status st = check_device(h, "bz_set_state_acc_f64");
+    if (st == BZ_OK)
+        h->forces_valid = true;
     return st;
 }
 
@@ -1102,6 +1227,20 @@ bz_status bz_interaction_counts(bz_handle* h, uint64_t* n_pp, uint64_t* n_pn)
         *n_pp = h->last_pp;
     if (n_pn)
         *n_pn = h->last_pn;
+    return BZ_OK;
+}
+
+bz_status bz_walk_counts(bz_handle* h, uint64_t* listed_pairs, uint64_t* evaluated_pairs,
+                         uint64_t* node_terms)
+{
+    if (!h)
+        return BZ_INVALID_ARGUMENT;
+    if (listed_pairs)
+        *listed_pairs = h->last_pp;
+    if (evaluated_pairs)
+        *evaluated_pairs = h->last_eval;
+    if (node_terms)
+        *node_terms = h->last_pn;
     return BZ_OK;
 }
 
@@ -1256,7 +1395,7 @@ bz_status adaptive_steps(bz_handle* h, double dt, uint32_t nsteps)
             for (int a = 0; a < 3; ++a)
                 cudaMemsetAsync(d.acc[a], 0, sizeof(float) * n, h->stream);
             record(h, kPhWalk);
-            cudaMemsetAsync(d.counters, 0, 2 * sizeof(unsigned long long), h->stream);
+            cudaMemsetAsync(d.counters, 0, 3 * sizeof(unsigned long long), h->stream);
             WalkOutputs o{};
             o.ax = d.acc[0];
             o.ay = d.acc[1];

@@ -172,7 +172,8 @@ struct WalkOutputs {
     float* pot;       // optional (+=)
     unsigned long long* n_pp;  // optional per-group counters
     unsigned long long* n_pn;
-    unsigned long long* totals; // optional [2] sums of the above
+    unsigned long long* totals; // optional [3]: listed pairs, node terms (x targets), pairs
+                                //   evaluated by the pair law (inside the cutoff)
     int* pair_src;    // optional [n * kPairSlots]: sorted source index of each recorded pair
     int* pair_cnt;    // [n]: recorded pairs per target (above kPairSlots raises kErrListCapacity)
 };

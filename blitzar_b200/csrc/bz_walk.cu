@@ -339,7 +339,8 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                                              const TreeArrays& t, const WalkParams& p,
                                              float inv2rs, bool cut, float tx, float ty, float tz,
                                              int self_index, Acc& acc, uint32_t& phase, int* err,
-                                             const WalkOutputs& o, int pair_row, int& npair)
+                                             const WalkOutputs& o, int pair_row, int& npair,
+                                             unsigned& evald)
 {
     // pairs closer than rcorr are recorded for the learned correction (pair_row < 0: a lane
     // without a target records nothing)
@@ -521,6 +522,7 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                     }
                 }
                 w.mask[wd][lane] = m;
+                evald += __popc(m);
             }
             int wd = 0;
             unsigned m = w.mask[0][lane];
@@ -555,6 +557,7 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                 const int gsrc0 = w.lstart[j] + (lo - pre);
                 const int off = lo - cbase;
                 const int cntp = hi - lo;
+                evald += cntp;  // every listed source goes through the pair law here
                 if (PERIODIC && w.lcode[j] == kPerPairImage) {
                     // rare slow path: nearest image chosen per pair
                     const float inv_box = 1.0f / p.box;
@@ -672,6 +675,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
         Acc acc;
         acc.zero();
         int npair = 0;
+        unsigned evald = 0;  // pairs this lane's target took through the pair law
         bool bail = false;
         while (top > 0 || gtop > 0) {
             if (top == 0) {  // refill from the spill area (uniform branch)
@@ -803,7 +807,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
             }
             if (nl >= 32 || lp >= kFlushParticles) {
                 flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, t, p, inv2rs, cut, me.x, me.y, me.z,
-                                                   ti, acc, phase, err, o, valid ? ti : -1, npair);
+                                                   ti, acc, phase, err, o, valid ? ti : -1, npair,
+                                                   evald);
                 nl = 0;
                 lp = 0;
             }
@@ -813,7 +818,8 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                 flush_nodes<PERIODIC, SPLIT, QUAD, POT>(w, nn, t, p, inv2rs, me.x, me.y, me.z, acc);
             if (nl > 0)
                 flush_leaves<PERIODIC, SPLIT, POT>(w, nl, pos4, t, p, inv2rs, cut, me.x, me.y, me.z,
-                                                   ti, acc, phase, err, o, valid ? ti : -1, npair);
+                                                   ti, acc, phase, err, o, valid ? ti : -1, npair,
+                                                   evald);
         }
         if (valid) {
             // the walk's sum is clamped, and so is its sum with a mesh force already in the
@@ -836,6 +842,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                     raise_error(err, kErrListCapacity);
             }
         }
+        const unsigned long long ev = __reduce_add_sync(kFullMask, valid ? evald : 0u);
         if (lane == 0) {
             if (o.n_pp)
                 o.n_pp[g] = cnt_pp;
@@ -845,6 +852,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                 const unsigned long long ng = static_cast<unsigned long long>(gn);
                 atomicAdd(&o.totals[0], cnt_pp * ng);
                 atomicAdd(&o.totals[1], cnt_pn * ng);
+                atomicAdd(&o.totals[2], ev);
             }
         }
         __syncwarp();

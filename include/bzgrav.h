@@ -190,6 +190,13 @@ bz_status bz_set_state_acc(bz_handle* h, const float* pos3n, const float* vel3n,
                            const float* acc3n, size_t n);
 bz_status bz_get_state_acc(bz_handle* h, float* pos3n, float* vel3n, float* acc3n);
 
+/* The same with the FP64 positions and velocities the engine integrates (accelerations stay
+ * FP32, the precision they are computed in), so that a state kept on the host between steps
+ * loses nothing to rounding.  Neither allocates device memory. */
+bz_status bz_set_state_acc_f64(bz_handle* h, const double* pos3n, const double* vel3n,
+                               const float* mass, const float* acc3n, size_t n);
+bz_status bz_get_state_acc_f64(bz_handle* h, double* pos3n, double* vel3n, float* acc3n);
+
 /* Morton keys of the current state, sorted, with the stable sort permutation (sorted
  * position -> caller index): buildMortonCodesKernel + thrust::sort_by_key
  * (engine/physics/octree/cuda/linear/OctKeyKernels.inl:22-46, OctBuild.inl:96). */
@@ -214,6 +221,13 @@ bz_status bz_reference_tree(bz_handle* h, int64_t* node_count, float* hot8, int3
 
 /* Interaction counts of the last force evaluation (particle-particle, particle-node). */
 bz_status bz_interaction_counts(bz_handle* h, uint64_t* n_pp, uint64_t* n_pn);
+
+/* Work counters of the last walk (no counterpart in the reference): listed_pairs = source
+ * particles listed for the targets (each listed pair is at least a distance test),
+ * evaluated_pairs = pairs taken through the pair law (with a cutoff, those inside it),
+ * node_terms = multipole interactions.  Any output may be NULL. */
+bz_status bz_walk_counts(bz_handle* h, uint64_t* listed_pairs, uint64_t* evaluated_pairs,
+                         uint64_t* node_terms);
 
 /* Per-phase device times of the last bz_step/bz_accelerations call, in milliseconds, from
  * CUDA events on the handle's stream: [0] keys, [1] sort, [2] permute, [3] tree, [4] mesh,

@@ -121,6 +121,13 @@ def ref():
         R.ref_octree_cpu_accel.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_float,
                                            C.c_float, C.c_float, C.c_float, C.c_int, C.c_float,
                                            C.c_float, C.c_void_p, C.c_int, _f32p, _f32p, _f32p]
+        R.ref_octree_cpu_build.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_float,
+                                           C.c_float, C.c_float, C.c_float, C.c_int, C.c_float,
+                                           C.c_float]
+        R.ref_octree_cpu_build.restype = C.c_void_p
+        R.ref_octree_cpu_walk.argtypes = [C.c_void_p, C.c_void_p, C.c_int, _f32p, _f32p, _f32p]
+        R.ref_octree_cpu_nodes.argtypes = [C.c_void_p]
+        R.ref_octree_cpu_free.argtypes = [C.c_void_p]
         R.ref_fp64_pairwise.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_float,
                                         C.c_float, _f32p, _f32p, _f32p]
         R.ref_pm_periodic.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int, C.c_int, C.c_double,

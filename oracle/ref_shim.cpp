@@ -321,34 +321,75 @@ int ref_octree_gpu_accel(const float* px, const float* py, const float* pz, cons
 // targets (octree/force/OctForces.cpp dispatch), clamp by maxAcceleration.
 // cutoffSquared/shortRangeScale > 0 select the TreePM short-range variant.
 // Returns the node count.
+// A built octree_cpu tree kept between calls, so that a caller can time the build once and
+// the walk over many target chunks (the bench's CPU baseline).
+struct RefOctreeCpu {
+    std::vector<ParticleHotData> hot;
+    Octree tree;
+    ForceLawPolicy law;
+    OctreeOpeningCriterion crit;
+    float maxAcceleration;
+    float cutoffSquared;
+};
+
+void* ref_octree_cpu_build(const float* px, const float* py, const float* pz, const float* mass,
+                           int n, float theta, float softening, float minDistance2,
+                           float maxAcceleration, int boundsCriterion, float shortRangeScale,
+                           float cutoffSquared)
+{
+    auto* t = new RefOctreeCpu();
+    t->hot.resize(n);
+    for (int i = 0; i < n; ++i)
+        t->hot[i] = ParticleHotData(px[i], py[i], pz[i], mass[i]);
+    t->tree.build(t->hot);
+    t->law = resolveForceLawPolicy(theta, softening, 0.0f, minDistance2, 0.0f);
+    t->law.treePmShortRangeScale = shortRangeScale;
+    t->crit = boundsCriterion ? OctreeOpeningCriterion::Bounds : OctreeOpeningCriterion::CenterOfMass;
+    t->maxAcceleration = maxAcceleration;
+    t->cutoffSquared = cutoffSquared;
+    return t;
+}
+
+// Forces on the listed targets (all particles when targets is NULL), clamped by
+// maxAcceleration as OctForces.cpp:128-132 does.
+void ref_octree_cpu_walk(void* handle, const int* targets, int nTargets, float* ax, float* ay,
+                         float* az)
+{
+    auto* t = static_cast<RefOctreeCpu*>(handle);
+    const int count = targets ? nTargets : static_cast<int>(t->hot.size());
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int k = 0; k < count; ++k) {
+        const int i = targets ? targets[k] : k;
+        Vector3 a = t->tree.computeForceOn(t->hot, static_cast<size_t>(i), t->law, t->crit,
+                                           t->cutoffSquared);
+        const float norm = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+        if (norm > t->maxAcceleration && norm > 1e-12f)
+            a = a * (t->maxAcceleration / norm);
+        ax[k] = a.x;
+        ay[k] = a.y;
+        az[k] = a.z;
+    }
+}
+
+int ref_octree_cpu_nodes(void* handle)
+{
+    return static_cast<int>(static_cast<RefOctreeCpu*>(handle)->tree.getNodeCount());
+}
+
+void ref_octree_cpu_free(void* handle) { delete static_cast<RefOctreeCpu*>(handle); }
+
 int ref_octree_cpu_accel(const float* px, const float* py, const float* pz, const float* mass,
                          int n, float theta, float softening, float minDistance2,
                          float maxAcceleration, int boundsCriterion, float shortRangeScale,
                          float cutoffSquared, const int* targets, int nTargets, float* ax,
                          float* ay, float* az)
 {
-    std::vector<ParticleHotData> hot(n);
-    for (int i = 0; i < n; ++i)
-        hot[i] = ParticleHotData(px[i], py[i], pz[i], mass[i]);
-    Octree tree;
-    tree.build(hot);
-    ForceLawPolicy law = resolveForceLawPolicy(theta, softening, 0.0f, minDistance2, 0.0f);
-    law.treePmShortRangeScale = shortRangeScale;
-    const OctreeOpeningCriterion crit =
-        boundsCriterion ? OctreeOpeningCriterion::Bounds : OctreeOpeningCriterion::CenterOfMass;
-    const int count = targets ? nTargets : n;
-#pragma omp parallel for schedule(dynamic, 64)
-    for (int t = 0; t < count; ++t) {
-        const int i = targets ? targets[t] : t;
-        Vector3 a = tree.computeForceOn(hot, static_cast<size_t>(i), law, crit, cutoffSquared);
-        const float norm = std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
-        if (norm > maxAcceleration && norm > 1e-12f)
-            a = a * (maxAcceleration / norm);
-        ax[t] = a.x;
-        ay[t] = a.y;
-        az[t] = a.z;
-    }
-    return static_cast<int>(tree.getNodeCount());
+    void* t = ref_octree_cpu_build(px, py, pz, mass, n, theta, softening, minDistance2,
+                                   maxAcceleration, boundsCriterion, shortRangeScale, cutoffSquared);
+    ref_octree_cpu_walk(t, targets, nTargets, ax, ay, az);
+    const int nodes = ref_octree_cpu_nodes(t);
+    ref_octree_cpu_free(t);
+    return nodes;
 }
 
 // ---------------------------------------------------------------- TreePM CPU templates

@@ -200,3 +200,46 @@ def test_state_round_trip_keeps_order(gpu):
         e.step(1e-3, 2)
         pb, vb = e.get_state(f64=True)
     assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+
+
+def test_state_with_accelerations_f64(gpu):
+    """The FP64 state-with-accelerations calls: a host round trip after every step leaves the
+    trajectory bit for bit that of a resident state (no FP32 rounding of positions and
+    velocities), and the FP64 download equals bz_get_state_f64."""
+    n = 20_000
+    pos = plummer(n, seed=10).astype(np.float64)
+    rng = np.random.default_rng(10)
+    vel = 0.1 * rng.standard_normal((n, 3))
+    m = np.full(n, 1.0 / n, np.float32)
+    with _engine(n) as e:
+        e.set_state(pos, vel, m, f64=True)
+        e.step(1e-3, 4)
+        pa, va = e.get_state(f64=True)
+    p3, v3 = np.empty(3 * n), np.empty(3 * n)
+    a3 = np.empty(3 * n, np.float32)
+    with _engine(n) as e:
+        e.set_state(pos, vel, m, f64=True)
+        for _ in range(4):
+            e.get_state_acc_f64_soa(p3, v3, a3)
+            e.set_state_acc_f64_soa(p3, v3, m, a3)  # same size: kept in the sorted order
+            e.step(1e-3, 1)
+        e.get_state_acc_f64_soa(p3, v3, a3)
+        pb, vb = e.get_state(f64=True)
+        again = e.accelerations()
+    assert np.array_equal(pa, pb) and np.array_equal(va, vb)
+    assert np.array_equal(p3.reshape(3, n).T, pb) and np.array_equal(v3.reshape(3, n).T, vb)
+    assert np.array_equal(a3.reshape(3, n).T, again)
+    # a fresh handle given the FP64 state and its accelerations steps like the resident one
+    with _engine(n) as e:
+        e.set_state(pos, vel, m, f64=True)
+        e.step(1e-3, 2)
+        pc, vc = e.get_state(f64=True)
+    with _engine(n) as e:
+        e.set_state(pos, vel, m, f64=True)
+        p0, v0, a0 = np.empty(3 * n), np.empty(3 * n), np.empty(3 * n, np.float32)
+        e.get_state_acc_f64_soa(p0, v0, a0)
+    with _engine(n) as e:
+        e.set_state_acc_f64_soa(p0, v0, m, a0)
+        e.step(1e-3, 2)
+        pd, vd = e.get_state(f64=True)
+    assert np.array_equal(pc, pd) and np.array_equal(vc, vd)
