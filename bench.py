@@ -1,18 +1,20 @@
 #!/usr/bin/env python
 """Benchmark: particle-steps/s of the periodic TreePM leapfrog step on one B200.
 
-Workload (default ``treepm128``): N = 128^3 = 2,097,152 equal-mass particles on a unit
-periodic box, grid positions displaced by a Zel'dovich field of a Gaussian random field with
-P(k) ~ k^-2 (3-D rms displacement 0.2 cell, seed 2), zero velocities; PM mesh 128^3 with
-Gaussian split r_s = 1.25 cells, theta = 0.5 with quadrupoles, Plummer softening 0.02 cell,
-FP64 leapfrog with dt = 5e-4.  Inputs are seeded synthetic data.  The default mesh settings
-(256^3 PCS mesh, spectral gradient, r_s = 1.0 mesh cell, cutoff 5 r_s, direct short range)
-are the cheapest found that hold the median force error under 1e-3 against FP64 Ewald on this
-box; ``treepm128_cic`` runs the reference mesh (128^3 CIC, centred differences, cutoff 4.5 r_s).
+Workload (default ``treepm256``, the box the metric's learned-vs-plain target is stated on):
+N = 256^3 = 16,777,216 equal-mass particles on a unit periodic box, grid positions displaced by
+a Zel'dovich field of a Gaussian random field with P(k) ~ k^-2 (3-D rms displacement 0.2 cell,
+seed 4), zero velocities, theta = 0.5, Plummer softening 0.02 lattice cell, FP64 leapfrog with
+dt = 5e-4.  Inputs are seeded synthetic data.  The mesh settings (512^3 PCS mesh, spectral
+gradient, r_s = 1.0 mesh cell, cutoff 5 r_s, no multipoles inside the cutoff) are the cheapest
+found that hold the median force error under 1e-3 against FP64 Ewald on this box (r_s = 0.9
+and 0.8 cells miss it; 4.5 r_s misses it); ``treepm128`` is the same recipe at 128^3 (seed 2)
+and ``treepm128_cic`` runs the reference mesh (128^3 CIC, centred differences, cutoff 4.5 r_s).
 
 A "step" is one KDK leapfrog step of the whole system (keys, sort, permutation, octree,
 mesh, group walk, kicks and drift), replayed from a CUDA graph.  The state (about 230 B per
-particle, ~480 MB) is larger than the 126 MB L2, so no flush is needed between steps.
+particle: ~3.9 GB at 256^3, ~480 MB at 128^3) is larger than the 126 MB L2, so no flush is
+needed between steps.
 
 Under torchrun (N > 1) every rank steps an independent replica (the force evaluation of one
 system does not shard) and `value` sums all ranks' particle-steps over the slowest rank's
@@ -73,7 +75,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="treepm128")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="treepm256")
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--error-sample", type=int, default=2048)
     ap.add_argument("--cpu-budget", type=float, default=20.0,

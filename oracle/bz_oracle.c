@@ -694,6 +694,7 @@ typedef struct {
     int64_t g0, g1;
     double* acc; /* per target in group */
     double* pot;
+    double* asum; /* optional: per target, sum of |a| over its pair and node terms */
     int64_t pp, pn;
 } walk_ctx;
 
@@ -762,6 +763,8 @@ static void direct_leaf(walk_ctx* w, int32_t k, const float sh[3], int per_pair_
             acc[0] += f * d[0];
             acc[1] += f * d[1];
             acc[2] += f * d[2];
+            if (w->asum)
+                w->asum[t - w->g0] += fabs(f) * sqrt(r2);
             if (w->pot && j != t) {
                 const double f0 = p->rsplit > 0.0f ? erfc(0.5 * s1 / p->rsplit) / s1 : 1.0 / s1;
                 w->pot[t - w->g0] -= (double)sp[3] * f0;
@@ -858,6 +861,8 @@ static void walk_node(walk_ctx* w, int32_t k)
             acc[2] += a[2];
             if (w->pot)
                 w->pot[t - w->g0] += phi;
+            if (w->asum)
+                w->asum[t - w->g0] += sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
         }
         return;
     }
@@ -944,16 +949,23 @@ int64_t or_tree_groups(const int32_t* start, const int32_t* count, const int32_t
     return g.ng;
 }
 
-void or_walk(const float* pos4, int64_t n, const int32_t* start, const int32_t* count,
-             const int32_t* child, const int32_t* nchild, const float* mono4,
-             const float* bmin3, const float* bmax3, const float* quad6,
-             const or_walk_params* prm, const int64_t* gstart, int64_t ngroups, double* acc3,
-             double* pot, int64_t* n_pp, int64_t* n_pn)
+/* Group walk.  only (may be NULL): walk just the groups only[0..n_only) (their targets' rows
+ * of acc3/pot/asum are written, the others are left untouched); asum (may be NULL): per
+ * target, the sum of the magnitudes of its pair and node terms (the scale of the rounding
+ * error of an FP32 sum of them). */
+void or_walk_ex(const float* pos4, int64_t n, const int32_t* start, const int32_t* count,
+                const int32_t* child, const int32_t* nchild, const float* mono4,
+                const float* bmin3, const float* bmax3, const float* quad6,
+                const or_walk_params* prm, const int64_t* gstart, int64_t ngroups, double* acc3,
+                double* pot, int64_t* n_pp, int64_t* n_pn, const int64_t* only, int64_t n_only,
+                double* asum)
 {
     const int G = prm->group > 0 ? prm->group : 32;
     const int64_t ng = gstart ? ngroups : (n + G - 1) / G;
+    const int64_t nw = only ? n_only : ng;
 #pragma omp parallel for schedule(dynamic, 4)
-    for (int64_t g = 0; g < ng; ++g) {
+    for (int64_t q = 0; q < nw; ++q) {
+        const int64_t g = only ? only[q] : q;
         walk_ctx w;
         memset(&w, 0, sizeof(w));
         w.pos4 = pos4;
@@ -989,12 +1001,26 @@ void or_walk(const float* pos4, int64_t n, const int32_t* start, const int32_t* 
         if (w.pot)
             for (int64_t t = 0; t < w.g1 - w.g0; ++t)
                 w.pot[t] = 0.0;
+        w.asum = asum ? asum + w.g0 : NULL;
+        if (w.asum)
+            for (int64_t t = 0; t < w.g1 - w.g0; ++t)
+                w.asum[t] = 0.0;
         walk_node(&w, 0);
         if (n_pp)
             n_pp[g] = w.pp;
         if (n_pn)
             n_pn[g] = w.pn;
     }
+}
+
+void or_walk(const float* pos4, int64_t n, const int32_t* start, const int32_t* count,
+             const int32_t* child, const int32_t* nchild, const float* mono4,
+             const float* bmin3, const float* bmax3, const float* quad6,
+             const or_walk_params* prm, const int64_t* gstart, int64_t ngroups, double* acc3,
+             double* pot, int64_t* n_pp, int64_t* n_pn)
+{
+    or_walk_ex(pos4, n, start, count, child, nchild, mono4, bmin3, bmax3, quad6, prm, gstart,
+               ngroups, acc3, pot, n_pp, n_pn, NULL, 0, NULL);
 }
 
 /* ======================================================================================
@@ -1260,6 +1286,16 @@ static inline double sinc(double v) { return fabs(v) < 1.0e-5 ? 1.0 : sin(v) / v
 int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rsplit, int order,
                    int gradient, double floor_w, double* acc3, double* density, double* phi)
 {
+    return or_pm_periodic_at(pos4, n, mesh, box, rsplit, order, gradient, floor_w, NULL, n, acc3,
+                             density, phi);
+}
+
+/* As or_pm_periodic, interpolating the mesh force only at targets[0..nt) (all particles when
+ * targets is NULL); acc3 holds 3 nt values in target order. */
+int or_pm_periodic_at(const float* pos4, int64_t n, int mesh, double box, double rsplit,
+                      int order, int gradient, double floor_w, const int64_t* targets, int64_t nt,
+                      double* acc3, double* density, double* phi)
+{
     const int64_t M = mesh, cells = M * M * M;
     const double h = box / (double)mesh, inv = 1.0 / h;
     double* rho = (double*)calloc((size_t)cells, sizeof(double));
@@ -1348,8 +1384,10 @@ int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rs
         }
         free(q);
     }
+    const int64_t nout = targets ? nt : n;
 #pragma omp parallel for schedule(static)
-    for (int64_t i = 0; i < n; ++i) {
+    for (int64_t o = 0; o < nout; ++o) {
+        const int64_t i = targets ? targets[o] : o;
         int ix[4], iy[4], iz[4];
         double wx[4], wy[4], wz[4];
         stencil_p(pos4[4 * i], inv, mesh, order, ix, wx);
@@ -1365,7 +1403,7 @@ int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rs
                         acc[a] += w * field[a][cell];
                 }
         for (int a = 0; a < 3; ++a)
-            acc3[3 * i + a] = acc[a];
+            acc3[3 * o + a] = acc[a];
     }
     for (int a = 0; a < 3; ++a)
         free(field[a]);

@@ -69,6 +69,14 @@ void or_walk(const float* pos4, int64_t n, const int32_t* start, const int32_t* 
              const float* bmin3, const float* bmax3, const float* quad6,
              const or_walk_params* prm, const int64_t* gstart, int64_t ngroups, double* acc3,
              double* pot, int64_t* n_pp, int64_t* n_pn);
+/* As or_walk for the groups only[0..n_only) (NULL: all); asum (may be NULL) receives, per
+ * target, the sum of the magnitudes of its pair and node terms. */
+void or_walk_ex(const float* pos4, int64_t n, const int32_t* start, const int32_t* count,
+                const int32_t* child, const int32_t* nchild, const float* mono4,
+                const float* bmin3, const float* bmax3, const float* quad6,
+                const or_walk_params* prm, const int64_t* gstart, int64_t ngroups, double* acc3,
+                double* pot, int64_t* n_pp, int64_t* n_pn, const int64_t* only, int64_t n_only,
+                double* asum);
 
 /* ---- direct sums --------------------------------------------------------------------- */
 void or_direct_f64(const float* pos4, int64_t n, const int64_t* targets, int64_t nt,
@@ -81,6 +89,10 @@ void or_ewald_f64(const float* pos4, int64_t n, const int64_t* targets, int64_t 
 void or_fft3d(double* re_im, int size, int inverse);
 int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rsplit, int order,
                    int gradient, double floor_w, double* acc3, double* density, double* phi);
+/* The same mesh, interpolated only at targets[0..nt) (all particles when NULL). */
+int or_pm_periodic_at(const float* pos4, int64_t n, int mesh, double box, double rsplit,
+                      int order, int gradient, double floor_w, const int64_t* targets, int64_t nt,
+                      double* acc3, double* density, double* phi);
 
 /* ---- split kernel helpers ---------------------------------------------------------------- */
 double or_split_weight(double s, double rsplit);

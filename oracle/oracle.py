@@ -85,6 +85,10 @@ def lib():
         L.or_walk.argtypes = [_f32p, C.c_int64, _i32p, _i32p, _i32p, _i32p, _f32p, _f32p,
                               _f32p, _f32p, C.POINTER(WalkParams), C.c_void_p, C.c_int64, _f64p,
                               C.c_void_p, _i64p, _i64p]
+        L.or_walk_ex.argtypes = L.or_walk.argtypes + [C.c_void_p, C.c_int64, C.c_void_p]
+        L.or_pm_periodic_at.argtypes = [_f32p, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int,
+                                        C.c_int, C.c_double, C.c_void_p, C.c_int64, _f64p,
+                                        C.c_void_p, C.c_void_p]
         L.or_direct_f64.argtypes = [_f32p, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
                                     C.c_double, C.c_double, C.c_double, _f64p, C.c_void_p]
         L.or_ewald_f64.argtypes = [_f32p, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
@@ -283,6 +287,33 @@ def walk(sorted_pos4, tree, theta=0.5, eps=0.01, rcut=0.0, box=0.0, rsplit=0.0,
     return out
 
 
+def walk_targets(sorted_pos4, tree, sorted_targets, theta=0.5, eps=0.01, rcut=0.0, box=0.0,
+                 rsplit=0.0, min_dist2=1e-12, quadrupole=True, max_node_size=0.0, gmax=32):
+    """Group walk (the engine's tree groups) of only the groups that hold the given sorted
+    target indices.  Returns (acc[len(targets), 3], asum[len(targets)]): the short-range
+    accelerations of those targets and, per target, the sum of the magnitudes of its terms."""
+    n = len(sorted_pos4)
+    prm = WalkParams(np.float32(theta) * np.float32(theta), np.float32(eps) * np.float32(eps),
+                     np.float32(rcut) * np.float32(rcut), box, rsplit, min_dist2,
+                     1 if quadrupole else 0, 32, max_node_size)
+    gstart = tree_groups(tree, gmax)
+    ng = len(gstart) - 1
+    tg = np.asarray(sorted_targets, np.int64)
+    only = np.unique(np.searchsorted(gstart, tg, side="right") - 1).astype(np.int64)
+    acc = np.zeros(3 * n, np.float64)
+    asum = np.zeros(n, np.float64)
+    npp = np.zeros(ng, np.int64)
+    npn = np.zeros(ng, np.int64)
+    lib().or_walk_ex(np.ascontiguousarray(sorted_pos4, np.float32), n, tree["start"], tree["count"],
+                     tree["child"], tree["nchild"], np.ascontiguousarray(tree["mono"].reshape(-1)),
+                     np.ascontiguousarray(tree["bmin"].reshape(-1)),
+                     np.ascontiguousarray(tree["bmax"].reshape(-1)),
+                     np.ascontiguousarray(tree["quad"].reshape(-1)), C.byref(prm),
+                     gstart.ctypes.data, ng, acc, None, npp, npn, only.ctypes.data, len(only),
+                     asum.ctypes.data)
+    return acc.reshape(n, 3)[tg], asum[tg]
+
+
 def direct(pos4_, targets=None, eps=0.01, box=0.0, rsplit=0.0, rcut=0.0, want_pot=False):
     p = np.ascontiguousarray(pos4_, np.float32)
     if targets is None:
@@ -325,6 +356,18 @@ def pm_periodic(pos4_, mesh, box, rsplit, want_fields=False, assignment="cic", s
                          None if phi is None else phi.ctypes.data)
     if want_fields:
         return acc.reshape(-1, 3), dens, phi
+    return acc.reshape(-1, 3)
+
+
+def pm_periodic_at(pos4_, targets, mesh, box, rsplit, assignment="cic", spectral=False,
+                   window_floor=0.08):
+    """pm_periodic's mesh force interpolated only at the given particle indices."""
+    p = np.ascontiguousarray(pos4_, np.float32)
+    tg = np.ascontiguousarray(targets, np.int64)
+    acc = np.zeros(3 * len(tg), np.float64)
+    lib().or_pm_periodic_at(p, len(p), mesh, box, rsplit, ASSIGNMENT_ORDER[assignment],
+                            1 if spectral else 0, window_floor, tg.ctypes.data, len(tg), acc,
+                            None, None)
     return acc.reshape(-1, 3)
 
 

@@ -1,0 +1,85 @@
+"""TreePM parity at the benchmark's sizes: engine accelerations on a seeded sample of 2048
+targets against the oracle's periodic PM interpolated at those targets plus the oracle's group
+walk of the groups that hold them (the sum the reference forms in treePmComputeAcceleration,
+engine/physics/treepm/short_range/TpmTreeForce.inl:9-25).
+
+The bound is 1e-5 relative per target.  The engine sums a target's pair and node terms in FP32
+(compensated), the oracle in FP64, so the two differ by a small multiple of the FP32 rounding
+of the terms, which scales with the sum of their magnitudes S = sum |a_j| + |a_mesh|, not with
+the net force.  A target whose net force is a cancellation (kappa = S / |a| above 20) is held
+to 1e-6 of S instead; the test reports how many targets that is."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+# the GRF boxes of the benchmark workloads (positions: grid displaced by a Zel'dovich field of
+# a P(k) ~ k^-2 Gaussian random field, 0.2 cell rms)
+CASES = {
+    # 128^3 box, 256^3 PCS mesh, spectral gradient, r_s = 1.0 cell, r_cut = 5 r_s, node cap
+    "treepm128": dict(n_side=128, seed=2, mesh=256, rs=1.0, rcf=5.0, assignment=2, spectral=True,
+                      floor=0.0, cap=0.5, order=1),
+    # the reference-literal mesh: 128^3 CIC, centred differences, r_s = 1.25 cells, 4.5 r_s
+    "treepm128_cic": dict(n_side=128, seed=2, mesh=128, rs=1.25, rcf=4.5, assignment=0,
+                          spectral=False, floor=0.08, cap=0.0, order=2),
+    # 256^3 box on the 512^3 mesh
+    "treepm256": dict(n_side=256, seed=4, mesh=512, rs=1.0, rcf=5.0, assignment=2, spectral=True,
+                      floor=0.0, cap=0.5, order=1),
+}
+ASSIGN_NAME = {0: "cic", 1: "tsc", 2: "pcs"}
+KAPPA = 20.0
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_treepm_parity_at_benchmark_scale(gpu, oracle, case):
+    from blitzar_b200 import ics
+    from blitzar_b200._lib import Engine
+
+    c = CASES[case]
+    pos, _, m = ics.grf_grid(c["n_side"], seed=c["seed"], rms_cells=0.2)
+    m = m.astype(np.float32)
+    n = len(m)
+    M = c["mesh"]
+    rs = c["rs"] / M
+    eps = 0.02 / c["n_side"]
+    with Engine(n, solver=1, box_length=1.0, treepm_grid_size=M, treepm_r_split_cells=c["rs"],
+                treepm_r_cut_factor=c["rcf"], treepm_assignment=c["assignment"],
+                treepm_gradient=1 if c["spectral"] else 0, treepm_window_floor=c["floor"],
+                treepm_node_size_factor=c["cap"], multipole_order=c["order"],
+                octree_softening=eps, physics_max_acceleration=1e30) as e:
+        e.set_state(pos, None, m, f64=True)
+        acc = e.accelerations().astype(np.float64)
+    rng = np.random.default_rng(101)
+    tg = np.sort(rng.choice(n, 2048, replace=False)).astype(np.int64)
+    p32 = pos.astype(np.float32)
+    p4 = oracle.pos4(p32, m)
+    keys = oracle.morton63(pos.astype(np.float64), [0.0, 0.0, 0.0], 1.0)
+    perm = oracle.stable_sort(keys)
+    inv = np.empty(n, np.int64)
+    inv[perm] = np.arange(n)
+    tree = oracle.build_tree(keys[perm], p4[perm], leaf_cap=16)
+    rsf = np.float32(c["rs"]) * np.float32(1.0 / M)
+    st = inv[tg]
+    order = np.argsort(st)
+    asr_s, asum_s = oracle.walk_targets(p4[perm], tree, st[order], theta=0.5, eps=eps,
+                                        rcut=np.float32(c["rcf"]) * rsf, box=1.0, rsplit=rsf,
+                                        quadrupole=c["order"] >= 2,
+                                        max_node_size=np.float32(c["cap"]) * rsf if c["cap"] else 0.0)
+    asr = np.empty_like(asr_s)
+    asum = np.empty_like(asum_s)
+    asr[order] = asr_s
+    asum[order] = asum_s
+    apm = oracle.pm_periodic_at(p4, tg, M, 1.0, rsf, assignment=ASSIGN_NAME[c["assignment"]],
+                                spectral=c["spectral"], window_floor=c["floor"])
+    ref = apm + asr
+    scale = asum + np.linalg.norm(apm, axis=1)
+    dev = np.linalg.norm(acc[tg] - ref, axis=1)
+    net = np.linalg.norm(ref, axis=1)
+    rel = dev / net
+    kappa = scale / net
+    cancel = kappa > KAPPA
+    print(f"{case}: median rel {np.median(rel):.2e}, max rel {rel.max():.2e} (kappa {kappa[rel.argmax()]:.1f}), "
+          f"max dev/S {(dev / scale).max():.2e}, {int(cancel.sum())} of {len(tg)} targets with kappa > {KAPPA:g}")
+    assert np.median(rel) < 1e-6
+    assert rel[~cancel].max() < 1e-5, (rel[~cancel].max(), kappa[~cancel][rel[~cancel].argmax()])
+    assert (dev[cancel] <= 1e-6 * scale[cancel]).all()
