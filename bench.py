@@ -146,12 +146,12 @@ def make_ics(w, rank):
 
 def engine_config(w):
     if w["kind"] == "treepm":
-        spectral = w["gradient"] == "spectral"
+        grad = {"centred-difference": 0, "spectral": 1, "analytic": 2}[w["gradient"]]
         return dict(solver=1, box_length=1.0, treepm_grid_size=w["mesh"],
                     treepm_r_split_cells=w["r_split_cells"], treepm_r_cut_factor=w["r_cut_factor"],
                     treepm_assignment={"cic": 0, "tsc": 1, "pcs": 2}[w["assignment"]],
-                    treepm_gradient=1 if spectral else 0,
-                    treepm_window_floor=0.0 if spectral else 0.08,
+                    treepm_gradient=grad,
+                    treepm_window_floor=0.0 if grad else 0.08,
                     treepm_node_size_factor=w["node_size_factor"],
                     octree_theta=w["theta"], octree_softening=w["eps_lattice"] / w["n_side"],
                     # with the node-size cap no node is accepted inside the cutoff on these

@@ -595,6 +595,7 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
         const int M = cfg->treepm_grid_size;
         if (cfg->box_length <= 0.0 || M < 8 || (M & (M - 1)) != 0 || cfg->treepm_r_split_cells <= 0.0f ||
             cfg->treepm_r_cut_factor <= 0.0f || cfg->treepm_assignment < 0 || cfg->treepm_assignment > 2 ||
+            cfg->treepm_gradient < 0 || cfg->treepm_gradient > 2 ||
             cfg->treepm_r_cut_factor * cfg->treepm_r_split_cells * 2.0 >= M) {
             delete h;
             return BZ_INVALID_ARGUMENT;
@@ -2108,8 +2109,10 @@ bz_status bz_pm_mesh(bz_handle* h, int which, float* out)
 {
     if (!h || !out || !h->pm || h->n == 0 || which < 0 || which > 4)
         return BZ_INVALID_ARGUMENT;
-    if (which == 1 && h->cfg.treepm_gradient != 0)
-        return fail(h, BZ_UNSUPPORTED, "the potential mesh exists in centred-difference mode only");
+    if (which == 1 && h->cfg.treepm_gradient == 1)
+        return fail(h, BZ_UNSUPPORTED, "the spectral-gradient mode keeps no potential mesh");
+    if (which >= 2 && h->cfg.treepm_gradient == 2)
+        return fail(h, BZ_UNSUPPORTED, "analytic differentiation keeps no force mesh");
     cudaSetDevice(h->device);
     bz_status s = ensure_forces(h);
     if (s != BZ_OK)

@@ -6,10 +6,16 @@
 //              to the mesh (one global atomic per tile cell instead of p^3 per particle);
 //              blocks whose stencils do not fit a tile use global atomics directly.
 //   solve    : cuFFT R2C -> Green's function with Gaussian split, window deconvolution and 1/M^3
-//              (precomputed in FP64) -> either the potential (reference centred differences,
-//              then a gradient kernel) or, fused in the same k-space pass, the three spectral
-//              gradients i k phi_k -> three cuFFT C2R -> interleaved float4 force mesh.
-//   interp   : the same order-p stencil gathers the force mesh at each particle.
+//              (precomputed in FP64) -> one of
+//              - the potential (reference centred differences, then a gradient kernel into an
+//                interleaved float4 force mesh);
+//              - fused in the same k-space pass, the three spectral gradients i k phi_k ->
+//                three cuFFT C2R -> interleaved float4 force mesh;
+//              - the potential alone (one C2R): analytic differentiation, below.
+//   interp   : the same order-p stencil gathers the force mesh at each particle; with analytic
+//              differentiation it gathers the potential with the gradient of the stencil
+//              weights, a = sum_c phi_c grad W(x - x_c), so that one inverse transform and a
+//              scalar mesh replace three transforms and a four-component mesh.
 //
 // Formulas follow the reference CPU templates driven with a periodic grid
 // (engine/physics/treepm/deposit/TpmAssignment.inl:39-199, engine/physics/treepm/field/
@@ -32,7 +38,7 @@ struct PmPlan {
     double box = 0.0;
     double rsplit = 0.0;
     int order = 2;
-    int gradient = 0;          // 0 centred differences of phi (reference), 1 spectral
+    int gradient = 0;          // 0 centred differences of phi (reference), 1 spectral, 2 analytic
     double floor = 0.08;
     float* rho = nullptr;      // M^3: density, then potential (centred-difference mode)
     cufftComplex* spec = nullptr;     // M*M*(M/2+1)
@@ -97,6 +103,62 @@ __device__ __forceinline__ int stencil(float coord, float inv_h, int mesh, float
         w[1] = pcs_w(s - fl);
         w[2] = pcs_w(s - (fl + 1.0f));
         w[3] = pcs_w(s - (fl + 2.0f));
+        return static_cast<int>(fl) - 1;
+    }
+}
+
+// Derivatives of the weights with respect to the particle coordinate in cells.
+__device__ __forceinline__ float tsc_dw(float d)
+{
+    const float a = fabsf(d);
+    if (a < 0.5f)
+        return -2.0f * d;
+    if (a < 1.5f)
+        return copysignf(a - 1.5f, d);
+    return 0.0f;
+}
+__device__ __forceinline__ float pcs_dw(float d)
+{
+    const float a = fabsf(d);
+    if (a < 1.0f)
+        return d * (1.5f * a - 2.0f);
+    if (a < 2.0f) {
+        const float t = 2.0f - a;
+        return copysignf(-0.5f * t * t, d);
+    }
+    return 0.0f;
+}
+
+// As stencil<P>, with the derivatives dw of the weights (per cell of coordinate).
+template <int P>
+__device__ __forceinline__ int stencil_d(float coord, float inv_h, int mesh, float* w, float* dw)
+{
+    const float raw = coord * inv_h;
+    const float m = static_cast<float>(mesh);
+    const float s = raw - floorf(raw / m) * m;
+    if (P == 2) {
+        const float fl = floorf(s);
+        const float f = s - fl;
+        w[0] = 1.0f - f;
+        w[1] = f;
+        dw[0] = -1.0f;
+        dw[1] = 1.0f;
+        return static_cast<int>(fl);
+    } else if (P == 3) {
+        const float c = floorf(s + 0.5f);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            w[k] = tsc_w(s - (c - 1.0f + k));
+            dw[k] = tsc_dw(s - (c - 1.0f + k));
+        }
+        return static_cast<int>(c) - 1;
+    } else {
+        const float fl = floorf(s);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            w[k] = pcs_w(s - (fl - 1.0f + k));
+            dw[k] = pcs_dw(s - (fl - 1.0f + k));
+        }
         return static_cast<int>(fl) - 1;
     }
 }
@@ -419,6 +481,63 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
     }
 }
 
+// Analytic differentiation: four lanes per particle as in k_interp, lane q taking stencil
+// column x = bx + q of the scalar potential mesh; the weight of cell (a, b, c) in the x
+// component is dW_x(a) W_y(b) W_z(c), and likewise for y and z.  The potential mesh holds one
+// float per cell, so a quad reads 16-byte row segments.
+template <int P>
+__global__ void __launch_bounds__(kThreads) k_interp_ad(const float4* __restrict__ pos4, int n, int mesh,
+                                                         float inv_h, const float* __restrict__ phi,
+                                                         float* __restrict__ ax, float* __restrict__ ay,
+                                                         float* __restrict__ az)
+{
+    const size_t M = static_cast<size_t>(mesh);
+    const int q = threadIdx.x & 3;
+    constexpr int kRound = (kThreads / 32) * 8;
+    const int per_block = ((n + gridDim.x - 1) / gridDim.x + kRound - 1) / kRound * kRound;
+    const int start = blockIdx.x * per_block;
+    const int stop = min(start + per_block, n);
+    for (int i0 = start + (threadIdx.x >> 5) * 8; i0 < stop; i0 += kRound) {
+        const int i = i0 + ((threadIdx.x & 31) >> 2);
+        float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+        if (i < stop && q < P) {
+            const float4 p = pos4[i];
+            float wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
+            const int bx = stencil_d<P>(p.x, inv_h, mesh, wx, dx);
+            const int by = stencil_d<P>(p.y, inv_h, mesh, wy, dy);
+            const int bz = stencil_d<P>(p.z, inv_h, mesh, wz, dz);
+            const float wq = column_weight<P>(wx, q);
+            const float dq = column_weight<P>(dx, q);
+            const int xs = wrap1(bx + q, mesh);
+#pragma unroll
+            for (int c = 0; c < P; ++c) {
+                const size_t zrow = static_cast<size_t>(wrap1(bz + c, mesh)) * M;
+                float sx = 0.0f, sy = 0.0f;  // this z plane's sums over y: W_y and dW_y weighted
+#pragma unroll
+                for (int b = 0; b < P; ++b) {
+                    const float v = __ldg(&phi[(zrow + wrap1(by + b, mesh)) * M + xs]);
+                    sx = fmaf(v, wy[b], sx);
+                    sy = fmaf(v, dy[b], sy);
+                }
+                gx = fmaf(sx * dq, wz[c], gx);
+                gy = fmaf(sy * wq, wz[c], gy);
+                gz = fmaf(sx * wq, dz[c], gz);
+            }
+        }
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+            gx += __shfl_xor_sync(kFullMask, gx, o);
+            gy += __shfl_xor_sync(kFullMask, gy, o);
+            gz += __shfl_xor_sync(kFullMask, gz, o);
+        }
+        if (i < stop && q == 0) {
+            ax[i] = gx * inv_h;
+            ay[i] = gy * inv_h;
+            az[i] = gz * inv_h;
+        }
+    }
+}
+
 int sm_count()
 {
     int dev = 0, sms = 148;
@@ -437,16 +556,17 @@ PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, 
     p->box = box;
     p->rsplit = rsplit;
     p->order = order < 2 ? 2 : (order > 4 ? 4 : order);
-    p->gradient = gradient ? 1 : 0;
+    p->gradient = gradient < 0 ? 0 : (gradient > 2 ? 2 : gradient);
     p->floor = window_floor;
     const size_t cells = static_cast<size_t>(mesh) * mesh * mesh;
     const size_t half = static_cast<size_t>(mesh) * mesh * (mesh / 2 + 1);
     *cuda_err = 0;
     bool ok = cudaMalloc(&p->rho, cells * sizeof(float)) == cudaSuccess &&
               cudaMalloc(&p->spec, half * sizeof(cufftComplex)) == cudaSuccess &&
-              cudaMalloc(&p->green, half * sizeof(float)) == cudaSuccess &&
-              cudaMalloc(&p->force, cells * sizeof(float4)) == cudaSuccess;
-    if (ok && p->gradient)
+              cudaMalloc(&p->green, half * sizeof(float)) == cudaSuccess;
+    if (ok && p->gradient != 2)  // analytic differentiation needs no force mesh
+        ok = cudaMalloc(&p->force, cells * sizeof(float4)) == cudaSuccess;
+    if (ok && p->gradient == 1)
         ok = cudaMalloc(&p->spec3, 3 * half * sizeof(cufftComplex)) == cudaSuccess &&
              cudaMalloc(&p->field3, 3 * cells * sizeof(float)) == cudaSuccess;
     if (!ok) {
@@ -465,8 +585,9 @@ PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, 
     size_t ws1 = 0, ws2 = 0;
     cufftGetSize(p->r2c, &ws1);
     cufftGetSize(p->c2r, &ws2);
-    p->bytes = cells * (sizeof(float) + sizeof(float4)) + half * (sizeof(cufftComplex) + sizeof(float)) +
-               (p->gradient ? 3 * (half * sizeof(cufftComplex) + cells * sizeof(float)) : 0) + ws1 + ws2;
+    p->bytes = cells * (sizeof(float) + (p->gradient != 2 ? sizeof(float4) : 0)) +
+               half * (sizeof(cufftComplex) + sizeof(float)) +
+               (p->gradient == 1 ? 3 * (half * sizeof(cufftComplex) + cells * sizeof(float)) : 0) + ws1 + ws2;
     count_launch();
     k_green_table<<<sm_count() * 4, 256, 0, s>>>(mesh, box, rsplit, p->order, window_floor, p->green);
     return p;
@@ -538,7 +659,7 @@ int pm_solve(PmPlan* p, cudaStream_t s)
     cufftSetStream(p->c2r, s);
     if (cufftExecR2C(p->r2c, p->rho, p->spec) != CUFFT_SUCCESS)
         return 1;
-    if (p->gradient) {
+    if (p->gradient == 1) {
         count_launch();
         k_green_gradient<<<sms * 4, kThreads, 0, s>>>(p->spec, p->green, M, p->box, p->spec3);
         const size_t cells = static_cast<size_t>(M) * M * M;
@@ -552,8 +673,11 @@ int pm_solve(PmPlan* p, cudaStream_t s)
         k_apply_green<<<sms * 4, kThreads, 0, s>>>(p->spec, p->green, half);
         if (cufftExecC2R(p->c2r, p->spec, p->rho) != CUFFT_SUCCESS)
             return 2;
-        count_launch();
-        k_fd_gradient<<<sms * 4, kThreads, 0, s>>>(p->rho, M, static_cast<float>(0.5 * M / p->box), p->force);
+        if (p->gradient == 0) {
+            count_launch();
+            k_fd_gradient<<<sms * 4, kThreads, 0, s>>>(p->rho, M, static_cast<float>(0.5 * M / p->box),
+                                                       p->force);
+        }
     }
     return 0;
 }
@@ -566,6 +690,15 @@ void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float
     int b = (n + kThreads / 4 - 1) / (kThreads / 4);  // four lanes per particle
     b = b < sm_count() * 8 ? b : sm_count() * 8;
     count_launch();
+    if (p->gradient == 2) {
+        if (p->order == 2)
+            k_interp_ad<2><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->rho, ax, ay, az);
+        else if (p->order == 3)
+            k_interp_ad<3><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->rho, ax, ay, az);
+        else
+            k_interp_ad<4><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->rho, ax, ay, az);
+        return;
+    }
     if (p->order == 2)
         k_interp<2><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->force, ax, ay, az);
     else if (p->order == 3)

@@ -302,7 +302,7 @@ bool resolve(const std::map<std::string, std::string>& kv, GravitySystem& sys, R
             }
         }
         if (const std::string* s = lookup(kv, {"treepm_gradient"})) {
-            c.treepm_gradient = *s == "spectral" ? 1 : 0;
+            c.treepm_gradient = *s == "spectral" ? 1 : (*s == "analytic" ? 2 : 0);
             c.treepm_window_floor = c.treepm_gradient ? 0.0f : 0.08f;
         }
     } else {

@@ -70,7 +70,10 @@ typedef struct bz_config {
     float treepm_r_cut_factor;     /* short-range cutoff r_cut = factor * r_s */
     int32_t treepm_assignment;     /* treepm_assignment: 0 cic, 1 tsc, 2 pcs */
     int32_t treepm_gradient;       /* 0 centred differences of the potential (reference),
-                                      1 spectral i k gradient fused with the Green's function */
+                                      1 spectral i k gradient fused with the Green's function
+                                      (three inverse transforms), 2 analytic differentiation:
+                                      one inverse transform to the potential, interpolated
+                                      with the gradient of the assignment weights */
     float treepm_window_floor;     /* lower bound of the deconvolution window (reference 0.08) */
     float treepm_node_size_factor; /* short range: tree nodes at least this many r_s across are
                                       never accepted as multipoles (0 = no cap) */
@@ -243,7 +246,8 @@ bz_status bz_force_errors(bz_handle* h, int32_t nsample, uint64_t seed, float* e
                           int32_t* idx, double* median, double* p99);
 
 /* Debug access to the PM mesh of the current state: which = 0 density after the deposit,
- * 1 potential after the solve (centred-difference mode only), 2/3/4 the x/y/z force mesh.
+ * 1 potential after the solve (gradient modes 0 and 2), 2/3/4 the x/y/z force mesh (modes 0
+ * and 1).
  * out holds grid^3 floats, index (z*M + y)*M + x. */
 bz_status bz_pm_mesh(bz_handle* h, int which, float* out);
 

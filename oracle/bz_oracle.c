@@ -1252,6 +1252,59 @@ static double pcs_w(double d)
         return (2.0 - a) * (2.0 - a) * (2.0 - a) / 6.0;
     return 0.0;
 }
+/* Derivatives of the assignment kernels with respect to the particle coordinate (cells). */
+static double cic_dw(double d) { return fabs(d) < 1.0 ? (d > 0.0 ? -1.0 : 1.0) : 0.0; }
+static double tsc_dw(double d)
+{
+    const double a = fabs(d), sg = d > 0.0 ? 1.0 : -1.0;
+    if (a < 0.5)
+        return -2.0 * d;
+    if (a < 1.5)
+        return -sg * (1.5 - a);
+    return 0.0;
+}
+static double pcs_dw(double d)
+{
+    const double a = fabs(d), sg = d > 0.0 ? 1.0 : -1.0;
+    if (a < 1.0)
+        return -2.0 * d + 1.5 * d * a;
+    if (a < 2.0)
+        return -sg * 0.5 * (2.0 - a) * (2.0 - a);
+    return 0.0;
+}
+/* Stencil weights and their derivatives d w / d s (s = coordinate in cells). */
+static void stencil_dp(double coord01, double inv_cell, int mesh, int order, int idx[4], double w[4],
+                       double dw[4])
+{
+    const double raw = coord01 * inv_cell;
+    const double s = raw - floor(raw / (double)mesh) * (double)mesh;
+    if (order == 2) {
+        const double fl = floor(s);
+        for (int k = 0; k < 2; ++k) {
+            idx[k] = wrapi((int)fl + k, mesh);
+            const double d = s - (fl + k);
+            w[k] = 1.0 - fabs(d);
+            dw[k] = cic_dw(d);
+        }
+    } else if (order == 3) {
+        const double c = floor(s + 0.5);
+        for (int k = 0; k < 3; ++k) {
+            idx[k] = wrapi((int)c - 1 + k, mesh);
+            const double d = s - (c - 1.0 + k);
+            w[k] = tsc_w(d);
+            dw[k] = tsc_dw(d);
+        }
+    } else {
+        const double fl = floor(s);
+        for (int k = 0; k < 4; ++k) {
+            idx[k] = wrapi((int)fl - 1 + k, mesh);
+            const double d = s - (fl - 1.0 + k);
+            w[k] = pcs_w(d);
+            dw[k] = pcs_dw(d);
+        }
+    }
+}
+
 static void stencil_p(double coord01, double inv_cell, int mesh, int order, int idx[4], double w[4])
 {
     const double raw = coord01 * inv_cell;
@@ -1280,7 +1333,9 @@ static void stencil_p(double coord01, double inv_cell, int mesh, int order, int 
 static inline double sinc(double v) { return fabs(v) < 1.0e-5 ? 1.0 : sin(v) / v; }
 
 /* Periodic PM accelerations.  order: 2/3/4; gradient: 0 centred differences of the potential
- * (TpmField.inl:48-89), 1 spectral i k (Nyquist derivative terms zero); floor_w: lower bound
+ * (TpmField.inl:48-89), 1 spectral i k (Nyquist derivative terms zero), 2 analytic
+ * differentiation (the potential interpolated with the gradient of the assignment weights;
+ * Hockney & Eastwood's "ad" scheme); floor_w: lower bound
  * of the deconvolution window.  density/phi (optional) receive the deposited density and
  * (centred-difference mode) the potential. */
 int or_pm_periodic(const float* pos4, int64_t n, int mesh, double box, double rsplit, int order,
@@ -1345,6 +1400,45 @@ int or_pm_periodic_at(const float* pos4, int64_t n, int mesh, double box, double
     double* field[3] = {NULL, NULL, NULL};
     for (int a = 0; a < 3; ++a)
         field[a] = (double*)malloc(sizeof(double) * (size_t)cells);
+    if (gradient == 2) {
+        /* analytic differentiation: the force is the gradient of the interpolated potential,
+         * a = sum_c psi_c grad W(x - x_c), with psi the inverse transform of the (negated)
+         * potential spectrum; one inverse transform instead of three */
+        double* q = (double*)malloc(sizeof(double) * 2 * (size_t)cells);
+        memcpy(q, sp, sizeof(double) * 2 * (size_t)cells);
+        or_fft3d(q, mesh, 1);
+        double* psi = (double*)malloc(sizeof(double) * (size_t)cells);
+        for (int64_t c = 0; c < cells; ++c)
+            psi[c] = q[2 * c];
+        free(q);
+        const int64_t nout = targets ? nt : n;
+#pragma omp parallel for schedule(static)
+        for (int64_t o = 0; o < nout; ++o) {
+            const int64_t i = targets ? targets[o] : o;
+            int ix[4], iy[4], iz[4];
+            double wx[4], wy[4], wz[4], dx[4], dy[4], dz[4];
+            stencil_dp(pos4[4 * i], inv, mesh, order, ix, wx, dx);
+            stencil_dp(pos4[4 * i + 1], inv, mesh, order, iy, wy, dy);
+            stencil_dp(pos4[4 * i + 2], inv, mesh, order, iz, wz, dz);
+            double acc[3] = {0, 0, 0};
+            for (int c = 0; c < order; ++c)
+                for (int b = 0; b < order; ++b)
+                    for (int a2 = 0; a2 < order; ++a2) {
+                        const double v = psi[(iz[c] * M + iy[b]) * M + ix[a2]];
+                        acc[0] += v * dx[a2] * wy[b] * wz[c];
+                        acc[1] += v * wx[a2] * dy[b] * wz[c];
+                        acc[2] += v * wx[a2] * wy[b] * dz[c];
+                    }
+            for (int a = 0; a < 3; ++a)
+                acc3[3 * o + a] = acc[a] * inv;
+        }
+        free(psi);
+        for (int a = 0; a < 3; ++a)
+            free(field[a]);
+        free(rho);
+        free(sp);
+        return 0;
+    }
     if (gradient == 0) {
         double* q = (double*)malloc(sizeof(double) * 2 * (size_t)cells);
         memcpy(q, sp, sizeof(double) * 2 * (size_t)cells);

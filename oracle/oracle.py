@@ -344,14 +344,17 @@ ASSIGNMENT_ORDER = {"cic": 2, "tsc": 3, "pcs": 4}
 
 
 def pm_periodic(pos4_, mesh, box, rsplit, want_fields=False, assignment="cic", spectral=False,
-                window_floor=0.08):
+                window_floor=0.08, gradient=None):
+    """Periodic PM accelerations; gradient: 0 centred differences, 1 spectral (spectral=True),
+    2 analytic differentiation of the assignment weights (overrides spectral when given)."""
     p = np.ascontiguousarray(pos4_, np.float32)
+    mode = gradient if gradient is not None else (1 if spectral else 0)
     acc = np.zeros(3 * len(p), np.float64)
     cells = mesh ** 3
     dens = np.zeros(cells, np.float64) if want_fields else None
     phi = np.zeros(cells, np.float64) if want_fields else None
     lib().or_pm_periodic(p, len(p), mesh, box, rsplit, ASSIGNMENT_ORDER[assignment],
-                         1 if spectral else 0, window_floor, acc,
+                         mode, window_floor, acc,
                          None if dens is None else dens.ctypes.data,
                          None if phi is None else phi.ctypes.data)
     if want_fields:
@@ -360,13 +363,14 @@ def pm_periodic(pos4_, mesh, box, rsplit, want_fields=False, assignment="cic", s
 
 
 def pm_periodic_at(pos4_, targets, mesh, box, rsplit, assignment="cic", spectral=False,
-                   window_floor=0.08):
+                   window_floor=0.08, gradient=None):
     """pm_periodic's mesh force interpolated only at the given particle indices."""
     p = np.ascontiguousarray(pos4_, np.float32)
+    mode = gradient if gradient is not None else (1 if spectral else 0)
     tg = np.ascontiguousarray(targets, np.int64)
     acc = np.zeros(3 * len(tg), np.float64)
     lib().or_pm_periodic_at(p, len(p), mesh, box, rsplit, ASSIGNMENT_ORDER[assignment],
-                            1 if spectral else 0, window_floor, tg.ctypes.data, len(tg), acc,
+                            mode, window_floor, tg.ctypes.data, len(tg), acc,
                             None, None)
     return acc.reshape(-1, 3)
 

@@ -38,51 +38,69 @@ def test_density_and_potential(gpu, oracle, mesh, assignment):
     assert np.abs(phi - ophi).max() / np.abs(ophi).max() < 1e-4
 
 
-@pytest.mark.parametrize("assignment", ["cic", "pcs"])
-def test_spectral_force_mesh(gpu, oracle, assignment):
-    """Fused Green x i k gradient: the interpolated mesh force matches the oracle."""
+@pytest.mark.parametrize("gradient", [1, 2])
+@pytest.mark.parametrize("assignment", ["cic", "tsc", "pcs"])
+def test_spectral_force_mesh(gpu, oracle, assignment, gradient):
+    """Mesh forces of the fused Green x i k gradient (1) and of analytic differentiation (2: the
+    potential interpolated with the gradient of the assignment weights) match the oracle."""
     n, mesh = 20_000, 32
     pos = _box_particles(n, 12)
     m = np.full(n, 1.0 / n, np.float32)
     rs = 1.25 / mesh
     with _engine(n, solver=1, box_length=1.0, treepm_grid_size=mesh, treepm_assignment=ASSIGN[assignment],
-                 treepm_gradient=1, treepm_window_floor=0.0, treepm_r_cut_factor=1e-3) as e:
+                 treepm_gradient=gradient, treepm_window_floor=0.0, treepm_r_cut_factor=1e-3) as e:
         e.set_state(pos, None, m)
         acc = e.accelerations().astype(np.float64)
-    ref = oracle.pm_periodic(oracle.pos4(pos, m), mesh, 1.0, rs, assignment=assignment, spectral=True,
-                             window_floor=0.0)
-    err = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
-    assert np.median(err) < 1e-5 and err.max() < 1e-3, (np.median(err), err.max())
+    ref = oracle.pm_periodic(oracle.pos4(pos, m), mesh, 1.0, rs, assignment=assignment,
+                             window_floor=0.0, gradient=gradient)
+    dev = np.linalg.norm(acc - ref, axis=1)
+    net = np.linalg.norm(ref, axis=1)
+    # FP32 transforms (cuFFT) against FP64 ones: 1e-5 relative, or 1e-5 of the rms mesh force
+    # for particles whose mesh force is far below it (the transforms' rounding is global)
+    rms = np.sqrt((net ** 2).mean())
+    assert np.median(dev / net) < 1e-5
+    assert (dev <= 1e-5 * np.maximum(net, rms)).all(), ((dev / np.maximum(net, rms)).max())
 
 
-@pytest.mark.parametrize("variant", ["reference", "production"])
+@pytest.mark.parametrize("variant", ["reference", "production", "analytic"])
 def test_treepm_forces_match_oracle(gpu, oracle, variant):
+    """reference: CIC, centred differences; production: PCS with the spectral gradient;
+    analytic: PCS with analytic differentiation of the assignment weights."""
     n = 16_384
     mesh = 32
     pos = _box_particles(n, 4)
     m = np.full(n, 1.0 / n, np.float32)
     rs = 1.25 / mesh
-    prod = variant == "production"
+    prod = variant != "reference"
+    grad = {"reference": 0, "production": 1, "analytic": 2}[variant]
     rcf = 5.5 if prod else 4.5
     rc = rcf * rs
     eps = 0.02 / mesh
-    kw = dict(treepm_assignment=2, treepm_gradient=1, treepm_window_floor=0.0) if prod else {}
+    kw = dict(treepm_assignment=2, treepm_gradient=grad, treepm_window_floor=0.0) if prod else {}
     with _engine(n, solver=1, box_length=1.0, treepm_grid_size=mesh, octree_softening=eps,
                  treepm_r_cut_factor=rcf, **kw) as e:
         e.set_state(pos, None, m)
         acc = e.accelerations().astype(np.float64)
     p4 = oracle.pos4(pos, m)
-    apm = oracle.pm_periodic(p4, mesh, 1.0, rs, assignment="pcs" if prod else "cic", spectral=prod,
+    apm = oracle.pm_periodic(p4, mesh, 1.0, rs, assignment="pcs" if prod else "cic", gradient=grad,
                              window_floor=0.0 if prod else 0.08)
     keys = oracle.morton63(pos.astype(np.float64), [0, 0, 0], 1.0)
     perm = oracle.stable_sort(keys)
     t = oracle.build_tree(keys[perm], p4[perm], leaf_cap=16)
-    w = oracle.walk(p4[perm], t, theta=0.5, eps=eps, rcut=rc, box=1.0, rsplit=rs)
-    asr = np.empty_like(w["acc"])
-    asr[perm] = w["acc"]
+    a_s, s_s = oracle.walk_targets(p4[perm], t, np.arange(n), theta=0.5, eps=eps, rcut=rc, box=1.0,
+                                   rsplit=rs, quadrupole=True)
+    asr = np.empty_like(a_s)
+    asr[perm] = a_s
+    asum = np.empty_like(s_s)
+    asum[perm] = s_s
     ref = apm + asr
-    err = np.linalg.norm(acc - ref, axis=1) / np.linalg.norm(ref, axis=1)
-    assert np.median(err) < 1e-5 and err.max() < 1e-3, (np.median(err), err.max())
+    dev = np.linalg.norm(acc - ref, axis=1)
+    net = np.linalg.norm(ref, axis=1)
+    # 1e-5 relative, or the worst-case rounding of an FP32 sum of 64 terms of total magnitude
+    # S = sum |a_j| + |a_mesh| where the net force is a cancellation (see test_gpu_treepm_scale)
+    bound = 64.0 * 2.0 ** -24 * (asum + np.linalg.norm(apm, axis=1))
+    assert np.median(dev / net) < 1e-5
+    assert (dev <= np.maximum(1e-5 * net, bound)).all(), (dev / net).max()
 
 
 @pytest.mark.parametrize("schedule", [0, 2])

@@ -3,11 +3,13 @@ targets against the oracle's periodic PM interpolated at those targets plus the 
 walk of the groups that hold them (the sum the reference forms in treePmComputeAcceleration,
 engine/physics/treepm/short_range/TpmTreeForce.inl:9-25).
 
-The bound is 1e-5 relative per target.  The engine sums a target's pair and node terms in FP32
-(compensated), the oracle in FP64, so the two differ by a small multiple of the FP32 rounding
-of the terms, which scales with the sum of their magnitudes S = sum |a_j| + |a_mesh|, not with
-the net force.  A target whose net force is a cancellation (kappa = S / |a| above 20) is held
-to 1e-6 of S instead; the test reports how many targets that is."""
+The bound is 1e-5 relative per target, or the FP32 rounding bound of the engine's sums where
+that is larger.  The engine sums a target's pair terms in FP32 (a tile of up to 128 listed
+sources at a time, the tiles combined with a two-sum), the oracle in FP64; the difference is
+bounded by a multiple of 2^-24 of the sum of the magnitudes of the terms, S = sum |a_j| +
+|a_mesh|, not of the net force |a|.  Where the net force is a cancellation (kappa = S / |a|
+large) 1e-5 |a| can lie below that bound; those targets are held to 64 * 2^-24 * S (the
+worst-case rounding of an FP32 sum of 64 terms) and counted in the output."""
 import numpy as np
 import pytest
 
@@ -27,7 +29,7 @@ CASES = {
                       floor=0.0, cap=0.5, order=1),
 }
 ASSIGN_NAME = {0: "cic", 1: "tsc", 2: "pcs"}
-KAPPA = 20.0
+FP32_SUM_BOUND = 64.0 * 2.0 ** -24
 
 
 @pytest.mark.parametrize("case", list(CASES))
@@ -77,9 +79,11 @@ def test_treepm_parity_at_benchmark_scale(gpu, oracle, case):
     net = np.linalg.norm(ref, axis=1)
     rel = dev / net
     kappa = scale / net
-    cancel = kappa > KAPPA
+    bound = FP32_SUM_BOUND * scale
+    held = 1e-5 * net < bound  # targets where the FP32 rounding bound exceeds 1e-5 |a|
     print(f"{case}: median rel {np.median(rel):.2e}, max rel {rel.max():.2e} (kappa {kappa[rel.argmax()]:.1f}), "
-          f"max dev/S {(dev / scale).max():.2e}, {int(cancel.sum())} of {len(tg)} targets with kappa > {KAPPA:g}")
+          f"max dev/S {(dev / scale).max():.2e}, {int((rel > 1e-5).sum())} of {len(tg)} targets above "
+          f"1e-5, {int(held.sum())} with kappa > {1e-5 / FP32_SUM_BOUND:.1f}")
     assert np.median(rel) < 1e-6
-    assert rel[~cancel].max() < 1e-5, (rel[~cancel].max(), kappa[~cancel][rel[~cancel].argmax()])
-    assert (dev[cancel] <= 1e-6 * scale[cancel]).all()
+    assert (dev <= np.maximum(1e-5 * net, bound)).all(), \
+        (rel.max(), kappa[rel.argmax()], (dev / scale).max())
