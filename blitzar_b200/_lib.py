@@ -29,7 +29,7 @@ EXPORTS = (
     "bz_learn_set", "bz_learn_get", "bz_learn_enable", "bz_learn_forward", "bz_learn_gradient",
     "bz_set_ensemble", "bz_adaptive_levels", "bz_adaptive_updates", "bz_set_mesh_schedule",
     "bz_walk_blocks_per_sm", "bz_set_state_acc", "bz_get_state_acc", "bz_set_state_acc_f64",
-    "bz_get_state_acc_f64", "bz_walk_counts",
+    "bz_get_state_acc_f64", "bz_walk_counts", "bz_pm_grid",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -64,6 +64,7 @@ class BzConfig(C.Structure):
         ("walk_group_size", C.c_int32),
         ("adaptive_max_level", C.c_int32),
         ("adaptive_eta", C.c_float),
+        ("treepm_cell_floor", C.c_float),
     ]
 
 
@@ -104,6 +105,7 @@ def load():
     L.bz_force_errors.argtypes = [_vp, C.c_int32, C.c_uint64, _vp, _vp, C.POINTER(C.c_double),
                                   C.POINTER(C.c_double)]
     L.bz_pm_mesh.argtypes = [_vp, C.c_int, _vp]
+    L.bz_pm_grid.argtypes = [_vp, _vp]
     L.bz_particle_count.argtypes = [_vp]
     L.bz_particle_count.restype = C.c_size_t
     L.bz_device_bytes.argtypes = [_vp]
@@ -426,10 +428,16 @@ class Engine:
         return dict(median=med.value, p99=p99.value, errs=errs, idx=idx)
 
     def pm_mesh(self, which):
-        M = self.cfg.treepm_grid_size
+        M = self.cfg.treepm_grid_size * (2 if self.cfg.box_length <= 0.0 else 1)
         out = np.empty(M ** 3, np.float32)
         self._check(self.L.bz_pm_mesh(self.h, which, _ptr(out)), "bz_pm_mesh")
         return out
+
+    def pm_grid(self):
+        """Mesh grid of the last force evaluation: dict(origin, cell, rsplit, rcut)."""
+        v = np.zeros(6, np.float64)
+        self._check(self.L.bz_pm_grid(self.h, _ptr(v)), "bz_pm_grid")
+        return dict(origin=v[:3].copy(), cell=v[3], rsplit=v[4], rcut=v[5])
 
     def launches_per_step(self):
         k = C.c_uint64(0)

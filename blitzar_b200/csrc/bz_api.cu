@@ -84,6 +84,7 @@ struct bz_handle {
     TreeArrays tree{};
     GroupTable groups{};
     PmPlan* pm = nullptr;
+    IsoGrid* iso = nullptr;  // isolated TreePM: grid of the current evaluation (device)
     int spill_slots = 0;
     size_t bytes = 0;
     std::vector<void*> allocations;
@@ -157,6 +158,8 @@ template <class T> bool dalloc(bz_handle* h, T** p, size_t count)
 }
 
 bool periodic(const bz_handle* h) { return h->cfg.solver == BZ_SOLVER_TREEPM && h->cfg.box_length > 0.0; }
+// Open-boundary TreePM: the reference's GPU TreePM on a doubled, particle-centred mesh.
+bool isolated(const bz_handle* h) { return h->cfg.solver == BZ_SOLVER_TREEPM && h->cfg.box_length <= 0.0; }
 
 float rsplit_len(const bz_handle* h)
 {
@@ -192,7 +195,14 @@ WalkParams walk_params(const bz_handle* h, bool want_pot)
     p.quadrupole = h->cfg.multipole_order >= 2 ? 1 : 0;
     p.want_pot = want_pot ? 1 : 0;
     p.max_acc = h->cfg.physics_max_acceleration;
-    if (h->cfg.solver == BZ_SOLVER_TREEPM) {
+    if (isolated(h)) {
+        // split scale, cutoff and node cap follow the mesh cell of each evaluation: the walk
+        // reads them from the device-held grid (the values here only select its variant)
+        p.rsplit = 1.0f;
+        p.rcut2 = 1.0f;
+        p.box = 0.0f;
+        p.iso = h->iso;
+    } else if (h->cfg.solver == BZ_SOLVER_TREEPM) {
         const float rs = rsplit_len(h);
         const float rc = h->cfg.treepm_r_cut_factor * rs;
         p.rsplit = rs;
@@ -242,6 +252,11 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
 {
     const int n = static_cast<int>(h->n);
     DeviceBuffers& d = h->d;
+    // isolated TreePM: this evaluation's mesh grid, from the bounds the ordering just reduced
+    if (isolated(h))
+        launch_iso_grid(d.box, h->cfg.treepm_grid_size, h->cfg.treepm_cell_floor,
+                        h->cfg.octree_softening, h->cfg.treepm_r_split_cells, h->cfg.treepm_r_cut_factor,
+                        h->cfg.treepm_node_size_factor, h->iso, h->stream);
     // TreePM: the mesh leg needs only the ordered positions, so it runs on a second stream
     // while this one builds the tree and walks; joined before the kick
     const bool overlap = mesh_concurrent(h);
@@ -324,7 +339,8 @@ void enqueue_step(bz_handle* h)
     const int n = static_cast<int>(h->n);
     DeviceBuffers& d = h->d;
     double* const* s = d.st[h->cur];
-    const bool early = mesh_concurrent(h) && h->mesh_overlap == 2;
+    // (the isolated mesh's grid needs the new bounds first: no early fork there)
+    const bool early = mesh_concurrent(h) && h->mesh_overlap == 2 && !isolated(h);
     launch_kick_drift(s[0], s[1], s[2], s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt,
                       periodic(h) ? h->cfg.box_length : 0.0, nullptr, h->stream,
                       early ? d.mass[h->cur] : nullptr, early ? d.pos4_drift : nullptr);
@@ -524,6 +540,7 @@ bz_status bz_config_init(bz_config* c)
     c->treepm_gradient = 0;
     c->treepm_window_floor = 0.08f;
     c->treepm_node_size_factor = 0.0f;
+    c->treepm_cell_floor = 0.25f;  // the reference's isolated-mesh cell floor (TpmGridBuild.inl:100)
     c->box_length = 0.0;
     c->key_mode = BZ_KEYS_PRODUCTION;
     c->device = 0;
@@ -591,7 +608,16 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     h->cfg = *cfg;
     h->device = cfg->device;
     h->capacity = capacity;
-    if (cfg->solver == BZ_SOLVER_TREEPM) {
+    if (cfg->solver == BZ_SOLVER_TREEPM && cfg->box_length <= 0.0) {
+        // isolated mesh of 2G cells, G = treepm_grid_size
+        if (cfg->treepm_grid_size < 8 || cfg->treepm_grid_size > 1024 || !(cfg->treepm_r_split_cells > 0.0f) ||
+            !(cfg->treepm_r_cut_factor > 0.0f) || !(cfg->treepm_cell_floor > 0.0f) ||
+            cfg->treepm_assignment < 0 || cfg->treepm_assignment > 2 || cfg->treepm_gradient < 0 ||
+            cfg->treepm_gradient > 2 || cfg->treepm_node_size_factor < 0.0f) {
+            delete h;
+            return BZ_INVALID_ARGUMENT;
+        }
+    } else if (cfg->solver == BZ_SOLVER_TREEPM) {
         const int M = cfg->treepm_grid_size;
         if (cfg->box_length <= 0.0 || M < 8 || (M & (M - 1)) != 0 || cfg->treepm_r_split_cells <= 0.0f ||
             cfg->treepm_r_cut_factor <= 0.0f || cfg->treepm_assignment < 0 || cfg->treepm_assignment > 2 ||
@@ -686,9 +712,21 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     cudaMemsetAsync(d.err, 0, sizeof(int), h->stream);
     if (cfg->solver == BZ_SOLVER_TREEPM) {
         int perr = 0;
-        h->pm = pm_create(cfg->treepm_grid_size, cfg->box_length, rsplit_len(h),
-                          cfg->treepm_assignment + 2, cfg->treepm_gradient,
-                          cfg->treepm_window_floor, h->stream, &perr);
+        if (isolated(h)) {
+            void* g = nullptr;
+            if (cudaMalloc(&g, sizeof(IsoGrid)) != cudaSuccess) {
+                bz_destroy(h);
+                return BZ_OUT_OF_MEMORY;
+            }
+            h->allocations.push_back(g);
+            h->iso = static_cast<IsoGrid*>(g);
+            h->pm = pm_create(2 * cfg->treepm_grid_size, 0.0, 0.0, cfg->treepm_assignment + 2,
+                              cfg->treepm_gradient, cfg->treepm_window_floor, h->stream, &perr, h->iso);
+        } else {
+            h->pm = pm_create(cfg->treepm_grid_size, cfg->box_length, rsplit_len(h),
+                              cfg->treepm_assignment + 2, cfg->treepm_gradient,
+                              cfg->treepm_window_floor, h->stream, &perr);
+        }
         if (!h->pm) {
             bz_destroy(h);
             return BZ_OUT_OF_MEMORY;
@@ -1736,7 +1774,7 @@ bz_status bz_learn_generate(bz_handle* h, int64_t nsamples, uint64_t seed, float
 {
     if (!h || nsamples <= 0 || !x6 || !y3)
         return BZ_INVALID_ARGUMENT;
-    if (h->cfg.solver != BZ_SOLVER_TREEPM || !h->pm)
+    if (h->cfg.solver != BZ_SOLVER_TREEPM || !h->pm || isolated(h))
         return fail(h, BZ_UNSUPPORTED, "bz_learn_generate: residuals are defined for the periodic TreePM solver");
     cudaSetDevice(h->device);
     const int M = h->cfg.treepm_grid_size;
@@ -2117,7 +2155,11 @@ bz_status bz_pm_mesh(bz_handle* h, int which, float* out)
     bz_status s = ensure_forces(h);
     if (s != BZ_OK)
         return s;
-    const size_t M = static_cast<size_t>(h->cfg.treepm_grid_size);
+    const size_t M = static_cast<size_t>(h->cfg.treepm_grid_size) * (isolated(h) ? 2 : 1);
+    if (isolated(h))  // the grid of the current state (the one its forces were computed on)
+        launch_iso_grid(h->d.box, h->cfg.treepm_grid_size, h->cfg.treepm_cell_floor,
+                        h->cfg.octree_softening, h->cfg.treepm_r_split_cells, h->cfg.treepm_r_cut_factor,
+                        h->cfg.treepm_node_size_factor, h->iso, h->stream);
     pm_deposit(h->pm, h->d.pos4, static_cast<int>(h->n), h->stream);
     if (which == 0) {
         cudaMemcpyAsync(out, pm_mesh(h->pm), M * M * M * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
@@ -2137,6 +2179,27 @@ bz_status bz_pm_mesh(bz_handle* h, int which, float* out)
         return s;
     for (size_t c = 0; c < f.size(); ++c)
         out[c] = which == 2 ? f[c].x : (which == 3 ? f[c].y : f[c].z);
+    return BZ_OK;
+}
+
+bz_status bz_pm_grid(bz_handle* h, double* out6)
+{
+    if (!h || !out6 || h->cfg.solver != BZ_SOLVER_TREEPM)
+        return BZ_INVALID_ARGUMENT;
+    if (isolated(h)) {
+        cudaSetDevice(h->device);
+        IsoGrid g{};
+        if (cudaMemcpy(&g, h->iso, sizeof(g), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return fail(h, BZ_CUDA_ERROR, "bz_pm_grid");
+        const float rc = std::sqrt(g.rcut2);
+        const double v[6] = {g.origin[0], g.origin[1], g.origin[2], g.h, g.rsplit, rc};
+        std::copy(v, v + 6, out6);
+        return BZ_OK;
+    }
+    const double cell = h->cfg.box_length / h->cfg.treepm_grid_size;
+    const float rs = rsplit_len(h);
+    const double v[6] = {0.0, 0.0, 0.0, cell, rs, h->cfg.treepm_r_cut_factor * rs};
+    std::copy(v, v + 6, out6);
     return BZ_OK;
 }
 

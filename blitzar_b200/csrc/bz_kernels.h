@@ -132,6 +132,7 @@ void launch_reference_leaf(const float* x, const float* y, const float* z, const
                            const uint32_t* sorted_index, int n, float* hot8, cudaStream_t s);
 
 // ---------------------------------------------------------------- walk (bz_walk.cu)
+struct IsoGrid;
 struct WalkParams {
     float theta2;
     float eps2;
@@ -148,6 +149,7 @@ struct WalkParams {
                                   // for kernels of a concurrent stream); 0 = as many as fit
     float max_acc;                // acceleration clamp of the walk's sum (and of the total)
     int clamp_total;              // the output already holds the mesh force: clamp the sum
+    const IsoGrid* iso;           // isolated TreePM: rsplit, rcut2, max_node_size read here
 };
 // ---------------------------------------------------------------- target groups (bz_groups.cu)
 constexpr int kGroupMax = 32;  // largest walk group (one warp)
@@ -192,10 +194,29 @@ void launch_reference_walk(const float4* pos_orig, const float4* pos_sorted,
 
 // ---------------------------------------------------------------- PM (bz_pm.cu)
 struct PmPlan;
-// order: 2 CIC, 3 TSC, 4 PCS; gradient: 0 centred differences of phi, 1 spectral (i k);
-// window_floor: lower bound of the deconvolution window (the reference uses 0.08).
+// Grid of the isolated (open-boundary) mesh, recomputed on the device for every force
+// evaluation from the particles' bounds (the reference's TpmGridBuild.inl:98-171): a cubic
+// mesh of `mesh` = 2G cells of size h = max(cell_floor, extent / (G - 2)), centred on the
+// bounds; the split scale and cutoff follow h.
+struct IsoGrid {
+    float origin[3];
+    float h;
+    float inv_h;
+    float rsplit;
+    float rcut2;
+    float max_node_size;
+};
+// order: 2 CIC, 3 TSC, 4 PCS; gradient: 0 centred differences of phi, 1 spectral (i k), 2
+// analytic differentiation; window_floor: lower bound of the deconvolution window (the
+// reference uses 0.08).  iso != NULL: isolated mesh whose grid the device holds at iso (box
+// and rsplit unused); the Green's function is then evaluated in the solve, not tabulated.
 PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, double window_floor,
-                  cudaStream_t s, int* cuda_err);
+                  cudaStream_t s, int* cuda_err, const IsoGrid* iso = nullptr);
+// Isolated grid from the FP64 bounding box of the positions: grid_half = G, r_split_cells and
+// r_cut_factor in units of the cell, node_size_factor in units of r_s.
+void launch_iso_grid(const BoxF64* box, int grid_half, float cell_floor, float softening,
+                     float r_split_cells, float r_cut_factor, float node_size_factor, IsoGrid* out,
+                     cudaStream_t s);
 void pm_destroy(PmPlan* p);
 size_t pm_bytes(const PmPlan* p);
 // Deposit, FFT Poisson solve with split + deconvolution, then interpolate the centred-

@@ -48,6 +48,7 @@ struct PmPlan {
     float* green = nullptr;           // M*M*(M/2+1), computed in FP64
     cufftHandle r2c = 0, c2r = 0;
     size_t bytes = 0;
+    const IsoGrid* iso = nullptr;     // isolated mesh: grid on the device, Green in the solve
 };
 
 namespace {
@@ -78,7 +79,21 @@ __device__ __forceinline__ float pcs_w(float d)
     return 0.0f;
 }
 
-// Stencil of order P along one axis: first (unwrapped) node index and P weights.
+// Mesh frame of a plan: periodic meshes start at 0 with a fixed cell; an isolated mesh reads
+// its origin and cell from the device-held grid of the current force evaluation.
+struct MeshFrame {
+    float ox, oy, oz, inv_h;
+};
+__device__ __forceinline__ MeshFrame mesh_frame(const IsoGrid* iso, float inv_h)
+{
+    if (iso)
+        return MeshFrame{iso->origin[0], iso->origin[1], iso->origin[2], iso->inv_h};
+    return MeshFrame{0.0f, 0.0f, 0.0f, inv_h};
+}
+
+// Stencil of order P along one axis: first (unwrapped) node index and P weights.  coord is
+// the position relative to the mesh origin; for an isolated mesh the particles lie in its
+// central half, so the periodic fold below never applies there.
 template <int P>
 __device__ __forceinline__ int stencil(float coord, float inv_h, int mesh, float* w)
 {
@@ -114,7 +129,7 @@ __device__ __forceinline__ float tsc_dw(float d)
     if (a < 0.5f)
         return -2.0f * d;
     if (a < 1.5f)
-        return copysignf(a - 1.5f, d);
+        return -copysignf(1.5f - a, d);  // -(1.5 - |d|) sign(d)
     return 0.0f;
 }
 __device__ __forceinline__ float pcs_dw(float d)
@@ -124,7 +139,7 @@ __device__ __forceinline__ float pcs_dw(float d)
         return d * (1.5f * a - 2.0f);
     if (a < 2.0f) {
         const float t = 2.0f - a;
-        return copysignf(-0.5f * t * t, d);
+        return -copysignf(0.5f * t * t, d);  // -(2 - |d|)^2 / 2 sign(d)
     }
     return 0.0f;
 }
@@ -185,9 +200,13 @@ __device__ __forceinline__ float column_weight(const float* w, int q)
 
 template <int P>
 __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __restrict__ pos4, int n,
-                                                             int chunk, int mesh, float inv_h,
-                                                             float inv_h3, float* __restrict__ rho)
+                                                             int chunk, int mesh, float inv_h_fixed,
+                                                             float inv_h3_fixed, const IsoGrid* iso,
+                                                             float* __restrict__ rho)
 {
+    const MeshFrame fr = mesh_frame(iso, inv_h_fixed);
+    const float inv_h = fr.inv_h;
+    const float inv_h3 = iso ? 1.0f / (iso->h * iso->h * iso->h) : inv_h3_fixed;
     // The tile accumulates in 32-bit fixed point: integer shared-memory atomics are native and
     // about three times the rate of float ones, and integer sums are exact and independent of
     // the order of the additions.  The block's scale 2^k keeps any cell sum below 2^31 / 1.01: a
@@ -212,8 +231,8 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
         float w[P];
-        const int b[3] = {stencil<P>(p.x, inv_h, mesh, w), stencil<P>(p.y, inv_h, mesh, w),
-                          stencil<P>(p.z, inv_h, mesh, w)};
+        const int b[3] = {stencil<P>(p.x - fr.ox, inv_h, mesh, w), stencil<P>(p.y - fr.oy, inv_h, mesh, w),
+                          stencil<P>(p.z - fr.oz, inv_h, mesh, w)};
         for (int a = 0; a < 3; ++a) {
             lo[a] = min(lo[a], b[a]);
             hi[a] = max(hi[a], b[a] + P - 1);
@@ -253,9 +272,9 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
         float wx[P], wy[P], wz[P];
-        const int bx = stencil<P>(p.x, inv_h, mesh, wx);
-        const int by = stencil<P>(p.y, inv_h, mesh, wy);
-        const int bz = stencil<P>(p.z, inv_h, mesh, wz);
+        const int bx = stencil<P>(p.x - fr.ox, inv_h, mesh, wx);
+        const int by = stencil<P>(p.y - fr.oy, inv_h, mesh, wy);
+        const int bz = stencil<P>(p.z - fr.oz, inv_h, mesh, wz);
         const float m = p.w * inv_h3;
 #pragma unroll
         for (int c = 0; c < P; ++c)
@@ -348,6 +367,89 @@ __global__ void k_green_table(int mesh, double box, double rsplit, int order, do
     }
 }
 
+// Isolated mesh: the Green x window deconvolution x 1/M^3 of k_green_table, evaluated per
+// mode in FP64 from the device-held grid of this evaluation (its cell and split scale change
+// with the particles' extent).  gradient 1 writes the three spectral gradients as
+// k_green_gradient does; otherwise the potential spectrum is scaled in place.
+__global__ void __launch_bounds__(kThreads) k_green_iso(cufftComplex* __restrict__ spec, int mesh,
+                                                         int order, double floor_w, const IsoGrid* iso,
+                                                         int gradient, cufftComplex* __restrict__ out3)
+{
+    const int hx = mesh / 2 + 1;
+    const size_t total = static_cast<size_t>(mesh) * mesh * hx;
+    const double h = iso->h, rs = iso->rsplit;
+    const double ks = 2.0 * 3.14159265358979323846 / (mesh * h);
+    const double norm = 1.0 / (static_cast<double>(mesh) * mesh * mesh);
+    for (size_t idx = blockIdx.x * static_cast<size_t>(blockDim.x) + threadIdx.x; idx < total;
+         idx += static_cast<size_t>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(idx % hx);
+        const size_t pl = idx / hx;
+        const int y = static_cast<int>(pl % mesh);
+        const int z = static_cast<int>(pl / mesh);
+        const int sy = y <= mesh / 2 ? y : y - mesh;
+        const int sz = z <= mesh / 2 ? z : z - mesh;
+        const double kx = x * ks, ky = sy * ks, kz = sz * ks;
+        const double k2 = kx * kx + ky * ky + kz * kz;
+        float g = 0.0f;
+        if (k2 > 1.0e-12) {
+            const double s3 = sinc_d(0.5 * kx * h) * sinc_d(0.5 * ky * h) * sinc_d(0.5 * kz * h);
+            double W = 1.0;
+            for (int i = 0; i < 2 * order; ++i)
+                W *= s3;
+            if (W < floor_w)
+                W = floor_w;
+            g = static_cast<float>(4.0 * 3.14159265358979323846 * exp(-k2 * rs * rs) / (k2 * W) * norm);
+        }
+        const cufftComplex c = spec[idx];
+        const float pr = c.x * g, pi = c.y * g;
+        if (gradient == 1) {
+            const int tx = x == mesh / 2 ? 0 : x;
+            const int ty = y == mesh / 2 ? 0 : sy;
+            const int tz = z == mesh / 2 ? 0 : sz;
+            const float k[3] = {static_cast<float>(tx * ks), static_cast<float>(ty * ks),
+                                static_cast<float>(tz * ks)};
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                cufftComplex o;
+                o.x = -k[a] * pi;
+                o.y = k[a] * pr;
+                out3[a * total + idx] = o;
+            }
+        } else {
+            spec[idx] = make_cuFloatComplex(pr, pi);
+        }
+    }
+}
+
+// Grid of an isolated mesh from the FP64 bounds of the positions (one thread).  The formulas
+// and their FP32 rounding are the reference's (TpmGridBuild.inl:98-171): FP32 bounds, extent =
+// max(span x, y, z, softening), cell = max(cell_floor, extent / (G - 2)), the 2G mesh centred
+// on the bounds.
+__global__ void k_iso_grid(const BoxF64* box, int grid_half, float cell_floor, float softening,
+                           float r_split_cells, float r_cut_factor, float node_size_factor, IsoGrid* out)
+{
+    float mn[3], mx[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        mn[a] = static_cast<float>(double_from_ordered(box->mn[a]));
+        mx[a] = static_cast<float>(double_from_ordered(box->mx[a]));
+    }
+    const float extent = fmaxf(fmaxf(fmaxf(mx[0] - mn[0], mx[1] - mn[1]), mx[2] - mn[2]), softening);
+    const float h = fmaxf(cell_floor, extent / static_cast<float>(grid_half - 2));
+    const float half_extent = 0.5f * static_cast<float>(2 * grid_half) * h;
+    IsoGrid g;
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+        g.origin[a] = 0.5f * (mn[a] + mx[a]) - half_extent;
+    g.h = h;
+    g.inv_h = 1.0f / h;
+    g.rsplit = r_split_cells * h;
+    const float rc = r_cut_factor * g.rsplit;
+    g.rcut2 = rc * rc;
+    g.max_node_size = node_size_factor > 0.0f ? node_size_factor * g.rsplit : 0.0f;
+    *out = g;
+}
+
 __global__ void __launch_bounds__(kThreads) k_apply_green(cufftComplex* __restrict__ spec,
                                                            const float* __restrict__ green,
                                                            size_t total)
@@ -395,14 +497,22 @@ __global__ void __launch_bounds__(kThreads) k_green_gradient(const cufftComplex*
     }
 }
 
-// Centred-difference gradient of phi into the interleaved force mesh (reference mode).
+// Centred-difference gradient of phi into the interleaved force mesh (reference mode).  An
+// isolated mesh (iso != NULL) takes its cell from the device-held grid and, as the reference's
+// non-periodic gradient does (TpmFft.inl:108-141), leaves its outer layer of cells at zero.
 __global__ void __launch_bounds__(kThreads) k_fd_gradient(const float* __restrict__ phi, int mesh,
-                                                           float half_inv_h, float4* __restrict__ force)
+                                                           float half_inv_h_fixed, const IsoGrid* iso,
+                                                           float4* __restrict__ force)
 {
     const size_t M = static_cast<size_t>(mesh), total = M * M * M;
+    const float half_inv_h = iso ? 0.5f * iso->inv_h : half_inv_h_fixed;
     for (size_t i = blockIdx.x * static_cast<size_t>(kThreads) + threadIdx.x; i < total;
          i += static_cast<size_t>(gridDim.x) * kThreads) {
         const int x = static_cast<int>(i % M), y = static_cast<int>((i / M) % M), z = static_cast<int>(i / (M * M));
+        if (iso && (x == 0 || y == 0 || z == 0 || x == mesh - 1 || y == mesh - 1 || z == mesh - 1)) {
+            force[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            continue;
+        }
         const int xp = x + 1 == mesh ? 0 : x + 1, xm = x == 0 ? mesh - 1 : x - 1;
         const int yp = y + 1 == mesh ? 0 : y + 1, ym = y == 0 ? mesh - 1 : y - 1;
         const int zp = z + 1 == mesh ? 0 : z + 1, zm = z == 0 ? mesh - 1 : z - 1;
@@ -430,10 +540,13 @@ __global__ void __launch_bounds__(kThreads) k_pack_force(const float* __restrict
 // by L1 wavefronts).
 template <int P>
 __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ pos4, int n, int mesh,
-                                                      float inv_h, const float4* __restrict__ force,
+                                                      float inv_h_fixed, const IsoGrid* iso,
+                                                      const float4* __restrict__ force,
                                                       float* __restrict__ ax, float* __restrict__ ay,
                                                       float* __restrict__ az)
 {
+    const MeshFrame fr = mesh_frame(iso, inv_h_fixed);
+    const float inv_h = fr.inv_h;
     const size_t M = static_cast<size_t>(mesh);
     const int q = threadIdx.x & 3;
     // each block walks one contiguous (Morton-ordered) range, 64 particles at a time, so that
@@ -448,9 +561,9 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
         if (i < stop && q < P) {
             const float4 p = pos4[i];
             float wx[P], wy[P], wz[P];
-            const int bx = stencil<P>(p.x, inv_h, mesh, wx);
-            const int by = stencil<P>(p.y, inv_h, mesh, wy);
-            const int bz = stencil<P>(p.z, inv_h, mesh, wz);
+            const int bx = stencil<P>(p.x - fr.ox, inv_h, mesh, wx);
+            const int by = stencil<P>(p.y - fr.oy, inv_h, mesh, wy);
+            const int bz = stencil<P>(p.z - fr.oz, inv_h, mesh, wz);
             const float wq = column_weight<P>(wx, q);
             const int xs = wrap1(bx + q, mesh);
 #pragma unroll
@@ -487,10 +600,13 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
 // float per cell, so a quad reads 16-byte row segments.
 template <int P>
 __global__ void __launch_bounds__(kThreads) k_interp_ad(const float4* __restrict__ pos4, int n, int mesh,
-                                                         float inv_h, const float* __restrict__ phi,
+                                                         float inv_h_fixed, const IsoGrid* iso,
+                                                         const float* __restrict__ phi,
                                                          float* __restrict__ ax, float* __restrict__ ay,
                                                          float* __restrict__ az)
 {
+    const MeshFrame fr = mesh_frame(iso, inv_h_fixed);
+    const float inv_h = fr.inv_h;
     const size_t M = static_cast<size_t>(mesh);
     const int q = threadIdx.x & 3;
     constexpr int kRound = (kThreads / 32) * 8;
@@ -503,9 +619,9 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad(const float4* __restrict
         if (i < stop && q < P) {
             const float4 p = pos4[i];
             float wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
-            const int bx = stencil_d<P>(p.x, inv_h, mesh, wx, dx);
-            const int by = stencil_d<P>(p.y, inv_h, mesh, wy, dy);
-            const int bz = stencil_d<P>(p.z, inv_h, mesh, wz, dz);
+            const int bx = stencil_d<P>(p.x - fr.ox, inv_h, mesh, wx, dx);
+            const int by = stencil_d<P>(p.y - fr.oy, inv_h, mesh, wy, dy);
+            const int bz = stencil_d<P>(p.z - fr.oz, inv_h, mesh, wz, dz);
             const float wq = column_weight<P>(wx, q);
             const float dq = column_weight<P>(dx, q);
             const int xs = wrap1(bx + q, mesh);
@@ -549,9 +665,10 @@ int sm_count()
 } // namespace
 
 PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, double window_floor,
-                  cudaStream_t s, int* cuda_err)
+                  cudaStream_t s, int* cuda_err, const IsoGrid* iso)
 {
     PmPlan* p = new PmPlan();
+    p->iso = iso;
     p->mesh = mesh;
     p->box = box;
     p->rsplit = rsplit;
@@ -563,7 +680,7 @@ PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, 
     *cuda_err = 0;
     bool ok = cudaMalloc(&p->rho, cells * sizeof(float)) == cudaSuccess &&
               cudaMalloc(&p->spec, half * sizeof(cufftComplex)) == cudaSuccess &&
-              cudaMalloc(&p->green, half * sizeof(float)) == cudaSuccess;
+              (iso || cudaMalloc(&p->green, half * sizeof(float)) == cudaSuccess);
     if (ok && p->gradient != 2)  // analytic differentiation needs no force mesh
         ok = cudaMalloc(&p->force, cells * sizeof(float4)) == cudaSuccess;
     if (ok && p->gradient == 1)
@@ -586,10 +703,12 @@ PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, 
     cufftGetSize(p->r2c, &ws1);
     cufftGetSize(p->c2r, &ws2);
     p->bytes = cells * (sizeof(float) + (p->gradient != 2 ? sizeof(float4) : 0)) +
-               half * (sizeof(cufftComplex) + sizeof(float)) +
+               half * (sizeof(cufftComplex) + (iso ? 0 : sizeof(float))) +
                (p->gradient == 1 ? 3 * (half * sizeof(cufftComplex) + cells * sizeof(float)) : 0) + ws1 + ws2;
-    count_launch();
-    k_green_table<<<sm_count() * 4, 256, 0, s>>>(mesh, box, rsplit, p->order, window_floor, p->green);
+    if (!iso) {
+        count_launch();
+        k_green_table<<<sm_count() * 4, 256, 0, s>>>(mesh, box, rsplit, p->order, window_floor, p->green);
+    }
     return p;
 }
 
@@ -618,7 +737,7 @@ void pm_deposit(PmPlan* p, const float4* pos4, int n, cudaStream_t s)
 {
     const int M = p->mesh;
     const size_t cells = static_cast<size_t>(M) * M * M;
-    const double h = p->box / M;
+    const double h = p->iso ? 1.0 : p->box / M;  // isolated: the kernels read the cell
     const float inv_h = static_cast<float>(1.0 / h);
     const float inv_h3 = static_cast<float>(1.0 / (h * h * h));
     cudaMemsetAsync(p->rho, 0, cells * sizeof(float), s);
@@ -626,11 +745,11 @@ void pm_deposit(PmPlan* p, const float4* pos4, int n, cudaStream_t s)
     const int b = (n + chunk - 1) / chunk;
     count_launch();
     if (p->order == 2)
-        k_deposit_tiled<2><<<b, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, inv_h3, p->rho);
+        k_deposit_tiled<2><<<b, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, inv_h3, p->iso, p->rho);
     else if (p->order == 3)
-        k_deposit_tiled<3><<<b, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, inv_h3, p->rho);
+        k_deposit_tiled<3><<<b, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, inv_h3, p->iso, p->rho);
     else
-        k_deposit_tiled<4><<<b, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, inv_h3, p->rho);
+        k_deposit_tiled<4><<<b, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, inv_h3, p->iso, p->rho);
 }
 
 int pm_deposit_chunk(const PmPlan* p, int n)
@@ -659,6 +778,27 @@ int pm_solve(PmPlan* p, cudaStream_t s)
     cufftSetStream(p->c2r, s);
     if (cufftExecR2C(p->r2c, p->rho, p->spec) != CUFFT_SUCCESS)
         return 1;
+    if (p->iso) {
+        count_launch();
+        k_green_iso<<<sms * 4, kThreads, 0, s>>>(p->spec, M, p->order, p->floor, p->iso, p->gradient,
+                                                 p->spec3);
+        const size_t cells = static_cast<size_t>(M) * M * M;
+        if (p->gradient == 1) {
+            for (int a = 0; a < 3; ++a)
+                if (cufftExecC2R(p->c2r, p->spec3 + a * half, p->field3 + a * cells) != CUFFT_SUCCESS)
+                    return 2;
+            count_launch();
+            k_pack_force<<<sms * 4, kThreads, 0, s>>>(p->field3, cells, p->force);
+            return 0;
+        }
+        if (cufftExecC2R(p->c2r, p->spec, p->rho) != CUFFT_SUCCESS)
+            return 2;
+        if (p->gradient == 0) {
+            count_launch();
+            k_fd_gradient<<<sms * 4, kThreads, 0, s>>>(p->rho, M, 0.0f, p->iso, p->force);
+        }
+        return 0;
+    }
     if (p->gradient == 1) {
         count_launch();
         k_green_gradient<<<sms * 4, kThreads, 0, s>>>(p->spec, p->green, M, p->box, p->spec3);
@@ -676,7 +816,7 @@ int pm_solve(PmPlan* p, cudaStream_t s)
         if (p->gradient == 0) {
             count_launch();
             k_fd_gradient<<<sms * 4, kThreads, 0, s>>>(p->rho, M, static_cast<float>(0.5 * M / p->box),
-                                                       p->force);
+                                                       nullptr, p->force);
         }
     }
     return 0;
@@ -686,25 +826,34 @@ void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float
                cudaStream_t s)
 {
     const int M = p->mesh;
-    const float inv_h = static_cast<float>(M / p->box);
+    const float inv_h = p->iso ? 1.0f : static_cast<float>(M / p->box);  // isolated: read on the device
     int b = (n + kThreads / 4 - 1) / (kThreads / 4);  // four lanes per particle
     b = b < sm_count() * 8 ? b : sm_count() * 8;
     count_launch();
     if (p->gradient == 2) {
         if (p->order == 2)
-            k_interp_ad<2><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->rho, ax, ay, az);
+            k_interp_ad<2><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->iso, p->rho, ax, ay, az);
         else if (p->order == 3)
-            k_interp_ad<3><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->rho, ax, ay, az);
+            k_interp_ad<3><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->iso, p->rho, ax, ay, az);
         else
-            k_interp_ad<4><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->rho, ax, ay, az);
+            k_interp_ad<4><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->iso, p->rho, ax, ay, az);
         return;
     }
     if (p->order == 2)
-        k_interp<2><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->force, ax, ay, az);
+        k_interp<2><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->iso, p->force, ax, ay, az);
     else if (p->order == 3)
-        k_interp<3><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->force, ax, ay, az);
+        k_interp<3><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->iso, p->force, ax, ay, az);
     else
-        k_interp<4><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->force, ax, ay, az);
+        k_interp<4><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->iso, p->force, ax, ay, az);
+}
+
+void launch_iso_grid(const BoxF64* box, int grid_half, float cell_floor, float softening,
+                     float r_split_cells, float r_cut_factor, float node_size_factor, IsoGrid* out,
+                     cudaStream_t s)
+{
+    count_launch();
+    k_iso_grid<<<1, 1, 0, s>>>(box, grid_half, cell_floor, softening, r_split_cells, r_cut_factor,
+                               node_size_factor, out);
 }
 
 int pm_forces(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float* az,

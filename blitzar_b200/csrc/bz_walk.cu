@@ -618,10 +618,18 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                                                        TreeArrays t, const int* __restrict__ gstart,
                                                        const int* __restrict__ groot,
                                                        const int* __restrict__ ngroups_ptr,
-                                                       WalkParams p, float inv_box,
+                                                       WalkParams p_in, float inv_box,
                                                        WalkOutputs o, unsigned* queue,
                                                        int* spill_base, int* err)
 {
+    // The isolated TreePM's split scale and cutoff follow its mesh cell, which the device
+    // recomputes from the particles' bounds for every evaluation: read them here.
+    WalkParams p = p_in;
+    if (!PERIODIC && SPLIT && p_in.iso != nullptr) {
+        p.rsplit = p_in.iso->rsplit;
+        p.rcut2 = p_in.iso->rcut2;
+        p.max_node_size = p_in.iso->max_node_size;
+    }
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     WarpSmem& w = reinterpret_cast<WarpSmem*>(smem_raw)[warp];

@@ -280,15 +280,45 @@ bool resolve(const std::map<std::string, std::string>& kv, GravitySystem& sys, R
     get_num(kv, {"physics_min_theta"}, c.physics_min_theta);
     if (rc.solver == "octree_reference") {
         c.solver = BZ_SOLVER_OCTREE_REFERENCE;
+    } else if (rc.treepm && !lookup(kv, {"treepm_box_length", "box_length"})) {
+        // the reference's TreePM keys (CfgEntriesCore.cpp:75-117, defaults CfgConfig.hpp:49-62)
+        // through the reference's setter: the isolated TreePM of octree_gpu
+        std::string model = "auto", layout = "auto", precision = "fp32", assignment = "cic";
+        bool local_grid = true, gravity_only = true;
+        int grid = 64, jacobi = 12, max_neighbors = 64, particle_limit = 0, dense = 64;
+        float cutoff = 1.0f;
+        if (const std::string* s = lookup(kv, {"treepm_model"}))
+            model = *s;
+        if (const std::string* s = lookup(kv, {"treepm_layout"}))
+            layout = *s;
+        if (const std::string* s = lookup(kv, {"treepm_precision"}))
+            precision = *s;
+        if (const std::string* s = lookup(kv, {"treepm_assignment"}))
+            assignment = *s;
+        if (const std::string* s = lookup(kv, {"treepm_local_grid"}))
+            local_grid = truthy(*s);
+        if (const std::string* s = lookup(kv, {"treepm_gravity_only_buffers"}))
+            gravity_only = truthy(*s);
+        get_num(kv, {"treepm_grid_size"}, grid);
+        get_num(kv, {"treepm_jacobi_iterations"}, jacobi);
+        get_num(kv, {"treepm_cutoff_factor"}, cutoff);
+        get_num(kv, {"treepm_max_local_neighbors"}, max_neighbors);
+        get_num(kv, {"treepm_particle_limit"}, particle_limit);
+        get_num(kv, {"treepm_dense_cell_threshold"}, dense);
+        sys.setTreePmParameters(true, model, layout, precision, assignment, local_grid, grid, jacobi,
+                                cutoff, max_neighbors, particle_limit, dense, gravity_only);
     } else if (rc.treepm) {
+        // this engine's periodic TreePM (a box length given): grid, split and cutoff in cells
         c.solver = BZ_SOLVER_TREEPM;
         get_num(kv, {"treepm_grid_size"}, c.treepm_grid_size);
         get_num(kv, {"treepm_r_split_cells"}, c.treepm_r_split_cells);
-        get_num(kv, {"treepm_r_cut_factor", "treepm_cutoff_factor"}, c.treepm_r_cut_factor);
+        get_num(kv, {"treepm_r_cut_factor"}, c.treepm_r_cut_factor);
         get_num(kv, {"treepm_node_size_factor"}, c.treepm_node_size_factor);
         get_num(kv, {"treepm_box_length", "box_length"}, c.box_length);
-        if (c.box_length <= 0.0)
-            c.box_length = 1.0;
+        if (c.box_length <= 0.0) {
+            err = "treepm box_length must be positive (omit it for the isolated TreePM)";
+            return false;
+        }
         if (const std::string* s = lookup(kv, {"treepm_assignment"})) {
             if (*s == "cic")
                 c.treepm_assignment = 0;
@@ -318,11 +348,11 @@ void print_json(const RunConfig& rc, const bz_config& c)
                 "\"physics_max_acceleration\": %.9g, \"treepm_grid_size\": %d, "
                 "\"treepm_r_split_cells\": %.9g, \"treepm_r_cut_factor\": %.9g, "
                 "\"treepm_assignment\": %d, \"treepm_gradient\": %d, \"box_length\": %.17g, "
-                "\"input\": \"%s\"}\n",
+                "\"treepm_cell_floor\": %.9g, \"input\": \"%s\"}\n",
                 c.solver, rc.integrator.c_str(), rc.dt, c.octree_theta, c.octree_softening,
                 c.leaf_capacity, c.multipole_order, c.physics_max_acceleration, c.treepm_grid_size,
                 c.treepm_r_split_cells, c.treepm_r_cut_factor, c.treepm_assignment,
-                c.treepm_gradient, c.box_length, rc.input.c_str());
+                c.treepm_gradient, c.box_length, c.treepm_cell_floor, rc.input.c_str());
 }
 
 } // namespace

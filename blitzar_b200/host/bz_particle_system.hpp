@@ -58,9 +58,74 @@ public:
         cfg_.physics_min_theta = min_theta;
         invalidate();
     }
-    // the periodic TreePM subset of setTreePmParameters (PhyParticleSystem.hpp:204-208)
-    void setTreePmParameters(int grid_size, float r_split_cells, float r_cut_factor,
-                             int assignment, int gradient, double box_length)
+    // setTreePmParameters with the reference's signature (PhyParticleSystem.hpp:204-207) and
+    // clamps (CudSolverConfiguration.inl:55-74), for the path of octree_gpu that integrates
+    // leapfrog (CudOctreeGpuIntegrators.inl:75-110), the integrator of this engine:
+    //   - TreePM runs when enabled and model != "exact_tree" (the reference's octree_gpu runs
+    //     TreePM for every other model when it integrates leapfrog, CudOctreeGpuUpdate.inl:37;
+    //     exact_tree names the CPU FP64 pairwise sum, so the octree solver stays);
+    //   - it is the reference's isolated TreePM: a mesh of 2 x clamp(gridSize, 32, 128) cells of
+    //     max(0.25, extent / (G - 2)) centred on the particles, cutoff clamp(cutoffFactor, 1, 2)
+    //     cells, r_s = cutoff / 4.5, CIC / TSC / PCS (any other name: CIC), centred differences
+    //     with the 0.08 window floor;
+    //   - layout, precision, localGrid, jacobiIterations, maxLocalNeighbors, particleLimit,
+    //     denseCellThreshold and gravityOnlyBuffers select the reference's memory layouts, its
+    //     CPU precision, its Euler-only local-grid and hybrid kernels and its finite-difference
+    //     fallback solver; the reference's leapfrog path does not read them and neither does
+    //     this engine (they are kept, clamped as the reference clamps them, for the getters).
+    // Returns true (every combination maps); it takes effect at the next update().
+    bool setTreePmParameters(bool enabled, const std::string& model, const std::string& layout,
+                             const std::string& precision, const std::string& assignment,
+                             bool localGrid, int gridSize, int jacobiIterations, float cutoffFactor,
+                             int maxLocalNeighbors, int particleLimit, int denseCellThreshold,
+                             bool gravityOnlyBuffers)
+    {
+        tpm_.enabled = enabled;
+        tpm_.model = model;
+        tpm_.layout = layout;
+        tpm_.precision = precision == "fp64" ? "fp64" : "fp32";
+        tpm_.assignment = assignment == "tsc" || assignment == "pcs" ? assignment : "cic";
+        tpm_.localGrid = localGrid;
+        tpm_.gridSize = clampi(gridSize, 32, 128);
+        tpm_.jacobiIterations = clampi(jacobiIterations, 4, 64);
+        tpm_.cutoffFactor = cutoffFactor < 1.0f ? 1.0f : (cutoffFactor > 2.0f ? 2.0f : cutoffFactor);
+        tpm_.maxLocalNeighbors = clampi(maxLocalNeighbors, 0, 256);
+        tpm_.particleLimit = particleLimit > 0 ? particleLimit : 0;
+        tpm_.denseCellThreshold = denseCellThreshold > 1 ? denseCellThreshold : 1;
+        tpm_.gravityOnlyBuffers = gravityOnlyBuffers;
+        if (!enabled || model == "exact_tree") {
+            cfg_.solver = BZ_SOLVER_OCTREE;
+        } else {
+            cfg_.solver = BZ_SOLVER_TREEPM;
+            cfg_.box_length = 0.0;  // isolated mesh
+            cfg_.treepm_grid_size = tpm_.gridSize;
+            cfg_.treepm_cell_floor = 0.25f;
+            cfg_.treepm_r_split_cells = tpm_.cutoffFactor / 4.5f;
+            cfg_.treepm_r_cut_factor = 4.5f;
+            cfg_.treepm_assignment = tpm_.assignment == "tsc" ? 1 : (tpm_.assignment == "pcs" ? 2 : 0);
+            cfg_.treepm_gradient = 0;
+            cfg_.treepm_window_floor = 0.08f;
+            cfg_.treepm_node_size_factor = 0.0f;
+        }
+        invalidate();
+        return true;
+    }
+    // the reference's TreePM settings as last set (getters of the same fields)
+    struct TreePmSettings {
+        bool enabled = false;
+        std::string model = "auto", layout = "auto", precision = "fp32", assignment = "cic";
+        bool localGrid = true;
+        int gridSize = 64, jacobiIterations = 12;
+        float cutoffFactor = 1.0f;
+        int maxLocalNeighbors = 64, particleLimit = 0, denseCellThreshold = 64;
+        bool gravityOnlyBuffers = true;
+    };
+    const TreePmSettings& treePmSettings() const { return tpm_; }
+
+    // the periodic TreePM of this engine (no counterpart in the reference's GPU solvers, whose
+    // periodic PM is the comoving PM-only cosmology): grid, split and cutoff in mesh cells
+    void setPeriodicTreePmParameters(int grid_size, float r_split_cells, float r_cut_factor,
+                                     int assignment, int gradient, double box_length)
     {
         cfg_.treepm_grid_size = grid_size;
         cfg_.treepm_r_split_cells = r_split_cells;
@@ -72,6 +137,7 @@ public:
         invalidate();
     }
     void setTreePmNodeSizeFactor(float f) { cfg_.treepm_node_size_factor = f; invalidate(); }
+    void setTreePmCellFloor(float f) { cfg_.treepm_cell_floor = f; invalidate(); }
     void setDevice(int device) { cfg_.device = device; invalidate(); }
     bz_config& config() { return cfg_; }
 
@@ -116,6 +182,7 @@ public:
     const std::string& lastError() const { return err_; }
 
 private:
+    static int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
     void invalidate()
     {
         if (h_) {
@@ -166,6 +233,7 @@ private:
 
     std::vector<Particle> particles_;
     bz_config cfg_{};
+    TreePmSettings tpm_;
     bz_handle* h_ = nullptr;
     std::string err_;
 };

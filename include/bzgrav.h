@@ -65,7 +65,11 @@ typedef struct bz_config {
     float physics_min_softening;   /* physics_min_softening */
     float physics_min_distance2;   /* physics_min_distance2 */
     float physics_min_theta;       /* physics_min_theta */
-    int32_t treepm_grid_size;      /* treepm_grid_size: PM mesh cells per side */
+    int32_t treepm_grid_size;      /* treepm_grid_size: PM mesh cells per side; with box_length
+                                      = 0 (isolated TreePM, the reference's GPU TreePM) the
+                                      mesh has 2 x this many cells per side, of size max(
+                                      treepm_cell_floor, extent / (grid - 2)), centred on the
+                                      particles and recomputed for every force evaluation */
     float treepm_r_split_cells;    /* Gaussian split scale r_s in mesh cells */
     float treepm_r_cut_factor;     /* short-range cutoff r_cut = factor * r_s */
     int32_t treepm_assignment;     /* treepm_assignment: 0 cic, 1 tsc, 2 pcs */
@@ -77,7 +81,8 @@ typedef struct bz_config {
     float treepm_window_floor;     /* lower bound of the deconvolution window (reference 0.08) */
     float treepm_node_size_factor; /* short range: tree nodes at least this many r_s across are
                                       never accepted as multipoles (0 = no cap) */
-    double box_length;             /* periodic box length (TreePM); 0 = open boundaries */
+    double box_length;             /* periodic box length (TreePM); 0 = open boundaries (TreePM:
+                                      the isolated doubled mesh) */
     int32_t key_mode;              /* bz_key_mode */
     int32_t device;                /* CUDA device ordinal */
     uint64_t stream;               /* cudaStream_t to run on, or 0 for a private stream */
@@ -86,6 +91,8 @@ typedef struct bz_config {
     int32_t adaptive_max_level;    /* adaptive(max_level): 0 = fixed steps; k > 0: power-of-two
                                       block steps dt / 2^l, l <= k (octree solver) */
     float adaptive_eta;            /* adaptive(eta): stable dt = eta * min(sqrt(eps/|a|), eps/|v|) */
+    float treepm_cell_floor;       /* isolated TreePM (box_length = 0): smallest mesh cell (the
+                                      reference's 0.25, TpmGridBuild.inl:100) */
 } bz_config;
 
 typedef struct bz_handle bz_handle;
@@ -246,10 +253,17 @@ bz_status bz_force_errors(bz_handle* h, int32_t nsample, uint64_t seed, float* e
                           int32_t* idx, double* median, double* p99);
 
 /* Debug access to the PM mesh of the current state: which = 0 density after the deposit,
- * 1 potential after the solve (gradient modes 0 and 2), 2/3/4 the x/y/z force mesh (modes 0
- * and 1).
+ * 1 potential after the solve (gradient modes 0 and 2; the negated potential, whose gradient is
+ * the acceleration), 2/3/4 the x/y/z force mesh (modes 0 and 1).  Isolated meshes have 2 grid
+ * cells per side.
  * out holds grid^3 floats, index (z*M + y)*M + x. */
 bz_status bz_pm_mesh(bz_handle* h, int which, float* out);
+
+/* Mesh grid of the last force evaluation (TreePM): out6 = {origin x, y, z, cell, r_s, r_cut}.
+ * Periodic: origin 0, cell = box / grid.  Isolated: the doubled mesh's grid, which follows the
+ * particles' bounds (TpmGridBuild.inl:98-171).  No counterpart in the reference's C ABI (its
+ * grid is internal). */
+bz_status bz_pm_grid(bz_handle* h, double* out6);
 
 /* Kernel launches of this library enqueued so far (cuFFT's own kernels excluded), and the
  * number one bz_step step enqueues. */

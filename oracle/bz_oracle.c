@@ -1507,6 +1507,214 @@ int or_pm_periodic_at(const float* pos4, int64_t n, int mesh, double box, double
 }
 
 /* ======================================================================================
+ * Isolated (open-boundary) PM of the reference's GPU TreePM: a cubic mesh of 2G cells, the
+ * periodic convolution isolated by the empty half of the doubled domain.
+ *   grid   : engine/physics/treepm/cuda/deposit/TpmGridBuild.inl:98-171 (FP32 bounds, cell =
+ *            max(cell_floor, extent / (G - 2)), extent = max(span x, y, z, softening), origin
+ *            centring the mesh on the bounds);
+ *   deposit: TpmDeposit.inl:9-61 (scaled coordinate clamped to [0, 2G - 1], nodes
+ *            floor(s + 0.5) - 2 .. + 2 clamped, kernel weights of TpmMath.inl:84-108);
+ *   solve  : TpmFft.inl:9-54 (phi_k = -4 pi e^{-k^2 r_s^2} rho_k / (k^2 max(W, floor)), W =
+ *            prod sinc^{2p}(k h / 2)), TpmFftRuntime.inl (C2R, / cells);
+ *   gradient 0: TpmFft.inl:108-141 (a = -(phi[i+1] - phi[i-1]) / 2h, outer cells zero);
+ *            1 spectral i k, 2 analytic differentiation (the engine's production options);
+ *   sample : TpmMath.inl:110-158 (the deposit's stencil).
+ * params8 (may be NULL) receives {cell, origin x, y, z, mesh, r_s (given), extent, 0}. */
+static double iso_w(double d, int order)
+{
+    return order == 2 ? (fabs(d) < 1.0 ? 1.0 - fabs(d) : 0.0) : (order == 3 ? tsc_w(d) : pcs_w(d));
+}
+static double iso_dw(double d, int order)
+{
+    return order == 2 ? cic_dw(d) : (order == 3 ? tsc_dw(d) : pcs_dw(d));
+}
+
+int or_pm_isolated(const float* pos4, int64_t n, int grid_half, float cell_floor, float softening,
+                   double rsplit_cells, int order, int gradient, double floor_w,
+                   const int64_t* targets, int64_t nt, double* acc3, double* params8,
+                   double* density, double* phi_out)
+{
+    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int64_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = fminf_(mn[a], pos4[4 * i + a]);
+            mx[a] = fmaxf_(mx[a], pos4[4 * i + a]);
+        }
+    float extent = softening;
+    for (int a = 0; a < 3; ++a)
+        extent = fmaxf_(extent, mx[a] - mn[a]);
+    const float cell = fmaxf_(cell_floor, extent / (float)(grid_half - 2));
+    const int M = 2 * grid_half;
+    const float inv = 1.0f / cell;
+    const float half_ext = 0.5f * (float)M * cell;
+    float origin[3];
+    for (int a = 0; a < 3; ++a)
+        origin[a] = 0.5f * (mn[a] + mx[a]) - half_ext;
+    const double h = cell, rs = rsplit_cells * (double)cell;
+    if (params8) {
+        params8[0] = cell;
+        for (int a = 0; a < 3; ++a)
+            params8[1 + a] = origin[a];
+        params8[4] = M;
+        params8[5] = rs;
+        params8[6] = extent;
+        params8[7] = 0.0;
+    }
+    const int64_t MM = M, cells = MM * MM * MM;
+    double* rho = (double*)calloc((size_t)cells, sizeof(double));
+    const double vinv = 1.0 / (h * h * h);
+    for (int64_t i = 0; i < n; ++i) {
+        float sc[3];
+        int c0[3];
+        for (int a = 0; a < 3; ++a) {
+            const float s0 = (pos4[4 * i + a] - origin[a]) * inv;
+            sc[a] = fminf_(fmaxf_(s0, 0.0f), (float)M - 1.0f);
+            int c = (int)floorf(sc[a] + 0.5f);
+            c0[a] = c < 0 ? 0 : (c > M - 1 ? M - 1 : c);
+        }
+        const double md = (double)pos4[4 * i + 3] * vinv;
+        for (int dz = -2; dz <= 2; ++dz) {
+            const int z = c0[2] + dz < 0 ? 0 : (c0[2] + dz > M - 1 ? M - 1 : c0[2] + dz);
+            const double wz = iso_w((double)sc[2] - (double)(c0[2] + dz), order);
+            for (int dy = -2; dy <= 2; ++dy) {
+                const int y = c0[1] + dy < 0 ? 0 : (c0[1] + dy > M - 1 ? M - 1 : c0[1] + dy);
+                const double wy = iso_w((double)sc[1] - (double)(c0[1] + dy), order);
+                for (int dx = -2; dx <= 2; ++dx) {
+                    const int x = c0[0] + dx < 0 ? 0 : (c0[0] + dx > M - 1 ? M - 1 : c0[0] + dx);
+                    const double wx = iso_w((double)sc[0] - (double)(c0[0] + dx), order);
+                    rho[(z * MM + y) * MM + x] += md * wx * wy * wz;
+                }
+            }
+        }
+    }
+    if (density)
+        memcpy(density, rho, sizeof(double) * (size_t)cells);
+    double* sp = (double*)malloc(sizeof(double) * 2 * (size_t)cells);
+    for (int64_t c = 0; c < cells; ++c) {
+        sp[2 * c] = rho[c];
+        sp[2 * c + 1] = 0.0;
+    }
+    or_fft3d(sp, M, 0);
+    const double ks = 2.0 * M_PI / ((double)M * h);
+    for (int64_t z = 0; z < MM; ++z)
+        for (int64_t y = 0; y < MM; ++y)
+            for (int64_t x = 0; x < MM; ++x) {
+                const int64_t sx = x <= MM / 2 ? x : x - MM, sy = y <= MM / 2 ? y : y - MM,
+                              sz = z <= MM / 2 ? z : z - MM;
+                const double kx = sx * ks, ky = sy * ks, kz = sz * ks;
+                const double k2 = kx * kx + ky * ky + kz * kz;
+                const int64_t c = (z * MM + y) * MM + x;
+                if (k2 <= 1.0e-12) {
+                    sp[2 * c] = sp[2 * c + 1] = 0.0;
+                    continue;
+                }
+                const double s3 = sinc(0.5 * kx * h) * sinc(0.5 * ky * h) * sinc(0.5 * kz * h);
+                double W = 1.0;
+                for (int i = 0; i < 2 * order; ++i)
+                    W *= s3;
+                if (W < floor_w)
+                    W = floor_w;
+                /* the physical potential (negative Green function): acceleration = -grad phi */
+                const double f = -4.0 * M_PI * exp(-k2 * rs * rs) / (k2 * W);
+                sp[2 * c] *= f;
+                sp[2 * c + 1] *= f;
+            }
+    double* phi = (double*)malloc(sizeof(double) * (size_t)cells);
+    double* field[3] = {NULL, NULL, NULL};
+    {
+        double* q = (double*)malloc(sizeof(double) * 2 * (size_t)cells);
+        memcpy(q, sp, sizeof(double) * 2 * (size_t)cells);
+        or_fft3d(q, M, 1); /* the inverse transform includes the 1/cells */
+        for (int64_t c = 0; c < cells; ++c)
+            phi[c] = q[2 * c];
+        free(q);
+    }
+    if (phi_out)
+        memcpy(phi_out, phi, sizeof(double) * (size_t)cells);
+    if (gradient != 2)
+        for (int a = 0; a < 3; ++a)
+            field[a] = (double*)calloc((size_t)cells, sizeof(double));
+    if (gradient == 0) {
+        for (int64_t Z = 1; Z < MM - 1; ++Z)
+            for (int64_t Y = 1; Y < MM - 1; ++Y)
+                for (int64_t X = 1; X < MM - 1; ++X) {
+                    const int64_t c = (Z * MM + Y) * MM + X;
+                    field[0][c] = -(phi[c + 1] - phi[c - 1]) * 0.5 / h;
+                    field[1][c] = -(phi[c + MM] - phi[c - MM]) * 0.5 / h;
+                    field[2][c] = -(phi[c + MM * MM] - phi[c - MM * MM]) * 0.5 / h;
+                }
+    } else if (gradient == 1) {
+        double* q = (double*)malloc(sizeof(double) * 2 * (size_t)cells);
+        for (int a = 0; a < 3; ++a) {
+            for (int64_t z = 0; z < MM; ++z)
+                for (int64_t y = 0; y < MM; ++y)
+                    for (int64_t x = 0; x < MM; ++x) {
+                        const int64_t idx3[3] = {x, y, z};
+                        const int64_t v = idx3[a];
+                        const int64_t sv = v == MM / 2 ? 0 : (v < MM / 2 ? v : v - MM);
+                        const double k = sv * ks;
+                        const int64_t c = (z * MM + y) * MM + x;
+                        /* a = -i k phi_k */
+                        q[2 * c] = k * sp[2 * c + 1];
+                        q[2 * c + 1] = -k * sp[2 * c];
+                    }
+            or_fft3d(q, M, 1);
+            for (int64_t c = 0; c < cells; ++c)
+                field[a][c] = q[2 * c];
+        }
+        free(q);
+    }
+    const int64_t nout = targets ? nt : n;
+#pragma omp parallel for schedule(static)
+    for (int64_t o = 0; o < nout; ++o) {
+        const int64_t i = targets ? targets[o] : o;
+        float sc[3];
+        int c0[3];
+        for (int a = 0; a < 3; ++a) {
+            const float s0 = (pos4[4 * i + a] - origin[a]) * inv;
+            sc[a] = fminf_(fmaxf_(s0, 0.0f), (float)M - 1.0f);
+            int c = (int)floorf(sc[a] + 0.5f);
+            c0[a] = c < 0 ? 0 : (c > M - 1 ? M - 1 : c);
+        }
+        double acc[3] = {0, 0, 0};
+        for (int dz = -2; dz <= 2; ++dz) {
+            const int z = c0[2] + dz < 0 ? 0 : (c0[2] + dz > M - 1 ? M - 1 : c0[2] + dz);
+            const double dzd = (double)sc[2] - (double)(c0[2] + dz);
+            const double wz = iso_w(dzd, order), gz = iso_dw(dzd, order);
+            for (int dy = -2; dy <= 2; ++dy) {
+                const int y = c0[1] + dy < 0 ? 0 : (c0[1] + dy > M - 1 ? M - 1 : c0[1] + dy);
+                const double dyd = (double)sc[1] - (double)(c0[1] + dy);
+                const double wy = iso_w(dyd, order), gy = iso_dw(dyd, order);
+                for (int dx = -2; dx <= 2; ++dx) {
+                    const int x = c0[0] + dx < 0 ? 0 : (c0[0] + dx > M - 1 ? M - 1 : c0[0] + dx);
+                    const double dxd = (double)sc[0] - (double)(c0[0] + dx);
+                    const double wx = iso_w(dxd, order), gx = iso_dw(dxd, order);
+                    const int64_t cc = (z * MM + y) * MM + x;
+                    if (gradient == 2) {
+                        /* a = -grad phi(x) = -(1/h) sum_c phi_c grad_s W */
+                        acc[0] -= phi[cc] * gx * wy * wz / h;
+                        acc[1] -= phi[cc] * wx * gy * wz / h;
+                        acc[2] -= phi[cc] * wx * wy * gz / h;
+                    } else {
+                        const double w = wx * wy * wz;
+                        for (int a = 0; a < 3; ++a)
+                            acc[a] += field[a][cc] * w;
+                    }
+                }
+            }
+        }
+        for (int a = 0; a < 3; ++a)
+            acc3[3 * o + a] = acc[a];
+    }
+    for (int a = 0; a < 3; ++a)
+        free(field[a]);
+    free(phi);
+    free(rho);
+    free(sp);
+    return 0;
+}
+
+/* ======================================================================================
  * Learned pair correction: the MLP of blitzar_b200/csrc/bz_mlp.cu restated on the CPU with
  * the same BF16 rounding points (features, weights, hidden activations and back-propagated
  * errors are rounded to BF16 before each product; products accumulate in FP64 here, FP32 on

@@ -94,6 +94,12 @@ int or_pm_periodic_at(const float* pos4, int64_t n, int mesh, double box, double
                       int order, int gradient, double floor_w, const int64_t* targets, int64_t nt,
                       double* acc3, double* density, double* phi);
 
+/* Isolated PM of the reference's GPU TreePM (doubled mesh of 2 grid_half cells). */
+int or_pm_isolated(const float* pos4, int64_t n, int grid_half, float cell_floor, float softening,
+                   double rsplit_cells, int order, int gradient, double floor_w,
+                   const int64_t* targets, int64_t nt, double* acc3, double* params8,
+                   double* density, double* phi_out);
+
 /* ---- split kernel helpers ---------------------------------------------------------------- */
 double or_split_weight(double s, double rsplit);
 

@@ -89,6 +89,9 @@ def lib():
         L.or_pm_periodic_at.argtypes = [_f32p, C.c_int64, C.c_int, C.c_double, C.c_double, C.c_int,
                                         C.c_int, C.c_double, C.c_void_p, C.c_int64, _f64p,
                                         C.c_void_p, C.c_void_p]
+        L.or_pm_isolated.argtypes = [_f32p, C.c_int64, C.c_int, C.c_float, C.c_float, C.c_double,
+                                     C.c_int, C.c_int, C.c_double, C.c_void_p, C.c_int64, _f64p,
+                                     _f64p, C.c_void_p, C.c_void_p]
         L.or_direct_f64.argtypes = [_f32p, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
                                     C.c_double, C.c_double, C.c_double, _f64p, C.c_void_p]
         L.or_ewald_f64.argtypes = [_f32p, C.c_int64, C.c_void_p, C.c_int64, C.c_double,
@@ -373,6 +376,30 @@ def pm_periodic_at(pos4_, targets, mesh, box, rsplit, assignment="cic", spectral
                             mode, window_floor, tg.ctypes.data, len(tg), acc,
                             None, None)
     return acc.reshape(-1, 3)
+
+
+def pm_isolated(pos4_, grid_half, rsplit_cells, assignment="cic", gradient=0, window_floor=0.08,
+                cell_floor=0.25, softening=0.0, targets=None, want_fields=False):
+    """The reference GPU TreePM's isolated PM (doubled mesh of 2 grid_half cells centred on the
+    particle bounds, cell = max(cell_floor, extent / (grid_half - 2)), r_s = rsplit_cells x
+    cell): returns (acc[n or len(targets), 3], params) with params = {cell, origin, mesh,
+    rsplit, extent}, plus (density, phi) meshes when want_fields."""
+    p = np.ascontiguousarray(pos4_, np.float32)
+    tg = None if targets is None else np.ascontiguousarray(targets, np.int64)
+    nt = len(p) if tg is None else len(tg)
+    acc = np.zeros(3 * nt, np.float64)
+    par = np.zeros(8, np.float64)
+    M = 2 * grid_half
+    dens = np.zeros(M ** 3, np.float64) if want_fields else None
+    phi = np.zeros(M ** 3, np.float64) if want_fields else None
+    lib().or_pm_isolated(p, len(p), grid_half, cell_floor, softening, rsplit_cells,
+                         ASSIGNMENT_ORDER[assignment], gradient, window_floor,
+                         None if tg is None else tg.ctypes.data, nt, acc, par,
+                         None if dens is None else dens.ctypes.data,
+                         None if phi is None else phi.ctypes.data)
+    params = dict(cell=par[0], origin=par[1:4].copy(), mesh=int(par[4]), rsplit=par[5], extent=par[6])
+    out = (acc.reshape(-1, 3), params)
+    return out + (dens, phi) if want_fields else out
 
 
 def fft3d(cube_complex, inverse=False):

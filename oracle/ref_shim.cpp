@@ -87,6 +87,55 @@ namespace refgpu {
 #include "physics/octree/cuda/linear/OctParentKernels.inl"
 #include "physics/octree/cuda/linear/OctLinkKernels.inl"
 #include "physics/octree/cuda/force/OctGpu.inl"
+
+// The GPU TreePM's isolated-mesh kernels (deposit, Green, gradient, sampling), run on the host:
+// cuFFT's types stand in as plain structs, atomics as plain updates (the shim runs the
+// deposit serially), and the transforms are done around the kernels below.
+typedef int cufftResult;
+constexpr int CUFFT_SUCCESS = 0;
+struct cufftComplex {
+    float x, y;
+};
+static inline cufftComplex make_cuFloatComplex(float r, float i) { return cufftComplex{r, i}; }
+static inline float atomicAdd(float* p, float v)
+{
+    const float o = *p;
+    *p = o + v;
+    return o;
+}
+static inline unsigned atomicOr(unsigned* p, unsigned v)
+{
+    const unsigned o = *p;
+    *p = o | v;
+    return o;
+}
+static inline int max(int a, int b) { return a > b ? a : b; }
+static inline int min(int a, int b) { return a < b ? a : b; }
+static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
+// The grid parameter block the TreePM kernels take (field list of
+// engine/physics/core/cuda/prelude/CudConfiguration.inl:42-60).
+struct TreePmGridParams {
+    int gridSize;
+    int totalCells;
+    int assignment;
+    int periodic;
+    float cellSize;
+    float invCellSize;
+    float originX;
+    float originY;
+    float originZ;
+    float boundaryMass;
+    float boundaryCenterX;
+    float boundaryCenterY;
+    float boundaryCenterZ;
+    float boundarySoftening;
+    float shortRangeScale;
+    float densityScale;
+    float poissonCoefficient;
+};
+#include "physics/treepm/cuda/field/TpmMath.inl"
+#include "physics/treepm/cuda/fft/TpmFft.inl"
+#include "physics/treepm/cuda/deposit/TpmDeposit.inl"
 } // namespace refgpu
 
 extern "C" {
@@ -523,3 +572,125 @@ void ref_short_range_pair(const float* self3, const float* src3, float srcMass, 
 
 int ref_omp_threads(void) { return omp_get_max_threads(); }
 } // extern "C"
+
+// ---------------------------------------------------------------- isolated GPU TreePM mesh
+// The reference's isolated TreePM mesh (octree_gpu with treepm enabled), its kernels run on
+// the host.  Grid set-up restated from engine/physics/treepm/cuda/deposit/TpmGridBuild.inl:98-171
+// (FP32 bounds, cell = max(0.25, extent / (G - 2)), doubled mesh centred on the bounds,
+// r_s = clamp(cutoffFactor, 1, 2) x cell / 4.5); deposit treePmDepositMassKernel; transforms
+// as buildTreePmFftField (TpmFftRuntime.inl): R2C, treePmApplyFftKernel, C2R and the division
+// by the cell count (here: the reference CPU fft3d on the Hermitian-completed spectrum, whose
+// inverse divides by the cell count); treePmPotentialGradientKernel; treePmSampleAcceleration.
+// params8 = {cell, origin x, y, z, mesh, r_s, cutoff, extent}.
+extern "C" int ref_treepm_isolated(const float* px, const float* py, const float* pz,
+                                   const float* mass, int n, int gridSize, float softening,
+                                   float cutoffFactor, int assignment, double* params8,
+                                   float* densityOut, float* potentialOut, float* ax, float* ay,
+                                   float* az)
+{
+    float mn[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, mx[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int i = 0; i < n; ++i) {
+        const float q[3] = {px[i], py[i], pz[i]};
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = fminf(mn[a], q[a]);
+            mx[a] = fmaxf(mx[a], q[a]);
+        }
+    }
+    const int requested = std::clamp(gridSize, 32, 128);
+    const float extent = std::max({mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2], softening});
+    const float cellSize = std::max(0.25f, extent / static_cast<float>(requested - 2));
+    const int G = requested * 2;
+    const int total = G * G * G;
+    refgpu::TreePmGridParams grid{};
+    grid.gridSize = G;
+    grid.totalCells = total;
+    grid.assignment = assignment;
+    grid.periodic = 0;
+    grid.cellSize = cellSize;
+    grid.invCellSize = 1.0f / cellSize;
+    const float halfGridExtent = 0.5f * static_cast<float>(G) * cellSize;
+    grid.originX = 0.5f * (mn[0] + mx[0]) - halfGridExtent;
+    grid.originY = 0.5f * (mn[1] + mx[1]) - halfGridExtent;
+    grid.originZ = 0.5f * (mn[2] + mx[2]) - halfGridExtent;
+    const float cutoff = std::clamp(cutoffFactor, 1.0f, 2.0f) * cellSize;
+    grid.shortRangeScale = cutoff / 4.5f;
+    grid.densityScale = 1.0f;
+    grid.poissonCoefficient = 0.0f;
+    if (params8) {
+        params8[0] = cellSize;
+        params8[1] = grid.originX;
+        params8[2] = grid.originY;
+        params8[3] = grid.originZ;
+        params8[4] = G;
+        params8[5] = grid.shortRangeScale;
+        params8[6] = cutoff;
+        params8[7] = extent;
+    }
+    ParticleSoAView view{};
+    view.posX = const_cast<float*>(px);
+    view.posY = const_cast<float*>(py);
+    view.posZ = const_cast<float*>(pz);
+    view.mass = const_cast<float*>(mass);
+    view.count = n;
+    std::vector<float> density(total, 0.0f);
+    std::vector<unsigned> mask((total + 31) / 32, 0u);
+    shimLaunch(n, [&] {
+        refgpu::blitzar_cuda_tree_pm_gpu::treePmDepositMassKernel(view, n, n, grid, density.data(),
+                                                                  mask.data());
+    });
+    if (densityOut)
+        std::copy(density.begin(), density.end(), densityOut);
+    // R2C: forward transform, keep x <= G / 2
+    std::vector<std::complex<float>> full(total);
+    for (int c = 0; c < total; ++c)
+        full[c] = std::complex<float>(density[c], 0.0f);
+    refpm::fft3d<float>(full, G, false);
+    const int hx = G / 2 + 1;
+    const int spectrumCells = G * G * hx;
+    std::vector<refgpu::cufftComplex> spec(spectrumCells), pot(spectrumCells);
+    for (int z = 0; z < G; ++z)
+        for (int y = 0; y < G; ++y)
+            for (int x = 0; x < hx; ++x) {
+                const std::complex<float> v = full[(z * G + y) * G + x];
+                spec[(z * G + y) * hx + x] = refgpu::cufftComplex{v.real(), v.imag()};
+            }
+    shimLaunch(spectrumCells, [&] {
+        refgpu::blitzar_cuda_tree_pm_gpu::treePmApplyFftKernel(spec.data(), pot.data(), grid,
+                                                               softening);
+    });
+    // C2R + normalisation: the Hermitian completion, then the inverse transform (which
+    // divides by the cell count, as treePmNormalizeFftFieldKernel does after cuFFT)
+    for (int z = 0; z < G; ++z)
+        for (int y = 0; y < G; ++y)
+            for (int x = 0; x < G; ++x) {
+                std::complex<float> v;
+                if (x < hx) {
+                    const refgpu::cufftComplex c = pot[(z * G + y) * hx + x];
+                    v = std::complex<float>(c.x, c.y);
+                } else {
+                    const int xs = G - x, ys = (G - y) % G, zs = (G - z) % G;
+                    const refgpu::cufftComplex c = pot[(zs * G + ys) * hx + xs];
+                    v = std::complex<float>(c.x, -c.y);
+                }
+                full[(z * G + y) * G + x] = v;
+            }
+    refpm::fft3d<float>(full, G, true);
+    std::vector<float> potential(total);
+    for (int c = 0; c < total; ++c)
+        potential[c] = full[c].real();
+    if (potentialOut)
+        std::copy(potential.begin(), potential.end(), potentialOut);
+    std::vector<float> gx(total), gy(total), gz(total);
+    shimLaunch(total, [&] {
+        refgpu::blitzar_cuda_tree_pm_gpu::treePmPotentialGradientKernel(potential.data(), gx.data(),
+                                                                        gy.data(), gz.data(), grid);
+    });
+    for (int i = 0; i < n; ++i) {
+        const Vector3 a = refgpu::blitzar_cuda_tree_pm_gpu::treePmSampleAcceleration(
+            grid, Vector3(px[i], py[i], pz[i]), gx.data(), gy.data(), gz.data());
+        ax[i] = a.x;
+        ay[i] = a.y;
+        az[i] = a.z;
+    }
+    return 0;
+}

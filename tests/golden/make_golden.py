@@ -5,7 +5,7 @@ The reference sources are compiled where they lie into oracle/_ref/libbzref.so
 are stored as small .npz files that travel with the repository, so the oracle restatement can
 be pinned to the reference on machines that do not have the reference tree.
 
-Run: python tests/golden/make_golden.py
+Run: python tests/golden/make_golden.py [isolated]   (a name: regenerate that fixture only)
 """
 from __future__ import annotations
 
@@ -35,11 +35,48 @@ def soa(p):
     return [np.ascontiguousarray(p[:, a]) for a in range(3)]
 
 
-def main():
+def isolated_treepm(R):
+    """6. the reference GPU TreePM's isolated mesh (its kernels run on the host): grid, density,
+    potential and the sampled mesh accelerations, CIC / TSC / PCS, for an open cluster."""
+    n = 3000
+    rng = np.random.default_rng(105)
+    pos = (rng.standard_normal((n, 3)) * 1.5).astype(np.float32)
+    mass = (rng.random(n).astype(np.float32) + 0.5) / n
+    x, y, z = soa(pos)
+    fn = R.ref_treepm_isolated
+    fn.argtypes = [np.ctypeslib.ndpointer(np.float32)] * 4 + [C.c_int, C.c_int, C.c_float, C.c_float,
+                                                              C.c_int, np.ctypeslib.ndpointer(np.float64),
+                                                              C.c_void_p, C.c_void_p] + \
+        [np.ctypeslib.ndpointer(np.float32)] * 3
+    out = {}
+    G, softening, cutoff_factor = 32, 0.01, 1.5
+    for code, name in ((0, "cic"), (1, "tsc"), (2, "pcs")):
+        params = np.zeros(8)
+        dens = np.zeros((2 * G) ** 3, np.float32)
+        phi = np.zeros((2 * G) ** 3, np.float32)
+        ax, ay, az = [np.zeros(n, np.float32) for _ in range(3)]
+        fn(x, y, z, mass, n, G, softening, cutoff_factor, code, params, dens.ctypes.data,
+           phi.ctypes.data, ax, ay, az)
+        out[f"{name}_params"] = params
+        out[f"{name}_density"] = dens
+        # the potential is dense: a seeded sample of its cells keeps the fixture small
+        cells = np.sort(np.random.default_rng(106).choice(dens.size, 8192, replace=False))
+        out[f"{name}_potential_cells"] = cells
+        out[f"{name}_potential"] = phi[cells]
+        out[f"{name}_acc"] = np.stack([ax, ay, az], 1)
+    np.savez_compressed(os.path.join(HERE, "ref_treepm_isolated.npz"), pos=pos, mass=mass, grid=G,
+                        softening=softening, cutoff_factor=cutoff_factor, **out)
+
+
+def main(only=None):
     O.build(ref=True)
     R = O.ref()
     if R is None:
         raise SystemExit("oracle/_ref/libbzref.so is not built (needs the reference tree)")
+    if only == "isolated":
+        isolated_treepm(R)
+        print("golden fixture written to", HERE)
+        return
 
     # 1. Morton keys, stable sort permutation and topology (reference octree_gpu build)
     n = 2000
@@ -113,8 +150,9 @@ def main():
     np.savez_compressed(os.path.join(HERE, "ref_misc.npz"), sep=sep, pair=pair, pair_mass=0.7,
                         pair_softening=0.002, pair_split=0.01, fft_in=cube,
                         fft_out=(flat[0::2] + 1j * flat[1::2]).reshape(8, 8, 8))
+    isolated_treepm(R)
     print("golden fixtures written to", HERE)
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1] if len(sys.argv) > 1 else None)

@@ -289,3 +289,55 @@ def test_node_cap_walk_needs_no_multipoles(gpu):
             assert pn == 0 and pp > 0
     scale = np.linalg.norm(out[0], axis=1).max()
     assert np.abs(out[1] - out[0]).max() < 1e-6 * scale
+
+
+@pytest.mark.parametrize("assignment,gradient", [("cic", 0), ("tsc", 0), ("pcs", 0), ("pcs", 2)])
+def test_isolated_treepm_matches_oracle(gpu, oracle, assignment, gradient):
+    """Open-boundary TreePM (box_length 0), the reference's GPU TreePM: a doubled mesh of 2G
+    cells of max(0.25, extent / (G - 2)), centred on the particles, r_s = cutoffFactor x cell
+    / 4.5 (here cutoffFactor 1.5), r_cut = 4.5 r_s.  The device-computed grid equals the
+    oracle's FP32 grid; density, and forces (isolated PM + open cutoff walk), match."""
+    n, G = 20_000, 32
+    rng = np.random.default_rng(51)
+    pos = (rng.standard_normal((n, 3)) * 1.5).astype(np.float32)
+    m = np.full(n, 1.0 / n, np.float32)
+    eps = 0.01
+    rs_cells = np.float32(1.5 / 4.5)
+    with _engine(n, solver=1, box_length=0.0, treepm_grid_size=G, treepm_r_split_cells=rs_cells,
+                 treepm_r_cut_factor=4.5, treepm_assignment=ASSIGN[assignment],
+                 treepm_gradient=gradient, treepm_window_floor=0.08 if gradient == 0 else 0.0,
+                 octree_softening=eps) as e:
+        e.set_state(pos, None, m)
+        acc = e.accelerations().astype(np.float64)
+        grid = e.pm_grid()
+        rho = e.pm_mesh(0).astype(np.float64)
+    p4 = oracle.pos4(pos, m)
+    apm, par, orho, _ = oracle.pm_isolated(p4, G, float(rs_cells), assignment=assignment,
+                                           gradient=gradient,
+                                           window_floor=0.08 if gradient == 0 else 0.0,
+                                           cell_floor=0.25, softening=eps, want_fields=True)
+    assert np.float32(grid["cell"]) == np.float32(par["cell"])
+    assert np.array_equal(np.asarray(grid["origin"], np.float32), np.asarray(par["origin"], np.float32))
+    assert np.abs(rho - orho).max() < 1e-5 * np.abs(orho).max()
+    rs = np.float32(rs_cells) * np.float32(grid["cell"])
+    assert np.float32(grid["rsplit"]) == rs
+    p64 = pos.astype(np.float64)
+    lo = p64.min(0)
+    size = float((p64.max(0) - lo).max())
+    keys = oracle.morton63(p64, lo, size)
+    perm = oracle.stable_sort(keys)
+    t = oracle.build_tree(keys[perm], p4[perm], leaf_cap=16)
+    a_s, s_s = oracle.walk_targets(p4[perm], t, np.arange(n), theta=0.5, eps=eps,
+                                   rcut=np.float32(4.5) * rs, box=0.0, rsplit=rs, quadrupole=True)
+    asr = np.empty_like(a_s)
+    asr[perm] = a_s
+    asum = np.empty_like(s_s)
+    asum[perm] = s_s
+    ref = apm + asr
+    dev = np.linalg.norm(acc - ref, axis=1)
+    net = np.linalg.norm(ref, axis=1)
+    bound = 64.0 * 2.0 ** -24 * (asum + np.linalg.norm(apm, axis=1))
+    # the mesh force in FP32 transforms: 1e-5 of the rms mesh force as a floor
+    rms_pm = np.sqrt((np.linalg.norm(apm, axis=1) ** 2).mean())
+    assert np.median(dev / net) < 1e-5
+    assert (dev <= np.maximum(np.maximum(1e-5 * net, bound), 1e-5 * rms_pm)).all(), (dev / net).max()

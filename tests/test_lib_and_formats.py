@@ -113,15 +113,31 @@ def test_headless_resolves_reference_config(tmp_path):
         "simulation(particle_count=3073, dt=0.002, solver=octree_gpu, integrator=leapfrog)\n"
         "octree(theta=0.7, softening=0.05, criterion=com, leaf_capacity=256)\n"
         "physics(max_acceleration=64, min_softening=0.0001, min_distance2=1e-12, min_theta=0.05)\n"
-        "treepm(enabled=true, assignment=pcs, grid_size=64, gradient=spectral)\n"
+        "treepm(enabled=true, assignment=pcs, grid_size=256, cutoff_factor=1.5, model=auto)\n"
         "input_file=state.bin\n")
     out = subprocess.run([_headless(), "--config", str(cfg), "--dry-run"], capture_output=True,
                          text=True, check=True).stdout
     d = json.loads(out)
-    assert d["solver"] == 1 and d["treepm_grid_size"] == 64 and d["treepm_assignment"] == 2
-    assert d["treepm_gradient"] == 1 and d["dt"] == 0.002 and d["box_length"] == 1.0
+    # the reference's TreePM keys: the isolated TreePM, grid clamped to 128 (mesh 256), the
+    # cutoff in cells clamped to [1, 2] with r_s = cutoff / 4.5, centred differences
+    assert d["solver"] == 1 and d["treepm_grid_size"] == 128 and d["treepm_assignment"] == 2
+    assert d["box_length"] == 0.0 and d["treepm_gradient"] == 0 and d["dt"] == 0.002
+    assert abs(d["treepm_r_split_cells"] - 1.5 / 4.5) < 1e-7 and d["treepm_r_cut_factor"] == 4.5
+    assert abs(d["treepm_cell_floor"] - 0.25) < 1e-7
     assert abs(d["octree_theta"] - 0.7) < 1e-7 and abs(d["physics_max_acceleration"] - 64) < 1e-6
     assert d["input"] == "state.bin"
+    # exact_tree names the reference's CPU FP64 pairwise sum: octree_gpu keeps the octree
+    cfg.write_text("simulation(solver=octree_gpu, integrator=leapfrog)\ntreepm(enabled=true, model=exact_tree)\n")
+    d = json.loads(subprocess.run([_headless(), "--config", str(cfg), "--dry-run"], capture_output=True,
+                                  text=True, check=True).stdout)
+    assert d["solver"] == 0
+    # a box length selects this engine's periodic TreePM with its own keys
+    cfg.write_text("simulation(solver=octree_gpu, integrator=leapfrog)\n"
+                   "treepm(enabled=true, box_length=1, assignment=pcs, grid_size=64, gradient=spectral)\n")
+    d = json.loads(subprocess.run([_headless(), "--config", str(cfg), "--dry-run"], capture_output=True,
+                                  text=True, check=True).stdout)
+    assert d["solver"] == 1 and d["box_length"] == 1.0 and d["treepm_gradient"] == 1
+    assert d["treepm_grid_size"] == 64
     bad = tmp_path / "bad.ini"
     bad.write_text("simulation(solver=octree_gpu, integrator=euler)\n")
     r = subprocess.run([_headless(), "--config", str(bad), "--dry-run"], capture_output=True, text=True)

@@ -98,3 +98,31 @@ def test_fft_matches_reference(oracle):
     d = load("ref_misc.npz")
     out = oracle.fft3d(d["fft_in"])
     assert np.abs(out - d["fft_out"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("assignment", ["cic", "tsc", "pcs"])
+def test_isolated_treepm_mesh_matches_reference(oracle, assignment):
+    """The oracle's isolated PM against the reference GPU TreePM's own kernels (run on the
+    host): FP32 grid set-up bit for bit, density, potential and mesh accelerations within the
+    FP32 rounding of the reference's arithmetic."""
+    d = load("ref_treepm_isolated.npz")
+    pos, mass, G = d["pos"], d["mass"], int(d["grid"])
+    cf = float(d["cutoff_factor"])
+    acc, par, dens, phi = oracle.pm_isolated(oracle.pos4(pos, mass), G, cf / 4.5,
+                                             assignment=assignment, gradient=0, window_floor=0.08,
+                                             cell_floor=0.25, softening=float(d["softening"]),
+                                             want_fields=True)
+    rp = d[f"{assignment}_params"]  # cell, origin, mesh, r_s, cutoff, extent
+    assert np.float32(par["cell"]) == np.float32(rp[0])
+    assert np.array_equal(np.float32(par["origin"]), np.float32(rp[1:4]))
+    assert par["mesh"] == int(rp[4])
+    assert abs(par["rsplit"] - rp[5]) <= 1e-6 * rp[5]
+    rd = d[f"{assignment}_density"].astype(np.float64)
+    assert np.abs(dens - rd).max() <= 1e-6 * np.abs(rd).max()
+    cells = d[f"{assignment}_potential_cells"]
+    rphi = d[f"{assignment}_potential"].astype(np.float64)
+    assert np.abs(phi[cells] - rphi).max() <= 1e-5 * np.abs(rphi).max()
+    ra = d[f"{assignment}_acc"].astype(np.float64)
+    assert np.abs(acc - ra).max() <= 1e-5 * np.abs(ra).max()
+    err = np.linalg.norm(acc - ra, axis=1) / np.linalg.norm(ra, axis=1)
+    assert np.median(err) < 1e-5
