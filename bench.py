@@ -50,16 +50,21 @@ NOMINAL_SM_MHZ = 1965.0
 WORKLOADS = {
     "treepm128": dict(kind="treepm", n_side=128, mesh=256, r_split_cells=1.0, r_cut_factor=5.0,
                       theta=0.5, eps_lattice=0.02, dt=5e-4, seed=2, rms_cells=0.2,
-                      assignment="pcs", gradient="spectral", node_size_factor=0.5),
-    "treepm256": dict(kind="treepm", n_side=256, mesh=512, r_split_cells=1.0, r_cut_factor=5.0,
+                      assignment="pcs", gradient="analytic", node_size_factor=0.5),
+    "treepm256": dict(kind="treepm", n_side=256, mesh=512, r_split_cells=0.95, r_cut_factor=5.0,
                       theta=0.5, eps_lattice=0.02, dt=5e-4, seed=4, rms_cells=0.2,
-                      assignment="pcs", gradient="spectral", node_size_factor=0.5),
+                      assignment="pcs", gradient="analytic", node_size_factor=0.5),
     "treepm128_cic": dict(kind="treepm", n_side=128, mesh=128, r_split_cells=1.25, r_cut_factor=4.5,
                           theta=0.5, eps_lattice=0.02, dt=5e-4, seed=2, rms_cells=0.2,
                           assignment="cic", gradient="centred-difference", node_size_factor=0.0),
     "treepm64": dict(kind="treepm", n_side=64, mesh=128, r_split_cells=1.0, r_cut_factor=5.0,
                      theta=0.5, eps_lattice=0.02, dt=5e-4, seed=2, rms_cells=0.2,
-                     assignment="pcs", gradient="spectral", node_size_factor=0.5),
+                     assignment="pcs", gradient="analytic", node_size_factor=0.5),
+    # the reference's own GPU TreePM (isolated doubled mesh) at its defaults for the 13 TreePM
+    # parameters (grid 64 -> mesh 128, cutoff 1 cell, CIC, centred differences) on a Plummer
+    # sphere of 1M particles
+    "treepm_open": dict(kind="treepm_open", ic="plummer", n=1 << 20, grid=64, cutoff_factor=1.0,
+                        assignment="cic", theta=0.5, eps=0.01, dt=1e-3, seed=1),
     "plummer65k": dict(kind="octree", ic="plummer", n=65536, theta=0.5, eps=0.01, dt=1e-3, seed=1),
     "hernquist4m": dict(kind="octree", ic="hernquist", n=4194304, theta=0.4, eps=0.005, dt=2e-4,
                         seed=3),
@@ -137,6 +142,8 @@ def make_ics(w, rank):
         return pos, vel, mass
     if w["kind"] == "treepm":
         pos, vel, mass = ics.grf_grid(w["n_side"], seed=w["seed"] + rank, rms_cells=w["rms_cells"])
+    elif w["kind"] == "treepm_open" or w["ic"] == "plummer":
+        pos, vel, mass = ics.plummer(w["n"], seed=w["seed"] + rank)
     elif w["ic"] == "hernquist":
         pos, vel, mass = ics.hernquist(w["n"], seed=w["seed"] + rank)
     else:
@@ -158,6 +165,14 @@ def engine_config(w):
                     # boxes (particle_node = 0 in the counters), so the walk needs no multipoles
                     # and the tree no second moments; the cic workload (no cap) keeps them
                     multipole_order=1 if w["node_size_factor"] > 0 else 2)
+    if w["kind"] == "treepm_open":
+        # the reference's isolated TreePM: setTreePmParameters(grid, cutoffFactor, assignment)
+        # maps to this mesh of 2 x grid cells, r_s = cutoff / 4.5, r_cut = 4.5 r_s
+        return dict(solver=1, box_length=0.0, treepm_grid_size=w["grid"],
+                    treepm_r_split_cells=w["cutoff_factor"] / 4.5, treepm_r_cut_factor=4.5,
+                    treepm_assignment={"cic": 0, "tsc": 1, "pcs": 2}[w["assignment"]],
+                    treepm_gradient=0, treepm_window_floor=0.08, octree_theta=w["theta"],
+                    octree_softening=w["eps"], multipole_order=2)
     cfg = dict(solver=0, octree_theta=w["theta"], octree_softening=w["eps"], multipole_order=2)
     if w.get("adaptive_levels"):
         cfg.update(adaptive_max_level=w["adaptive_levels"], adaptive_eta=w["adaptive_eta"])
@@ -286,7 +301,15 @@ def cpu_reference_step(w, pos, mass, budget_s, seed=7, chunk=65536):
         m = np.ascontiguousarray(mass, np.float32)
         targets = rng.permutation(n).astype(np.int32)
         treepm = w["kind"] == "treepm"
-        if treepm:
+        iso = w["kind"] == "treepm_open"
+        if iso:
+            # grid of the reference's isolated mesh: the cell follows the bounds
+            ext = max(float((p32[:, a].max() - p32[:, a].min())) for a in range(3))
+            cell = max(0.25, max(ext, w["eps"]) / (w["grid"] - 2))
+            rc = min(max(w["cutoff_factor"], 1.0), 2.0) * cell
+            rs = rc / 4.5
+            eps, theta = w["eps"], w["theta"]
+        elif treepm:
             M = w["mesh"]
             rs = w["r_split_cells"] / M
             rc = w["r_cut_factor"] * rs
@@ -300,6 +323,18 @@ def cpu_reference_step(w, pos, mass, budget_s, seed=7, chunk=65536):
                 ax, ay, az = [np.zeros(n, np.float32) for _ in range(3)]
                 t0 = time.perf_counter()
                 R.ref_pm_periodic(x, y, z, m, n, M, 1.0, rs, 0, b"cic", ax, ay, az, None, None)
+                pieces["pm_s"] = time.perf_counter() - t0
+            elif iso:
+                import ctypes as C
+                fn = R.ref_treepm_isolated
+                fn.argtypes = [np.ctypeslib.ndpointer(np.float32)] * 4 + [
+                    C.c_int, C.c_int, C.c_float, C.c_float, C.c_int,
+                    np.ctypeslib.ndpointer(np.float64), C.c_void_p, C.c_void_p] + \
+                    [np.ctypeslib.ndpointer(np.float32)] * 3
+                ax, ay, az = [np.zeros(n, np.float32) for _ in range(3)]
+                t0 = time.perf_counter()
+                fn(x, y, z, m, n, w["grid"], w["eps"], w["cutoff_factor"],
+                   {"cic": 0, "tsc": 1, "pcs": 2}[w["assignment"]], np.zeros(8), None, None, ax, ay, az)
                 pieces["pm_s"] = time.perf_counter() - t0
             t0 = time.perf_counter()
             tree = R.ref_octree_cpu_build(x, y, z, m, n, theta, eps, 1e-12, 1e30, 0, rs, rc * rc)
@@ -324,8 +359,11 @@ def cpu_reference_step(w, pos, mass, budget_s, seed=7, chunk=65536):
             text = ("reference CPU code built from its sources: " +
                     (f"periodic PM templates (TpmAssignment/TpmField, FP32 CIC, mesh {M}^3) over all "
                      f"{n} particles, " if treepm else "") +
+                    (f"its GPU TreePM's isolated-mesh kernels run on one host core (deposit, "
+                     f"cuFFT replaced by its CPU fft3d, gradient, sampling; mesh {2 * w['grid']}^3) "
+                     f"over all {n} particles, " if iso else "") +
                     f"octree_cpu build over all {n} (Octree::build) and its "
-                    + ("cutoff/erfc-split " if treepm else "") +
+                    + ("cutoff/erfc-split " if treepm or iso else "") +
                     f"walk (Octree::computeForceOn) for {walked} seeded targets"
                     + (f", walk time scaled to all {n}" if walked < n else "")
                     + (" (open-boundary short range: the reference has no periodic split)"
@@ -547,7 +585,7 @@ def run_ours(args, w, rank, world, local):
     ph = eng.phase_times()
     listed, evaluated, nodes = eng.walk_counts()
     eng.enable_timing(False)
-    split = w["kind"] == "treepm"
+    split = w["kind"] in ("treepm", "treepm_open")
     # algorithmic flops: pairs that went through the pair law (inside the cutoff) and
     # multipole terms; the distance tests of listed pairs outside the cutoff are not counted
     flops = evaluated * FLOP_PP[split] + nodes * FLOP_PN[(split, True)]

@@ -18,14 +18,18 @@ pytestmark = pytest.mark.gpu
 # the GRF boxes of the benchmark workloads (positions: grid displaced by a Zel'dovich field of
 # a P(k) ~ k^-2 Gaussian random field, 0.2 cell rms)
 CASES = {
-    # 128^3 box, 256^3 PCS mesh, spectral gradient, r_s = 1.0 cell, r_cut = 5 r_s, node cap
-    "treepm128": dict(n_side=128, seed=2, mesh=256, rs=1.0, rcf=5.0, assignment=2, spectral=True,
+    # 128^3 box, 256^3 PCS mesh, analytic differentiation, r_s = 1.0 cell, r_cut = 5 r_s,
+    # node cap (the bench's treepm128)
+    "treepm128": dict(n_side=128, seed=2, mesh=256, rs=1.0, rcf=5.0, assignment=2, gradient=2,
                       floor=0.0, cap=0.5, order=1),
+    # the same with the spectral gradient
+    "treepm128_spectral": dict(n_side=128, seed=2, mesh=256, rs=1.0, rcf=5.0, assignment=2,
+                               gradient=1, floor=0.0, cap=0.5, order=1),
     # the reference-literal mesh: 128^3 CIC, centred differences, r_s = 1.25 cells, 4.5 r_s
     "treepm128_cic": dict(n_side=128, seed=2, mesh=128, rs=1.25, rcf=4.5, assignment=0,
-                          spectral=False, floor=0.08, cap=0.0, order=2),
-    # 256^3 box on the 512^3 mesh
-    "treepm256": dict(n_side=256, seed=4, mesh=512, rs=1.0, rcf=5.0, assignment=2, spectral=True,
+                          gradient=0, floor=0.08, cap=0.0, order=2),
+    # 256^3 box on the 512^3 mesh (the bench's treepm256)
+    "treepm256": dict(n_side=256, seed=4, mesh=512, rs=0.95, rcf=5.0, assignment=2, gradient=2,
                       floor=0.0, cap=0.5, order=1),
 }
 ASSIGN_NAME = {0: "cic", 1: "tsc", 2: "pcs"}
@@ -46,7 +50,7 @@ def test_treepm_parity_at_benchmark_scale(gpu, oracle, case):
     eps = 0.02 / c["n_side"]
     with Engine(n, solver=1, box_length=1.0, treepm_grid_size=M, treepm_r_split_cells=c["rs"],
                 treepm_r_cut_factor=c["rcf"], treepm_assignment=c["assignment"],
-                treepm_gradient=1 if c["spectral"] else 0, treepm_window_floor=c["floor"],
+                treepm_gradient=c["gradient"], treepm_window_floor=c["floor"],
                 treepm_node_size_factor=c["cap"], multipole_order=c["order"],
                 octree_softening=eps, physics_max_acceleration=1e30) as e:
         e.set_state(pos, None, m, f64=True)
@@ -60,7 +64,7 @@ def test_treepm_parity_at_benchmark_scale(gpu, oracle, case):
     inv = np.empty(n, np.int64)
     inv[perm] = np.arange(n)
     tree = oracle.build_tree(keys[perm], p4[perm], leaf_cap=16)
-    rsf = np.float32(c["rs"]) * np.float32(1.0 / M)
+    rsf = np.float32(np.float64(np.float32(c["rs"])) / M)
     st = inv[tg]
     order = np.argsort(st)
     asr_s, asum_s = oracle.walk_targets(p4[perm], tree, st[order], theta=0.5, eps=eps,
@@ -72,7 +76,7 @@ def test_treepm_parity_at_benchmark_scale(gpu, oracle, case):
     asr[order] = asr_s
     asum[order] = asum_s
     apm = oracle.pm_periodic_at(p4, tg, M, 1.0, rsf, assignment=ASSIGN_NAME[c["assignment"]],
-                                spectral=c["spectral"], window_floor=c["floor"])
+                                gradient=c["gradient"], window_floor=c["floor"])
     ref = apm + asr
     scale = asum + np.linalg.norm(apm, axis=1)
     dev = np.linalg.norm(acc[tg] - ref, axis=1)
@@ -84,6 +88,8 @@ def test_treepm_parity_at_benchmark_scale(gpu, oracle, case):
     print(f"{case}: median rel {np.median(rel):.2e}, max rel {rel.max():.2e} (kappa {kappa[rel.argmax()]:.1f}), "
           f"max dev/S {(dev / scale).max():.2e}, {int((rel > 1e-5).sum())} of {len(tg)} targets above "
           f"1e-5, {int(held.sum())} with kappa > {1e-5 / FP32_SUM_BOUND:.1f}")
-    assert np.median(rel) < 1e-6
+    # centred differences of an FP32 potential lose digits to cancellation (the reference's
+    # own mesh does the same): its median is held to 1e-5, the spectral and analytic meshes' to 1e-6
+    assert np.median(rel) < (1e-5 if c["gradient"] == 0 else 1e-6)
     assert (dev <= np.maximum(1e-5 * net, bound)).all(), \
         (rel.max(), kappa[rel.argmax()], (dev / scale).max())
