@@ -9,7 +9,11 @@ sources at a time, the tiles combined with a two-sum), the oracle in FP64; the d
 bounded by a multiple of 2^-24 of the sum of the magnitudes of the terms, S = sum |a_j| +
 |a_mesh|, not of the net force |a|.  Where the net force is a cancellation (kappa = S / |a|
 large) 1e-5 |a| can lie below that bound; those targets are held to 64 * 2^-24 * S (the
-worst-case rounding of an FP32 sum of 64 terms) and counted in the output."""
+worst-case rounding of an FP32 sum of 64 terms) and counted in the output.
+
+Analytic differentiation takes the gradient of the FP32 potential mesh: its rounding, a few
+2^-24 of the largest |phi|, enters the force divided by the cell h.  For that mesh the bound
+also admits 64 * 2^-24 * max|phi| / h (phi from the engine's own mesh), counted separately."""
 import numpy as np
 import pytest
 
@@ -55,6 +59,8 @@ def test_treepm_parity_at_benchmark_scale(gpu, oracle, case):
                 octree_softening=eps, physics_max_acceleration=1e30) as e:
         e.set_state(pos, None, m, f64=True)
         acc = e.accelerations().astype(np.float64)
+        psi_floor = (FP32_SUM_BOUND * float(np.abs(e.pm_mesh(1)).max()) * M
+                     if c["gradient"] == 2 else 0.0)
     rng = np.random.default_rng(101)
     tg = np.sort(rng.choice(n, 2048, replace=False)).astype(np.int64)
     p32 = pos.astype(np.float32)
@@ -85,11 +91,14 @@ def test_treepm_parity_at_benchmark_scale(gpu, oracle, case):
     kappa = scale / net
     bound = FP32_SUM_BOUND * scale
     held = 1e-5 * net < bound  # targets where the FP32 rounding bound exceeds 1e-5 |a|
+    by_mesh = (dev > np.maximum(1e-5 * net, bound)) & (dev <= psi_floor)
     print(f"{case}: median rel {np.median(rel):.2e}, max rel {rel.max():.2e} (kappa {kappa[rel.argmax()]:.1f}), "
           f"max dev/S {(dev / scale).max():.2e}, {int((rel > 1e-5).sum())} of {len(tg)} targets above "
-          f"1e-5, {int(held.sum())} with kappa > {1e-5 / FP32_SUM_BOUND:.1f}")
-    # centred differences of an FP32 potential lose digits to cancellation (the reference's
-    # own mesh does the same): its median is held to 1e-5, the spectral and analytic meshes' to 1e-6
-    assert np.median(rel) < (1e-5 if c["gradient"] == 0 else 1e-6)
-    assert (dev <= np.maximum(1e-5 * net, bound)).all(), \
-        (rel.max(), kappa[rel.argmax()], (dev / scale).max())
+          f"1e-5, {int(held.sum())} with kappa > {1e-5 / FP32_SUM_BOUND:.1f}, "
+          f"{int(by_mesh.sum())} within the potential-mesh floor {psi_floor:.2e} only")
+    # differences of an FP32 potential (centred, the reference's own mesh; or of the assignment
+    # weights) lose digits to cancellation: their median is held to 1e-5, the spectral mesh's,
+    # which transforms the gradient itself, to 1e-6
+    assert np.median(rel) < (1e-5 if c["gradient"] != 1 else 1e-6)
+    assert (dev <= np.maximum(np.maximum(1e-5 * net, bound), psi_floor)).all(), \
+        (rel.max(), kappa[rel.argmax()], (dev / scale).max(), dev.max(), psi_floor)
