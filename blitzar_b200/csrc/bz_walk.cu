@@ -18,8 +18,6 @@
 // per-particle stackless walk is engine/physics/octree/cuda/force/OctGpu.inl:100-228 and the
 // TreePM pair law with the Gaussian split is engine/physics/core/cuda/prelude/
 // CudForceKernels.inl:62-89.
-#include <cuda_fp16.h>
-
 #include "bz_common.cuh"
 #include "bz_kernels.h"
 
@@ -48,18 +46,9 @@ struct __align__(16) WarpSmem {
         };
         unsigned mask[kTile / 32][32];  // leaf flush: per-lane in-cutoff bits of the tile
     };
-    union {
-        struct {
-            float2 nd_qb[32];
-            float nd_tr[32];  // -tr(Q) eps^2 / 3 of each node (traceless Newtonian form only)
-            int tidx[kTile];  // sorted index of each tile source (only when pairs are recorded)
-        };
-        // leaf flush with a cutoff: the tile's sources relative to the group centre in units
-        // of the cutoff, as half pairs {x, y, z} of sources 2k and 2k + 1 (the coarse filter)
-        uint4 htile[kTile / 2];
-    };
-    float4 gframe;    // group centre and its half-diagonal, both in units of the cutoff
-    float hthr;       // the coarse filter's threshold of r^2 / r_cut^2 for the current tile
+    float2 nd_qb[32];
+    float nd_tr[32];  // -tr(Q) eps^2 / 3 of each node (traceless Newtonian form only)
+    int tidx[kTile];  // sorted index of each tile source (only when pairs are recorded)
     int stack[kStack];
     int nlist[kList];
     int lstart[kList];
@@ -82,15 +71,6 @@ __device__ __forceinline__ float erfc_as(float u, float e)
     p = fmaf(p, t, 0.254829592f);
     return t * p * e;
 }
-
-// Two floats rounded to a half2 (lo in the low 16 bits) as its 32-bit image.
-__device__ __forceinline__ unsigned pack_half2(float lo, float hi)
-{
-    const __half2 h = __floats2half2_rn(lo, hi);
-    return *reinterpret_cast<const unsigned*>(&h);
-}
-__device__ __forceinline__ __half2 as_half2(unsigned u) { return *reinterpret_cast<const __half2*>(&u); }
-__device__ __forceinline__ unsigned as_u32(__half2 h) { return *reinterpret_cast<const unsigned*>(&h); }
 
 constexpr float kTwoOverSqrtPi = 1.1283791670955126f;
 constexpr float kFourOverSqrtPi = 2.2567583341910252f;
@@ -526,72 +506,10 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
             // r2 <= rcut2 exactly when r2 - next_float(rcut2) is negative (a float difference
             // has the exact sign), so the sign bit is the mask bit: one funnel shift appends it
             const float rc2n = __uint_as_float(__float_as_uint(p.rcut2) + 1u);
-            // Coarse filter in half precision, two sources per instruction: positions relative
-            // to the group centre in units of the cutoff, tested against a threshold widened by
-            // the rounding bound of that arithmetic, so that no source inside the cutoff is
-            // dropped.  The few extra sources (a shell a few per cent thick) go through the pair
-            // law with the exact test there and add exactly zero, so the sums are those of the
-            // exact filter.  Far-flung groups (coordinates beyond 64 cutoffs) and the learned
-            // path (its pair records share the half tile's space) keep the exact filter.
-            bool coarse = !rec;
-            if (coarse) {
-                const float4 gf = w.gframe;
-                const float irc = rsqrtf(p.rcut2);
-                constexpr float kFar = 16.0f;
-                float xm = gf.w;
-                for (int k = lane; k < nw * 16; k += 32) {
-                    const int q0 = 2 * k, q1 = q0 + 1;
-                    float a[3] = {kFar, kFar, kFar}, b[3] = {kFar, kFar, kFar};
-                    if (q0 < nb) {
-                        const float4 s4 = w.tile[q0];
-                        a[0] = (s4.x - gf.x) * irc;
-                        a[1] = (s4.y - gf.y) * irc;
-                        a[2] = (s4.z - gf.z) * irc;
-                        xm = fmaxf(xm, fmaxf(fabsf(a[0]), fmaxf(fabsf(a[1]), fabsf(a[2]))));
-                    }
-                    if (q1 < nb) {
-                        const float4 s4 = w.tile[q1];
-                        b[0] = (s4.x - gf.x) * irc;
-                        b[1] = (s4.y - gf.y) * irc;
-                        b[2] = (s4.z - gf.z) * irc;
-                        xm = fmaxf(xm, fmaxf(fabsf(b[0]), fmaxf(fabsf(b[1]), fabsf(b[2]))));
-                    }
-                    w.htile[k] = make_uint4(pack_half2(a[0], b[0]), pack_half2(a[1], b[1]),
-                                            pack_half2(a[2], b[2]), 0u);
-                }
-                for (int o = 16; o > 0; o >>= 1)
-                    xm = fmaxf(xm, __shfl_xor_sync(kFullMask, xm, o));
-                coarse = xm < 64.0f;
-                // |error of r^2| <= 6 ulp(max coordinate) + 4 ulp(1) near r^2 = 1 (inputs
-                // rounded to half, their differences, squares and sums rounded again)
-                const int e = static_cast<int>((__float_as_uint(fmaxf(xm, 1.0f)) >> 23) & 0xff) - 127;
-                if (lane == 0)
-                    w.hthr = 1.0f + 6.0f * ldexpf(1.0f, e - 10) + 0.0078125f;
-                __syncwarp();
-            }
             for (int wd = 0; wd < nw; ++wd) {
                 const int qb = wd << 5;
                 unsigned m = 0u;
-                if (coarse) {
-                    // this lane's target in the frame (recomputed per word: fewer live registers)
-                    const float4 gf = w.gframe;
-                    const float irc = rsqrtf(p.rcut2);
-                    const __half2 th2 = __float2half2_rn(w.hthr);
-                    const __half2 tx2 = __float2half2_rn((tx - gf.x) * irc);
-                    const __half2 ty2 = __float2half2_rn((ty - gf.y) * irc);
-                    const __half2 tz2 = __float2half2_rn((tz - gf.z) * irc);
-                    // pairs of sources, highest first; bits 2j, 2j + 1 = sources 2j, 2j + 1
-#pragma unroll 4
-                    for (int j = 15; j >= 0; --j) {
-                        const uint4 v = w.htile[wd * 16 + j];
-                        const __half2 dx = __hsub2(as_half2(v.x), tx2);
-                        const __half2 dy = __hsub2(as_half2(v.y), ty2);
-                        const __half2 dz = __hsub2(as_half2(v.z), tz2);
-                        const __half2 r2 = __hfma2(dx, dx, __hfma2(dy, dy, __hmul2(dz, dz)));
-                        const unsigned u = as_u32(__hsub2(r2, th2));  // sign bits 15 and 31
-                        m = (m << 2) | ((u >> 30) & 2u) | ((u >> 15) & 1u);
-                    }
-                } else if (qb + 32 <= nb) {
+                if (qb + 32 <= nb) {
                     // highest source first, shifting the mask left (short loop body)
 #pragma unroll 8
                     for (int b = 31; b >= 0; --b) {
@@ -610,8 +528,7 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                     }
                 }
                 w.mask[wd][lane] = m;
-                if (!coarse)
-                    evald += __popc(m);
+                evald += __popc(m);
             }
             int wd = 0;
             unsigned m = w.mask[0][lane];
@@ -623,12 +540,7 @@ __device__ __forceinline__ void flush_leaves(WarpSmem& w, int nl, const float4* 
                 const int b = __ffs(m) - 1;
                 m &= m - 1u;
                 const float4 s4 = w.tile[(wd << 5) + b];
-                if (coarse) {
-                    // the exact test: a source of the coarse filter's shell adds exactly zero
-                    evald += pair_fast<SPLIT>(s4, tx, ty, tz, p.eps2, p.rcut2, true, sk, fx, fy, fz);
-                } else {
-                    pair_fast<SPLIT>(s4, tx, ty, tz, p.eps2, p.rcut2, false, sk, fx, fy, fz);
-                }
+                pair_fast<SPLIT>(s4, tx, ty, tz, p.eps2, p.rcut2, false, sk, fx, fy, fz);
                 if (rec)
                     record(s4, w.tidx[(wd << 5) + b]);
             }
@@ -764,9 +676,6 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
             gc[a] = __fmul_rn(0.5f, __fadd_rn(gmin[a], gmax[a]));
             ghalf[a] = __fmul_rn(0.5f, __fsub_rn(gmax[a], gmin[a]));
         }
-        if (lane == 0 && cut)  // the coarse filter's frame (units of the cutoff)
-            w.gframe = make_float4(gc[0], gc[1], gc[2],
-                                   fmaxf(ghalf[0], fmaxf(ghalf[1], ghalf[2])) * rsqrtf(p.rcut2));
 
         if (lane == 0)
             w.stack[0] = groot[g];  // the group's system root (node 0 for a single system)
