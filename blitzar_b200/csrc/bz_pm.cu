@@ -594,63 +594,100 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
     }
 }
 
-// Analytic differentiation: four lanes per particle as in k_interp, lane q taking stencil
-// column x = bx + q of the scalar potential mesh; the weight of cell (a, b, c) in the x
-// component is dW_x(a) W_y(b) W_z(c), and likewise for y and z.  The potential mesh holds one
-// float per cell, so a quad reads 16-byte row segments.
+// Analytic differentiation with the potential staged in shared memory, the gather twin of
+// k_deposit_tiled: a block takes a chunk of Morton-consecutive particles (the deposit's chunk,
+// whose stencils fit one tile), loads the box of cells their stencils cover once, row by row,
+// and each thread then reads its particle's stencil from shared memory.  A chunk whose box
+// does not fit gathers from the global mesh instead.  The sums are those of k_interp_ad
+// (over x within a row, then y, then z): a = (1/h) sum_c phi_c grad W(x - x_c), the weight of
+// cell (a, b, c) in the x component being dW_x(a) W_y(b) W_z(c), and likewise for y and z.
 template <int P>
-__global__ void __launch_bounds__(kThreads) k_interp_ad(const float4* __restrict__ pos4, int n, int mesh,
-                                                         float inv_h_fixed, const IsoGrid* iso,
-                                                         const float* __restrict__ phi,
-                                                         float* __restrict__ ax, float* __restrict__ ay,
-                                                         float* __restrict__ az)
+__global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __restrict__ pos4, int n,
+                                                               int chunk, int mesh, float inv_h_fixed,
+                                                               const IsoGrid* iso,
+                                                               const float* __restrict__ phi,
+                                                               float* __restrict__ ax,
+                                                               float* __restrict__ ay,
+                                                               float* __restrict__ az)
 {
+    __shared__ float tile[kTileCells];
+    __shared__ int s_lo[3], s_hi[3];
     const MeshFrame fr = mesh_frame(iso, inv_h_fixed);
     const float inv_h = fr.inv_h;
+    const int base = blockIdx.x * chunk;
+    const int end = min(base + chunk, n);
+    if (threadIdx.x < 3) {
+        s_lo[threadIdx.x] = 1 << 30;
+        s_hi[threadIdx.x] = -(1 << 30);
+    }
+    __syncthreads();
+    int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
+    for (int i = base + threadIdx.x; i < end; i += kThreads) {
+        const float4 p = pos4[i];
+        float w[P];
+        const int b[3] = {stencil<P>(p.x - fr.ox, inv_h, mesh, w), stencil<P>(p.y - fr.oy, inv_h, mesh, w),
+                          stencil<P>(p.z - fr.oz, inv_h, mesh, w)};
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = min(lo[a], b[a]);
+            hi[a] = max(hi[a], b[a] + P - 1);
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        atomicMin(&s_lo[a], lo[a]);
+        atomicMax(&s_hi[a], hi[a]);
+    }
+    __syncthreads();
+    const int ox = s_lo[0], oy = s_lo[1], oz = s_lo[2];
+    const int ex = s_hi[0] - ox + 1, ey = s_hi[1] - oy + 1, ez = s_hi[2] - oz + 1;
+    const bool tiled = ex > 0 && ey > 0 && ez > 0 && static_cast<long long>(ex) * ey * ez <= kTileCells;
     const size_t M = static_cast<size_t>(mesh);
-    const int q = threadIdx.x & 3;
-    constexpr int kRound = (kThreads / 32) * 8;
-    const int per_block = ((n + gridDim.x - 1) / gridDim.x + kRound - 1) / kRound * kRound;
-    const int start = blockIdx.x * per_block;
-    const int stop = min(start + per_block, n);
-    for (int i0 = start + (threadIdx.x >> 5) * 8; i0 < stop; i0 += kRound) {
-        const int i = i0 + ((threadIdx.x & 31) >> 2);
+    if (tiled) {
+        const int cells = ex * ey * ez;
+        for (int c = threadIdx.x; c < cells; c += kThreads) {
+            const int x = c % ex, r = c / ex;
+            const int y = r % ey, z = r / ey;
+            tile[c] = __ldg(&phi[(static_cast<size_t>(wrapm(oz + z, mesh)) * M + wrapm(oy + y, mesh)) * M +
+                                 wrapm(ox + x, mesh)]);
+        }
+    }
+    __syncthreads();
+    for (int i = base + threadIdx.x; i < end; i += kThreads) {
+        const float4 p = pos4[i];
+        float wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
+        const int bx = stencil_d<P>(p.x - fr.ox, inv_h, mesh, wx, dx);
+        const int by = stencil_d<P>(p.y - fr.oy, inv_h, mesh, wy, dy);
+        const int bz = stencil_d<P>(p.z - fr.oz, inv_h, mesh, wz, dz);
         float gx = 0.0f, gy = 0.0f, gz = 0.0f;
-        if (i < stop && q < P) {
-            const float4 p = pos4[i];
-            float wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
-            const int bx = stencil_d<P>(p.x - fr.ox, inv_h, mesh, wx, dx);
-            const int by = stencil_d<P>(p.y - fr.oy, inv_h, mesh, wy, dy);
-            const int bz = stencil_d<P>(p.z - fr.oz, inv_h, mesh, wz, dz);
-            const float wq = column_weight<P>(wx, q);
-            const float dq = column_weight<P>(dx, q);
-            const int xs = wrap1(bx + q, mesh);
 #pragma unroll
-            for (int c = 0; c < P; ++c) {
-                const size_t zrow = static_cast<size_t>(wrap1(bz + c, mesh)) * M;
-                float sx = 0.0f, sy = 0.0f;  // this z plane's sums over y: W_y and dW_y weighted
+        for (int c = 0; c < P; ++c) {
+            float txd = 0.0f, tyw = 0.0f, tzw = 0.0f;
 #pragma unroll
-                for (int b = 0; b < P; ++b) {
-                    const float v = __ldg(&phi[(zrow + wrap1(by + b, mesh)) * M + xs]);
-                    sx = fmaf(v, wy[b], sx);
-                    sy = fmaf(v, dy[b], sy);
+            for (int b = 0; b < P; ++b) {
+                float rw = 0.0f, rd = 0.0f;  // this row's sums over x: W_x and dW_x weighted
+#pragma unroll
+                for (int a = 0; a < P; ++a) {
+                    float v;
+                    if (tiled)
+                        v = tile[((bz + c - oz) * ey + (by + b - oy)) * ex + (bx + a - ox)];
+                    else
+                        v = __ldg(&phi[(static_cast<size_t>(wrap1(bz + c, mesh)) * M + wrap1(by + b, mesh)) * M +
+                                       wrap1(bx + a, mesh)]);
+                    rw = fmaf(v, wx[a], rw);
+                    rd = fmaf(v, dx[a], rd);
                 }
-                gx = fmaf(sx * dq, wz[c], gx);
-                gy = fmaf(sy * wq, wz[c], gy);
-                gz = fmaf(sx * wq, dz[c], gz);
+                txd = fmaf(rd, wy[b], txd);
+                tyw = fmaf(rw, dy[b], tyw);
+                tzw = fmaf(rw, wy[b], tzw);
             }
+            gx = fmaf(txd, wz[c], gx);
+            gy = fmaf(tyw, wz[c], gy);
+            gz = fmaf(tzw, dz[c], gz);
         }
-#pragma unroll
-        for (int o = 1; o < 4; o <<= 1) {
-            gx += __shfl_xor_sync(kFullMask, gx, o);
-            gy += __shfl_xor_sync(kFullMask, gy, o);
-            gz += __shfl_xor_sync(kFullMask, gz, o);
-        }
-        if (i < stop && q == 0) {
-            ax[i] = gx * inv_h;
-            ay[i] = gy * inv_h;
-            az[i] = gz * inv_h;
-        }
+        ax[i] = gx * inv_h;
+        ay[i] = gy * inv_h;
+        az[i] = gz * inv_h;
     }
 }
 
@@ -831,12 +868,15 @@ void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float
     b = b < sm_count() * 8 ? b : sm_count() * 8;
     count_launch();
     if (p->gradient == 2) {
+        // the potential staged in shared memory per chunk of particles (the deposit's chunks)
+        const int chunk = pm_deposit_chunk(p, n);
+        const int blocks = (n + chunk - 1) / chunk;
         if (p->order == 2)
-            k_interp_ad<2><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->iso, p->rho, ax, ay, az);
+            k_interp_ad_tiled<2><<<blocks, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, p->iso, p->rho, ax, ay, az);
         else if (p->order == 3)
-            k_interp_ad<3><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->iso, p->rho, ax, ay, az);
+            k_interp_ad_tiled<3><<<blocks, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, p->iso, p->rho, ax, ay, az);
         else
-            k_interp_ad<4><<<b, kThreads, 0, s>>>(pos4, n, M, inv_h, p->iso, p->rho, ax, ay, az);
+            k_interp_ad_tiled<4><<<blocks, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, p->iso, p->rho, ax, ay, az);
         return;
     }
     if (p->order == 2)
