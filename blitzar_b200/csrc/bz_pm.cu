@@ -598,9 +598,9 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
 // k_deposit_tiled: a block takes a chunk of Morton-consecutive particles (the deposit's chunk,
 // whose stencils fit one tile), loads the box of cells their stencils cover once, row by row,
 // and each thread then reads its particle's stencil from shared memory.  A chunk whose box
-// does not fit gathers from the global mesh instead.  The sums are those of k_interp_ad
-// (over x within a row, then y, then z): a = (1/h) sum_c phi_c grad W(x - x_c), the weight of
-// cell (a, b, c) in the x component being dW_x(a) W_y(b) W_z(c), and likewise for y and z.
+// does not fit gathers from the global mesh instead.  The sums run over x within a row, then y,
+// then z: a = (1/h) sum_c phi_c grad W(x - x_c), the weight of cell (a, b, c) in the x component
+// being dW_x(a) W_y(b) W_z(c), and likewise for y and z.
 template <int P>
 __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __restrict__ pos4, int n,
                                                                int chunk, int mesh, float inv_h_fixed,
