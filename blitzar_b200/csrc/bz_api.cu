@@ -721,11 +721,12 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
             h->allocations.push_back(g);
             h->iso = static_cast<IsoGrid*>(g);
             h->pm = pm_create(2 * cfg->treepm_grid_size, 0.0, 0.0, cfg->treepm_assignment + 2,
-                              cfg->treepm_gradient, cfg->treepm_window_floor, h->stream, &perr, h->iso);
+                              cfg->treepm_gradient, cfg->treepm_window_floor, h->stream, &perr, h->iso,
+                              h->d.err);
         } else {
             h->pm = pm_create(cfg->treepm_grid_size, cfg->box_length, rsplit_len(h),
                               cfg->treepm_assignment + 2, cfg->treepm_gradient,
-                              cfg->treepm_window_floor, h->stream, &perr);
+                              cfg->treepm_window_floor, h->stream, &perr, nullptr, h->d.err);
         }
         if (!h->pm) {
             bz_destroy(h);

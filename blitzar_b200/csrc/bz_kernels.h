@@ -210,8 +210,10 @@ struct IsoGrid {
 // analytic differentiation; window_floor: lower bound of the deconvolution window (the
 // reference uses 0.08).  iso != NULL: isolated mesh whose grid the device holds at iso (box
 // and rsplit unused); the Green's function is then evaluated in the solve, not tabulated.
+// dev_err: the handle's device error bits (a staged gather whose bulk copies time out sets
+// kErrBulkWait there).
 PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, double window_floor,
-                  cudaStream_t s, int* cuda_err, const IsoGrid* iso = nullptr);
+                  cudaStream_t s, int* cuda_err, const IsoGrid* iso = nullptr, int* dev_err = nullptr);
 // Isolated grid from the FP64 bounding box of the positions: grid_half = G, r_split_cells and
 // r_cut_factor in units of the cell, node_size_factor in units of r_s.
 void launch_iso_grid(const BoxF64* box, int grid_half, float cell_floor, float softening,

@@ -49,6 +49,7 @@ struct PmPlan {
     cufftHandle r2c = 0, c2r = 0;
     size_t bytes = 0;
     const IsoGrid* iso = nullptr;     // isolated mesh: grid on the device, Green in the solve
+    int* err = nullptr;               // device error bits (bounded waits of the staged gathers)
 };
 
 namespace {
@@ -596,11 +597,14 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
 
 // Analytic differentiation with the potential staged in shared memory, the gather twin of
 // k_deposit_tiled: a block takes a chunk of Morton-consecutive particles (the deposit's chunk,
-// whose stencils fit one tile), loads the box of cells their stencils cover once, row by row,
-// and each thread then reads its particle's stencil from shared memory.  A chunk whose box
-// does not fit gathers from the global mesh instead.  The sums run over x within a row, then y,
-// then z: a = (1/h) sum_c phi_c grad W(x - x_c), the weight of cell (a, b, c) in the x component
-// being dW_x(a) W_y(b) W_z(c), and likewise for y and z.
+// whose stencils fit one tile) and stages the box of cells their stencils cover with bulk copies
+// (cp.async.bulk, global -> shared, no multicast), one per mesh row segment: rows start on a
+// 16-byte boundary (x rounded down to a multiple of 4 cells; the mesh side is a multiple of 4),
+// a row crossing the periodic x boundary takes two copies, and all complete on one mbarrier
+// (bounded wait).  Each thread then reads its particle's stencil from shared memory.  A chunk
+// whose box does not fit gathers from the global mesh instead.  The sums run over x within a
+// row, then y, then z: a = (1/h) sum_c phi_c grad W(x - x_c), the weight of cell (a, b, c) in the
+// x component being dW_x(a) W_y(b) W_z(c), and likewise for y and z.
 template <int P>
 __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __restrict__ pos4, int n,
                                                                int chunk, int mesh, float inv_h_fixed,
@@ -608,10 +612,11 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
                                                                const float* __restrict__ phi,
                                                                float* __restrict__ ax,
                                                                float* __restrict__ ay,
-                                                               float* __restrict__ az)
+                                                               float* __restrict__ az, int* err)
 {
-    __shared__ float tile[kTileCells];
+    __shared__ __align__(16) float tile[kTileCells];
     __shared__ int s_lo[3], s_hi[3];
+    __shared__ unsigned long long bar;
     const MeshFrame fr = mesh_frame(iso, inv_h_fixed);
     const float inv_h = fr.inv_h;
     const int base = blockIdx.x * chunk;
@@ -620,6 +625,9 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
         s_lo[threadIdx.x] = 1 << 30;
         s_hi[threadIdx.x] = -(1 << 30);
     }
+    if (threadIdx.x == 0)
+        mbar_init(&bar, 1);
+    fence_mbar_init();
     __syncthreads();
     int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
@@ -639,20 +647,31 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
         atomicMax(&s_hi[a], hi[a]);
     }
     __syncthreads();
-    const int ox = s_lo[0], oy = s_lo[1], oz = s_lo[2];
-    const int ex = s_hi[0] - ox + 1, ey = s_hi[1] - oy + 1, ez = s_hi[2] - oz + 1;
-    const bool tiled = ex > 0 && ey > 0 && ez > 0 && static_cast<long long>(ex) * ey * ez <= kTileCells;
+    // x rounded out to whole 16-byte groups of four cells
+    const int ox = s_lo[0] - (((s_lo[0] % 4) + 4) % 4);
+    const int oy = s_lo[1], oz = s_lo[2];
+    const int ex = ((s_hi[0] + 1 - ox) + 3) & ~3;
+    const int ey = s_hi[1] - oy + 1, ez = s_hi[2] - oz + 1;
+    const bool tiled = ex > 0 && ey > 0 && ez > 0 && ex <= mesh &&
+                       static_cast<long long>(ex) * ey * ez <= kTileCells && (mesh & 3) == 0;
     const size_t M = static_cast<size_t>(mesh);
     if (tiled) {
-        const int cells = ex * ey * ez;
-        for (int c = threadIdx.x; c < cells; c += kThreads) {
-            const int x = c % ex, r = c / ex;
+        const int rows = ey * ez;
+        if (threadIdx.x == 0)
+            mbar_arrive_expect_tx(&bar, static_cast<uint32_t>(rows) * static_cast<uint32_t>(ex) * 4u);
+        __syncthreads();
+        for (int r = threadIdx.x; r < rows; r += kThreads) {
             const int y = r % ey, z = r / ey;
-            tile[c] = __ldg(&phi[(static_cast<size_t>(wrapm(oz + z, mesh)) * M + wrapm(oy + y, mesh)) * M +
-                                 wrapm(ox + x, mesh)]);
+            const float* row = phi + (static_cast<size_t>(wrapm(oz + z, mesh)) * M + wrapm(oy + y, mesh)) * M;
+            float* dst = tile + static_cast<size_t>(r) * ex;
+            const int x0 = wrapm(ox, mesh);           // a multiple of four
+            const int first = min(ex, mesh - x0);      // cells before the periodic x boundary
+            bulk_g2s(dst, row + x0, static_cast<uint32_t>(first) * 4u, &bar);
+            if (first < ex)
+                bulk_g2s(dst + first, row, static_cast<uint32_t>(ex - first) * 4u, &bar);
         }
+        mbar_wait_bounded(&bar, 0u, err);
     }
-    __syncthreads();
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
         float wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
@@ -702,10 +721,11 @@ int sm_count()
 } // namespace
 
 PmPlan* pm_create(int mesh, double box, double rsplit, int order, int gradient, double window_floor,
-                  cudaStream_t s, int* cuda_err, const IsoGrid* iso)
+                  cudaStream_t s, int* cuda_err, const IsoGrid* iso, int* dev_err)
 {
     PmPlan* p = new PmPlan();
     p->iso = iso;
+    p->err = dev_err;
     p->mesh = mesh;
     p->box = box;
     p->rsplit = rsplit;
@@ -872,11 +892,14 @@ void pm_interp(PmPlan* p, const float4* pos4, int n, float* ax, float* ay, float
         const int chunk = pm_deposit_chunk(p, n);
         const int blocks = (n + chunk - 1) / chunk;
         if (p->order == 2)
-            k_interp_ad_tiled<2><<<blocks, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, p->iso, p->rho, ax, ay, az);
+            k_interp_ad_tiled<2><<<blocks, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, p->iso, p->rho, ax, ay, az,
+                                                                   p->err);
         else if (p->order == 3)
-            k_interp_ad_tiled<3><<<blocks, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, p->iso, p->rho, ax, ay, az);
+            k_interp_ad_tiled<3><<<blocks, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, p->iso, p->rho, ax, ay, az,
+                                                                   p->err);
         else
-            k_interp_ad_tiled<4><<<blocks, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, p->iso, p->rho, ax, ay, az);
+            k_interp_ad_tiled<4><<<blocks, kThreads, 0, s>>>(pos4, n, chunk, M, inv_h, p->iso, p->rho, ax, ay, az,
+                                                                   p->err);
         return;
     }
     if (p->order == 2)
