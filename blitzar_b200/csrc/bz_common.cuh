@@ -12,7 +12,7 @@ enum DeviceError : int {
     kErrSortSpin = 2,       // radix-sort look-back gave up waiting for a predecessor tile
     kErrTreeCapacity = 4,   // more octree nodes than the preallocated capacity
     kErrTreeSpin = 8,       // octree level look-back gave up waiting
-    kErrBulkWait = 16,      // a bulk-copy mbarrier wait ran out of iterations
+    kErrBulkWait = 16,      // a bulk-copy or MMA mbarrier wait ran out of time
     kErrListCapacity = 32,  // an interaction list exceeded its shared-memory capacity
 };
 
@@ -112,15 +112,41 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t 
     return ok != 0;
 }
 
-// Bounded wait: gives up after kSpinLimit polls, raising kErrBulkWait.
+// try_wait with a suspend-time hint: a thread whose phase has not completed sleeps (up to ns
+// nanoseconds, or until the phase completes) instead of polling, leaving its issue slots to
+// the other warps of the SM.
+__device__ __forceinline__ bool mbar_try_wait_suspend(unsigned long long* bar, uint32_t parity, uint32_t ns)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ uint64_t global_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: suspends on the mbarrier and gives up after about a second of device time
+// (global timer), raising kErrBulkWait.
+constexpr uint64_t kWaitLimitNs = 1000000000ull;
 __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, uint32_t parity, int* err)
 {
-    for (int it = 0; it < kSpinLimit; ++it) {
-        if (mbar_try_wait(bar, parity))
+    if (mbar_try_wait(bar, parity))
+        return true;
+    const uint64_t t0 = global_ns();
+    do {
+        if (mbar_try_wait_suspend(bar, parity, 20000u))
             return true;
-        if (it > 64)
-            __nanosleep(64);
-    }
+    } while (global_ns() - t0 < kWaitLimitNs);
     raise_error(err, kErrBulkWait);
     return false;
 }

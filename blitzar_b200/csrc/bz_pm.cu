@@ -57,29 +57,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kTileCells = 12000;      // 47 KB of float accumulators (static shared memory <= 48 KB)
 
-__device__ __forceinline__ float tsc_w(float d)
-{
-    const float a = fabsf(d);
-    if (a < 0.5f)
-        return 0.75f - a * a;
-    if (a < 1.5f) {
-        const float t = 1.5f - a;
-        return 0.5f * t * t;
-    }
-    return 0.0f;
-}
-__device__ __forceinline__ float pcs_w(float d)
-{
-    const float a = fabsf(d);
-    if (a < 1.0f)
-        return (4.0f - 6.0f * a * a + 3.0f * a * a * a) * (1.0f / 6.0f);
-    if (a < 2.0f) {
-        const float t = 2.0f - a;
-        return t * t * t * (1.0f / 6.0f);
-    }
-    return 0.0f;
-}
-
 // Mesh frame of a plan: periodic meshes start at 0 with a fixed cell; an isolated mesh reads
 // its origin and cell from the device-held grid of the current force evaluation.
 struct MeshFrame {
@@ -92,97 +69,94 @@ __device__ __forceinline__ MeshFrame mesh_frame(const IsoGrid* iso, float inv_h)
     return MeshFrame{0.0f, 0.0f, 0.0f, inv_h};
 }
 
-// Stencil of order P along one axis: first (unwrapped) node index and P weights.  coord is
-// the position relative to the mesh origin; for an isolated mesh the particles lie in its
-// central half, so the periodic fold below never applies there.
+// Stencil of order P along one axis.  coord is the position relative to the mesh origin; for an
+// isolated mesh the particles lie in its central half, so the periodic fold below never applies
+// there.  stencil_base returns the first (unwrapped) node index and the particle's offset t in
+// its stencil: the particle lies at base + t for CIC and at base + 1 + t for TSC and PCS, with t
+// in [0, 1) for CIC and PCS and in [-1/2, 1/2) for TSC (the offset from the nearest node).
 template <int P>
-__device__ __forceinline__ int stencil(float coord, float inv_h, int mesh, float* w)
+__device__ __forceinline__ int stencil_base(float coord, float inv_h, int mesh, float& t)
 {
     const float raw = coord * inv_h;
     const float m = static_cast<float>(mesh);
-    const float s = raw - floorf(raw / m) * m;  // [0, M]
-    if (P == 2) {
-        const float fl = floorf(s);
-        const float f = s - fl;
-        w[0] = 1.0f - f;
-        w[1] = f;
-        return static_cast<int>(fl);
-    } else if (P == 3) {
+    // fold into [0, M): the product with 1/M may miss the exact quotient by one period at a
+    // boundary, which the two compares put back
+    float s = raw - floorf(raw * (1.0f / m)) * m;
+    s = s < 0.0f ? s + m : s;
+    s = s >= m ? s - m : s;
+    if (P == 3) {
         const float c = floorf(s + 0.5f);
-        w[0] = tsc_w(s - (c - 1.0f));
-        w[1] = tsc_w(s - c);
-        w[2] = tsc_w(s - (c + 1.0f));
+        t = s - c;
         return static_cast<int>(c) - 1;
+    }
+    const float fl = floorf(s);
+    t = s - fl;
+    return static_cast<int>(fl) - (P == 4 ? 1 : 0);
+}
+
+// The assignment weights W(d) of the P nodes, d = particle - node in cells, written per node
+// for the offset t of stencil_base (no branches on |d|):
+//   CIC  W = 1 - |d|;
+//   TSC  W = 3/4 - d^2 (|d| < 1/2), (3/2 - |d|)^2 / 2 (|d| < 3/2);
+//   PCS  W = 2/3 - d^2 + |d|^3 / 2 (|d| < 1), (2 - |d|)^3 / 6 (|d| < 2).
+// dw holds dW/dd, the derivative with respect to the particle coordinate in cells.
+template <int P>
+__device__ __forceinline__ void stencil_weights(float t, float* w)
+{
+    if (P == 2) {
+        w[0] = 1.0f - t;
+        w[1] = t;
+    } else if (P == 3) {
+        const float a = 0.5f - t, b = 0.5f + t;
+        w[0] = 0.5f * a * a;
+        w[1] = 0.75f - t * t;
+        w[2] = 0.5f * b * b;
     } else {
-        const float fl = floorf(s);
-        w[0] = pcs_w(s - (fl - 1.0f));
-        w[1] = pcs_w(s - fl);
-        w[2] = pcs_w(s - (fl + 1.0f));
-        w[3] = pcs_w(s - (fl + 2.0f));
-        return static_cast<int>(fl) - 1;
+        const float u = 1.0f - t;
+        const float t2 = t * t, u2 = u * u;
+        w[0] = (1.0f / 6.0f) * u2 * u;
+        w[1] = (2.0f / 3.0f) - t2 * fmaf(-0.5f, t, 1.0f);
+        w[2] = (2.0f / 3.0f) - u2 * fmaf(-0.5f, u, 1.0f);
+        w[3] = (1.0f / 6.0f) * t2 * t;
+    }
+}
+template <int P>
+__device__ __forceinline__ void stencil_weights_d(float t, float* w, float* dw)
+{
+    stencil_weights<P>(t, w);
+    if (P == 2) {
+        dw[0] = -1.0f;
+        dw[1] = 1.0f;
+    } else if (P == 3) {
+        dw[0] = t - 0.5f;
+        dw[1] = -2.0f * t;
+        dw[2] = t + 0.5f;
+    } else {
+        const float u = 1.0f - t;
+        dw[0] = -0.5f * u * u;
+        dw[1] = t * fmaf(1.5f, t, -2.0f);
+        dw[2] = u * fmaf(-1.5f, u, 2.0f);
+        dw[3] = 0.5f * t * t;
     }
 }
 
-// Derivatives of the weights with respect to the particle coordinate in cells.
-__device__ __forceinline__ float tsc_dw(float d)
+template <int P>
+__device__ __forceinline__ int stencil(float coord, float inv_h, int mesh, float* w)
 {
-    const float a = fabsf(d);
-    if (a < 0.5f)
-        return -2.0f * d;
-    if (a < 1.5f)
-        return -copysignf(1.5f - a, d);  // -(1.5 - |d|) sign(d)
-    return 0.0f;
-}
-__device__ __forceinline__ float pcs_dw(float d)
-{
-    const float a = fabsf(d);
-    if (a < 1.0f)
-        return d * (1.5f * a - 2.0f);
-    if (a < 2.0f) {
-        const float t = 2.0f - a;
-        return -copysignf(0.5f * t * t, d);  // -(2 - |d|)^2 / 2 sign(d)
-    }
-    return 0.0f;
+    float t;
+    const int base = stencil_base<P>(coord, inv_h, mesh, t);
+    stencil_weights<P>(t, w);
+    return base;
 }
 
 // As stencil<P>, with the derivatives dw of the weights (per cell of coordinate).
 template <int P>
 __device__ __forceinline__ int stencil_d(float coord, float inv_h, int mesh, float* w, float* dw)
 {
-    const float raw = coord * inv_h;
-    const float m = static_cast<float>(mesh);
-    const float s = raw - floorf(raw / m) * m;
-    if (P == 2) {
-        const float fl = floorf(s);
-        const float f = s - fl;
-        w[0] = 1.0f - f;
-        w[1] = f;
-        dw[0] = -1.0f;
-        dw[1] = 1.0f;
-        return static_cast<int>(fl);
-    } else if (P == 3) {
-        const float c = floorf(s + 0.5f);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            w[k] = tsc_w(s - (c - 1.0f + k));
-            dw[k] = tsc_dw(s - (c - 1.0f + k));
-        }
-        return static_cast<int>(c) - 1;
-    } else {
-        const float fl = floorf(s);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            w[k] = pcs_w(s - (fl - 1.0f + k));
-            dw[k] = pcs_dw(s - (fl - 1.0f + k));
-        }
-        return static_cast<int>(fl) - 1;
-    }
-}
-
-__device__ __forceinline__ int wrapm(int i, int m)
-{
-    i %= m;
-    return i < 0 ? i + m : i;
+    float t;
+    const int base = stencil_base<P>(coord, inv_h, mesh, t);
+    stencil_weights_d<P>(t, w, dw);
+    return base;
 }
 
 // Index i + d, d in [-m, m], wrapped into [0, m).
@@ -197,6 +171,71 @@ __device__ __forceinline__ float column_weight(const float* w, int q)
     for (int a = 0; a < P; ++a)
         r = q == a ? w[a] : r;
     return r;
+}
+
+// Tile pitches of the staged interpolation and deposit boxes, padded so that the particles of a
+// warp, Morton neighbours, touch mostly distinct banks.  The interpolation serves a particle
+// with four lanes (eight particles a warp), the deposit with one thread: a bank model over the
+// 128^3 benchmark box gives about 1.5 and 4 shared-memory wavefronts per access with these pads,
+// against 3.4 and 11.5 unpadded.  All are multiples of 4 cells, so rows start on a 16-byte
+// boundary.
+constexpr int kRowPad = 8;
+constexpr int kPlanePad = 12;
+constexpr int kDepositRowPad = 12;
+constexpr int kDepositPlanePad = 12;
+
+// The scatter of k_deposit_tiled, one thread per particle: all threads of a warp add the same
+// stencil offset together, so two of them meet on one cell only when their particles share a
+// stencil base (four lanes per particle, one x column each, would collide whenever neighbours'
+// bases differ by under four cells along x).  Fixed point into the block's tile (TILED, with
+// red.shared on shared-window addresses), or floating point into the global mesh.
+template <int P, bool TILED>
+__device__ __forceinline__ void deposit_particles(const float4* __restrict__ pos4, int base, int end,
+                                                  const MeshFrame& fr, int mesh, float inv_h3, float scale,
+                                                  int* tile, int ox, int oy, int oz, int rp, int pp,
+                                                  float* __restrict__ rho)
+{
+    const size_t M = static_cast<size_t>(mesh);
+    for (int i = base + threadIdx.x; i < end; i += kThreads) {
+        const float4 p = pos4[i];
+        float tx, ty, tz;
+        const int bx = stencil_base<P>(p.x - fr.ox, fr.inv_h, mesh, tx);
+        const int by = stencil_base<P>(p.y - fr.oy, fr.inv_h, mesh, ty);
+        const int bz = stencil_base<P>(p.z - fr.oz, fr.inv_h, mesh, tz);
+        float wx[P], wy[P], wz[P];
+        stencil_weights<P>(tx, wx);
+        stencil_weights<P>(ty, wy);
+        stencil_weights<P>(tz, wz);
+        const float m = p.w * inv_h3;
+        if (TILED) {
+            const uint32_t corner = smem_u32(tile + (bz - oz) * pp + (by - oy) * rp + (bx - ox));
+#pragma unroll
+            for (int c = 0; c < P; ++c)
+#pragma unroll
+                for (int b = 0; b < P; ++b) {
+                    const float wzy = m * wz[c] * wy[b];
+                    const uint32_t row = corner + 4u * static_cast<uint32_t>(c * pp + b * rp);
+#pragma unroll
+                    for (int a = 0; a < P; ++a)
+                        asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(row + 4u * a),
+                                     "r"(__float2int_rn(wzy * wx[a] * scale))
+                                     : "memory");
+                }
+        } else {
+#pragma unroll
+            for (int c = 0; c < P; ++c) {
+                const size_t zrow = static_cast<size_t>(wrap1(bz + c, mesh)) * M;
+#pragma unroll
+                for (int b = 0; b < P; ++b) {
+                    const float wzy = m * wz[c] * wy[b];
+                    const size_t row = (zrow + wrap1(by + b, mesh)) * M;
+#pragma unroll
+                    for (int a = 0; a < P; ++a)
+                        atomicAdd(&rho[row + wrap1(bx + a, mesh)], wzy * wx[a]);
+                }
+            }
+        }
+    }
 }
 
 template <int P>
@@ -215,7 +254,7 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
     // rounding of at most chunk x P^3 contributions adds less than 2^15.  One unit is then
     // below 2 x 1.01 x (largest weight)^3 x sum |m| / h^3 / 2^31: with at most 512 particles a
     // chunk, a few 1e-7 of a mean cell.
-    __shared__ int tile[kTileCells];
+    __shared__ __align__(16) int tile[kTileCells];
     __shared__ int s_lo[3], s_hi[3];
     __shared__ float s_mass, s_scale, s_unscale;
     const int base = blockIdx.x * chunk;
@@ -231,9 +270,9 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
     float msum = 0.0f;
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
-        float w[P];
-        const int b[3] = {stencil<P>(p.x - fr.ox, inv_h, mesh, w), stencil<P>(p.y - fr.oy, inv_h, mesh, w),
-                          stencil<P>(p.z - fr.oz, inv_h, mesh, w)};
+        float t;
+        const int b[3] = {stencil_base<P>(p.x - fr.ox, inv_h, mesh, t), stencil_base<P>(p.y - fr.oy, inv_h, mesh, t),
+                          stencil_base<P>(p.z - fr.oz, inv_h, mesh, t)};
         for (int a = 0; a < 3; ++a) {
             lo[a] = min(lo[a], b[a]);
             hi[a] = max(hi[a], b[a] + P - 1);
@@ -241,8 +280,11 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
         msum += fabsf(p.w);
     }
     for (int a = 0; a < 3; ++a) {
-        atomicMin(&s_lo[a], lo[a]);
-        atomicMax(&s_hi[a], hi[a]);
+        const int wl = __reduce_min_sync(kFullMask, lo[a]), wh = __reduce_max_sync(kFullMask, hi[a]);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&s_lo[a], wl);
+            atomicMax(&s_hi[a], wh);
+        }
     }
     for (int o = 16; o > 0; o >>= 1)
         msum += __shfl_xor_sync(kFullMask, msum, o);
@@ -261,74 +303,64 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
         s_scale = ldexpf(1.0f, k);
         s_unscale = ldexpf(1.0f, -k);
     }
-    const int ex = s_hi[0] - s_lo[0] + 1, ey = s_hi[1] - s_lo[1] + 1, ez = s_hi[2] - s_lo[2] + 1;
-    const bool tiled = ex > 0 && ey > 0 && ez > 0 && static_cast<long long>(ex) * ey * ez <= kTileCells;
-    const int ox = s_lo[0], oy = s_lo[1], oz = s_lo[2];
+    // x rounded out to whole groups of four cells, so that the flush reads the tile in int4 and
+    // adds four cells at a time
+    const int ox = s_lo[0] - (((s_lo[0] % 4) + 4) % 4);
+    const int oy = s_lo[1], oz = s_lo[2];
+    const int ex = ((s_hi[0] + 1 - ox) + 3) & ~3;
+    const int ey = s_hi[1] - oy + 1, ez = s_hi[2] - oz + 1;
+    const int rp = ex + kDepositRowPad, pp = ey * rp + kDepositPlanePad;  // padded pitches
+    const bool tiled = ex > 0 && ey > 0 && ez > 0 && static_cast<long long>(pp) * ez <= kTileCells;
     if (tiled)
-        for (int c = threadIdx.x; c < ex * ey * ez; c += kThreads)
-            tile[c] = 0;
+        for (int c = threadIdx.x; c < pp * ez / 4; c += kThreads)
+            reinterpret_cast<int4*>(tile)[c] = make_int4(0, 0, 0, 0);
     __syncthreads();
     const float scale = s_scale, unscale = s_unscale;
-    const size_t M = static_cast<size_t>(mesh);
-    for (int i = base + threadIdx.x; i < end; i += kThreads) {
-        const float4 p = pos4[i];
-        float wx[P], wy[P], wz[P];
-        const int bx = stencil<P>(p.x - fr.ox, inv_h, mesh, wx);
-        const int by = stencil<P>(p.y - fr.oy, inv_h, mesh, wy);
-        const int bz = stencil<P>(p.z - fr.oz, inv_h, mesh, wz);
-        const float m = p.w * inv_h3;
-#pragma unroll
-        for (int c = 0; c < P; ++c)
-#pragma unroll
-            for (int b = 0; b < P; ++b) {
-                const float wzy = m * wz[c] * wy[b];
-#pragma unroll
-                for (int a = 0; a < P; ++a) {
-                    const float v = wzy * wx[a];
-                    if (tiled) {
-                        atomicAdd(&tile[((bz + c - oz) * ey + (by + b - oy)) * ex + (bx + a - ox)],
-                                  __float2int_rn(v * scale));
-                    } else {
-                        const size_t g = (static_cast<size_t>(wrapm(bz + c, mesh)) * M + wrapm(by + b, mesh)) * M +
-                                         wrapm(bx + a, mesh);
-                        atomicAdd(&rho[g], v);
-                    }
-                }
-            }
-    }
+    if (tiled)
+        deposit_particles<P, true>(pos4, base, end, fr, mesh, inv_h3, scale, tile, ox, oy, oz, rp, pp, rho);
+    else
+        deposit_particles<P, false>(pos4, base, end, fr, mesh, inv_h3, scale, tile, ox, oy, oz, rp, pp, rho);
     if (!tiled)
         return;
     __syncthreads();
-    // Flush the tile row by row.  Where a row segment is contiguous in the mesh (no periodic
-    // wrap) and 16-byte aligned, four cells go in one vector atomic (red.global.add.v4.f32).
-    const int quads = (ex + 3 + 3) / 4;  // enough 4-cell groups to cover a row from any alignment
-    for (int r = threadIdx.x; r < ey * ez * quads; r += kThreads) {
-        const int q = r % quads, row = r / quads;
-        const int y = row % ey, z = row / ey;
-        const size_t rowbase = (static_cast<size_t>(wrapm(oz + z, mesh)) * M + wrapm(oy + y, mesh)) * M;
-        // group q covers mesh x in [xa, xa + 4) with xa 4-aligned relative to the unwrapped origin
-        const int xa = ((ox >> 2) << 2) + 4 * q;
-        float v[4];
-        bool any = false;
+    // Flush the tile in groups of four cells: thread t takes groups t, t + kThreads, ... of the
+    // (z, y, group) range, its indices advanced by constant steps.  Where the group is
+    // contiguous in the mesh (no periodic wrap; the mesh side a multiple of 4), its four cells go
+    // in one vector atomic (red.global.add.v4.f32).
+    const size_t M = static_cast<size_t>(mesh);
+    const int quads = ex / 4;
+    const int items = ey * ez * quads;
+    int row = threadIdx.x / quads, qd = threadIdx.x - row * quads;
+    int z = row / ey, y = row - z * ey;
+    const int dq = kThreads % quads, drow = kThreads / quads;
+    const int dz = drow / ey, dy = drow - dz * ey;
+    for (int f = threadIdx.x; f < items; f += kThreads) {
+        const int4 c4 = *reinterpret_cast<const int4*>(tile + z * pp + y * rp + 4 * qd);
+        if ((c4.x | c4.y | c4.z | c4.w) != 0) {
+            const float v[4] = {static_cast<float>(c4.x) * unscale, static_cast<float>(c4.y) * unscale,
+                                static_cast<float>(c4.z) * unscale, static_cast<float>(c4.w) * unscale};
+            const size_t rowbase = (static_cast<size_t>(wrap1(oz + z, mesh)) * M + wrap1(oy + y, mesh)) * M;
+            const int gx = wrap1(ox + 4 * qd, mesh);
+            if (gx + 3 < mesh && (mesh & 3) == 0) {
+                float* dst = rho + rowbase + gx;
+                asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst), "f"(v[0]),
+                             "f"(v[1]), "f"(v[2]), "f"(v[3])
+                             : "memory");
+            } else {
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int tx = xa + j - ox;
-            v[j] = (tx >= 0 && tx < ex) ? static_cast<float>(tile[(z * ey + y) * ex + tx]) * unscale : 0.0f;
-            any = any || v[j] != 0.0f;
+                for (int j = 0; j < 4; ++j)
+                    if (v[j] != 0.0f)
+                        atomicAdd(&rho[rowbase + wrap1(gx + j, mesh)], v[j]);
+            }
         }
-        if (!any)
-            continue;
-        const int gx = wrapm(xa, mesh);
-        if (gx + 3 < mesh && (mesh & 3) == 0) {
-            float* dst = rho + rowbase + gx;
-            asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst), "f"(v[0]), "f"(v[1]),
-                         "f"(v[2]), "f"(v[3])
-                         : "memory");
-        } else {
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-                if (v[j] != 0.0f)
-                    atomicAdd(&rho[rowbase + wrapm(xa + j, mesh)], v[j]);
+        qd += dq;
+        const int carry = qd >= quads ? 1 : 0;
+        qd -= carry * quads;
+        y += dy + carry;
+        z += dz;
+        if (y >= ey) {
+            y -= ey;
+            ++z;
         }
     }
 }
@@ -595,6 +627,70 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
     }
 }
 
+// The gather of k_interp_ad_tiled: four lanes per particle, lane q taking stencil column
+// x = bx + q of every (y, z) row from the staged tile (TILED) or from the global mesh.  The loop
+// bound is uniform over the block, so every lane of a quad reaches the shuffles.
+template <int P, bool TILED>
+__device__ __forceinline__ void interp_ad_quads(const float4* __restrict__ pos4, int base, int end,
+                                                const MeshFrame& fr, int mesh, const float* tile,
+                                                int ox, int oy, int oz, int rp, int pp,
+                                                const float* __restrict__ phi, float* __restrict__ ax,
+                                                float* __restrict__ ay, float* __restrict__ az)
+{
+    const size_t M = static_cast<size_t>(mesh);
+    const int q = threadIdx.x & 3;
+    for (int i0 = base; i0 < end; i0 += kThreads / 4) {
+        const int i = i0 + (threadIdx.x >> 2);
+        float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+        if (i < end && q < P) {
+            const float4 p = pos4[i];
+            float tx, ty, tz;
+            const int bx = stencil_base<P>(p.x - fr.ox, fr.inv_h, mesh, tx);
+            const int by = stencil_base<P>(p.y - fr.oy, fr.inv_h, mesh, ty);
+            const int bz = stencil_base<P>(p.z - fr.oz, fr.inv_h, mesh, tz);
+            float wx[P], dx[P], wy[P], dy[P], wz[P], dz[P];
+            stencil_weights_d<P>(tx, wx, dx);
+            stencil_weights_d<P>(ty, wy, dy);
+            stencil_weights_d<P>(tz, wz, dz);
+            const float wq = column_weight<P>(wx, q);
+            const float dq = column_weight<P>(dx, q);
+            const int xs = bx + q;
+            const float* col = nullptr;
+            int xw = 0;
+            if (TILED)
+                col = tile + (bz - oz) * pp + (by - oy) * rp + (xs - ox);
+            else
+                xw = wrap1(xs, mesh);
+#pragma unroll
+            for (int c = 0; c < P; ++c) {
+                float sw = 0.0f, sd = 0.0f;  // this plane's column sums over y: W_y and dW_y weighted
+                const size_t zrow = TILED ? 0 : static_cast<size_t>(wrap1(bz + c, mesh)) * M;
+#pragma unroll
+                for (int b = 0; b < P; ++b) {
+                    const float v = TILED ? col[c * pp + b * rp]
+                                          : __ldg(&phi[(zrow + wrap1(by + b, mesh)) * M + xw]);
+                    sw = fmaf(v, wy[b], sw);
+                    sd = fmaf(v, dy[b], sd);
+                }
+                gx = fmaf(sw * dq, wz[c], gx);
+                gy = fmaf(sd * wq, wz[c], gy);
+                gz = fmaf(sw * wq, dz[c], gz);
+            }
+        }
+#pragma unroll
+        for (int o = 1; o < 4; o <<= 1) {
+            gx += __shfl_xor_sync(kFullMask, gx, o);
+            gy += __shfl_xor_sync(kFullMask, gy, o);
+            gz += __shfl_xor_sync(kFullMask, gz, o);
+        }
+        if (i < end && q == 0) {
+            ax[i] = gx * fr.inv_h;
+            ay[i] = gy * fr.inv_h;
+            az[i] = gz * fr.inv_h;
+        }
+    }
+}
+
 // Analytic differentiation with the potential staged in shared memory, the gather twin of
 // k_deposit_tiled: a block takes a chunk of Morton-consecutive particles (the deposit's chunk,
 // whose stencils fit one tile) and stages the box of cells their stencils cover with bulk copies
@@ -636,9 +732,9 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
     int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
-        float w[P];
-        const int b[3] = {stencil<P>(p.x - fr.ox, inv_h, mesh, w), stencil<P>(p.y - fr.oy, inv_h, mesh, w),
-                          stencil<P>(p.z - fr.oz, inv_h, mesh, w)};
+        float t;
+        const int b[3] = {stencil_base<P>(p.x - fr.ox, inv_h, mesh, t), stencil_base<P>(p.y - fr.oy, inv_h, mesh, t),
+                          stencil_base<P>(p.z - fr.oz, inv_h, mesh, t)};
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             lo[a] = min(lo[a], b[a]);
@@ -647,8 +743,11 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        atomicMin(&s_lo[a], lo[a]);
-        atomicMax(&s_hi[a], hi[a]);
+        const int wl = __reduce_min_sync(kFullMask, lo[a]), wh = __reduce_max_sync(kFullMask, hi[a]);
+        if ((threadIdx.x & 31) == 0) {
+            atomicMin(&s_lo[a], wl);
+            atomicMax(&s_hi[a], wh);
+        }
     }
     __syncthreads();
     // x rounded out to whole 16-byte groups of four cells
@@ -656,8 +755,7 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
     const int oy = s_lo[1], oz = s_lo[2];
     const int ex = ((s_hi[0] + 1 - ox) + 3) & ~3;
     const int ey = s_hi[1] - oy + 1, ez = s_hi[2] - oz + 1;
-    const int rp = ex + 8;            // padded row pitch: a multiple of 4, rows stay 16-byte aligned
-    const int pp = ey * rp + 12;      // padded plane pitch, also a multiple of 4
+    const int rp = ex + kRowPad, pp = ey * rp + kPlanePad;
     const bool tiled = ex > 0 && ey > 0 && ez > 0 && ex <= mesh &&
                        static_cast<long long>(pp) * ez <= kTileCells && (mesh & 3) == 0;
     const size_t M = static_cast<size_t>(mesh);
@@ -667,10 +765,10 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
             mbar_arrive_expect_tx(&bar, static_cast<uint32_t>(rows) * static_cast<uint32_t>(ex) * 4u);
         __syncthreads();
         for (int r = threadIdx.x; r < rows; r += kThreads) {
-            const int y = r % ey, z = r / ey;
-            const float* row = phi + (static_cast<size_t>(wrapm(oz + z, mesh)) * M + wrapm(oy + y, mesh)) * M;
+            const int z = r / ey, y = r - z * ey;
+            const float* row = phi + (static_cast<size_t>(wrap1(oz + z, mesh)) * M + wrap1(oy + y, mesh)) * M;
             float* dst = tile + z * pp + y * rp;
-            const int x0 = wrapm(ox, mesh);           // a multiple of four
+            const int x0 = wrap1(ox, mesh);           // a multiple of four
             const int first = min(ex, mesh - x0);      // cells before the periodic x boundary
             bulk_g2s(dst, row + x0, static_cast<uint32_t>(first) * 4u, &bar);
             if (first < ex)
@@ -678,51 +776,10 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
         }
         mbar_wait_bounded(&bar, 0u, err);
     }
-    // the loop bound is uniform over the block, so every lane of a quad reaches the shuffles
-    const int q = threadIdx.x & 3;
-    for (int i0 = base; i0 < end; i0 += kThreads / 4) {
-        const int i = i0 + (threadIdx.x >> 2);
-        float gx = 0.0f, gy = 0.0f, gz = 0.0f;
-        if (i < end && q < P) {
-            const float4 p = pos4[i];
-            float wx[P], wy[P], wz[P], dx[P], dy[P], dz[P];
-            const int bx = stencil_d<P>(p.x - fr.ox, inv_h, mesh, wx, dx);
-            const int by = stencil_d<P>(p.y - fr.oy, inv_h, mesh, wy, dy);
-            const int bz = stencil_d<P>(p.z - fr.oz, inv_h, mesh, wz, dz);
-            const float wq = column_weight<P>(wx, q);
-            const float dq = column_weight<P>(dx, q);
-            const int xs = bx + q;
-#pragma unroll
-            for (int c = 0; c < P; ++c) {
-                float sw = 0.0f, sd = 0.0f;  // this plane's column sums over y: W_y and dW_y weighted
-#pragma unroll
-                for (int b = 0; b < P; ++b) {
-                    float v;
-                    if (tiled)
-                        v = tile[(bz + c - oz) * pp + (by + b - oy) * rp + (xs - ox)];
-                    else
-                        v = __ldg(&phi[(static_cast<size_t>(wrap1(bz + c, mesh)) * M + wrap1(by + b, mesh)) * M +
-                                       wrap1(xs, mesh)]);
-                    sw = fmaf(v, wy[b], sw);
-                    sd = fmaf(v, dy[b], sd);
-                }
-                gx = fmaf(sw * dq, wz[c], gx);
-                gy = fmaf(sd * wq, wz[c], gy);
-                gz = fmaf(sw * wq, dz[c], gz);
-            }
-        }
-#pragma unroll
-        for (int o = 1; o < 4; o <<= 1) {
-            gx += __shfl_xor_sync(kFullMask, gx, o);
-            gy += __shfl_xor_sync(kFullMask, gy, o);
-            gz += __shfl_xor_sync(kFullMask, gz, o);
-        }
-        if (i < end && q == 0) {
-            ax[i] = gx * inv_h;
-            ay[i] = gy * inv_h;
-            az[i] = gz * inv_h;
-        }
-    }
+    if (tiled)
+        interp_ad_quads<P, true>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, phi, ax, ay, az);
+    else
+        interp_ad_quads<P, false>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, phi, ax, ay, az);
 }
 
 int sm_count()
