@@ -88,6 +88,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-autotune", action="store_true",
                     help="keep the default leaf capacity, group size and mesh overlap")
+    ap.add_argument("--tune", default="",
+                    help="LEAF,GROUP,SCHEDULE: pin the autotuner's three choices instead of "
+                         "tuning (to profile the configuration a tuned run picked)")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-correction comparison (TreePM workloads)")
     return ap.parse_args()
@@ -523,6 +526,12 @@ def run_ours(args, w, rank, world, local):
     n = len(mass)
     stream = torch.cuda.Stream()
     cfg = engine_config(w)
+    pinned = None
+    if args.tune:
+        leaf, group, schedule = (int(v) for v in args.tune.split(","))
+        cfg.update(leaf_capacity=leaf, walk_group_size=group)
+        pinned = dict(leaf_capacity=leaf, walk_group_size=group, mesh_schedule=schedule,
+                      walk_blocks_per_sm=0, pinned=True)
     eng = Engine(n, stream=stream.cuda_stream, device=local, **cfg)
     if systems is not None:
         offsets = eng.set_ensemble(systems)
@@ -530,7 +539,11 @@ def run_ours(args, w, rank, world, local):
         eng.set_state(pos, vel, mass, f64=True)
     dt = w["dt"]
     tuned = None
-    if not args.no_autotune and not w.get("adaptive_levels"):
+    if pinned is not None:
+        if cfg.get("solver") == 1:
+            eng.set_mesh_schedule(pinned["mesh_schedule"])
+        tuned = pinned
+    elif not args.no_autotune and not w.get("adaptive_levels"):
         eng.autotune(trials=5)  # untimed: picks leaf capacity, group size, mesh schedule
         tuned = eng.last_tune
     with torch.cuda.stream(stream):
