@@ -61,12 +61,14 @@ constexpr int kTileCells = 12000;      // 47 KB of float accumulators (static sh
 // its origin and cell from the device-held grid of the current force evaluation.
 struct MeshFrame {
     float ox, oy, oz, inv_h;
+    float inv_m;  // 1 / mesh side, for the periodic fold (one division per thread)
 };
-__device__ __forceinline__ MeshFrame mesh_frame(const IsoGrid* iso, float inv_h)
+__device__ __forceinline__ MeshFrame mesh_frame(const IsoGrid* iso, float inv_h, int mesh)
 {
+    const float inv_m = 1.0f / static_cast<float>(mesh);
     if (iso)
-        return MeshFrame{iso->origin[0], iso->origin[1], iso->origin[2], iso->inv_h};
-    return MeshFrame{0.0f, 0.0f, 0.0f, inv_h};
+        return MeshFrame{iso->origin[0], iso->origin[1], iso->origin[2], iso->inv_h, inv_m};
+    return MeshFrame{0.0f, 0.0f, 0.0f, inv_h, inv_m};
 }
 
 // Stencil of order P along one axis.  coord is the position relative to the mesh origin; for an
@@ -75,13 +77,13 @@ __device__ __forceinline__ MeshFrame mesh_frame(const IsoGrid* iso, float inv_h)
 // its stencil: the particle lies at base + t for CIC and at base + 1 + t for TSC and PCS, with t
 // in [0, 1) for CIC and PCS and in [-1/2, 1/2) for TSC (the offset from the nearest node).
 template <int P>
-__device__ __forceinline__ int stencil_base(float coord, float inv_h, int mesh, float& t)
+__device__ __forceinline__ int stencil_base(float coord, float inv_h, int mesh, float inv_m, float& t)
 {
     const float raw = coord * inv_h;
     const float m = static_cast<float>(mesh);
     // fold into [0, M): the product with 1/M may miss the exact quotient by one period at a
     // boundary, which the two compares put back
-    float s = raw - floorf(raw * (1.0f / m)) * m;
+    float s = raw - floorf(raw * inv_m) * m;
     s = s < 0.0f ? s + m : s;
     s = s >= m ? s - m : s;
     if (P == 3) {
@@ -141,20 +143,20 @@ __device__ __forceinline__ void stencil_weights_d(float t, float* w, float* dw)
 }
 
 template <int P>
-__device__ __forceinline__ int stencil(float coord, float inv_h, int mesh, float* w)
+__device__ __forceinline__ int stencil(float coord, float inv_h, int mesh, float inv_m, float* w)
 {
     float t;
-    const int base = stencil_base<P>(coord, inv_h, mesh, t);
+    const int base = stencil_base<P>(coord, inv_h, mesh, inv_m, t);
     stencil_weights<P>(t, w);
     return base;
 }
 
 // As stencil<P>, with the derivatives dw of the weights (per cell of coordinate).
 template <int P>
-__device__ __forceinline__ int stencil_d(float coord, float inv_h, int mesh, float* w, float* dw)
+__device__ __forceinline__ int stencil_d(float coord, float inv_h, int mesh, float inv_m, float* w, float* dw)
 {
     float t;
-    const int base = stencil_base<P>(coord, inv_h, mesh, t);
+    const int base = stencil_base<P>(coord, inv_h, mesh, inv_m, t);
     stencil_weights_d<P>(t, w, dw);
     return base;
 }
@@ -199,9 +201,9 @@ __device__ __forceinline__ void deposit_particles(const float4* __restrict__ pos
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
         float tx, ty, tz;
-        const int bx = stencil_base<P>(p.x - fr.ox, fr.inv_h, mesh, tx);
-        const int by = stencil_base<P>(p.y - fr.oy, fr.inv_h, mesh, ty);
-        const int bz = stencil_base<P>(p.z - fr.oz, fr.inv_h, mesh, tz);
+        const int bx = stencil_base<P>(p.x - fr.ox, fr.inv_h, mesh, fr.inv_m, tx);
+        const int by = stencil_base<P>(p.y - fr.oy, fr.inv_h, mesh, fr.inv_m, ty);
+        const int bz = stencil_base<P>(p.z - fr.oz, fr.inv_h, mesh, fr.inv_m, tz);
         float wx[P], wy[P], wz[P];
         stencil_weights<P>(tx, wx);
         stencil_weights<P>(ty, wy);
@@ -244,7 +246,7 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
                                                              float inv_h3_fixed, const IsoGrid* iso,
                                                              float* __restrict__ rho)
 {
-    const MeshFrame fr = mesh_frame(iso, inv_h_fixed);
+    const MeshFrame fr = mesh_frame(iso, inv_h_fixed, mesh);
     const float inv_h = fr.inv_h;
     const float inv_h3 = iso ? 1.0f / (iso->h * iso->h * iso->h) : inv_h3_fixed;
     // The tile accumulates in 32-bit fixed point: integer shared-memory atomics are native and
@@ -271,8 +273,8 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
         float t;
-        const int b[3] = {stencil_base<P>(p.x - fr.ox, inv_h, mesh, t), stencil_base<P>(p.y - fr.oy, inv_h, mesh, t),
-                          stencil_base<P>(p.z - fr.oz, inv_h, mesh, t)};
+        const int b[3] = {stencil_base<P>(p.x - fr.ox, inv_h, mesh, fr.inv_m, t), stencil_base<P>(p.y - fr.oy, inv_h, mesh, fr.inv_m, t),
+                          stencil_base<P>(p.z - fr.oz, inv_h, mesh, fr.inv_m, t)};
         for (int a = 0; a < 3; ++a) {
             lo[a] = min(lo[a], b[a]);
             hi[a] = max(hi[a], b[a] + P - 1);
@@ -578,7 +580,7 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
                                                       float* __restrict__ ax, float* __restrict__ ay,
                                                       float* __restrict__ az)
 {
-    const MeshFrame fr = mesh_frame(iso, inv_h_fixed);
+    const MeshFrame fr = mesh_frame(iso, inv_h_fixed, mesh);
     const float inv_h = fr.inv_h;
     const size_t M = static_cast<size_t>(mesh);
     const int q = threadIdx.x & 3;
@@ -594,9 +596,9 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
         if (i < stop && q < P) {
             const float4 p = pos4[i];
             float wx[P], wy[P], wz[P];
-            const int bx = stencil<P>(p.x - fr.ox, inv_h, mesh, wx);
-            const int by = stencil<P>(p.y - fr.oy, inv_h, mesh, wy);
-            const int bz = stencil<P>(p.z - fr.oz, inv_h, mesh, wz);
+            const int bx = stencil<P>(p.x - fr.ox, inv_h, mesh, fr.inv_m, wx);
+            const int by = stencil<P>(p.y - fr.oy, inv_h, mesh, fr.inv_m, wy);
+            const int bz = stencil<P>(p.z - fr.oz, inv_h, mesh, fr.inv_m, wz);
             const float wq = column_weight<P>(wx, q);
             const int xs = wrap1(bx + q, mesh);
 #pragma unroll
@@ -645,9 +647,9 @@ __device__ __forceinline__ void interp_ad_quads(const float4* __restrict__ pos4,
         if (i < end && q < P) {
             const float4 p = pos4[i];
             float tx, ty, tz;
-            const int bx = stencil_base<P>(p.x - fr.ox, fr.inv_h, mesh, tx);
-            const int by = stencil_base<P>(p.y - fr.oy, fr.inv_h, mesh, ty);
-            const int bz = stencil_base<P>(p.z - fr.oz, fr.inv_h, mesh, tz);
+            const int bx = stencil_base<P>(p.x - fr.ox, fr.inv_h, mesh, fr.inv_m, tx);
+            const int by = stencil_base<P>(p.y - fr.oy, fr.inv_h, mesh, fr.inv_m, ty);
+            const int bz = stencil_base<P>(p.z - fr.oz, fr.inv_h, mesh, fr.inv_m, tz);
             float wx[P], dx[P], wy[P], dy[P], wz[P], dz[P];
             stencil_weights_d<P>(tx, wx, dx);
             stencil_weights_d<P>(ty, wy, dy);
@@ -717,7 +719,7 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
     __shared__ __align__(16) float tile[kTileCells];
     __shared__ int s_lo[3], s_hi[3];
     __shared__ unsigned long long bar;
-    const MeshFrame fr = mesh_frame(iso, inv_h_fixed);
+    const MeshFrame fr = mesh_frame(iso, inv_h_fixed, mesh);
     const float inv_h = fr.inv_h;
     const int base = blockIdx.x * chunk;
     const int end = min(base + chunk, n);
@@ -733,8 +735,8 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
         const float4 p = pos4[i];
         float t;
-        const int b[3] = {stencil_base<P>(p.x - fr.ox, inv_h, mesh, t), stencil_base<P>(p.y - fr.oy, inv_h, mesh, t),
-                          stencil_base<P>(p.z - fr.oz, inv_h, mesh, t)};
+        const int b[3] = {stencil_base<P>(p.x - fr.ox, inv_h, mesh, fr.inv_m, t), stencil_base<P>(p.y - fr.oy, inv_h, mesh, fr.inv_m, t),
+                          stencil_base<P>(p.z - fr.oz, inv_h, mesh, fr.inv_m, t)};
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
             lo[a] = min(lo[a], b[a]);
