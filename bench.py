@@ -607,11 +607,13 @@ def run_ours(args, w, rank, world, local):
     peak_tf = SMS * FP32_LANES_PER_SM * 2 * NOMINAL_SM_MHZ * 1e6 / 1e12
     # DRAM traffic and issue utilisation come from an ncu capture committed under profiles/;
     # they are quoted only when that capture used this run's walk settings
-    prof = load_traffic(f"walk_{args.workload}")
     leaf_now = tuned["leaf_capacity"] if tuned else cfg.get("leaf_capacity", 16)
     group_now = tuned["walk_group_size"] if tuned else 32
-    prof_ok = (prof is not None and prof.get("leaf_capacity") == leaf_now
-               and prof.get("walk_group_size") == group_now)
+    prof = None
+    for cap in (load_traffic(f"walk_{args.workload}") or {}).get("captures", []):
+        if cap.get("leaf_capacity") == leaf_now and cap.get("walk_group_size") == group_now:
+            prof = cap
+    prof_ok = prof is not None
     roofline = {
         "kernel": "k_walk (group tree walk + pair/multipole arithmetic)",
         "bound": "fp32", "achieved": achieved_tf, "peak": peak_tf, "unit": "TFLOP/s",
@@ -619,7 +621,7 @@ def run_ours(args, w, rank, world, local):
         "peak_source": "nominal FP32 (148 SM x 128 lanes x 2 x 1965 MHz); no measured FP32 peak is provided",
         "traffic": prof.get("dram_bytes_per_launch") if prof_ok else None,
         "ncu_issue_active_pct": prof.get("issue_active_pct") if prof_ok else None,
-        "traffic_source": (f"profiles/walk_{args.workload}.json: one ncu capture at leaf "
+        "traffic_source": (f"profiles/walk_{args.workload}.json: ncu capture of one launch at leaf "
                            f"{prof.get('leaf_capacity')}, group {prof.get('walk_group_size')}"
                            if prof_ok else
                            "none: no committed ncu capture of this workload at this run's leaf "
