@@ -91,6 +91,9 @@ def parse():
     ap.add_argument("--tune", default="",
                     help="LEAF,GROUP,SCHEDULE: pin the autotuner's three choices instead of "
                          "tuning (to profile the configuration a tuned run picked)")
+    ap.add_argument("--learned-experiment", choices=["split", "cut"], default="split",
+                    help="split: plain and learned at a smaller split scale; cut: plain at "
+                         "r_cut 4.5 r_s against learned at 3.0 r_s")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-correction comparison (TreePM workloads)")
     return ap.parse_args()
@@ -455,19 +458,27 @@ def config_dict(w, args, n):
 
 
 LEARNED_RS = 0.8  # split scale (mesh cells) at which the learned correction is compared
+LEARNED_SAMPLES = 1 << 22  # training residuals
 
 
-def learned_comparison(w, pos, vel, mass, stream, local, dt, nsample):
-    """Plain TreePM and the learned pair correction at a smaller split scale (fewer short-range
-    pairs, larger mesh error): force errors against FP64 Ewald and device time per step of
-    each, plus the training cost.  The correction is trained here, on the GPU, on residuals
-    the engine generates for this mesh."""
+def learned_comparison(w, pos, vel, mass, stream, local, dt, nsample, experiment="split"):
+    """Plain TreePM against the learned pair correction: force errors against FP64 Ewald and
+    device time per step of each, plus the training cost.  The correction is trained here, on
+    the GPU, on residuals the engine generates for this mesh.
+
+    experiment "split": both at a smaller split scale (fewer short-range pairs, larger mesh
+    error), the same cutoff.  experiment "cut": the workload's split scale, plain at
+    r_cut = 4.5 r_s against the corrected walk at r_cut = 3.0 r_s."""
     import torch
 
     from blitzar_b200._lib import Engine
 
-    cfg = engine_config(dict(w, r_split_cells=LEARNED_RS))
-    out = {"r_split_cells": LEARNED_RS, "r_cut_factor": w["r_cut_factor"]}
+    if experiment == "cut":
+        rs, rcf_plain, rcf_learned = w["r_split_cells"], 4.5, 3.0
+    else:
+        rs, rcf_plain, rcf_learned = LEARNED_RS, w["r_cut_factor"], w["r_cut_factor"]
+    out = {"experiment": experiment, "r_split_cells": rs, "r_cut_factor": rcf_plain,
+           "r_cut_factor_learned": rcf_learned}
     n = len(mass)
 
     def timed(eng, steps=5):
@@ -480,13 +491,20 @@ def learned_comparison(w, pos, vel, mass, stream, local, dt, nsample):
         torch.cuda.synchronize()
         return a.elapsed_time(b) / steps
 
-    with Engine(n, stream=stream.cuda_stream, device=local, **cfg) as e:
+    with Engine(n, stream=stream.cuda_stream, device=local,
+                **engine_config(dict(w, r_split_cells=rs, r_cut_factor=rcf_plain))) as e:
         e.set_state(pos, vel, mass, f64=True)
         pe = e.force_errors(nsample=nsample, seed=11)
         ms_plain = timed(e)
+    with Engine(n, stream=stream.cuda_stream, device=local,
+                **engine_config(dict(w, r_split_cells=rs, r_cut_factor=rcf_learned))) as e:
         e.set_state(pos, vel, mass, f64=True)
+        if rcf_learned != rcf_plain:  # the shorter cutoff before its correction
+            ue = e.force_errors(nsample=nsample, seed=11)
+            out["uncorrected"] = {"median": ue["median"], "p99": ue["p99"], "ms_per_step": timed(e)}
+            e.set_state(pos, vel, mass, f64=True)
         t0 = time.perf_counter()
-        x, y = e.learn_generate(1 << 18, seed=7)
+        x, y = e.learn_generate(LEARNED_SAMPLES, seed=7)
         t1 = time.perf_counter()
         loss = e.learn_train(x, y, steps=12000, batch=4096, lr=3e-3, seed=1)
         t2 = time.perf_counter()
@@ -731,7 +749,8 @@ def run_ours(args, w, rank, world, local):
 
     learned = None
     if w["kind"] == "treepm" and not args.no_learned:
-        learned = learned_comparison(w, pos, vel, mass, stream, local, dt, args.error_sample)
+        learned = learned_comparison(w, pos, vel, mass, stream, local, dt, args.error_sample,
+                                     args.learned_experiment)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
