@@ -185,6 +185,13 @@ constexpr int kRowPad = 8;
 constexpr int kPlanePad = 12;
 constexpr int kDepositRowPad = 12;
 constexpr int kDepositPlanePad = 12;
+// Fixed pitches for the interpolation's boxes of the usual chunks (a chunk of 256 Morton-
+// consecutive particles at 8 cells per particle spans 12-16 x 17-19 x 17-19 cells): with the
+// strides known at compile time every stencil read is one shared-memory load with an immediate
+// offset (the kernel's integer instructions halve).  The pitches keep the banks of the padded
+// layout (mod 32: 24 and 12; the bank model gives 1.35 wavefronts).  Boxes that do not fit use
+// the padded pitches above.  (The deposit measured no faster with fixed pitches.)
+constexpr int kInterpRp = 24, kInterpPp = 492;  // rows of up to 24 cells, up to 20 rows a plane
 
 // The scatter of k_deposit_tiled, one thread per particle: all threads of a warp add the same
 // stencil offset together, so two of them meet on one cell only when their particles share a
@@ -632,14 +639,15 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
 // The gather of k_interp_ad_tiled: four lanes per particle, lane q taking stencil column
 // x = bx + q of every (y, z) row from the staged tile (TILED) or from the global mesh.  The loop
 // bound is uniform over the block, so every lane of a quad reaches the shuffles.
-template <int P, bool TILED>
+template <int P, bool TILED, int RP = 0, int PP = 0>
 __device__ __forceinline__ void interp_ad_quads(const float4* __restrict__ pos4, int base, int end,
                                                 const MeshFrame& fr, int mesh, const float* tile,
-                                                int ox, int oy, int oz, int rp, int pp,
+                                                int ox, int oy, int oz, int rp_dyn, int pp_dyn,
                                                 const float* __restrict__ phi, float* __restrict__ ax,
                                                 float* __restrict__ ay, float* __restrict__ az)
 {
     const size_t M = static_cast<size_t>(mesh);
+    const int rp = RP ? RP : rp_dyn, pp = PP ? PP : pp_dyn;  // RP, PP: pitches known at compile time
     const int q = threadIdx.x & 3;
     for (int i0 = base; i0 < end; i0 += kThreads / 4) {
         const int i = i0 + (threadIdx.x >> 2);
@@ -757,7 +765,10 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
     const int oy = s_lo[1], oz = s_lo[2];
     const int ex = ((s_hi[0] + 1 - ox) + 3) & ~3;
     const int ey = s_hi[1] - oy + 1, ez = s_hi[2] - oz + 1;
-    const int rp = ex + kRowPad, pp = ey * rp + kPlanePad;
+    const bool fixed = ex > 0 && ey > 0 && ez > 0 && ex <= kInterpRp && ey * kInterpRp <= kInterpPp &&
+                       ez * kInterpPp <= kTileCells;
+    const int rp = fixed ? kInterpRp : ex + kRowPad;
+    const int pp = fixed ? kInterpPp : ey * rp + kPlanePad;
     const bool tiled = ex > 0 && ey > 0 && ez > 0 && ex <= mesh &&
                        static_cast<long long>(pp) * ez <= kTileCells && (mesh & 3) == 0;
     const size_t M = static_cast<size_t>(mesh);
@@ -778,7 +789,10 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
         }
         mbar_wait_bounded(&bar, 0u, err);
     }
-    if (tiled)
+    if (tiled && fixed)
+        interp_ad_quads<P, true, kInterpRp, kInterpPp>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, phi,
+                                                       ax, ay, az);
+    else if (tiled)
         interp_ad_quads<P, true>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, phi, ax, ay, az);
     else
         interp_ad_quads<P, false>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, phi, ax, ay, az);
