@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libbzgrav.so")
 
 BZ_OK, BZ_INVALID_ARGUMENT, BZ_NOT_READY, BZ_TIMEOUT, BZ_INTERNAL_ERROR = 0, 1, 2, 3, 4
 BZ_CUDA_ERROR, BZ_OUT_OF_MEMORY, BZ_DEVICE_LIMIT, BZ_UNSUPPORTED = 5, 6, 7, 8
+BZ_INTEGRATOR_LEAPFROG, BZ_INTEGRATOR_EULER = 0, 1  # bz_integrator
 SOLVER_OCTREE, SOLVER_TREEPM, SOLVER_OCTREE_REFERENCE = 0, 1, 2
 KEYS_PRODUCTION, KEYS_REFERENCE = 0, 1
 
@@ -65,6 +66,7 @@ class BzConfig(C.Structure):
         ("adaptive_max_level", C.c_int32),
         ("adaptive_eta", C.c_float),
         ("treepm_cell_floor", C.c_float),
+        ("integrator", C.c_int32),
     ]
 
 

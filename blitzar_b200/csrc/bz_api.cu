@@ -341,9 +341,13 @@ void enqueue_step(bz_handle* h)
     double* const* s = d.st[h->cur];
     // (the isolated mesh's grid needs the new bounds first: no early fork there)
     const bool early = mesh_concurrent(h) && h->mesh_overlap == 2 && !isolated(h);
+    // leapfrog: the opening half kick (the closing one follows the force evaluation);
+    // symplectic Euler: the whole kick with the force of the step's start positions
+    const bool euler = h->cfg.integrator == BZ_INTEGRATOR_EULER;
     launch_kick_drift(s[0], s[1], s[2], s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt,
                       periodic(h) ? h->cfg.box_length : 0.0, nullptr, h->stream,
-                      early ? d.mass[h->cur] : nullptr, early ? d.pos4_drift : nullptr);
+                      early ? d.mass[h->cur] : nullptr, early ? d.pos4_drift : nullptr,
+                      euler ? 1.0 : 0.5);
     if (early) {
         // the mass deposit is a sum over particles in any order: start it and the field solve
         // now, concurrently with the keys, sort and permutation of this stream
@@ -353,7 +357,7 @@ void enqueue_step(bz_handle* h)
         pm_solve(h->pm, h->pm_stream);
     }
     enqueue_order(h);
-    enqueue_forces(h, true, false, early);
+    enqueue_forces(h, !euler, false, early);
 }
 
 bz_status check_device(bz_handle* h, const char* what)
@@ -549,6 +553,7 @@ bz_status bz_config_init(bz_config* c)
     c->walk_group_size = kGroupMax;
     c->adaptive_max_level = 0;
     c->adaptive_eta = 0.02f;
+    c->integrator = BZ_INTEGRATOR_LEAPFROG;
     return BZ_OK;
 }
 
@@ -632,7 +637,8 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     if (cfg->leaf_capacity < 1 || cfg->octree_theta <= 0.0f || cfg->walk_group_size < 1 ||
         !(cfg->physics_max_acceleration > 0.0f) ||
         cfg->walk_group_size > kGroupMax || cfg->adaptive_max_level < 0 || cfg->adaptive_max_level > 12 ||
-        (cfg->adaptive_max_level > 0 && (cfg->solver != BZ_SOLVER_OCTREE || !(cfg->adaptive_eta > 0.0f)))) {
+        (cfg->adaptive_max_level > 0 && (cfg->solver != BZ_SOLVER_OCTREE || !(cfg->adaptive_eta > 0.0f))) ||
+        (cfg->integrator != BZ_INTEGRATOR_LEAPFROG && cfg->integrator != BZ_INTEGRATOR_EULER)) {
         delete h;
         return BZ_INVALID_ARGUMENT;
     }

@@ -248,7 +248,7 @@ void launch_kick(double* vx, double* vy, double* vz, float* ax, float* ay, float
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
                        const float* ax, const float* ay, const float* az, int n,
                        const double* dt, double periodic_len, BoxF64* box, cudaStream_t s,
-                       const float* mass = nullptr, float4* pos4 = nullptr);
+                       const float* mass = nullptr, float4* pos4 = nullptr, double kick_frac = 0.5);
 // FP64 energy/momentum sums over the sorted state (scratch: energy_scratch_doubles(); the
 // five results land at scratch[5 * 1024 .. 5 * 1024 + 5)).
 size_t energy_scratch_doubles();

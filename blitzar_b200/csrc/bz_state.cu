@@ -93,8 +93,9 @@ __device__ __forceinline__ double wrap_periodic(double x, double L)
     return x >= L ? 0.0 : x;
 }
 
-// Half kick with the cached acceleration, full drift, periodic wrap; for open boundaries
-// the FP64 box of the drifted positions is reduced in the same pass.
+// Kick with the cached acceleration (kick_frac x dt: half for leapfrog, whole for symplectic
+// Euler), full drift with the kicked velocity, periodic wrap; for open boundaries the FP64 box
+// of the drifted positions is reduced in the same pass.
 __global__ void __launch_bounds__(kThreads) k_kick_drift(double* __restrict__ x,
                                                           double* __restrict__ y,
                                                           double* __restrict__ z,
@@ -107,10 +108,10 @@ __global__ void __launch_bounds__(kThreads) k_kick_drift(double* __restrict__ x,
                                                           const double* __restrict__ dtp,
                                                           double L, BoxF64* box,
                                                           const float* __restrict__ mass,
-                                                          float4* __restrict__ pos4)
+                                                          float4* __restrict__ pos4, double kick_frac)
 {
     const double dt = *dtp;
-    const double h = 0.5 * dt;
+    const double h = kick_frac * dt;
     double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
     for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
         const double ux = vx[i] + static_cast<double>(ax[i]) * h;
@@ -206,7 +207,7 @@ void launch_kick(double* vx, double* vy, double* vz, float* ax, float* ay, float
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
                        const float* ax, const float* ay, const float* az, int n,
                        const double* dt, double periodic_len, BoxF64* box, cudaStream_t s,
-                       const float* mass, float4* pos4)
+                       const float* mass, float4* pos4, double kick_frac)
 {
     if (box) {
         count_launch();
@@ -214,7 +215,7 @@ void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, 
     }
     count_launch();
     k_kick_drift<<<grid_for(n), kThreads, 0, s>>>(x, y, z, vx, vy, vz, ax, ay, az, n, dt,
-                                                  periodic_len, box, mass, pos4);
+                                                  periodic_len, box, mass, pos4, kick_frac);
 }
 
 void launch_scatter3(const float* ax, const float* ay, const float* az, const int* id, int n,

@@ -226,7 +226,7 @@ bool save(const std::string& path, const std::string& fmt, const std::vector<Par
 
 struct RunConfig {
     std::string solver = "octree_gpu";
-    std::string integrator = "leapfrog";
+    std::string integrator = "euler";  // the reference's default (CfgMain.cpp)
     bool treepm = false;
     double dt = 1e-3;
     std::string input, input_format = "auto";
@@ -253,11 +253,12 @@ bool resolve(const std::map<std::string, std::string>& kv, GravitySystem& sys, R
     }
     if (const std::string* s = lookup(kv, {"simulation_integrator", "integrator"}))
         rc.integrator = *s;
-    if (rc.integrator != "leapfrog") {
-        err = "integrator=" + rc.integrator + ": this engine integrates with leapfrog (KDK); "
-              "set integrator=leapfrog";
+    if (rc.integrator != "leapfrog" && rc.integrator != "euler") {
+        err = "integrator=" + rc.integrator + " is not provided with octree_gpu (euler or leapfrog)";
         return false;
     }
+    sys.setIntegratorMode(rc.integrator == "euler" ? GravitySystem::IntegratorMode::Euler
+                                                   : GravitySystem::IntegratorMode::Leapfrog);
     if (const std::string* s = lookup(kv, {"treepm_enabled"}))
         rc.treepm = truthy(*s);
     get_num(kv, {"substep_target_dt", "simulation_dt", "dt"}, rc.dt);

@@ -26,14 +26,36 @@ struct Particle {
 class GravitySystem {
 public:
     enum class SolverMode { OctreeGpu, TreePm, OctreeReference };
+    // ParticleSystem::IntegratorMode (PhyParticleSystem.hpp:131-135)
+    enum class IntegratorMode { Euler, Rk4, Leapfrog };
 
+    // The integrator starts as symplectic Euler, the reference's default (integrator=euler,
+    // SrvSimulationServer.hpp:410); setIntegratorMode(Leapfrog) selects kick-drift-kick.
     explicit GravitySystem(std::vector<Particle> particles) : particles_(std::move(particles))
     {
         bz_config_init(&cfg_);
+        cfg_.integrator = BZ_INTEGRATOR_EULER;
     }
     ~GravitySystem() { release(); }
     GravitySystem(const GravitySystem&) = delete;
     GravitySystem& operator=(const GravitySystem&) = delete;
+
+    // setIntegratorMode / getIntegratorMode (PhyParticleSystem.hpp:316-324).  RK4 is not
+    // provided (the reference rejects it with octree_gpu, CfgNormalize.cpp:103-106): false.
+    bool setIntegratorMode(IntegratorMode m)
+    {
+        if (m == IntegratorMode::Rk4) {
+            err_ = "integrator rk4 is not provided with the octree solvers (euler, leapfrog)";
+            return false;
+        }
+        cfg_.integrator = m == IntegratorMode::Euler ? BZ_INTEGRATOR_EULER : BZ_INTEGRATOR_LEAPFROG;
+        invalidate();
+        return true;
+    }
+    IntegratorMode getIntegratorMode() const
+    {
+        return cfg_.integrator == BZ_INTEGRATOR_EULER ? IntegratorMode::Euler : IntegratorMode::Leapfrog;
+    }
 
     // setters of PhyParticleSystem.hpp:187-252; they take effect at the next update()
     void setSolverMode(SolverMode m)

@@ -48,6 +48,21 @@ typedef enum bz_key_mode {
                                engine/physics/octree/cuda/linear/OctKeyKernels.inl:22-46) */
 } bz_key_mode;
 
+/* Time integrator of bz_step (simulation(integrator=...)); one force evaluation per step either
+   way, the accelerations of the step's end positions kept for the next step.
+   Replaces the integrator switch of ParticleSystem::updateOctreeGpuIntegrators
+   (engine/physics/core/cuda/integration/CudOctreeGpuIntegrators.inl:31-296). */
+typedef enum bz_integrator {
+    BZ_INTEGRATOR_LEAPFROG = 0, /* kick-drift-kick: v += a dt/2, x += v dt, a = F(x), v += a dt/2
+                                   (the reference's leapfrog, CudOctreeGpuIntegrators.inl:42-196) */
+    BZ_INTEGRATOR_EULER = 1     /* symplectic Euler, the reference's default integrator=euler:
+                                   a = F(x), v += a dt, x += v dt (updateParticlesOctree,
+                                   engine/physics/octree/cuda/force/OctGpu.inl:246-275).
+                                   Adaptive block steps (adaptive_max_level > 0) keep their own
+                                   scheme whatever this says, as the reference's adaptive path
+                                   does (CudOctreeGpuAdaptive.inl) */
+} bz_integrator;
+
 /* Configuration; field names follow the simulation.ini keys they mirror. */
 typedef struct bz_config {
     uint32_t struct_size;          /* sizeof(bz_config), set by bz_config_init */
@@ -93,6 +108,7 @@ typedef struct bz_config {
     float adaptive_eta;            /* adaptive(eta): stable dt = eta * min(sqrt(eps/|a|), eps/|v|) */
     float treepm_cell_floor;       /* isolated TreePM (box_length = 0): smallest mesh cell (the
                                       reference's 0.25, TpmGridBuild.inl:100) */
+    int32_t integrator;            /* bz_integrator: the time integrator of bz_step */
 } bz_config;
 
 typedef struct bz_handle bz_handle;

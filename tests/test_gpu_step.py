@@ -65,6 +65,48 @@ def test_kdk_matches_oracle_integration(gpu, oracle):
     assert np.abs(gv - v).max() < 1e-6
 
 
+def test_symplectic_euler_matches_oracle_integration(gpu, oracle):
+    """integrator = Euler: v += a(x) dt, x += v dt, one force evaluation a step, as the
+    reference's updateParticlesOctree (engine/physics/octree/cuda/force/OctGpu.inl:246-275)."""
+    from blitzar_b200._lib import BZ_INTEGRATOR_EULER
+
+    n = 4000
+    pos = plummer(n, seed=5).astype(np.float64)
+    rng = np.random.default_rng(5)
+    vel = 0.2 * rng.standard_normal((n, 3))
+    m = np.full(n, 1.0 / n, np.float32)
+    dt, steps = 1e-3, 5
+    with _engine(n, integrator=BZ_INTEGRATOR_EULER) as e:
+        e.set_state(pos, vel, m, f64=True)
+        e.step(dt, steps)
+        gp, gv = e.get_state(f64=True)
+
+    def force(p):
+        p32 = p.astype(np.float32)
+        lo = p.min(0)
+        size = float((p.max(0) - lo).max())
+        k = oracle.morton63(p, lo, size)
+        pm = oracle.stable_sort(k)
+        t = oracle.build_tree(k[pm], oracle.pos4(p32[pm], m[pm]), 16)
+        w = oracle.walk(oracle.pos4(p32[pm], m[pm]), t, theta=0.5, eps=0.01)
+        a = np.empty((n, 3))
+        a[pm] = w["acc"]
+        return a
+
+    x, v = pos.copy(), vel.copy()
+    for _ in range(steps):
+        v = v + dt * force(x)
+        x = x + dt * v
+    assert np.abs(gp - x).max() < 1e-9
+    assert np.abs(gv - v).max() < 1e-6
+    # and not the leapfrog result
+    with _engine(n) as e:
+        e.set_state(pos, vel, m, f64=True)
+        e.step(dt, steps)
+        lp, _ = e.get_state(f64=True)
+    assert np.abs(lp - x).max() > 1e-8
+
+
 def test_periodic_wrap_and_momentum(gpu):
     n = 32_768
     rng = np.random.default_rng(1)
@@ -118,20 +160,22 @@ def test_energy_drift_is_small(gpu):
     assert np.abs(p1 - p0).max() < 1e-4 * np.sqrt(2 * k0 * m.sum())
 
 
-def test_headless_driver_matches_engine(gpu, tmp_path):
+@pytest.mark.parametrize("integrator", ["leapfrog", "euler"])
+def test_headless_driver_matches_engine(gpu, tmp_path, integrator):
     """The C++ headless driver (reference config + NBSIMBIN in, NBSIMBIN out) steps exactly as
-    the engine driven through ctypes does."""
+    the engine driven through ctypes does, with either integrator."""
     import subprocess
 
     from blitzar_b200 import build as b
     from blitzar_b200 import ics, snapshot
+    from blitzar_b200._lib import BZ_INTEGRATOR_EULER, BZ_INTEGRATOR_LEAPFROG
 
     n = 4096
     pos, vel, m = ics.plummer(n, seed=8)
     pos, vel, m = pos.astype(np.float32), vel.astype(np.float32), m.astype(np.float32)
     snapshot.write_bin(tmp_path / "in.bin", pos, vel, m)
     (tmp_path / "sim.ini").write_text(
-        "simulation(dt=0.001, solver=octree_gpu, integrator=leapfrog)\n"
+        f"simulation(dt=0.001, solver=octree_gpu, integrator={integrator})\n"
         "octree(theta=0.6, softening=0.02)\n"
         f"input_file={tmp_path / 'in.bin'}\n")
     r = subprocess.run([b.HEADLESS, "--config", str(tmp_path / "sim.ini"), "--run",
@@ -141,7 +185,9 @@ def test_headless_driver_matches_engine(gpu, tmp_path):
     assert "[headless] done steps=10" in r.stdout
     p_h, v_h, m_h, _ = snapshot.read_bin(tmp_path / "out.bin")
     # the headless run keeps the reference's default clamp (64); so does this handle
-    with _engine(n, octree_theta=0.6, octree_softening=0.02, physics_max_acceleration=64.0) as e:
+    mode = BZ_INTEGRATOR_EULER if integrator == "euler" else BZ_INTEGRATOR_LEAPFROG
+    with _engine(n, octree_theta=0.6, octree_softening=0.02, physics_max_acceleration=64.0,
+                 integrator=mode) as e:
         e.set_state(pos, vel, m)
         e.step(1e-3, 10)
         p_e, v_e = e.get_state()

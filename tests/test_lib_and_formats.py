@@ -138,10 +138,16 @@ def test_headless_resolves_reference_config(tmp_path):
                                   text=True, check=True).stdout)
     assert d["solver"] == 1 and d["box_length"] == 1.0 and d["treepm_gradient"] == 1
     assert d["treepm_grid_size"] == 64
+    # the integrator: the reference's default is symplectic Euler; rk4 is not provided with
+    # octree_gpu (the reference rejects the pair too)
+    cfg.write_text("simulation(solver=octree_gpu)\n")
+    d = json.loads(subprocess.run([_headless(), "--config", str(cfg), "--dry-run"], capture_output=True,
+                                  text=True, check=True).stdout)
+    assert d["integrator"] == "euler"
     bad = tmp_path / "bad.ini"
-    bad.write_text("simulation(solver=octree_gpu, integrator=euler)\n")
+    bad.write_text("simulation(solver=octree_gpu, integrator=rk4)\n")
     r = subprocess.run([_headless(), "--config", str(bad), "--dry-run"], capture_output=True, text=True)
-    assert r.returncode == 2 and "leapfrog" in r.stderr
+    assert r.returncode == 2 and "not provided" in r.stderr
     bad.write_text("solver=pairwise_cuda\n")
     r = subprocess.run([_headless(), "--config", str(bad), "--dry-run"], capture_output=True, text=True)
     assert r.returncode == 2 and "not provided" in r.stderr
