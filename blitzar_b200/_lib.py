@@ -30,7 +30,7 @@ EXPORTS = (
     "bz_learn_set", "bz_learn_get", "bz_learn_enable", "bz_learn_forward", "bz_learn_gradient",
     "bz_set_ensemble", "bz_adaptive_levels", "bz_adaptive_updates", "bz_set_mesh_schedule",
     "bz_walk_blocks_per_sm", "bz_set_state_acc", "bz_get_state_acc", "bz_set_state_acc_f64",
-    "bz_get_state_acc_f64", "bz_walk_counts", "bz_pm_grid",
+    "bz_get_state_acc_f64", "bz_step_get_state_acc_f64", "bz_walk_counts", "bz_pm_grid",
 )
 
 PHASES = ("keys", "sort", "permute", "tree", "mesh", "walk", "integrate", "total")
@@ -127,6 +127,7 @@ def load():
     L.bz_get_state_acc.argtypes = [_vp, _vp, _vp, _vp]
     L.bz_set_state_acc_f64.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_size_t]
     L.bz_get_state_acc_f64.argtypes = [_vp, _vp, _vp, _vp]
+    L.bz_step_get_state_acc_f64.argtypes = [_vp, C.c_double, _vp, _vp, _vp]
     L.bz_adaptive_levels.argtypes = [_vp, _vp]
     L.bz_adaptive_updates.argtypes = [_vp, C.POINTER(C.c_uint64)]
     L.bz_set_ensemble.argtypes = [_vp, _vp, _vp, _vp, _vp, C.c_int32]
@@ -276,6 +277,12 @@ class Engine:
         """FP64 positions and velocities with the FP32 accelerations of the positions (SoA)."""
         self._check(self.L.bz_get_state_acc_f64(self.h, _ptr(pos_soa3), _ptr(vel_soa3),
                                                 _ptr(acc_soa3)), "bz_get_state_acc_f64")
+
+    def step_get_state_acc_f64_soa(self, dt, pos_soa3, vel_soa3, acc_soa3):
+        """One step, then the FP64 state and FP32 accelerations (SoA), the position download
+        overlapping the step (bz_step_get_state_acc_f64)."""
+        self._check(self.L.bz_step_get_state_acc_f64(self.h, dt, _ptr(pos_soa3), _ptr(vel_soa3),
+                                                     _ptr(acc_soa3)), "bz_step_get_state_acc_f64")
 
     def get_state_soa(self, pos_soa3, vel_soa3):
         self._check(self.L.bz_get_state(self.h, _ptr(pos_soa3), _ptr(vel_soa3)), "bz_get_state")

@@ -93,6 +93,11 @@ struct bz_handle {
     bool timing = false;
     cudaEvent_t ev[kNumPhases + 2] = {};
     bool stepping = false;  // last timed call was bz_step (has an opening kick-drift)
+    // bz_step_get_state_acc_f64: the drifted positions leave on io_stream while the step runs
+    cudaStream_t io_stream = nullptr;
+    cudaEvent_t ev_drift = nullptr, ev_io = nullptr;
+    double* io_pos = nullptr;       // 3 x capacity doubles of caller-order positions
+    double* io_host_pos = nullptr;  // set only while that call enqueues its step
     float phase_ms[kNumPhases] = {};
     // graphs (one per state-buffer parity)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};
@@ -334,6 +339,8 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
     }
 }
 
+void enqueue_io_positions(bz_handle* h);
+
 void enqueue_step(bz_handle* h)
 {
     const int n = static_cast<int>(h->n);
@@ -348,6 +355,8 @@ void enqueue_step(bz_handle* h)
                       periodic(h) ? h->cfg.box_length : 0.0, nullptr, h->stream,
                       early ? d.mass[h->cur] : nullptr, early ? d.pos4_drift : nullptr,
                       euler ? 1.0 : 0.5);
+    if (h->io_host_pos)  // the step's positions are final here: send them while the step runs
+        enqueue_io_positions(h);
     if (early) {
         // the mass deposit is a sum over particles in any order: start it and the field solve
         // now, concurrently with the keys, sort and permutation of this stream
@@ -592,6 +601,14 @@ bz_status bz_destroy(bz_handle* h)
         cudaEventDestroy(h->ev_sorted);
     if (h->pm_stream)
         cudaStreamDestroy(h->pm_stream);
+    if (h->io_stream) {
+        cudaStreamSynchronize(h->io_stream);
+        cudaStreamDestroy(h->io_stream);
+    }
+    if (h->ev_drift)
+        cudaEventDestroy(h->ev_drift);
+    if (h->ev_io)
+        cudaEventDestroy(h->ev_io);
     for (void* p : h->allocations)
         cudaFree(p);
     if (h->h_dt)
@@ -1009,6 +1026,36 @@ static void enqueue_get_f64(bz_handle* h, double* pos, double* vel)
                             h->stream);
 }
 
+}  // extern "C"
+
+namespace {
+
+// The drifted positions of the step being enqueued, gathered into caller order and copied to
+// the host on io_stream (they stay untouched in buffer `cur` for the rest of the step: the
+// permutation writes the other buffer); ev_io marks the copies done.
+void enqueue_io_positions(bz_handle* h)
+{
+    const size_t n = h->n;
+    DeviceBuffers& d = h->d;
+    double* const* s = d.st[h->cur];
+    Soa6 out{};
+    for (int a = 0; a < 3; ++a)
+        out.a[a] = h->io_pos + a * n;
+    cudaEventRecord(h->ev_drift, h->stream);
+    cudaStreamWaitEvent(h->io_stream, h->ev_drift, 0);
+    count_launch();
+    k_gather_f64_soa<<<blocks_for(n), 256, 0, h->io_stream>>>(s[0], s[1], s[2], s[3], s[4], s[5],
+                                                              d.id[h->cur], static_cast<int>(n), out, 0);
+    for (int a = 0; a < 3; ++a)
+        cudaMemcpyAsync(h->io_host_pos + a * n, out.a[a], n * sizeof(double), cudaMemcpyDeviceToHost,
+                        h->io_stream);
+    cudaEventRecord(h->ev_io, h->io_stream);
+}
+
+} // namespace
+
+extern "C" {
+
 // Uploads and unpacks an FP32 state (caller order, buffer 0) on the handle's stream.
 static void enqueue_set_state(bz_handle* h, const float* pos, const float* vel, const float* mass,
                               size_t n)
@@ -1200,6 +1247,62 @@ bz_status bz_get_state_acc_f64(bz_handle* h, double* pos, double* vel, float* ac
     enqueue_get_f64(h, pos, vel);
     cudaMemcpyAsync(acc, d.stage + 6 * n, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
     return check_device(h, "bz_get_state_acc_f64");
+}
+
+bz_status bz_step_get_state_acc_f64(bz_handle* h, double dt, double* pos, double* vel, float* acc)
+{
+    if (!h || !pos || !vel || !acc || h->n == 0)
+        return BZ_INVALID_ARGUMENT;
+    if (h->cfg.solver == BZ_SOLVER_OCTREE_REFERENCE)
+        return fail(h, BZ_UNSUPPORTED, "the reference formulation is a parity mode; step with BZ_SOLVER_OCTREE");
+    if (h->cfg.adaptive_max_level > 0)
+        return fail(h, BZ_UNSUPPORTED, "adaptive steps keep per-particle accelerations of their own");
+    cudaSetDevice(h->device);
+    if (!h->io_stream) {
+        if (cudaStreamCreateWithFlags(&h->io_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_drift, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&h->ev_io, cudaEventDisableTiming) != cudaSuccess)
+            return fail(h, BZ_CUDA_ERROR, "bz_step_get_state_acc_f64: stream or events");
+        if (!dalloc(h, &h->io_pos, 3 * h->capacity))
+            return fail(h, BZ_OUT_OF_MEMORY, "bz_step_get_state_acc_f64: position staging");
+    }
+    h->h_dt[0] = dt;
+    h->h_dt[1] = 0.5 * dt;
+    cudaMemcpyAsync(h->d.dt, h->h_dt, 2 * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    bz_status s = ensure_forces(h);
+    if (s != BZ_OK)
+        return s;
+    h->stepping = true;
+    // one step enqueued eagerly, so that the position download can start inside it
+    const bool timing = h->timing;
+    h->timing = false;
+    h->io_host_pos = pos;
+    enqueue_step(h);
+    h->io_host_pos = nullptr;
+    h->timing = timing;
+    // velocities and accelerations of the step's end; the alternate state buffer that stages
+    // the velocities is the one io_stream reads positions from, so wait for it first
+    cudaStreamWaitEvent(h->stream, h->ev_io, 0);
+    const size_t n = h->n;
+    DeviceBuffers& d = h->d;
+    launch_scatter3(d.acc[0], d.acc[1], d.acc[2], d.id[h->cur], static_cast<int>(n), d.stage + 6 * n,
+                    h->stream);
+    double* const* st = d.st[h->cur];
+    double* const* alt = d.st[h->cur ^ 1];
+    Soa6 out{};
+    for (int a = 0; a < 3; ++a)
+        out.a[a] = alt[3 + a];
+    count_launch();
+    k_gather_f64_soa<<<blocks_for(n), 256, 0, h->stream>>>(st[3], st[4], st[5], st[3], st[4], st[5],
+                                                           d.id[h->cur], static_cast<int>(n), out, 0);
+    for (int a = 0; a < 3; ++a)
+        cudaMemcpyAsync(vel + a * n, alt[3 + a], n * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    cudaMemcpyAsync(acc, d.stage + 6 * n, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, h->stream);
+    s = check_device(h, "bz_step_get_state_acc_f64");
+    if (s != BZ_OK)
+        return s;
+    read_counters(h);
+    return BZ_OK;
 }
 
 bz_status bz_set_state_acc_f64(bz_handle* h, const double* pos, const double* vel, const float* mass,

@@ -223,6 +223,17 @@ bz_status bz_set_state_acc_f64(bz_handle* h, const double* pos3n, const double* 
                                const float* mass, const float* acc3n, size_t n);
 bz_status bz_get_state_acc_f64(bz_handle* h, double* pos3n, double* vel3n, float* acc3n);
 
+/* One bz_step(h, dt, 1) followed by bz_get_state_acc_f64, with the download of the positions
+ * overlapping the step: the positions are final after the step's drift, so they are copied to
+ * the host on a second stream while the tree, mesh and walk run; velocities and accelerations
+ * follow the step.  The result equals that of the two calls bit for bit (the step is launched
+ * eagerly rather than as the captured graph).  The first call allocates a staging buffer of
+ * 3 x capacity doubles and a stream; not with adaptive block steps.  For hosts that keep the
+ * state between steps (bz_set_state_acc_f64 / this call), where each step otherwise pays both
+ * transfers in full; no counterpart in the reference, whose state stays on the device. */
+bz_status bz_step_get_state_acc_f64(bz_handle* h, double dt, double* pos3n, double* vel3n,
+                                    float* acc3n);
+
 /* Morton keys of the current state, sorted, with the stable sort permutation (sorted
  * position -> caller index): buildMortonCodesKernel + thrust::sort_by_key
  * (engine/physics/octree/cuda/linear/OctKeyKernels.inl:22-46, OctBuild.inl:96). */

@@ -225,6 +225,47 @@ def test_state_with_accelerations(gpu):
     assert np.array_equal(a3.reshape(3, n).T, again)
 
 
+@pytest.mark.parametrize("case", ["octree", "treepm"])
+def test_step_with_overlapped_download(gpu, case):
+    """bz_step_get_state_acc_f64 (the position download overlapping the step) returns, step
+    after step, what bz_step followed by bz_get_state_acc_f64 returns: bit for bit for the
+    octree; for TreePM to the mesh's own run-to-run spread (its deposit adds the blocks' tiles
+    into the mesh with float reductions, in no fixed order: ~1e-12 in positions after a few
+    steps, the same between two bz_step runs)."""
+    n = 20_000
+    rng = np.random.default_rng(12)
+    if case == "octree":
+        pos = plummer(n, seed=12).astype(np.float64)
+        kw = {}
+    else:  # periodic TreePM, its mesh leg on the second stream
+        pos = rng.random((n, 3))
+        kw = dict(solver=1, box_length=1.0, treepm_grid_size=32, octree_softening=0.02 / 32)
+    vel = 0.1 * rng.standard_normal((n, 3))
+    m = np.full(n, 1.0 / n, np.float32)
+    outs = []
+    for fused in (False, True):
+        with _engine(n, **kw) as e:
+            e.set_state(pos, vel, m, f64=True)
+            p3, v3 = np.empty(3 * n), np.empty(3 * n)
+            a3 = np.empty(3 * n, np.float32)
+            got = []
+            for _ in range(3):
+                if fused:
+                    e.step_get_state_acc_f64_soa(1e-3, p3, v3, a3)
+                else:
+                    e.step(1e-3, 1)
+                    e.get_state_acc_f64_soa(p3, v3, a3)
+                got.append((p3.copy(), v3.copy(), a3.copy()))
+                e.set_state_acc_f64_soa(p3, v3, m, a3)
+            outs.append(got)
+    for (pa, va, aa), (pb, vb, ab) in zip(*outs):
+        if case == "octree":
+            assert np.array_equal(pa, pb) and np.array_equal(va, vb) and np.array_equal(aa, ab)
+        else:
+            assert np.abs(pa - pb).max() < 1e-10 and np.abs(va - vb).max() < 1e-7
+            assert np.abs(aa - ab).max() < 1e-4 * np.abs(aa).max()
+
+
 def test_state_round_trip_keeps_order(gpu):
     """Uploading a held state back (same size) keeps the device's particle order; the steps that
     follow match those of a fresh engine given the same state and accelerations."""
