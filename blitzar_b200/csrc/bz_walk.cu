@@ -705,11 +705,15 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
             if (k >= 0) {
                 const float4 b0 = t.box0[k];
                 const float4 b1 = t.box1[k];
-                const float4 mo = t.mono[k];
+                // the centre of mass matters only to a node that may be accepted; with a node
+                // size cap (TreePM) most nodes are too large, and skip the load
+                const bool capped = p.max_node_size > 0.0f;
+                float4 mo = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (!capped)
+                    mo = t.mono[k];
                 link = __float_as_int(b0.w);
                 info = __float_as_int(b1.w);
                 const float bmin[3] = {b0.x, b0.y, b0.z}, bmax[3] = {b1.x, b1.y, b1.z};
-                const float com[3] = {mo.x, mo.y, mo.z};
                 float sh[3] = {0.0f, 0.0f, 0.0f};
                 bool amb = false;
                 if (PERIODIC) {
@@ -748,19 +752,27 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                     pruned = d2 > p.rcut2;
                 }
                 if (!pruned && !(PERIODIC && amb)) {
-                    float e2 = 0.0f, l = 0.0f;
+                    float l = 0.0f;
 #pragma unroll
-                    for (int a = 0; a < 3; ++a) {
-                        const float c = __fsub_rn(com[a], sh[a]);
-                        const float e = fmaxf(fmaxf(__fsub_rn(gmin[a], c), __fsub_rn(c, gmax[a])), 0.0f);
-                        e2 = __fadd_rn(e2, __fmul_rn(e, e));
+                    for (int a = 0; a < 3; ++a)
                         l = fmaxf(l, __fsub_rn(bmax[a], bmin[a]));
-                    }
                     // The split kernel varies on the scale r_s, so its expansion error depends on
                     // the node size itself, not only on l/d: nodes at least max_node_size large
                     // are never accepted.
-                    accept = __fmul_rn(l, l) < __fmul_rn(p.theta2, e2) &&
-                             (p.max_node_size <= 0.0f || l < p.max_node_size);
+                    const bool small = !capped || l < p.max_node_size;
+                    if (small) {
+                        if (capped)
+                            mo = t.mono[k];
+                        const float com[3] = {mo.x, mo.y, mo.z};
+                        float e2 = 0.0f;
+#pragma unroll
+                        for (int a = 0; a < 3; ++a) {
+                            const float c = __fsub_rn(com[a], sh[a]);
+                            const float e = fmaxf(fmaxf(__fsub_rn(gmin[a], c), __fsub_rn(c, gmax[a])), 0.0f);
+                            e2 = __fadd_rn(e2, __fmul_rn(e, e));
+                        }
+                        accept = __fmul_rn(l, l) < __fmul_rn(p.theta2, e2);
+                    }
                     if (!accept) {
                         if (info < 0)
                             leaf = true;
