@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
 {
     constexpr int kNodesPerTile = kThreads / TPN;
     __shared__ int s_tile;
-    __shared__ int s_scan[kThreads];
+    __shared__ int s_scan[kThreads / 32];
     __shared__ int s_prefix;
     const int first = t.lvl_first[l];
     // after a capacity overflow the recorded count can exceed the arrays: clamp
@@ -157,17 +157,22 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
             for (int d = 0; d < 8; ++d)
                 nch += b[d + 1] > b[d] ? 1 : 0;
         }
-        // block exclusive scan of child counts (only the leader of each node contributes)
-        s_scan[threadIdx.x] = nch;
+        // block scan of child counts (only the leader of each node contributes): warp scans,
+        // then one warp scans the warp totals
+        const int wincl = warp_incl_scan(nch);
+        const int warp = threadIdx.x >> 5;
+        if (lane == 31)
+            s_scan[warp] = wincl;
         __syncthreads();
-        for (int o = 1; o < kThreads; o <<= 1) {
-            const int v = threadIdx.x >= o ? s_scan[threadIdx.x - o] : 0;
-            __syncthreads();
-            s_scan[threadIdx.x] += v;
-            __syncthreads();
+        if (threadIdx.x < 32) {
+            int v = threadIdx.x < kThreads / 32 ? s_scan[threadIdx.x] : 0;
+            v = warp_incl_scan(v);
+            if (threadIdx.x < kThreads / 32)
+                s_scan[threadIdx.x] = v;
         }
-        const int incl = s_scan[threadIdx.x];
-        const int total = s_scan[kThreads - 1];
+        __syncthreads();
+        const int incl = wincl + (warp > 0 ? s_scan[warp - 1] : 0);
+        const int total = s_scan[kThreads / 32 - 1];
         if (threadIdx.x == 0) {
             unsigned long long excl = 0;
             if (tile == 0) {
@@ -423,8 +428,9 @@ void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4
         const bool wide = bound <= 4096;  // top levels: few, large nodes
         const long long per_tile = wide ? kThreads / 8 : kThreads;
         long long blocks = (bound + per_tile - 1) / per_tile;
-        if (blocks > 2LL * sms)
-            blocks = 2LL * sms;
+        // the tiles are latency-bound (loads, scan, look-back): fill the SMs (8 blocks each)
+        if (blocks > 8LL * sms)
+            blocks = 8LL * sms;
         count_launch();
         if (wide)
             k_tree_level<8><<<static_cast<int>(blocks), kThreads, 0, s>>>(sorted_keys, l, leaf_cap,
