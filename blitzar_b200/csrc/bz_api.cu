@@ -716,7 +716,7 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
          dalloc(h, &t.q64, 6 * cap) && dalloc(h, &t.box0, cap) && dalloc(h, &t.box1, cap) &&
          dalloc(h, &t.mono, cap) && dalloc(h, &t.quadA, cap) && dalloc(h, &t.quadB, cap);
     GroupTable& gt = h->groups;
-    ok = ok && dalloc(h, &gt.flag, n) && dalloc(h, &gt.gstart, n + 1) && dalloc(h, &gt.ngroups, 1) &&
+    ok = ok && dalloc(h, &gt.flag, group_flag_bytes(static_cast<int>(n))) && dalloc(h, &gt.gstart, n + 1) && dalloc(h, &gt.ngroups, 1) &&
          dalloc(h, &gt.groot, n + 1) && dalloc(h, &gt.sysroot, kMaxSystems) &&
          (cfg->adaptive_max_level == 0 ||
           (dalloc(h, &h->ad.st.level, n) && dalloc(h, &h->ad.st.ax, n) && dalloc(h, &h->ad.st.ay, n) &&

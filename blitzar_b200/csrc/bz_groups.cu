@@ -24,14 +24,17 @@ namespace bz {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kItems = 16;
+constexpr int kItems = 16;                 // flags per thread: one 16-byte load
 constexpr int kChunk = kThreads * kItems;  // flags per compaction block
 
 constexpr float kSparseRatio = 0.5f;
 
-// The system root of node k: its ancestor at root_level (the tree root when root_level = 0).
+// The system root of node k: its ancestor at root_level (node 0, the tree root, when
+// root_level = 0).
 __device__ __forceinline__ int system_root(const TreeArrays& t, int k, int root_level)
 {
+    if (root_level == 0)
+        return 0;
     for (int guard = 0; guard <= kMaxLevels + 1 && t.level[k] > root_level; ++guard)
         k = t.parent[k];
     return k;
@@ -77,7 +80,7 @@ __device__ bool node_split(const TreeArrays& t, int k, int gmax, int root_level,
 }
 
 __global__ void __launch_bounds__(kThreads) k_group_flags(TreeArrays t, int n, int gmax,
-                                                           int root_level, int* __restrict__ flag)
+                                                           int root_level, unsigned char* __restrict__ flag)
 {
     const int nodes = *t.n_nodes;
     for (int k = blockIdx.x * kThreads + threadIdx.x; k < nodes; k += gridDim.x * kThreads) {
@@ -128,15 +131,19 @@ __global__ void k_system_roots(TreeArrays t, int root_level, const unsigned long
             sysroot[static_cast<int>(keys[t.start[k]] >> 54)] = k;
 }
 
-__global__ void __launch_bounds__(kThreads) k_flag_count(const int* __restrict__ flag, int n,
+// Flags set among the 16 bytes of v (each byte 0 or 1).
+__device__ __forceinline__ int flags_in(const uint4 v)
+{
+    return __popc(v.x & 0x01010101u) + __popc(v.y & 0x01010101u) + __popc(v.z & 0x01010101u) +
+           __popc(v.w & 0x01010101u);
+}
+
+__global__ void __launch_bounds__(kThreads) k_flag_count(const unsigned char* __restrict__ flag, int n,
                                                           int* __restrict__ block_sums)
 {
-    const int base = blockIdx.x * kChunk;
-    int c = 0;
-    for (int i = threadIdx.x; i < kChunk; i += kThreads) {
-        const int idx = base + i;
-        c += (idx < n && flag[idx]) ? 1 : 0;
-    }
+    // the flag array is zero past n up to a whole chunk: every thread reads its 16 bytes
+    const uint4 v = reinterpret_cast<const uint4*>(flag + static_cast<size_t>(blockIdx.x) * kChunk)[threadIdx.x];
+    int c = flags_in(v);
     for (int o = 16; o > 0; o >>= 1)
         c += __shfl_xor_sync(kFullMask, c, o);
     __shared__ int ws[kThreads / 32];
@@ -185,8 +192,10 @@ __global__ void __launch_bounds__(1024) k_flag_scan(int* __restrict__ block_sums
         *ngroups = carry;
 }
 
-// Writes the sorted index of every flagged position at its rank, plus the end sentinel n.
-__global__ void __launch_bounds__(kThreads) k_flag_emit(const int* __restrict__ flag, int n,
+// Writes the sorted index of every flagged position at its rank, plus the end sentinel n.  Thread
+// t of a block takes the 16 consecutive flags at t * 16 of the block's chunk: a warp scan of the
+// threads' counts and one scan of the warp totals place every flag.
+__global__ void __launch_bounds__(kThreads) k_flag_emit(const unsigned char* __restrict__ flag, int n,
                                                          const int* __restrict__ block_offsets,
                                                          const int* __restrict__ ngroups,
                                                          int* __restrict__ gstart,
@@ -194,31 +203,29 @@ __global__ void __launch_bounds__(kThreads) k_flag_emit(const int* __restrict__ 
                                                          const unsigned long long* __restrict__ keys,
                                                          const int* __restrict__ sysroot)
 {
-    const int base = blockIdx.x * kChunk;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int base = blockIdx.x * kChunk + threadIdx.x * kItems;
+    const uint4 v = reinterpret_cast<const uint4*>(flag + static_cast<size_t>(blockIdx.x) * kChunk)[threadIdx.x];
+    const int c = flags_in(v);
+    const int incl = warp_incl_scan(c);
     __shared__ int ws[kThreads / 32];
-    __shared__ int carry;
-    if (threadIdx.x == 0)
-        carry = block_offsets[blockIdx.x];
+    if (lane == 31)
+        ws[warp] = incl;
     __syncthreads();
-    for (int it = 0; it < kItems; ++it) {
-        const int idx = base + it * kThreads + threadIdx.x;
-        const int f = (idx < n && flag[idx]) ? 1 : 0;
-        const int x = warp_incl_scan(f);
-        if (lane == 31)
-            ws[warp] = x;
-        __syncthreads();
-        int before = carry;
-        for (int w = 0; w < warp; ++w)
-            before += ws[w];
-        if (f) {
-            gstart[before + x - 1] = idx;
-            groot[before + x - 1] = sysroot ? sysroot[static_cast<int>(keys[idx] >> 54)] : 0;
+    int before = block_offsets[blockIdx.x] + incl - c;
+    for (int w = 0; w < warp; ++w)
+        before += ws[w];
+    if (c > 0) {
+        const unsigned words[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < kItems; ++j) {
+            if ((words[j >> 2] >> (8 * (j & 3))) & 1u) {
+                const int idx = base + j;  // flags are zero past n
+                gstart[before] = idx;
+                groot[before] = sysroot ? sysroot[static_cast<int>(keys[idx] >> 54)] : 0;
+                ++before;
+            }
         }
-        __syncthreads();
-        if (threadIdx.x == kThreads - 1)
-            carry = before + x;
-        __syncthreads();
     }
     if (blockIdx.x == 0 && threadIdx.x == 0)
         gstart[*ngroups] = n;
@@ -235,12 +242,13 @@ int sms_now()
 } // namespace
 
 int group_count_blocks(int n) { return (n + kChunk - 1) / kChunk > 0 ? (n + kChunk - 1) / kChunk : 1; }
+size_t group_flag_bytes(int n) { return static_cast<size_t>(group_count_blocks(n)) * kChunk; }
 
 void launch_groups(const TreeArrays& t, int n, int gmax, int root_level,
                    const unsigned long long* keys, GroupTable& g, cudaStream_t s)
 {
     gmax = gmax < 1 ? 1 : (gmax > kGroupMax ? kGroupMax : gmax);
-    cudaMemsetAsync(g.flag, 0, sizeof(int) * static_cast<size_t>(n), s);
+    cudaMemsetAsync(g.flag, 0, group_flag_bytes(n), s);
     const int sms = sms_now();
     int fb = (t.cap + kThreads - 1) / kThreads;
     fb = fb < 8 * sms ? fb : 8 * sms;

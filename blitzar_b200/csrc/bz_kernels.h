@@ -154,7 +154,7 @@ struct WalkParams {
 // ---------------------------------------------------------------- target groups (bz_groups.cu)
 constexpr int kGroupMax = 32;  // largest walk group (one warp)
 struct GroupTable {
-    int* flag;        // [n] group-start flags
+    unsigned char* flag;  // [group_flag_bytes(n)] group-start flags (0 / 1), zero past n
     int* gstart;      // [n + 1] group start indices in sorted order, then the end sentinel
     int* ngroups;     // [1]
     int* block_sums;  // [group_count_blocks(n)]
@@ -162,6 +162,7 @@ struct GroupTable {
     int* sysroot;     // [kMaxSystems]: root node of each system (ensembles)
 };
 int group_count_blocks(int n);
+size_t group_flag_bytes(int n);
 // root_level: level of the system roots (0 for one system, kSystemLevels for ensembles, whose
 // system id the sorted keys carry in bits 54..62)
 void launch_groups(const TreeArrays& t, int n, int gmax, int root_level,
