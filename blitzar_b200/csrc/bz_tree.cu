@@ -377,11 +377,11 @@ __global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restr
             const int p = t.parent[node];
             if (p < 0)
                 break;
-            __threadfence();
-            const int old = atomicAdd(&t.arrive[p], 1);
+            // release this node's moments and, for the last child, acquire its siblings'
+            int old;
+            asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(old) : "l"(&t.arrive[p]) : "memory");
             if (old != t.nchild[p] - 1)
                 break;
-            __threadfence();
             internal_moments<QUAD>(p, t);
             node = p;
         }
