@@ -707,7 +707,7 @@ __global__ void __launch_bounds__(kWarps * 32) k_walk(const float4* __restrict__
                 const float4 b1 = t.box1[k];
                 // the centre of mass matters only to a node that may be accepted; with a node
                 // size cap (TreePM) most nodes are too large, and skip the load
-                const bool capped = p.max_node_size > 0.0f;
+                const bool capped = SPLIT && p.max_node_size > 0.0f;  // the cap is a TreePM setting
                 float4 mo = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                 if (!capped)
                     mo = t.mono[k];
