@@ -218,6 +218,12 @@ __device__ __forceinline__ void deposit_particles(const float4* __restrict__ pos
         const float m = p.w * inv_h3;
         if (TILED) {
             const uint32_t corner = smem_u32(tile + (bz - oz) * pp + (by - oy) * rp + (bx - ox));
+            // the fixed-point scale is a power of two: folding it into the x weights rounds
+            // exactly as applying it to each product
+            float wxs[P];
+#pragma unroll
+            for (int a = 0; a < P; ++a)
+                wxs[a] = wx[a] * scale;
 #pragma unroll
             for (int c = 0; c < P; ++c)
 #pragma unroll
@@ -227,7 +233,7 @@ __device__ __forceinline__ void deposit_particles(const float4* __restrict__ pos
 #pragma unroll
                     for (int a = 0; a < P; ++a)
                         asm volatile("red.shared.add.s32 [%0], %1;" ::"r"(row + 4u * a),
-                                     "r"(__float2int_rn(wzy * wx[a] * scale))
+                                     "r"(__float2int_rn(wzy * wxs[a]))
                                      : "memory");
                 }
         } else {

@@ -483,14 +483,32 @@ __global__ void __launch_bounds__(kThreads) k_inv_emit(const unsigned long long*
     }
 }
 
-// ctl[1] |= 1 when U is not sorted.
+// ctl[1] |= 1 when U is not sorted.  Each thread checks a run of kVerifyRun consecutive keys
+// (16-byte loads) and the pair across the run's end.
+constexpr int kVerifyRun = 16;
 __global__ void __launch_bounds__(kThreads) k_inv_verify(const unsigned long long* __restrict__ ukeys,
                                                           int n, int* __restrict__ ctl)
 {
-    const int m = n - ctl[0];
+    const long long m = n - ctl[0];
     bool bad = false;
-    for (int j = blockIdx.x * kThreads + threadIdx.x; j + 1 < m; j += gridDim.x * kThreads)
-        bad = bad || ukeys[j] > ukeys[j + 1];
+    const long long stride = static_cast<long long>(gridDim.x) * kThreads * kVerifyRun;
+    for (long long s0 = (static_cast<long long>(blockIdx.x) * kThreads + threadIdx.x) * kVerifyRun;
+         s0 + 1 < m; s0 += stride) {
+        if (s0 + kVerifyRun < m) {
+            const ulonglong2* p = reinterpret_cast<const ulonglong2*>(ukeys + s0);  // 128-byte aligned
+            unsigned long long prev = 0;
+#pragma unroll
+            for (int q = 0; q < kVerifyRun / 2; ++q) {
+                const ulonglong2 v = p[q];
+                bad = bad || (q > 0 && prev > v.x) || v.x > v.y;
+                prev = v.y;
+            }
+            bad = bad || prev > ukeys[s0 + kVerifyRun];
+        } else {
+            for (long long j = s0; j + 1 < m; ++j)
+                bad = bad || ukeys[j] > ukeys[j + 1];
+        }
+    }
     if (__any_sync(kFullMask, bad) && (threadIdx.x & 31) == 0)
         atomicOr(&ctl[1], 1);
 }
