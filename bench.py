@@ -402,13 +402,57 @@ def cpu_reference_step(w, pos, mass, budget_s, seed=7, chunk=65536):
             "extrapolated": bool(extrapolated), "pieces": pieces}
 
 
+def reference_gpu_step(w, pos, vel, mass, warmup=2, steps=5):
+    """The reference's own GPU octree on the same particles: its CUDA kernels and octree_gpu
+    symplectic-Euler step compiled for sm_100a from its sources (oracle/_ref/libbzrefgpu.so),
+    at its defaults (leaf capacity 256, minimum distance² 1e-12, acceleration clamp 64), timed
+    with CUDA events on the stream it launches on.  Octree workloads of at most 2^18 particles:
+    the reference's 10-bit key spread puts every particle in one leaf, so its walk is a direct
+    sum, O(N^2) a step.  None for other workloads or without the library."""
+    if w["kind"] != "octree" or len(mass) > 1 << 18:
+        return None
+    import ctypes as C
+
+    from oracle import oracle as O
+
+    R = O.ref_gpu()
+    if R is None:
+        return None
+    n = len(mass)
+    soa = [np.ascontiguousarray(a[:, k], np.float32) for a in (pos, vel) for k in range(3)]
+    m = np.ascontiguousarray(mass, np.float32)
+    h = R.refgpu_create(n, 256, *soa, m)
+    if not h:
+        return None
+    try:
+        law = (w["theta"], w["eps"], 1e-12, 64.0, 0)
+        acc = [np.zeros(n, np.float32) for _ in range(3)]
+        nodes, leaves = C.c_int(), C.c_int()
+        if R.refgpu_accel(h, *law, *acc, C.byref(nodes), C.byref(leaves)) != 0:
+            return None
+        ms = C.c_double()
+        rc = R.refgpu_time_steps(h, warmup, steps, w["dt"], *law, C.byref(ms))
+    finally:
+        R.refgpu_destroy(h)
+    if rc != 0:
+        return None
+    return {"value": n / (ms.value * 1e-3), "unit": "particle-steps/s", "ms_per_step": ms.value,
+            "steps": steps, "warmup": warmup, "tree_nodes": nodes.value,
+            "tree_leaves": leaves.value,
+            "kind": "reference octree_gpu: its linear-octree build and updateParticlesOctree "
+                    "kernels compiled for sm_100a from its sources",
+            "note": "one leaf holds every particle (10-bit key spread), so the walk is an "
+                    "O(N^2) direct sum; CUDA events on the legacy default stream"}
+
+
 # --------------------------------------------------------------------------- arms
 
 def run_reference(args, w, rank, world):
     """The reference's own CPU implementation of the path on this box's host cores: whole
     force evaluations (cpu_reference_step) repeated while they fit in a few minutes; rank 0
     only.  "steps" is the number actually timed; a step whose walk did not finish within the
-    budget is extrapolated and marked so."""
+    budget is extrapolated and marked so.  Octree workloads add "reference_gpu", the
+    reference's own GPU octree timed on this GPU (reference_gpu_step)."""
     if rank != 0:
         return 0
     pos, vel, mass = make_ics(w, 0)
@@ -443,6 +487,9 @@ def run_reference(args, w, rank, world):
         "e2e": {"value": value, "unit": "particle-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    gpu = reference_gpu_step(w, pos, vel, mass)
+    if gpu is not None:
+        line["reference_gpu"] = gpu
     print(json.dumps(line))
     return 0
 

@@ -1,11 +1,15 @@
 """ctypes bindings for the oracle libraries -- TEST INFRASTRUCTURE ONLY.
 
-Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg import this module,
-and only as the checker: the product (``blitzar_b200``) never calls into it.
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg and reference arm
+import this module, and only as the checker or the reference being timed: the product
+(``blitzar_b200``) never calls into it.
 
 * ``liboracle.so`` -- the C restatement in ``bz_oracle.c`` (built from committed sources).
 * ``_ref/libbzref.so`` -- the reference's own sources compiled where they lie
   (``ref_shim.cpp``); present only where the reference tree was available at build time.
+* ``_ref/libbzrefgpu.so`` -- the reference's GPU linear octree and octree_gpu Euler step
+  compiled for sm_100a from its sources (``ref_gpu_shim.cu``), run on the GPU as the
+  reference arm's GPU comparator and as a checker in the GPU tests.
 """
 from __future__ import annotations
 
@@ -18,6 +22,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
 _REF = None
+_REF_GPU = None
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
@@ -440,3 +445,33 @@ def mlp_grad(params, x6, y3):
     lib().or_mlp_grad(np.ascontiguousarray(params, np.float32), x, np.ascontiguousarray(y3, np.float32),
                       len(x), g, C.byref(loss))
     return g, loss.value
+
+
+def ref_gpu():
+    """The reference's own GPU octree (``_ref/libbzrefgpu.so``), or None when not built.
+
+    ``refgpu_create(n, leaf_capacity, px, py, pz, vx, vy, vz, mass)`` -> handle;
+    ``refgpu_step(h, dt, theta, softening, min_distance2, max_acceleration, criterion)``;
+    ``refgpu_time_steps(h, warmup, steps, dt, ..., criterion, &ms)``;
+    ``refgpu_accel(h, theta, softening, min_distance2, max_acceleration, criterion, ax, ay, az,
+    &nodes, &leaves)``; ``refgpu_get_state(h, px, py, pz, vx, vy, vz)``; ``refgpu_destroy(h)``.
+    Status 0 is success; negative values are argument (-1), CUDA (-2), capacity (-3) or tree
+    (-4) errors."""
+    global _REF_GPU
+    if _REF_GPU is None:
+        path = os.path.join(HERE, "_ref", "libbzrefgpu.so")
+        if not os.path.exists(path):
+            return None
+        R = C.CDLL(path)
+        R.refgpu_create.argtypes = [C.c_int, C.c_int] + [_f32p] * 7
+        R.refgpu_create.restype = C.c_void_p
+        R.refgpu_destroy.argtypes = [C.c_void_p]
+        law = [C.c_float, C.c_float, C.c_float, C.c_float, C.c_int]
+        R.refgpu_step.argtypes = [C.c_void_p, C.c_float] + law
+        R.refgpu_time_steps.argtypes = ([C.c_void_p, C.c_int, C.c_int, C.c_float] + law +
+                                        [C.POINTER(C.c_double)])
+        R.refgpu_accel.argtypes = ([C.c_void_p] + law + [_f32p, _f32p, _f32p, C.POINTER(C.c_int),
+                                                         C.POINTER(C.c_int)])
+        R.refgpu_get_state.argtypes = [C.c_void_p] + [_f32p] * 6
+        _REF_GPU = R
+    return _REF_GPU
