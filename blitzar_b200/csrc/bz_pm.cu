@@ -187,12 +187,11 @@ constexpr int kPlanePad = 12;
 constexpr int kDepositRowPad = 12;
 constexpr int kDepositPlanePad = 4;
 // Fixed pitches for the interpolation's boxes of the usual chunks (a chunk of 256 Morton-
-// consecutive particles at 8 cells per particle spans 12-16 x 17-19 x 17-19 cells): with the
-// strides known at compile time every stencil read is one shared-memory load with an immediate
-// offset (the kernel's integer instructions halve).  The pitches keep the banks of the padded
-// layout (mod 32: 24 and 12; the bank model gives 1.35 wavefronts).  Boxes that do not fit use
-// the padded pitches above.  (The deposit measured no faster with fixed pitches.)
-constexpr int kInterpRp = 24, kInterpPp = 492;  // rows of up to 24 cells, up to 20 rows a plane
+// consecutive particles at 8 cells per particle spans about 20 x 20 x 12 cells): with the
+// staggered visiting order of interp_ad_single the bank model over the benchmark box gives 1.74
+// wavefronts a load for these pitches (2.1 for the padded ones above, which boxes that do not
+// fit use).  (The deposit measured no faster with fixed pitches.)
+constexpr int kInterpRp = 28, kInterpPp = 572;  // rows of up to 28 cells, up to 20 rows a plane
 
 // The scatter of k_deposit_tiled, one thread per particle: all threads of a warp add the same
 // stencil offset together, so two of them meet on one cell only when their particles share a
@@ -304,6 +303,72 @@ __device__ __forceinline__ void deposit_particles(const float4* __restrict__ pos
     }
 }
 
+// Adds four tile cells (fixed point, times unscale) into the mesh at linear cell index g with
+// one vector reduction.
+__device__ __forceinline__ void flush_quad(const int4 c4, float unscale, float* dst)
+{
+    asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst),
+                 "f"(static_cast<float>(c4.x) * unscale), "f"(static_cast<float>(c4.y) * unscale),
+                 "f"(static_cast<float>(c4.z) * unscale), "f"(static_cast<float>(c4.w) * unscale)
+                 : "memory");
+}
+
+// Flush of k_deposit_tiled's tile in groups of four cells: thread t takes groups t,
+// t + kThreads, ... of the (z, y, group) range, its indices advanced by constant steps.  A box
+// inside the mesh (no periodic wrap on any axis; almost every box) adds each group with one
+// vector reduction at a 32-bit cell index; a box that wraps folds each index and adds a group
+// that straddles the x boundary cell by cell.
+__device__ __forceinline__ void flush_tile(const int* tile, int ox, int oy, int oz, int ex, int ey,
+                                           int ez, int rp, int pp, int mesh, float unscale,
+                                           float* __restrict__ rho)
+{
+    const int quads = ex / 4;
+    const int items = ey * ez * quads;
+    int row = threadIdx.x / quads, qd = threadIdx.x - row * quads;
+    int z = row / ey, y = row - z * ey;
+    const int dq = kThreads % quads, drow = kThreads / quads;
+    const int dz = drow / ey, dy = drow - dz * ey;
+    // 32-bit cell indices need mesh^3 < 2^31; the mesh side is a multiple of 4 for the vector
+    // reductions
+    const bool inside = ox >= 0 && oy >= 0 && oz >= 0 && ox + ex <= mesh && oy + ey <= mesh &&
+                        oz + ez <= mesh && mesh <= 1024 && (mesh & 3) == 0;
+    const size_t M = static_cast<size_t>(mesh);
+    for (int f = threadIdx.x; f < items; f += kThreads) {
+        const int4 c4 = *reinterpret_cast<const int4*>(tile + z * pp + y * rp + 4 * qd);
+        if ((c4.x | c4.y | c4.z | c4.w) != 0) {
+            if (inside) {
+                const unsigned g = (static_cast<unsigned>(oz + z) * static_cast<unsigned>(mesh) +
+                                    static_cast<unsigned>(oy + y)) * static_cast<unsigned>(mesh) +
+                                   static_cast<unsigned>(ox + 4 * qd);
+                flush_quad(c4, unscale, rho + g);
+            } else {
+                const size_t rowbase =
+                    (static_cast<size_t>(wrap1(oz + z, mesh)) * M + wrap1(oy + y, mesh)) * M;
+                const int gx = wrap1(ox + 4 * qd, mesh);
+                if (gx + 3 < mesh && (mesh & 3) == 0) {
+                    flush_quad(c4, unscale, rho + rowbase + gx);
+                } else {
+                    const float v[4] = {static_cast<float>(c4.x) * unscale, static_cast<float>(c4.y) * unscale,
+                                        static_cast<float>(c4.z) * unscale, static_cast<float>(c4.w) * unscale};
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                        if (v[j] != 0.0f)
+                            atomicAdd(&rho[rowbase + wrap1(gx + j, mesh)], v[j]);
+                }
+            }
+        }
+        qd += dq;
+        const int carry = qd >= quads ? 1 : 0;
+        qd -= carry * quads;
+        y += dy + carry;
+        z += dz;
+        if (y >= ey) {
+            y -= ey;
+            ++z;
+        }
+    }
+}
+
 template <int P>
 __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __restrict__ pos4, int n,
                                                              int chunk, int mesh, float inv_h_fixed,
@@ -389,46 +454,7 @@ __global__ void __launch_bounds__(kThreads) k_deposit_tiled(const float4* __rest
     if (!tiled)
         return;
     __syncthreads();
-    // Flush the tile in groups of four cells: thread t takes groups t, t + kThreads, ... of the
-    // (z, y, group) range, its indices advanced by constant steps.  Where the group is
-    // contiguous in the mesh (no periodic wrap; the mesh side a multiple of 4), its four cells go
-    // in one vector atomic (red.global.add.v4.f32).
-    const size_t M = static_cast<size_t>(mesh);
-    const int quads = ex / 4;
-    const int items = ey * ez * quads;
-    int row = threadIdx.x / quads, qd = threadIdx.x - row * quads;
-    int z = row / ey, y = row - z * ey;
-    const int dq = kThreads % quads, drow = kThreads / quads;
-    const int dz = drow / ey, dy = drow - dz * ey;
-    for (int f = threadIdx.x; f < items; f += kThreads) {
-        const int4 c4 = *reinterpret_cast<const int4*>(tile + z * pp + y * rp + 4 * qd);
-        if ((c4.x | c4.y | c4.z | c4.w) != 0) {
-            const float v[4] = {static_cast<float>(c4.x) * unscale, static_cast<float>(c4.y) * unscale,
-                                static_cast<float>(c4.z) * unscale, static_cast<float>(c4.w) * unscale};
-            const size_t rowbase = (static_cast<size_t>(wrap1(oz + z, mesh)) * M + wrap1(oy + y, mesh)) * M;
-            const int gx = wrap1(ox + 4 * qd, mesh);
-            if (gx + 3 < mesh && (mesh & 3) == 0) {
-                float* dst = rho + rowbase + gx;
-                asm volatile("red.global.add.v4.f32 [%0], {%1, %2, %3, %4};" ::"l"(dst), "f"(v[0]),
-                             "f"(v[1]), "f"(v[2]), "f"(v[3])
-                             : "memory");
-            } else {
-#pragma unroll
-                for (int j = 0; j < 4; ++j)
-                    if (v[j] != 0.0f)
-                        atomicAdd(&rho[rowbase + wrap1(gx + j, mesh)], v[j]);
-            }
-        }
-        qd += dq;
-        const int carry = qd >= quads ? 1 : 0;
-        qd -= carry * quads;
-        y += dy + carry;
-        z += dz;
-        if (y >= ey) {
-            y -= ey;
-            ++z;
-        }
-    }
+    flush_tile(tile, ox, oy, oz, ex, ey, ez, rp, pp, mesh, unscale, rho);
 }
 
 __device__ __forceinline__ double sinc_d(double v) { return fabs(v) < 1.0e-5 ? 1.0 : sin(v) / v; }
@@ -696,6 +722,96 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
 // The gather of k_interp_ad_tiled: four lanes per particle, lane q taking stencil column
 // x = bx + q of every (y, z) row from the staged tile (TILED) or from the global mesh.  The loop
 // bound is uniform over the block, so every lane of a quad reaches the shuffles.
+// Analytic differentiation from the staged tile, one thread per particle.  Per stencil row
+// (b, c) the thread forms the row's W_x and dW_x weighted sums, then accumulates them with the y
+// and z weights, so every tile value is read once and the bases and weights are computed once a
+// particle.  For the four-point stencil each lane visits the rows and columns in its own order
+// (offset k of an axis at step k ^ s, s from lane bits, as the deposit does): a warp's
+// particles are Morton neighbours about two cells apart, and the staggered orders spread a
+// warp's loads over more banks (a bank model over the benchmark box: 1.7 wavefronts a load
+// with the fixed pitches below).
+template <int P>
+__device__ __forceinline__ void interp_ad_single(const float4* __restrict__ pos4, int base, int end,
+                                                 const MeshFrame& fr, int mesh, const float* tile,
+                                                 int ox, int oy, int oz, int rp, int pp,
+                                                 float* __restrict__ ax, float* __restrict__ ay,
+                                                 float* __restrict__ az)
+{
+    for (int i = base + threadIdx.x; i < end; i += kThreads) {
+        const float4 p = pos4[i];
+        float tx, ty, tz;
+        const int bx = stencil_base<P>(p.x - fr.ox, fr.inv_h, mesh, fr.inv_m, tx);
+        const int by = stencil_base<P>(p.y - fr.oy, fr.inv_h, mesh, fr.inv_m, ty);
+        const int bz = stencil_base<P>(p.z - fr.oz, fr.inv_h, mesh, fr.inv_m, tz);
+        float wx[P], dx[P], wy[P], dy[P], wz[P], dz[P];
+        stencil_weights_d<P>(tx, wx, dx);
+        stencil_weights_d<P>(ty, wy, dy);
+        stencil_weights_d<P>(tz, wz, dz);
+        const float* corner = tile + (bz - oz) * pp + (by - oy) * rp + (bx - ox);
+        float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+        if constexpr (P == 4) {
+            const int lane = threadIdx.x & 31;
+            const int sy = lane & 3, sz = (lane >> 2) & 3, sx = (lane >> 4) & 1;
+            xor_permute4(wx, sx);
+            xor_permute4(dx, sx);
+            xor_permute4(wy, sy);
+            xor_permute4(dy, sy);
+            xor_permute4(wz, sz);
+            xor_permute4(dz, sz);
+            int yoff[4], zoff[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                yoff[k] = (k ^ sy) * rp;
+                zoff[k] = (k ^ sz) * pp;
+            }
+            // x offsets a ^ sx: a = 0, 2 from the even base, a = 1, 3 from the odd one
+            const float* ce = corner + sx;
+            const float* co = corner + 1 - sx;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                float sw = 0.0f, sd = 0.0f, sg = 0.0f;  // plane sums: W_y W_x, dW_y W_x, W_y dW_x
+#pragma unroll
+                for (int b = 0; b < 4; ++b) {
+                    const int r = zoff[c] + yoff[b];
+                    const float v0 = ce[r], v1 = co[r], v2 = ce[r + 2], v3 = co[r + 2];
+                    const float rw = fmaf(wx[3], v3, fmaf(wx[2], v2, fmaf(wx[1], v1, wx[0] * v0)));
+                    const float rd = fmaf(dx[3], v3, fmaf(dx[2], v2, fmaf(dx[1], v1, dx[0] * v0)));
+                    sw = fmaf(wy[b], rw, sw);
+                    sd = fmaf(dy[b], rw, sd);
+                    sg = fmaf(wy[b], rd, sg);
+                }
+                gx = fmaf(wz[c], sg, gx);
+                gy = fmaf(wz[c], sd, gy);
+                gz = fmaf(dz[c], sw, gz);
+            }
+        } else {
+#pragma unroll
+            for (int c = 0; c < P; ++c) {
+                float sw = 0.0f, sd = 0.0f, sg = 0.0f;
+#pragma unroll
+                for (int b = 0; b < P; ++b) {
+                    const float* row = corner + c * pp + b * rp;
+                    float rw = 0.0f, rd = 0.0f;
+#pragma unroll
+                    for (int a = 0; a < P; ++a) {
+                        rw = fmaf(wx[a], row[a], rw);
+                        rd = fmaf(dx[a], row[a], rd);
+                    }
+                    sw = fmaf(wy[b], rw, sw);
+                    sd = fmaf(dy[b], rw, sd);
+                    sg = fmaf(wy[b], rd, sg);
+                }
+                gx = fmaf(wz[c], sg, gx);
+                gy = fmaf(wz[c], sd, gy);
+                gz = fmaf(dz[c], sw, gz);
+            }
+        }
+        ax[i] = gx * fr.inv_h;
+        ay[i] = gy * fr.inv_h;
+        az[i] = gz * fr.inv_h;
+    }
+}
+
 template <int P, bool TILED, int RP = 0, int PP = 0>
 __device__ __forceinline__ void interp_ad_quads(const float4* __restrict__ pos4, int base, int end,
                                                 const MeshFrame& fr, int mesh, const float* tile,
@@ -764,12 +880,11 @@ __device__ __forceinline__ void interp_ad_quads(const float4* __restrict__ pos4,
 // (cp.async.bulk, global -> shared, no multicast), one per mesh row segment: rows start on a
 // 16-byte boundary (x rounded down to a multiple of 4 cells; the mesh side is a multiple of 4),
 // a row crossing the periodic x boundary takes two copies, and all complete on one mbarrier
-// (bounded wait).  Four lanes then serve one particle, lane q reading stencil column
-// x = bx + q of every (y, z) row, and the quad adds its partial sums.  The tile's row and plane
-// pitches are padded by 8 and 12 cells so that the eight particles of a warp, Morton neighbours,
-// read mostly distinct banks: a bank model over the 128^3 benchmark box gives about 1.5
-// shared-memory wavefronts per load, against 11 for one thread per particle on an unpadded tile.
-// A chunk whose box does not fit gathers from the global mesh instead.  The sum is
+// (bounded wait).  One thread then serves one particle (interp_ad_single), each lane of a warp
+// visiting the stencil in its own order over a tile with fixed or padded pitches: about 1.7
+// shared-memory wavefronts a load, against 11 in one order on an unpadded tile.  A chunk whose
+// box does not fit gathers from the global mesh instead, four lanes a particle
+// (interp_ad_quads), lane q reading stencil column x = bx + q.  The sum is
 // a = (1/h) sum_c phi_c grad W(x - x_c), the weight of cell (a, b, c) in the x component being
 // dW_x(a) W_y(b) W_z(c), and likewise for y and z.
 template <int P>
@@ -846,11 +961,8 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
         }
         mbar_wait_bounded(&bar, 0u, err);
     }
-    if (tiled && fixed)
-        interp_ad_quads<P, true, kInterpRp, kInterpPp>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, phi,
-                                                       ax, ay, az);
-    else if (tiled)
-        interp_ad_quads<P, true>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, phi, ax, ay, az);
+    if (tiled)
+        interp_ad_single<P>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, ax, ay, az);
     else
         interp_ad_quads<P, false>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, phi, ax, ay, az);
 }
