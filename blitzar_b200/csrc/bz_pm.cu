@@ -187,10 +187,8 @@ constexpr int kPlanePad = 12;
 constexpr int kDepositRowPad = 12;
 constexpr int kDepositPlanePad = 4;
 // Fixed pitches for the interpolation's boxes of the usual chunks (a chunk of 256 Morton-
-// consecutive particles at 8 cells per particle spans about 20 x 20 x 12 cells): with the
-// staggered visiting order of interp_ad_single the bank model over the benchmark box gives 1.74
-// wavefronts a load for these pitches (2.1 for the padded ones above, which boxes that do not
-// fit use).  (The deposit measured no faster with fixed pitches.)
+// consecutive particles at 8 cells per particle spans about 20 x 20 x 12 cells); boxes that do
+// not fit use the padded pitches above.  (The deposit measured no faster with fixed pitches.)
 constexpr int kInterpRp = 28, kInterpPp = 572;  // rows of up to 28 cells, up to 20 rows a plane
 
 // The scatter of k_deposit_tiled, one thread per particle: all threads of a warp add the same
@@ -722,94 +720,145 @@ __global__ void __launch_bounds__(kThreads) k_interp(const float4* __restrict__ 
 // The gather of k_interp_ad_tiled: four lanes per particle, lane q taking stencil column
 // x = bx + q of every (y, z) row from the staged tile (TILED) or from the global mesh.  The loop
 // bound is uniform over the block, so every lane of a quad reaches the shuffles.
-// Analytic differentiation from the staged tile, one thread per particle.  Per stencil row
-// (b, c) the thread forms the row's W_x and dW_x weighted sums, then accumulates them with the y
-// and z weights, so every tile value is read once and the bases and weights are computed once a
-// particle.  For the four-point stencil each lane visits the rows and columns in its own order
-// (offset k of an axis at step k ^ s, s from lane bits, as the deposit does): a warp's
-// particles are Morton neighbours about two cells apart, and the staggered orders spread a
-// warp's loads over more banks (a bank model over the benchmark box: 1.7 wavefronts a load
-// with the fixed pitches below).
-template <int P>
-__device__ __forceinline__ void interp_ad_single(const float4* __restrict__ pos4, int base, int end,
-                                                 const MeshFrame& fr, int mesh, const float* tile,
-                                                 int ox, int oy, int oz, int rp, int pp,
-                                                 float* __restrict__ ax, float* __restrict__ ay,
-                                                 float* __restrict__ az)
+// Stages the box [ox, ox + ex) x [oy, oy + ey) x [oz, oz + ez) of the mesh into the tile
+// (row pitch rp, plane pitch pp) with 16-byte asynchronous copies (cp.async, one per thread and
+// group of four cells; the caller waits with cp.async.wait_all and a block barrier).  ox, ex,
+// rp, pp and the mesh side are multiples of 4, so every group is 16-byte aligned at both ends
+// and lies on one side of the periodic x boundary.  Thread t takes groups t, t + kThreads, ...
+// of the (z, y, group) range, its indices advanced by constant steps; a box inside the mesh
+// reads at a 32-bit cell index without folding.
+__device__ __forceinline__ void stage_box(const float* __restrict__ phi, int mesh, int ox, int oy, int oz,
+                                          int ex, int ey, int ez, int rp, int pp, float* tile)
 {
-    for (int i = base + threadIdx.x; i < end; i += kThreads) {
-        const float4 p = pos4[i];
-        float tx, ty, tz;
-        const int bx = stencil_base<P>(p.x - fr.ox, fr.inv_h, mesh, fr.inv_m, tx);
-        const int by = stencil_base<P>(p.y - fr.oy, fr.inv_h, mesh, fr.inv_m, ty);
-        const int bz = stencil_base<P>(p.z - fr.oz, fr.inv_h, mesh, fr.inv_m, tz);
-        float wx[P], dx[P], wy[P], dy[P], wz[P], dz[P];
-        stencil_weights_d<P>(tx, wx, dx);
-        stencil_weights_d<P>(ty, wy, dy);
-        stencil_weights_d<P>(tz, wz, dz);
-        const float* corner = tile + (bz - oz) * pp + (by - oy) * rp + (bx - ox);
-        float gx = 0.0f, gy = 0.0f, gz = 0.0f;
-        if constexpr (P == 4) {
-            const int lane = threadIdx.x & 31;
-            const int sy = lane & 3, sz = (lane >> 2) & 3, sx = (lane >> 4) & 1;
-            xor_permute4(wx, sx);
-            xor_permute4(dx, sx);
-            xor_permute4(wy, sy);
-            xor_permute4(dy, sy);
-            xor_permute4(wz, sz);
-            xor_permute4(dz, sz);
-            int yoff[4], zoff[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                yoff[k] = (k ^ sy) * rp;
-                zoff[k] = (k ^ sz) * pp;
-            }
-            // x offsets a ^ sx: a = 0, 2 from the even base, a = 1, 3 from the odd one
-            const float* ce = corner + sx;
-            const float* co = corner + 1 - sx;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                float sw = 0.0f, sd = 0.0f, sg = 0.0f;  // plane sums: W_y W_x, dW_y W_x, W_y dW_x
-#pragma unroll
-                for (int b = 0; b < 4; ++b) {
-                    const int r = zoff[c] + yoff[b];
-                    const float v0 = ce[r], v1 = co[r], v2 = ce[r + 2], v3 = co[r + 2];
-                    const float rw = fmaf(wx[3], v3, fmaf(wx[2], v2, fmaf(wx[1], v1, wx[0] * v0)));
-                    const float rd = fmaf(dx[3], v3, fmaf(dx[2], v2, fmaf(dx[1], v1, dx[0] * v0)));
-                    sw = fmaf(wy[b], rw, sw);
-                    sd = fmaf(dy[b], rw, sd);
-                    sg = fmaf(wy[b], rd, sg);
-                }
-                gx = fmaf(wz[c], sg, gx);
-                gy = fmaf(wz[c], sd, gy);
-                gz = fmaf(dz[c], sw, gz);
-            }
-        } else {
-#pragma unroll
-            for (int c = 0; c < P; ++c) {
-                float sw = 0.0f, sd = 0.0f, sg = 0.0f;
-#pragma unroll
-                for (int b = 0; b < P; ++b) {
-                    const float* row = corner + c * pp + b * rp;
-                    float rw = 0.0f, rd = 0.0f;
-#pragma unroll
-                    for (int a = 0; a < P; ++a) {
-                        rw = fmaf(wx[a], row[a], rw);
-                        rd = fmaf(dx[a], row[a], rd);
-                    }
-                    sw = fmaf(wy[b], rw, sw);
-                    sd = fmaf(dy[b], rw, sd);
-                    sg = fmaf(wy[b], rd, sg);
-                }
-                gx = fmaf(wz[c], sg, gx);
-                gy = fmaf(wz[c], sd, gy);
-                gz = fmaf(dz[c], sw, gz);
-            }
+    const int quads = ex / 4;
+    const int items = ey * ez * quads;
+    int row = threadIdx.x / quads, qd = threadIdx.x - row * quads;
+    int z = row / ey, y = row - z * ey;
+    const int dq = kThreads % quads, drow = kThreads / quads;
+    const int dz = drow / ey, dy = drow - dz * ey;
+    const bool inside = ox >= 0 && oy >= 0 && oz >= 0 && ox + ex <= mesh && oy + ey <= mesh &&
+                        oz + ez <= mesh && mesh <= 1024;
+    const size_t M = static_cast<size_t>(mesh);
+    for (int f = threadIdx.x; f < items; f += kThreads) {
+        const float* src;
+        if (inside)
+            src = phi + ((static_cast<unsigned>(oz + z) * static_cast<unsigned>(mesh) +
+                          static_cast<unsigned>(oy + y)) * static_cast<unsigned>(mesh) +
+                         static_cast<unsigned>(ox + 4 * qd));
+        else
+            src = phi + (static_cast<size_t>(wrap1(oz + z, mesh)) * M + wrap1(oy + y, mesh)) * M +
+                  wrap1(ox + 4 * qd, mesh);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(tile + z * pp + y * rp + 4 * qd)),
+                     "l"(src)
+                     : "memory");
+        qd += dq;
+        const int carry = qd >= quads ? 1 : 0;
+        qd -= carry * quads;
+        y += dy + carry;
+        z += dz;
+        if (y >= ey) {
+            y -= ey;
+            ++z;
         }
-        ax[i] = gx * fr.inv_h;
-        ay[i] = gy * fr.inv_h;
-        az[i] = gz * fr.inv_h;
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
+}
+
+// Analytic differentiation from the staged tile, one thread per particle, in two parts so
+// that a particle's bases and weights are computed while the tile is still being staged:
+// AdStencil holds them, ad_stencil computes them (the tile offset of the stencil's first cell
+// and the W and dW weights of each axis), ad_gather reads the particle's 64 tile values once
+// and forms per stencil row the W_x- and dW_x-weighted sums before the y and z weights.
+template <int P>
+struct AdStencil {
+    int corner;  // tile offset of the stencil's first cell
+    float wx[P], dx[P], wy[P], dy[P], wz[P], dz[P];
+};
+
+template <int P>
+__device__ __forceinline__ AdStencil<P> ad_stencil(const float4 p, const MeshFrame& fr, int mesh, int ox,
+                                                   int oy, int oz, int rp, int pp)
+{
+    AdStencil<P> st;
+    float tx, ty, tz;
+    const int bx = stencil_base<P>(p.x - fr.ox, fr.inv_h, mesh, fr.inv_m, tx);
+    const int by = stencil_base<P>(p.y - fr.oy, fr.inv_h, mesh, fr.inv_m, ty);
+    const int bz = stencil_base<P>(p.z - fr.oz, fr.inv_h, mesh, fr.inv_m, tz);
+    stencil_weights_d<P>(tx, st.wx, st.dx);
+    stencil_weights_d<P>(ty, st.wy, st.dy);
+    stencil_weights_d<P>(tz, st.wz, st.dz);
+    st.corner = (bz - oz) * pp + (by - oy) * rp + (bx - ox);
+    return st;
+}
+
+// Returns the acceleration of the stencil's particle in mesh units (times 1/h afterwards).
+template <int P>
+__device__ __forceinline__ float3 ad_gather(AdStencil<P> st, const float* tile, int rp, int pp)
+{
+    const float* corner = tile + st.corner;
+    float gx = 0.0f, gy = 0.0f, gz = 0.0f;
+    if constexpr (P == 4) {
+        // Each lane visits the rows and columns in its own order (offset k of an axis at step
+        // k ^ s, s from lane bits, as the deposit does): a warp's particles are Morton
+        // neighbours about two cells apart, and the staggered orders spread a warp's loads
+        // over more banks (1.73 wavefronts a load measured, about 4 in one common order).
+        const int lane = threadIdx.x & 31;
+        const int sy = lane & 3, sz = (lane >> 2) & 3, sx = (lane >> 4) & 1;
+        xor_permute4(st.wx, sx);
+        xor_permute4(st.dx, sx);
+        xor_permute4(st.wy, sy);
+        xor_permute4(st.dy, sy);
+        xor_permute4(st.wz, sz);
+        xor_permute4(st.dz, sz);
+        int yoff[4], zoff[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            yoff[k] = (k ^ sy) * rp;
+            zoff[k] = (k ^ sz) * pp;
+        }
+        // x offsets a ^ sx: a = 0, 2 from the even base, a = 1, 3 from the odd one
+        const float* ce = corner + sx;
+        const float* co = corner + 1 - sx;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float sw = 0.0f, sd = 0.0f, sg = 0.0f;  // plane sums: W_y W_x, dW_y W_x, W_y dW_x
+#pragma unroll
+            for (int b = 0; b < 4; ++b) {
+                const int r = zoff[c] + yoff[b];
+                const float v0 = ce[r], v1 = co[r], v2 = ce[r + 2], v3 = co[r + 2];
+                const float rw = fmaf(st.wx[3], v3, fmaf(st.wx[2], v2, fmaf(st.wx[1], v1, st.wx[0] * v0)));
+                const float rd = fmaf(st.dx[3], v3, fmaf(st.dx[2], v2, fmaf(st.dx[1], v1, st.dx[0] * v0)));
+                sw = fmaf(st.wy[b], rw, sw);
+                sd = fmaf(st.dy[b], rw, sd);
+                sg = fmaf(st.wy[b], rd, sg);
+            }
+            gx = fmaf(st.wz[c], sg, gx);
+            gy = fmaf(st.wz[c], sd, gy);
+            gz = fmaf(st.dz[c], sw, gz);
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < P; ++c) {
+            float sw = 0.0f, sd = 0.0f, sg = 0.0f;
+#pragma unroll
+            for (int b = 0; b < P; ++b) {
+                const float* row = corner + c * pp + b * rp;
+                float rw = 0.0f, rd = 0.0f;
+#pragma unroll
+                for (int a = 0; a < P; ++a) {
+                    rw = fmaf(st.wx[a], row[a], rw);
+                    rd = fmaf(st.dx[a], row[a], rd);
+                }
+                sw = fmaf(st.wy[b], rw, sw);
+                sd = fmaf(st.dy[b], rw, sd);
+                sg = fmaf(st.wy[b], rd, sg);
+            }
+            gx = fmaf(st.wz[c], sg, gx);
+            gy = fmaf(st.wz[c], sd, gy);
+            gz = fmaf(st.dz[c], sw, gz);
+        }
+    }
+    return make_float3(gx, gy, gz);
 }
 
 template <int P, bool TILED, int RP = 0, int PP = 0>
@@ -880,15 +929,15 @@ __device__ __forceinline__ void interp_ad_quads(const float4* __restrict__ pos4,
 // (cp.async.bulk, global -> shared, no multicast), one per mesh row segment: rows start on a
 // 16-byte boundary (x rounded down to a multiple of 4 cells; the mesh side is a multiple of 4),
 // a row crossing the periodic x boundary takes two copies, and all complete on one mbarrier
-// (bounded wait).  One thread then serves one particle (interp_ad_single), each lane of a warp
-// visiting the stencil in its own order over a tile with fixed or padded pitches: about 1.7
-// shared-memory wavefronts a load, against 11 in one order on an unpadded tile.  A chunk whose
-// box does not fit gathers from the global mesh instead, four lanes a particle
-// (interp_ad_quads), lane q reading stencil column x = bx + q.  The sum is
+// (bounded wait).  One thread then serves one particle (ad_stencil, ad_gather) over a tile with
+// fixed or padded pitches (the padding spreads a warp's loads over the banks: 11 shared-memory
+// wavefronts a load on an unpadded tile).  A chunk whose box does not fit gathers from the
+// global mesh instead, four lanes a particle (interp_ad_quads), lane q reading stencil column
+// x = bx + q.  The sum is
 // a = (1/h) sum_c phi_c grad W(x - x_c), the weight of cell (a, b, c) in the x component being
 // dW_x(a) W_y(b) W_z(c), and likewise for y and z.
 template <int P>
-__global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __restrict__ pos4, int n,
+__global__ void __launch_bounds__(kThreads, 4) k_interp_ad_tiled(const float4* __restrict__ pos4, int n,
                                                                int chunk, int mesh, float inv_h_fixed,
                                                                const IsoGrid* iso,
                                                                const float* __restrict__ phi,
@@ -898,7 +947,6 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
 {
     __shared__ __align__(16) float tile[kTileCells];
     __shared__ int s_lo[3], s_hi[3];
-    __shared__ unsigned long long bar;
     const MeshFrame fr = mesh_frame(iso, inv_h_fixed, mesh);
     const float inv_h = fr.inv_h;
     const int base = blockIdx.x * chunk;
@@ -907,9 +955,6 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
         s_lo[threadIdx.x] = 1 << 30;
         s_hi[threadIdx.x] = -(1 << 30);
     }
-    if (threadIdx.x == 0)
-        mbar_init(&bar, 1);
-    fence_mbar_init();
     __syncthreads();
     int lo[3] = {1 << 30, 1 << 30, 1 << 30}, hi[3] = {-(1 << 30), -(1 << 30), -(1 << 30)};
     for (int i = base + threadIdx.x; i < end; i += kThreads) {
@@ -943,27 +988,25 @@ __global__ void __launch_bounds__(kThreads) k_interp_ad_tiled(const float4* __re
     const int pp = fixed ? kInterpPp : ey * rp + kPlanePad;
     const bool tiled = ex > 0 && ey > 0 && ez > 0 && ex <= mesh &&
                        static_cast<long long>(pp) * ez <= kTileCells && (mesh & 3) == 0;
-    const size_t M = static_cast<size_t>(mesh);
+    (void)err;  // the staging has no wait of its own to bound (cp.async.wait_all)
     if (tiled) {
-        const int rows = ey * ez;
-        if (threadIdx.x == 0)
-            mbar_arrive_expect_tx(&bar, static_cast<uint32_t>(rows) * static_cast<uint32_t>(ex) * 4u);
+        stage_box(phi, mesh, ox, oy, oz, ex, ey, ez, rp, pp, tile);
+        // the first particle's stencil is prepared while the copies land
+        const int i0 = base + threadIdx.x;
+        AdStencil<P> st = {};
+        if (i0 < end)
+            st = ad_stencil<P>(pos4[i0], fr, mesh, ox, oy, oz, rp, pp);
+        asm volatile("cp.async.wait_all;" ::: "memory");
         __syncthreads();
-        for (int r = threadIdx.x; r < rows; r += kThreads) {
-            const int z = r / ey, y = r - z * ey;
-            const float* row = phi + (static_cast<size_t>(wrap1(oz + z, mesh)) * M + wrap1(oy + y, mesh)) * M;
-            float* dst = tile + z * pp + y * rp;
-            const int x0 = wrap1(ox, mesh);           // a multiple of four
-            const int first = min(ex, mesh - x0);      // cells before the periodic x boundary
-            bulk_g2s(dst, row + x0, static_cast<uint32_t>(first) * 4u, &bar);
-            if (first < ex)
-                bulk_g2s(dst + first, row, static_cast<uint32_t>(ex - first) * 4u, &bar);
+        for (int i = i0; i < end; i += kThreads) {
+            if (i != i0)
+                st = ad_stencil<P>(pos4[i], fr, mesh, ox, oy, oz, rp, pp);
+            const float3 g = ad_gather<P>(st, tile, rp, pp);
+            ax[i] = g.x * inv_h;
+            ay[i] = g.y * inv_h;
+            az[i] = g.z * inv_h;
         }
-        mbar_wait_bounded(&bar, 0u, err);
-    }
-    if (tiled)
-        interp_ad_single<P>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, ax, ay, az);
-    else
+    } else
         interp_ad_quads<P, false>(pos4, base, end, fr, mesh, tile, ox, oy, oz, rp, pp, phi, ax, ay, az);
 }
 
