@@ -30,6 +30,47 @@ def test_graph_equals_eager(gpu):
     assert np.array_equal(out[0][1], out[1][1])
 
 
+@pytest.mark.parametrize("case", ["octree", "treepm"])
+def test_steps_in_one_call_equal_single_steps(gpu, case):
+    """A leapfrog call of several steps folds each closing kick into the next step's opening
+    kernel (and kicks once after the last step): the same arithmetic as single-step calls, so
+    the octree state agrees bit for bit.  TreePM agrees to the mesh's run-to-run spread (its
+    float reductions into the mesh run in no fixed order), and its accelerations, completed by
+    the mesh leg's in the closing kick, agree too."""
+    n = 16_384
+    rng = np.random.default_rng(12)
+    if case == "octree":
+        pos = plummer(n, seed=12)
+        cfg = {}
+    else:
+        pos = rng.random((n, 3)).astype(np.float32)
+        cfg = dict(solver=1, box_length=1.0, treepm_grid_size=32, octree_softening=1e-3,
+                   treepm_assignment=2, treepm_gradient=2)
+    vel = (0.1 * rng.standard_normal((n, 3))).astype(np.float32)
+    m = np.full(n, 1.0 / n, np.float32)
+    out = []
+    for split in (False, True):
+        with _engine(n, **cfg) as e:
+            e.set_state(pos, vel, m)
+            if split:
+                for _ in range(6):
+                    e.step(1e-3, 1)
+            else:
+                e.step(1e-3, 6)
+            p, v = e.get_state(f64=True)
+            a = np.empty(3 * n, np.float32)
+            e.get_state_acc_soa(np.empty(3 * n, np.float32), np.empty(3 * n, np.float32), a)
+            out.append((p, v, a))
+    if case == "octree":
+        for x, y in zip(out[0], out[1]):
+            assert np.array_equal(x, y)
+    else:
+        assert np.abs(out[0][0] - out[1][0]).max() < 1e-10
+        assert np.abs(out[0][1] - out[1][1]).max() < 1e-7
+        a0, a1 = out[0][2].reshape(3, n), out[1][2].reshape(3, n)
+        assert np.abs(a0 - a1).max() < 1e-4 * np.abs(a1).max()
+
+
 def test_kdk_matches_oracle_integration(gpu, oracle):
     n = 4000
     pos = plummer(n, seed=4).astype(np.float64)
