@@ -129,6 +129,12 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(unsigned long long* keys_
     uint32_t* dst_v = (np & 1) ? vals_a : vals_b;
 
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    const int shift = 8 * pass;
+    const unsigned lt = lanemask_lt();
+    // Persistent blocks take tiles in ticket order until the (device-side) count is covered:
+    // a tile's look-back waits only on tiles taken earlier by running blocks.  A grid sized
+    // for a larger capacity than the job costs a few idle blocks, not a wave per tile.
+    for (;;) {
     if (tid == 0)
         sm.tile = static_cast<int>(atomicAdd(&ws.ticket[pass], 1u));
     for (int i = tid; i < kWarps * 256; i += kThreads)
@@ -137,9 +143,7 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(unsigned long long* keys_
     const int tile = sm.tile;
     const long long base = static_cast<long long>(tile) * kTile;
     if (base >= n)
-        return;  // a grid sized for a larger capacity: no later tile waits for this one
-    const int shift = 8 * pass;
-    const unsigned lt = lanemask_lt();
+        return;  // no later tile waits for this one
 
     unsigned long long kr[kIter];
     uint32_t vr[kIter];
@@ -234,6 +238,8 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(unsigned long long* keys_
         dst_k[out] = key;
         dst_v[out] = sm.vals[j];
     }
+    __syncthreads();  // the next tile reuses the shared memory
+    }
 }
 
 // After the passes the data sits in the alternate buffers when an odd number of passes ran;
@@ -299,10 +305,20 @@ void enqueue_sort(unsigned long long* keys, uint32_t* vals, int n, int bits, Sor
         if (dev >= 0 && dev < kMaxDevices)
             attr_set[dev].store(true);
     }
+    // persistent grid: the resident blocks (at most one per tile)
+    static std::atomic<int> resident[kMaxDevices];
+    int per_sm = dev >= 0 && dev < kMaxDevices ? resident[dev].load() : 0;
+    if (per_sm <= 0) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_onesweep, kThreads, smem);
+        per_sm = per_sm > 0 ? per_sm : 1;
+        if (dev >= 0 && dev < kMaxDevices)
+            resident[dev].store(per_sm);
+    }
+    const int grid = tiles < per_sm * sms ? tiles : per_sm * sms;
     for (int p = 0; p < passes; ++p) {
         count_launch();
-        k_onesweep<<<tiles, kThreads, smem, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, p, ws,
-                                                 err, job);
+        k_onesweep<<<grid, kThreads, smem, s>>>(keys, vals, ws.keys_alt, ws.vals_alt, n, p, ws,
+                                                err, job);
     }
     int fb = (n + 255) / 256;
     fb = fb < 4 * sms ? fb : 4 * sms;
