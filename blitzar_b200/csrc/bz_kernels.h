@@ -102,7 +102,6 @@ struct TreeArrays {
     int* n_nodes;      // [1]
     uint32_t* ticket;  // [kMaxLevels+2]
     unsigned long long* lookback;  // [tree_lookback_words(cap)]
-    int* arrive;       // [cap] bottom-up arrival counters
     double* m64;       // [cap] FP64 mass
     double* s64;       // [3*cap] FP64 first moments
     double* c64;       // [3*cap] FP64 centre of mass

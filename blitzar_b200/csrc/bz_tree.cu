@@ -38,7 +38,6 @@ __global__ void k_tree_init(TreeArrays t, int n)
         t.count[0] = n;
         t.parent[0] = -1;
         t.level[0] = 0;
-        t.arrive[0] = 0;
     }
 }
 
@@ -223,7 +222,6 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
                         t.count[c] = b[d + 1] - b[d];
                         t.parent[c] = k;
                         t.level[c] = l + 1;
-                        t.arrive[c] = 0;
                         ++c;
                     }
                 }
@@ -285,11 +283,13 @@ __device__ void leaf_moments(const float4* __restrict__ pos4, int k, TreeArrays&
     t.s64[3 * k] = sx;
     t.s64[3 * k + 1] = sy;
     t.s64[3 * k + 2] = sz;
-    t.c64[3 * k] = cx;
-    t.c64[3 * k + 1] = cy;
-    t.c64[3 * k + 2] = cz;
-    for (int j = 0; j < 6; ++j)
-        t.q64[6 * k + j] = q[j];
+    if (QUAD) {  // the FP64 centre and second moments feed only the parents' second moments
+        t.c64[3 * k] = cx;
+        t.c64[3 * k + 1] = cy;
+        t.c64[3 * k + 2] = cz;
+        for (int j = 0; j < 6; ++j)
+            t.q64[6 * k + j] = q[j];
+    }
     t.box0[k] = make_float4(mn[0], mn[1], mn[2], __int_as_float(s));
     t.box1[k] = make_float4(mx[0], mx[1], mx[2], __int_as_float(-(e - s)));
     t.mono[k] = make_float4((float)cx, (float)cy, (float)cz, (float)tm);
@@ -349,11 +349,13 @@ __device__ void internal_moments(int k, TreeArrays& t)
     t.s64[3 * k] = sx;
     t.s64[3 * k + 1] = sy;
     t.s64[3 * k + 2] = sz;
-    t.c64[3 * k] = cx;
-    t.c64[3 * k + 1] = cy;
-    t.c64[3 * k + 2] = cz;
-    for (int j = 0; j < 6; ++j)
-        t.q64[6 * k + j] = q[j];
+    if (QUAD) {  // the FP64 centre and second moments feed only the parents' second moments
+        t.c64[3 * k] = cx;
+        t.c64[3 * k + 1] = cy;
+        t.c64[3 * k + 2] = cz;
+        for (int j = 0; j < 6; ++j)
+            t.q64[6 * k + j] = q[j];
+    }
     t.box0[k] = make_float4(mn[0], mn[1], mn[2], __int_as_float(c0));
     t.box1[k] = make_float4(mx[0], mx[1], mx[2], __int_as_float(nc));
     t.mono[k] = make_float4((float)cx, (float)cy, (float)cz, (float)tm);
@@ -361,30 +363,58 @@ __device__ void internal_moments(int k, TreeArrays& t)
     t.quadB[k] = make_float2((float)q[4], (float)q[5]);
 }
 
-// One thread per leaf computes its moments, then climbs: the child that arrives last at a
-// parent (atomic counter) computes the parent from all children in octant order.
+// Moments bottom-up, level-synchronous: every leaf from its particles in one pass
+// (k_leaf_moments), then the internal nodes of each level from their children, deepest level
+// first (k_level_moments, one launch per level).  Each node is computed once from complete
+// children, in the same order of sums as a climb would, without atomics or fences.
 template <bool QUAD>
-__global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restrict__ pos4,
+__global__ void __launch_bounds__(kThreads) k_leaf_moments(const float4* __restrict__ pos4,
                                                             TreeArrays t)
 {
     const int nn = t.n_nodes[0];
-    for (int k = blockIdx.x * kThreads + threadIdx.x; k < nn; k += gridDim.x * kThreads) {
-        if (t.nchild[k] != 0)
-            continue;
-        leaf_moments<QUAD>(pos4, k, t);
-        int node = k;
-        for (;;) {
-            const int p = t.parent[node];
-            if (p < 0)
-                break;
-            // release this node's moments and, for the last child, acquire its siblings'
-            int old;
-            asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(old) : "l"(&t.arrive[p]) : "memory");
-            if (old != t.nchild[p] - 1)
-                break;
-            internal_moments<QUAD>(p, t);
-            node = p;
-        }
+    for (int k = blockIdx.x * kThreads + threadIdx.x; k < nn; k += gridDim.x * kThreads)
+        if (t.nchild[k] == 0)
+            leaf_moments<QUAD>(pos4, k, t);
+}
+
+template <bool QUAD>
+__global__ void __launch_bounds__(kThreads) k_level_moments(TreeArrays t, int l)
+{
+    const int first = t.lvl_first[l];
+    const int cnt = min(t.lvl_count[l], t.cap - first);
+    for (int i = blockIdx.x * kThreads + threadIdx.x; i < cnt; i += gridDim.x * kThreads) {
+        const int k = first + i;
+        if (t.nchild[k] > 0)
+            internal_moments<QUAD>(k, t);
+    }
+}
+
+void enqueue_moments(const float4* pos4, TreeArrays& t, int max_level, int sms, cudaStream_t s,
+                     bool quad)
+{
+    long long mb = (static_cast<long long>(t.cap) + kThreads - 1) / kThreads;
+    if (mb > 16LL * sms)
+        mb = 16LL * sms;
+    count_launch();
+    if (quad)
+        k_leaf_moments<true><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+    else
+        k_leaf_moments<false><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+    // internal nodes sit at levels 0 .. max_level - 1; level l holds at most min(8^l, cap)
+    for (int l = max_level - 1; l >= 0; --l) {
+        long long bound = 1;
+        for (int j = 0; j < l && bound < t.cap; ++j)
+            bound *= 8;
+        if (bound > t.cap)
+            bound = t.cap;
+        long long blocks = (bound + kThreads - 1) / kThreads;
+        if (blocks > 8LL * sms)
+            blocks = 8LL * sms;
+        count_launch();
+        if (quad)
+            k_level_moments<true><<<static_cast<int>(blocks), kThreads, 0, s>>>(t, l);
+        else
+            k_level_moments<false><<<static_cast<int>(blocks), kThreads, 0, s>>>(t, l);
     }
 }
 
@@ -395,15 +425,7 @@ void launch_tree_refit(const float4* pos4, TreeArrays& t, cudaStream_t s, bool q
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    cudaMemsetAsync(t.arrive, 0, sizeof(int) * static_cast<size_t>(t.cap), s);
-    long long mb = (static_cast<long long>(t.cap) + kThreads - 1) / kThreads;
-    if (mb > 16LL * sms)
-        mb = 16LL * sms;
-    count_launch();
-    if (quad)
-        k_tree_moments<true><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
-    else
-        k_tree_moments<false><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+    enqueue_moments(pos4, t, kMaxLevels, sms, s, quad);
 }
 
 size_t tree_lookback_words(int cap) { return static_cast<size_t>(cap) / kLookbackNodes + 2 * kMaxLevels + 8; }
@@ -441,14 +463,7 @@ void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4
     }
     count_launch();
     k_tree_finish_last<<<sms, 256, 0, s>>>(t, max_level);
-    long long mb = (static_cast<long long>(t.cap) + kThreads - 1) / kThreads;
-    if (mb > 16LL * sms)
-        mb = 16LL * sms;
-    count_launch();
-    if (quad)
-        k_tree_moments<true><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
-    else
-        k_tree_moments<false><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+    enqueue_moments(pos4, t, max_level, sms, s, quad);
 }
 
 } // namespace bz
