@@ -99,6 +99,7 @@ struct TreeArrays {
     int* level;
     int* lvl_first;    // [kMaxLevels+2]
     int* lvl_count;    // [kMaxLevels+2]
+    int* lvl_maxcnt;   // [kMaxLevels+2] largest particle count of a node of the level
     int* n_nodes;      // [1]
     uint32_t* ticket;  // [kMaxLevels+2]
     unsigned long long* lookback;  // [tree_lookback_words(cap)]

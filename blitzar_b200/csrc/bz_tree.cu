@@ -29,10 +29,12 @@ __global__ void k_tree_init(TreeArrays t, int n)
     if (i < kMaxLevels + 2) {
         t.lvl_first[i] = 0;
         t.lvl_count[i] = 0;
+        t.lvl_maxcnt[i] = 0;
         t.ticket[i] = 0;
     }
     if (i == 0) {
         t.lvl_count[0] = 1;
+        t.lvl_maxcnt[0] = n;
         t.n_nodes[0] = 1;
         t.start[0] = 0;
         t.count[0] = n;
@@ -86,8 +88,21 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
     const int cnt = min(t.lvl_count[l], t.cap - first);
     if (cnt <= 0)
         return;
-    const int ntiles = (cnt + kNodesPerTile - 1) / kNodesPerTile;
     const int next_first = first + cnt;
+    if (t.lvl_maxcnt[l] <= leaf_cap && l >= min_split) {
+        // no node of this level holds more than a leaf: all are leaves, no children, no scan
+        for (int i = blockIdx.x * kThreads + threadIdx.x; i < cnt; i += gridDim.x * kThreads) {
+            t.child[first + i] = -1;
+            t.nchild[first + i] = 0;
+        }
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            t.lvl_first[l + 1] = next_first;
+            t.lvl_count[l + 1] = 0;
+            t.n_nodes[0] = min(next_first, t.cap);
+        }
+        return;
+    }
+    const int ntiles = (cnt + kNodesPerTile - 1) / kNodesPerTile;
     unsigned long long* lb = t.lookback + (first / kLookbackNodes + 2 * l);
     const int shift = 3 * (max_level - l - 1);
     const int slot = threadIdx.x / TPN, sub = threadIdx.x % TPN, lane = threadIdx.x & 31;
@@ -208,6 +223,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
             }
         }
         __syncthreads();
+        int cmax = 0;
         if (k < next_first && sub == 0) {
             int c = next_first + s_prefix + incl - nch;
             if (split && c + nch > t.cap)
@@ -222,11 +238,16 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
                         t.count[c] = b[d + 1] - b[d];
                         t.parent[c] = k;
                         t.level[c] = l + 1;
+                        cmax = max(cmax, b[d + 1] - b[d]);
                         ++c;
                     }
                 }
             }
         }
+        // the largest child of the next level decides whether that level can split at all
+        cmax = __reduce_max_sync(kFullMask, cmax);
+        if (lane == 0 && cmax > 0)
+            atomicMax(&t.lvl_maxcnt[l + 1], cmax);
         __syncthreads();
     }
 }
