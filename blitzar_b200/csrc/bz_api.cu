@@ -771,9 +771,9 @@ bz_status bz_create(const bz_config* cfg, size_t capacity, bz_handle** out)
     ok = ok && dalloc(h, &t.start, cap) && dalloc(h, &t.count, cap) && dalloc(h, &t.child, cap) &&
          dalloc(h, &t.nchild, cap) && dalloc(h, &t.parent, cap) && dalloc(h, &t.level, cap) &&
          dalloc(h, &t.lvl_first, kMaxLevels + 2) && dalloc(h, &t.lvl_count, kMaxLevels + 2) &&
-         dalloc(h, &t.lvl_maxcnt, kMaxLevels + 2) &&
+         dalloc(h, &t.lvl_split, kMaxLevels + 2) &&
          dalloc(h, &t.n_nodes, 1) && dalloc(h, &t.ticket, kMaxLevels + 2) &&
-         dalloc(h, &t.lookback, tree_lookback_words(t.cap)) &&
+         dalloc(h, &t.lookback, tree_lookback_words(t.cap)) && dalloc(h, &t.arrive, cap) &&
          dalloc(h, &t.m64, cap) && dalloc(h, &t.s64, 3 * cap) && dalloc(h, &t.c64, 3 * cap) &&
          dalloc(h, &t.q64, 6 * cap) && dalloc(h, &t.box0, cap) && dalloc(h, &t.box1, cap) &&
          dalloc(h, &t.mono, cap) && dalloc(h, &t.quadA, cap) && dalloc(h, &t.quadB, cap);

@@ -99,9 +99,10 @@ struct TreeArrays {
     int* level;
     int* lvl_first;    // [kMaxLevels+2]
     int* lvl_count;    // [kMaxLevels+2]
-    int* lvl_maxcnt;   // [kMaxLevels+2] largest particle count of a node of the level
+    int* lvl_split;    // [kMaxLevels+2] 1 when some node of the level holds more than a leaf
     int* n_nodes;      // [1]
     uint32_t* ticket;  // [kMaxLevels+2]
+    int* arrive;       // [cap] bottom-up arrival counters of the moments climb
     unsigned long long* lookback;  // [tree_lookback_words(cap)]
     double* m64;       // [cap] FP64 mass
     double* s64;       // [3*cap] FP64 first moments

@@ -238,6 +238,9 @@ __global__ void __launch_bounds__(kThreads) k_onesweep(unsigned long long* keys_
         dst_k[out] = key;
         dst_v[out] = sm.vals[j];
     }
+    // a grid with a block for every tile of this count takes no second ticket
+    if (static_cast<long long>(gridDim.x) * kTile >= n)
+        return;
     __syncthreads();  // the next tile reuses the shared memory
     }
 }

@@ -29,17 +29,18 @@ __global__ void k_tree_init(TreeArrays t, int n)
     if (i < kMaxLevels + 2) {
         t.lvl_first[i] = 0;
         t.lvl_count[i] = 0;
-        t.lvl_maxcnt[i] = 0;
+        t.lvl_split[i] = 0;
         t.ticket[i] = 0;
     }
     if (i == 0) {
         t.lvl_count[0] = 1;
-        t.lvl_maxcnt[0] = n;
+        t.lvl_split[0] = 1;  // the root level goes the general way
         t.n_nodes[0] = 1;
         t.start[0] = 0;
         t.count[0] = n;
         t.parent[0] = -1;
         t.level[0] = 0;
+        t.arrive[0] = 0;
     }
 }
 
@@ -89,7 +90,7 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
     if (cnt <= 0)
         return;
     const int next_first = first + cnt;
-    if (t.lvl_maxcnt[l] <= leaf_cap && l >= min_split) {
+    if (__ldcg(&t.lvl_split[l]) == 0 && l >= min_split) {
         // no node of this level holds more than a leaf: all are leaves, no children, no scan
         for (int i = blockIdx.x * kThreads + threadIdx.x; i < cnt; i += gridDim.x * kThreads) {
             t.child[first + i] = -1;
@@ -238,16 +239,17 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
                         t.count[c] = b[d + 1] - b[d];
                         t.parent[c] = k;
                         t.level[c] = l + 1;
+                        t.arrive[c] = 0;
                         cmax = max(cmax, b[d + 1] - b[d]);
                         ++c;
                     }
                 }
             }
         }
-        // the largest child of the next level decides whether that level can split at all
-        cmax = __reduce_max_sync(kFullMask, cmax);
-        if (lane == 0 && cmax > 0)
-            atomicMax(&t.lvl_maxcnt[l + 1], cmax);
+        // a child larger than a leaf lets the next level split: flag it (plain stores of the
+        // same value, skipped once the flag reads set, instead of contended atomics)
+        if (__any_sync(kFullMask, cmax > leaf_cap) && lane == 0 && __ldcg(&t.lvl_split[l + 1]) == 0)
+            t.lvl_split[l + 1] = 1;
         __syncthreads();
     }
 }
@@ -384,59 +386,48 @@ __device__ void internal_moments(int k, TreeArrays& t)
     t.quadB[k] = make_float2((float)q[4], (float)q[5]);
 }
 
-// Moments bottom-up, level-synchronous: every leaf from its particles in one pass
-// (k_leaf_moments), then the internal nodes of each level from their children, deepest level
-// first (k_level_moments, one launch per level).  Each node is computed once from complete
-// children, in the same order of sums as a climb would, without atomics or fences.
+// One thread per leaf computes its moments, then climbs: the child that arrives last at a
+// parent (atomic counter) computes the parent from all children in octant order.
 template <bool QUAD>
-__global__ void __launch_bounds__(kThreads) k_leaf_moments(const float4* __restrict__ pos4,
+__global__ void __launch_bounds__(kThreads) k_tree_moments(const float4* __restrict__ pos4,
                                                             TreeArrays t)
 {
     const int nn = t.n_nodes[0];
-    for (int k = blockIdx.x * kThreads + threadIdx.x; k < nn; k += gridDim.x * kThreads)
-        if (t.nchild[k] == 0)
-            leaf_moments<QUAD>(pos4, k, t);
-}
-
-template <bool QUAD>
-__global__ void __launch_bounds__(kThreads) k_level_moments(TreeArrays t, int l)
-{
-    const int first = t.lvl_first[l];
-    const int cnt = min(t.lvl_count[l], t.cap - first);
-    for (int i = blockIdx.x * kThreads + threadIdx.x; i < cnt; i += gridDim.x * kThreads) {
-        const int k = first + i;
-        if (t.nchild[k] > 0)
-            internal_moments<QUAD>(k, t);
+    for (int k = blockIdx.x * kThreads + threadIdx.x; k < nn; k += gridDim.x * kThreads) {
+        if (t.nchild[k] != 0)
+            continue;
+        leaf_moments<QUAD>(pos4, k, t);
+        int node = k;
+        for (;;) {
+            const int p = t.parent[node];
+            if (p < 0)
+                break;
+            // release this node's moments and, for the last child, acquire its siblings'
+            int old;
+            asm volatile("atom.add.acq_rel.gpu.s32 %0, [%1], 1;" : "=r"(old) : "l"(&t.arrive[p]) : "memory");
+            if (old != t.nchild[p] - 1)
+                break;
+            internal_moments<QUAD>(p, t);
+            node = p;
+        }
     }
 }
 
-void enqueue_moments(const float4* pos4, TreeArrays& t, int max_level, int sms, cudaStream_t s,
-                     bool quad)
+
+// clear_arrive: the arrival counters are not fresh from a build (a refit of an existing tree)
+void enqueue_moments(const float4* pos4, TreeArrays& t, int sms, cudaStream_t s, bool quad,
+                     bool clear_arrive)
 {
+    if (clear_arrive)
+        cudaMemsetAsync(t.arrive, 0, sizeof(int) * static_cast<size_t>(t.cap), s);
     long long mb = (static_cast<long long>(t.cap) + kThreads - 1) / kThreads;
     if (mb > 16LL * sms)
         mb = 16LL * sms;
     count_launch();
     if (quad)
-        k_leaf_moments<true><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
+        k_tree_moments<true><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
     else
-        k_leaf_moments<false><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
-    // internal nodes sit at levels 0 .. max_level - 1; level l holds at most min(8^l, cap)
-    for (int l = max_level - 1; l >= 0; --l) {
-        long long bound = 1;
-        for (int j = 0; j < l && bound < t.cap; ++j)
-            bound *= 8;
-        if (bound > t.cap)
-            bound = t.cap;
-        long long blocks = (bound + kThreads - 1) / kThreads;
-        if (blocks > 8LL * sms)
-            blocks = 8LL * sms;
-        count_launch();
-        if (quad)
-            k_level_moments<true><<<static_cast<int>(blocks), kThreads, 0, s>>>(t, l);
-        else
-            k_level_moments<false><<<static_cast<int>(blocks), kThreads, 0, s>>>(t, l);
-    }
+        k_tree_moments<false><<<static_cast<int>(mb), kThreads, 0, s>>>(pos4, t);
 }
 
 } // namespace
@@ -446,7 +437,7 @@ void launch_tree_refit(const float4* pos4, TreeArrays& t, cudaStream_t s, bool q
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    enqueue_moments(pos4, t, kMaxLevels, sms, s, quad);
+    enqueue_moments(pos4, t, sms, s, quad, true);
 }
 
 size_t tree_lookback_words(int cap) { return static_cast<size_t>(cap) / kLookbackNodes + 2 * kMaxLevels + 8; }
@@ -484,7 +475,7 @@ void launch_tree_build(const unsigned long long* sorted_keys, const float4* pos4
     }
     count_launch();
     k_tree_finish_last<<<sms, 256, 0, s>>>(t, max_level);
-    enqueue_moments(pos4, t, max_level, sms, s, quad);
+    enqueue_moments(pos4, t, sms, s, quad, false);
 }
 
 } // namespace bz
