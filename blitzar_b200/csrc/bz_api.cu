@@ -99,11 +99,8 @@ struct bz_handle {
     double* io_pos = nullptr;       // 3 x capacity doubles of caller-order positions
     double* io_host_pos = nullptr;  // set only while that call enqueues its step
     float phase_ms[kNumPhases] = {};
-    // graphs of a step (kind x state-buffer parity): kStepWhole opens, evaluates and closes;
-    // kStepFirst opens and evaluates, leaving the closing kick to the next step's opening
-    // kernel; kStepNext also applies the previous step's closing kick (leapfrog calls of several
-    // steps: first, next, ..., next, then one closing kick)
-    cudaGraphExec_t graph[3][2] = {};
+    // graphs (one per state-buffer parity)
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};
     bool graph_failed = false;
     double* h_dt = nullptr;  // pinned {dt, dt/2}
     unsigned long long last_pp = 0, last_pn = 0, last_eval = 0;
@@ -138,19 +135,6 @@ struct bz_handle {
 };
 
 namespace {
-
-// Step kinds (the graph array's first index).
-constexpr int kStepWhole = 0, kStepFirst = 1, kStepNext = 2;
-
-void release_graphs(bz_handle* h)
-{
-    for (auto& kind : h->graph)
-        for (auto& ex : kind) {
-            if (ex)
-                cudaGraphExecDestroy(ex);
-            ex = nullptr;
-        }
-}
 
 bz_status fail(bz_handle* h, bz_status s, const std::string& msg)
 {
@@ -267,19 +251,9 @@ bool mesh_concurrent(const bz_handle* h)
            !h->timing;
 }
 
-// The learned correction adds into the walk's accelerations after the mesh leg has joined.
-bool learned_on(const bz_handle* h)
-{
-    return h->learn.enabled && h->learn.trained && h->cfg.solver == BZ_SOLVER_TREEPM;
-}
-
 // Forces of the (already ordered) state into d.acc; optional closing kick.  `mesh_forked`: the
-// step already forked the deposit and field solve onto pm_stream (mesh mode 2).  `defer_close`:
-// the closing kick is left to the next step's opening kernel (or a closing kick after the
-// last step), which also completes d.acc with the mesh leg's accelerations where the closing
-// kick would have.
-void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = false,
-                    bool defer_close = false)
+// step already forked the deposit and field solve onto pm_stream (mesh mode 2).
+void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = false)
 {
     const int n = static_cast<int>(h->n);
     DeviceBuffers& d = h->d;
@@ -331,7 +305,7 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
     wp.blocks_per_sm = h->walk_blocks_per_sm;
     // the mesh force computed in line is already in d.acc: the walk clamps the sum
     wp.clamp_total = h->cfg.solver == BZ_SOLVER_TREEPM && h->pm && !overlap ? 1 : 0;
-    const bool learned = learned_on(h);
+    const bool learned = h->learn.enabled && h->learn.trained && h->cfg.solver == BZ_SOLVER_TREEPM;
     if (learned) {
         o.pair_src = h->learn.pair_src;
         o.pair_cnt = h->learn.pair_cnt;
@@ -341,7 +315,7 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
     }
     launch_walk(d.pos4, n, h->tree, h->groups, wp, o, d.queue, d.spill, d.err, h->stream);
     // the mesh leg's accelerations complete d.acc here, or inside the closing kick
-    const bool add_in_kick = overlap && (kick || defer_close) && !learned;
+    const bool add_in_kick = overlap && kick && !learned;
     if (overlap) {
         cudaStreamWaitEvent(h->stream, h->ev_join, 0);
         if (!add_in_kick)
@@ -367,43 +341,20 @@ void enqueue_forces(bz_handle* h, bool kick, bool want_pot, bool mesh_forked = f
 
 void enqueue_io_positions(bz_handle* h);
 
-// The mesh leg's accelerations wait in d.acc_pm for the closing kick to complete d.acc.
-bool mesh_added_in_kick(const bz_handle* h) { return mesh_concurrent(h) && !learned_on(h); }
-
-// The closing kick of a leapfrog call of several steps, after its last step.
-void enqueue_close(bz_handle* h)
-{
-    DeviceBuffers& d = h->d;
-    double* const* s = d.st[h->cur];
-    const int n = static_cast<int>(h->n);
-    if (mesh_added_in_kick(h))
-        launch_kick(s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt + 1, h->stream,
-                    d.acc_pm[0], d.acc_pm[1], d.acc_pm[2], h->cfg.physics_max_acceleration);
-    else
-        launch_kick(s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt + 1, h->stream);
-}
-
-// One step of the given kind (kStepWhole, kStepFirst, kStepNext; symplectic Euler has no
-// closing kick, so its kinds coincide).
-void enqueue_step(bz_handle* h, int kind = kStepWhole)
+void enqueue_step(bz_handle* h)
 {
     const int n = static_cast<int>(h->n);
     DeviceBuffers& d = h->d;
     double* const* s = d.st[h->cur];
     // (the isolated mesh's grid needs the new bounds first: no early fork there)
     const bool early = mesh_concurrent(h) && h->mesh_overlap == 2 && !isolated(h);
-    // leapfrog: the opening half kick (the closing one follows the force evaluation, or the
-    // next step's opening kernel applies it first); symplectic Euler: the whole kick with the
-    // force of the step's start positions
+    // leapfrog: the opening half kick (the closing one follows the force evaluation);
+    // symplectic Euler: the whole kick with the force of the step's start positions
     const bool euler = h->cfg.integrator == BZ_INTEGRATOR_EULER;
-    const bool close_prev = !euler && kind == kStepNext;
-    const bool pm = close_prev && mesh_added_in_kick(h);
     launch_kick_drift(s[0], s[1], s[2], s[3], s[4], s[5], d.acc[0], d.acc[1], d.acc[2], n, d.dt,
                       periodic(h) ? h->cfg.box_length : 0.0, nullptr, h->stream,
                       early ? d.mass[h->cur] : nullptr, early ? d.pos4_drift : nullptr,
-                      euler ? 1.0 : 0.5, pm ? d.acc_pm[0] : nullptr, pm ? d.acc_pm[1] : nullptr,
-                      pm ? d.acc_pm[2] : nullptr, h->cfg.physics_max_acceleration,
-                      close_prev ? 0.5 : 0.0);
+                      euler ? 1.0 : 0.5);
     if (h->io_host_pos)  // the step's positions are final here: send them while the step runs
         enqueue_io_positions(h);
     if (early) {
@@ -415,8 +366,7 @@ void enqueue_step(bz_handle* h, int kind = kStepWhole)
         pm_solve(h->pm, h->pm_stream);
     }
     enqueue_order(h);
-    const bool defer = !euler && kind != kStepWhole;
-    enqueue_forces(h, !euler && !defer, false, early, defer);
+    enqueue_forces(h, !euler, false, early);
 }
 
 bz_status check_device(bz_handle* h, const char* what)
@@ -497,28 +447,15 @@ bz_status ensure_forces(bz_handle* h)
 
 // One-time capture of a step for each state-buffer parity.  Capturing records the work
 // without executing it; the host-side parity is restored afterwards.
-// Two steps as a bz_step call of two enqueues them.
-void enqueue_two_steps(bz_handle* h)
+void build_graphs(bz_handle* h)
 {
-    if (h->cfg.integrator == BZ_INTEGRATOR_EULER) {
-        enqueue_step(h);
-        enqueue_step(h);
-        return;
-    }
-    enqueue_step(h, kStepFirst);
-    enqueue_step(h, kStepNext);
-    enqueue_close(h);
-}
-
-void build_graphs(bz_handle* h, int kind)
-{
-    if (h->graph_failed || (h->graph[kind][0] && h->graph[kind][1]))
+    if (h->graph_failed || (h->graph[0] && h->graph[1]))
         return;
     const int orig = h->cur;
     const bool saved = h->timing;
     h->timing = false;
     for (int parity = 0; parity < 2 && !h->graph_failed; ++parity) {
-        if (h->graph[kind][parity])
+        if (h->graph[parity])
             continue;
         h->cur = parity;
         cudaGraph_t g = nullptr;
@@ -526,7 +463,7 @@ void build_graphs(bz_handle* h, int kind)
             h->graph_failed = true;
             break;
         }
-        enqueue_step(h, kind);
+        enqueue_step(h);
         const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
         cudaGraphExec_t ex = nullptr;
         if (e != cudaSuccess || !g || cudaGraphInstantiate(&ex, g, 0) != cudaSuccess) {
@@ -536,7 +473,7 @@ void build_graphs(bz_handle* h, int kind)
             break;
         }
         cudaGraphDestroy(g);
-        h->graph[kind][parity] = ex;
+        h->graph[parity] = ex;
     }
     if (h->graph_failed)
         cudaGetLastError();
@@ -565,7 +502,7 @@ bz_status bz_launches_per_step(bz_handle* h, uint64_t* launches)
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return fail(h, BZ_CUDA_ERROR, "capture for launch count");
-    enqueue_step(h, kStepNext);  // a step inside a call of several (leapfrog: no closing kick)
+    enqueue_step(h);
     cudaStreamEndCapture(h->stream, &g);
     if (g)
         cudaGraphDestroy(g);
@@ -647,7 +584,9 @@ bz_status bz_destroy(bz_handle* h)
     cudaSetDevice(h->device);
     if (h->stream)
         cudaStreamSynchronize(h->stream);
-    release_graphs(h);
+    for (int i = 0; i < 2; ++i)
+        if (h->graph[i])
+            cudaGraphExecDestroy(h->graph[i]);
     for (int i = 0; i <= kEvStepStart; ++i)
         if (h->ev[i])
             cudaEventDestroy(h->ev[i]);
@@ -1677,27 +1616,19 @@ bz_status bz_step(bz_handle* h, double dt, uint32_t nsteps)
     h->stepping = true;
     if (h->cfg.adaptive_max_level > 0)
         return adaptive_steps(h, dt, nsteps);
-    // leapfrog calls of several steps fold each closing kick into the next step's opening
-    // kernel and close once after the last step (bit for bit the same arithmetic)
-    const bool fold = nsteps > 1 && h->cfg.integrator != BZ_INTEGRATOR_EULER;
-    auto kind_of = [&](uint32_t i) { return !fold ? kStepWhole : (i == 0 ? kStepFirst : kStepNext); };
     uint32_t done = 0;
     if (h->cfg.use_graph && !h->timing) {
-        build_graphs(h, kind_of(0));
-        if (nsteps > 1)
-            build_graphs(h, kind_of(1));
+        build_graphs(h);
         if (!h->graph_failed)
             for (; done < nsteps; ++done) {
-                cudaGraphLaunch(h->graph[kind_of(done)][h->cur], h->stream);
+                cudaGraphLaunch(h->graph[h->cur], h->stream);
                 h->cur ^= 1;
             }
     }
     for (; done < nsteps; ++done) {
         record(h, kEvStepStart);
-        enqueue_step(h, kind_of(done));
+        enqueue_step(h);
     }
-    if (fold)
-        enqueue_close(h);
     if (h->timing)
         record(h, kNumPhases);
     s = check_device(h, "bz_step");
@@ -1714,7 +1645,11 @@ bz_status bz_walk_blocks_per_sm(bz_handle* h, int32_t set_value, int32_t* curren
         return BZ_INVALID_ARGUMENT;
     if (set_value >= 0 && set_value != h->walk_blocks_per_sm) {
         h->walk_blocks_per_sm = set_value;
-        release_graphs(h);  // captured steps hold the old grid
+        for (int i = 0; i < 2; ++i) {  // captured steps hold the old grid
+            if (h->graph[i])
+                cudaGraphExecDestroy(h->graph[i]);
+            h->graph[i] = nullptr;
+        }
     }
     if (current)
         *current = h->walk_blocks_per_sm;
@@ -1727,7 +1662,11 @@ bz_status bz_set_mesh_schedule(bz_handle* h, int32_t schedule)
         return BZ_INVALID_ARGUMENT;
     if (h->mesh_overlap != schedule) {
         h->mesh_overlap = schedule;
-        release_graphs(h);  // captured steps hold the old schedule
+        for (int i = 0; i < 2; ++i) {  // captured steps hold the old schedule
+            if (h->graph[i])
+                cudaGraphExecDestroy(h->graph[i]);
+            h->graph[i] = nullptr;
+        }
     }
     return BZ_OK;
 }
@@ -1767,7 +1706,8 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
         bool graph = h->cfg.use_graph && !h->graph_failed;
         if (graph) {
             if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-                enqueue_two_steps(h);
+                enqueue_step(h);
+                enqueue_step(h);
                 if (cudaStreamEndCapture(h->stream, &g) != cudaSuccess || !g ||
                     cudaGraphInstantiate(&ex, g, 0) != cudaSuccess)
                     graph = false;
@@ -1785,7 +1725,8 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
             if (graph) {
                 cudaGraphLaunch(ex, h->stream);
             } else {
-                enqueue_two_steps(h);
+                enqueue_step(h);
+                enqueue_step(h);
             }
         };
         run();  // warm-up with these parameters
@@ -1857,7 +1798,11 @@ bz_status bz_autotune(bz_handle* h, int32_t trials, int32_t* leaf_capacity, int3
     h->mesh_overlap = st == BZ_OK ? best_overlap : overlap0;
     h->walk_blocks_per_sm = st == BZ_OK ? best_bps : bps0;
     // the captured step holds the old parameters: capture again on the next bz_step
-    release_graphs(h);
+    for (int i = 0; i < 2; ++i) {
+        if (h->graph[i])
+            cudaGraphExecDestroy(h->graph[i]);
+        h->graph[i] = nullptr;
+    }
     h->forces_valid = false;
     if (st != BZ_OK)
         return st;
@@ -1897,7 +1842,11 @@ bool learn_pairs_alloc(bz_handle* h)
 
 void drop_graphs(bz_handle* h)
 {
-    release_graphs(h);
+    for (int i = 0; i < 2; ++i) {
+        if (h->graph[i])
+            cudaGraphExecDestroy(h->graph[i]);
+        h->graph[i] = nullptr;
+    }
     h->forces_valid = false;
 }
 

@@ -247,15 +247,10 @@ void launch_permute(const uint32_t* perm, int n, const double* const* src, doubl
 void launch_kick(double* vx, double* vy, double* vz, float* ax, float* ay, float* az, int n,
                  const double* dt_half, cudaStream_t s, const float* bx = nullptr,
                  const float* by = nullptr, const float* bz = nullptr, float max_acc = 0.0f);
-// Opening kick (kick_frac x dt) and drift.  close_frac > 0 first applies the previous step's
-// closing kick (close_frac x dt) as launch_kick would, with b (may be NULL) completing the
-// accelerations, without storing them.
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
                        const float* ax, const float* ay, const float* az, int n,
                        const double* dt, double periodic_len, BoxF64* box, cudaStream_t s,
-                       const float* mass = nullptr, float4* pos4 = nullptr, double kick_frac = 0.5,
-                       const float* bx = nullptr, const float* by = nullptr,
-                       const float* bz = nullptr, float max_acc = 0.0f, double close_frac = 0.0);
+                       const float* mass = nullptr, float4* pos4 = nullptr, double kick_frac = 0.5);
 // FP64 energy/momentum sums over the sorted state (scratch: energy_scratch_doubles(); the
 // five results land at scratch[5 * 1024 .. 5 * 1024 + 5)).
 size_t energy_scratch_doubles();

@@ -95,11 +95,7 @@ __device__ __forceinline__ double wrap_periodic(double x, double L)
 
 // Kick with the cached acceleration (kick_frac x dt: half for leapfrog, whole for symplectic
 // Euler), full drift with the kicked velocity, periodic wrap; for open boundaries the FP64 box
-// of the drifted positions is reduced in the same pass.  close_frac > 0: the previous leapfrog
-// step's closing kick (close_frac x dt) is applied first, with the same arithmetic as k_kick
-// (and, with bx, the same completion of the accelerations by the mesh leg's), so the result
-// is bit for bit that of k_kick followed by this kernel; the completed accelerations are not
-// stored (the force evaluation of this step replaces them).
+// of the drifted positions is reduced in the same pass.
 __global__ void __launch_bounds__(kThreads) k_kick_drift(double* __restrict__ x,
                                                           double* __restrict__ y,
                                                           double* __restrict__ z,
@@ -112,33 +108,15 @@ __global__ void __launch_bounds__(kThreads) k_kick_drift(double* __restrict__ x,
                                                           const double* __restrict__ dtp,
                                                           double L, BoxF64* box,
                                                           const float* __restrict__ mass,
-                                                          float4* __restrict__ pos4, double kick_frac,
-                                                          const float* __restrict__ bx,
-                                                          const float* __restrict__ by,
-                                                          const float* __restrict__ bz, float max_acc,
-                                                          double close_frac)
+                                                          float4* __restrict__ pos4, double kick_frac)
 {
     const double dt = *dtp;
     const double h = kick_frac * dt;
-    const double hc = close_frac * dt;
     double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
     for (int i = blockIdx.x * kThreads + threadIdx.x; i < n; i += gridDim.x * kThreads) {
-        float a[3] = {ax[i], ay[i], az[i]};
-        double ux = vx[i], uy = vy[i], uz = vz[i];
-        if (close_frac > 0.0) {
-            if (bx) {
-                a[0] += bx[i];
-                a[1] += by[i];
-                a[2] += bz[i];
-                clamp_acceleration(a[0], a[1], a[2], max_acc);
-            }
-            ux += static_cast<double>(a[0]) * hc;
-            uy += static_cast<double>(a[1]) * hc;
-            uz += static_cast<double>(a[2]) * hc;
-        }
-        ux = ux + static_cast<double>(a[0]) * h;
-        uy = uy + static_cast<double>(a[1]) * h;
-        uz = uz + static_cast<double>(a[2]) * h;
+        const double ux = vx[i] + static_cast<double>(ax[i]) * h;
+        const double uy = vy[i] + static_cast<double>(ay[i]) * h;
+        const double uz = vz[i] + static_cast<double>(az[i]) * h;
         vx[i] = ux;
         vy[i] = uy;
         vz[i] = uz;
@@ -229,8 +207,7 @@ void launch_kick(double* vx, double* vy, double* vz, float* ax, float* ay, float
 void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, double* vz,
                        const float* ax, const float* ay, const float* az, int n,
                        const double* dt, double periodic_len, BoxF64* box, cudaStream_t s,
-                       const float* mass, float4* pos4, double kick_frac, const float* bx,
-                       const float* by, const float* bz, float max_acc, double close_frac)
+                       const float* mass, float4* pos4, double kick_frac)
 {
     if (box) {
         count_launch();
@@ -238,8 +215,7 @@ void launch_kick_drift(double* x, double* y, double* z, double* vx, double* vy, 
     }
     count_launch();
     k_kick_drift<<<grid_for(n), kThreads, 0, s>>>(x, y, z, vx, vy, vz, ax, ay, az, n, dt,
-                                                  periodic_len, box, mass, pos4, kick_frac, bx, by,
-                                                  bz, max_acc, close_frac);
+                                                  periodic_len, box, mass, pos4, kick_frac);
 }
 
 void launch_scatter3(const float* ax, const float* ay, const float* az, const int* id, int n,

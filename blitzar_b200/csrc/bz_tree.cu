@@ -85,12 +85,13 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
     __shared__ int s_scan[kThreads / 32];
     __shared__ int s_prefix;
     const int first = t.lvl_first[l];
+    const int level_splits = t.lvl_split[l];  // loaded with the level's range, one round trip
     // after a capacity overflow the recorded count can exceed the arrays: clamp
     const int cnt = min(t.lvl_count[l], t.cap - first);
     if (cnt <= 0)
         return;
     const int next_first = first + cnt;
-    if (__ldcg(&t.lvl_split[l]) == 0 && l >= min_split) {
+    if (level_splits == 0 && l >= min_split) {
         // no node of this level holds more than a leaf: all are leaves, no children, no scan
         for (int i = blockIdx.x * kThreads + threadIdx.x; i < cnt; i += gridDim.x * kThreads) {
             t.child[first + i] = -1;
@@ -247,8 +248,8 @@ __global__ void __launch_bounds__(kThreads) k_tree_level(const unsigned long lon
             }
         }
         // a child larger than a leaf lets the next level split: flag it (plain stores of the
-        // same value, skipped once the flag reads set, instead of contended atomics)
-        if (__any_sync(kFullMask, cmax > leaf_cap) && lane == 0 && __ldcg(&t.lvl_split[l + 1]) == 0)
+        // same value, which no thread waits for, instead of contended atomics)
+        if (__any_sync(kFullMask, cmax > leaf_cap) && lane == 0)
             t.lvl_split[l + 1] = 1;
         __syncthreads();
     }

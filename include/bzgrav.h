@@ -293,8 +293,7 @@ bz_status bz_pm_mesh(bz_handle* h, int which, float* out);
 bz_status bz_pm_grid(bz_handle* h, double* out6);
 
 /* Kernel launches of this library enqueued so far (cuFFT's own kernels excluded), and the
- * number one step of a bz_step call of several steps enqueues (a leapfrog call adds one
- * closing kick after its last step). */
+ * number one bz_step step enqueues. */
 uint64_t bz_kernel_launches(void);
 bz_status bz_launches_per_step(bz_handle* h, uint64_t* launches);
 
