@@ -26,6 +26,19 @@ def test_library_exports_header_symbols():
     assert L.bz_version().startswith(b"bzgrav")
 
 
+def test_reference_gpu_comparator_exports():
+    """The reference's GPU octree comparator (oracle/_ref/libbzrefgpu.so, built where a reference
+    checkout was at hand) loads and exports its entry points; no GPU call is made here."""
+    from oracle import oracle as O
+
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libbzrefgpu.so")):
+        pytest.skip("reference GPU comparator not built (no reference checkout at build time)")
+    R = O.ref_gpu()
+    for name in ("refgpu_create", "refgpu_destroy", "refgpu_step", "refgpu_time_steps",
+                 "refgpu_accel", "refgpu_get_state"):
+        assert hasattr(R, name), name
+
+
 def test_config_defaults_and_argument_checks():
     import ctypes as C
 
