@@ -74,7 +74,7 @@ __host__ __device__ inline double double_from_ordered(unsigned long long u)
 #endif
 }
 
-// ---- mbarrier + bulk copy (global -> shared, no multicast) -------------------------
+// ---- mbarrier + bulk copy (global -> shared, into this CTA only) -------------------------
 __device__ __forceinline__ uint32_t smem_u32(const void* p)
 {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -152,7 +152,7 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, uint3
 }
 
 // 1-D bulk copy global -> shared completing on an mbarrier (cp.async.bulk, non-tensor,
-// no multicast).  dst, src 16-byte aligned; bytes a multiple of 16.
+// into this CTA only).  dst, src 16-byte aligned; bytes a multiple of 16.
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, uint32_t bytes, unsigned long long* bar)
 {
     asm volatile(

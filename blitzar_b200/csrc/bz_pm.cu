@@ -945,7 +945,7 @@ __device__ __forceinline__ void interp_ad_quads(const float4* __restrict__ pos4,
 // Analytic differentiation with the potential staged in shared memory, the gather twin of
 // k_deposit_tiled: a block takes a chunk of Morton-consecutive particles (the deposit's chunk,
 // whose stencils fit one tile) and stages the box of cells their stencils cover with bulk copies
-// (cp.async.bulk, global -> shared, no multicast), one per mesh row segment: rows start on a
+// (cp.async.bulk, global -> shared, into this CTA only), one per mesh row segment: rows start on a
 // 16-byte boundary (x rounded down to a multiple of 4 cells; the mesh side is a multiple of 4),
 // a row crossing the periodic x boundary takes two copies, and all complete on one mbarrier
 // (bounded wait).  One thread then serves one particle (ad_stencil, ad_gather) over a tile with

@@ -9,7 +9,7 @@
 //   - opened internal nodes -> children pushed on a shared-memory stack (shuffle scan).
 // Full lists are flushed: every lane evaluates its own target against each listed node, and
 // leaf particles are pulled into a shared-memory tile with cp.async.bulk (global -> shared,
-// completing on an mbarrier; no cluster multicast) and summed with FP32 pair arithmetic.
+// completing on an mbarrier, into this CTA only) and summed with FP32 pair arithmetic.
 // Per-flush partial sums are folded into the running force with a two-sum (compensated
 // accumulation).
 //
